@@ -1,0 +1,211 @@
+/*
+ * manapy_b200 -- C ABI of the B200 (sm_100a) explicit finite-volume step.
+ *
+ * Every entry point takes device pointers, plain sizes and a CUDA stream
+ * (cudaStream_t passed as void*), returns 0 on success or a negative MB_E*
+ * code, and never allocates device memory.  Field arrays are indexed in the
+ * numbering of the mb_mesh they are passed with: either manapy's own (the
+ * numbering of manapy/ddm/domain.py:294-334) or any relabelling of cells, faces
+ * and nodes the caller applied consistently to every table (the Python layer
+ * uses a Morton-curve relabelling for locality; per-cell lists keep manapy's
+ * order, so accumulation order is unchanged).  Vectors are [n][3].
+ *
+ * A mesh is described once by mb_mesh (device tables built on the host from
+ * manapy's Domain arrays); the per-variable ghost rules by mb_bc.  The
+ * kernels reproduce manapy's per-cell accumulation order: a cell gathers its
+ * faces instead of faces scattering into cells, so there are no atomics and
+ * the results do not depend on scheduling.
+ *
+ * Each function below names the manapy function it replaces (file:line in
+ * the manapy source tree).
+ */
+#ifndef MANAPY_B200_H
+#define MANAPY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MB_OK 0
+#define MB_EINVAL (-1)   /* bad argument (null pointer, bad size, bad dim) */
+#define MB_ECUDA (-2)    /* a CUDA launch or call failed */
+
+/* Ghost rule of a boundary face (manapy/boundary/bc_utils.py:45-68). */
+#define MB_G_NONE 0
+#define MB_G_DIRICHLET 1     /* ghost = value[f] */
+#define MB_G_NEUMANN 2       /* ghost = w[c0] */
+#define MB_G_NONSLIP 3       /* ghost = -w[c0] */
+#define MB_G_NEUMANN_NH 4    /* ghost = w[c0] + value[f] * dist[f] */
+#define MB_G_CELL_AT_FACE 5  /* ghost = w[(int)value[f]]: manapy reads its cell array at the
+                                face's own index; value[f] holds that cell index */
+
+typedef struct mb_mesh {
+  int32_t dim;       /* 2 (triangles) or 3 (tetrahedra) */
+  int32_t nbcells;
+  int32_t nbfaces;
+  int32_t nbnodes;
+  int32_t nlf;       /* faces per cell: 3 or 4 */
+  int32_t pad_;
+  /* cells */
+  const double *cell_center;    /* [nbcells][3] */
+  const double *cell_volume;    /* [nbcells] */
+  const int32_t *cell_faces;    /* [nbcells][4], manapy's local face order (cells.faceid) */
+  const uint8_t *cell_order;    /* [nbcells], 2 bits per slot: slot visited k-th in ascending face id */
+  const int32_t *cellnid_ptr;   /* [nbcells+1] CSR of vertex neighbours (cells.cellnid) */
+  const int32_t *cellnid_idx;
+  const int32_t *ghostnid_ptr;  /* [nbcells+1] CSR of stencil boundary faces (cells.ghostnid) */
+  const int32_t *ghostnid_idx;
+  /* faces */
+  const int32_t *face_cellid;   /* [nbfaces][2], second = -1 on boundary faces (faces.cellid) */
+  const int32_t *face_nodeid;   /* [nbfaces][4] (faces.nodeid without the count column) */
+  const int32_t *face_name;     /* [nbfaces] (faces.name) */
+  const double *face_normal;    /* [nbfaces][3] */
+  const double *face_center;    /* [nbfaces][3] */
+  const double *face_mesure;    /* [nbfaces] */
+  const double *face_ghostcenter; /* [nbfaces][3] ghost cell centre (faces.ghostcenter) */
+  const double *face_air;       /* [nbfaces] diamond measure (faces.airDiamond) */
+  const double *face_f;         /* 2D: [nbfaces][4][2] = f_1..f_4; 3D: [nbfaces][2][3] = f_1, f_2 */
+  const double *face_dist;      /* [nbfaces] (faces.dist_ortho) */
+  /* nodes */
+  const int32_t *n2c_ptr;       /* [nbnodes+1] CSR node -> cells (nodes.cellid) */
+  const int32_t *n2c_idx;
+  const double *n2c_alpha;      /* centre->vertex weight of each node->cell incidence */
+  const int32_t *n2g_ptr;       /* [nbnodes+1] CSR node -> boundary faces (nodes.ghostid) */
+  const int32_t *n2g_idx;
+  const double *n2g_alpha;
+  /* SW bathymetry source (2D): cells.cellfid [nbcells][4], cells.nf [nbcells][3][3],
+   * vertex of local node 1 of each cell [nbcells][2] */
+  const int32_t *cell_cellfid;
+  const double *cell_nf;
+  const double *cell_vertex1;
+} mb_mesh;
+
+typedef struct mb_bc {
+  const int8_t *kind;   /* [nbfaces] MB_G_* */
+  const double *value;  /* [nbfaces] dirichlet value / neumannNH gradient */
+  /* faces whose diamond gradient manapy computes: inner, dirichlet and
+   * neumann-list faces (manapy/ast/core.py:480-490); 1 = computed */
+  const uint8_t *face_grad_on;
+} mb_bc;
+
+/* ---- reference kernels, one entry point each ---------------------------------- */
+
+/* manapy/ast/ast_utils.py:8-18 facetocell */
+int mb_facetocell(const mb_mesh *m, const double *u_face, double *u_cell, void *stream);
+
+/* manapy/boundary/bc_utils.py:45-68 ghost_value_* for every boundary face (Variable.update_ghost_value,
+ * manapy/ast/core.py:492-497) */
+int mb_ghost_value(const mb_mesh *m, const mb_bc *bc, const double *w_c, double *w_ghost, void *stream);
+
+/* manapy/ast/functions2d.py:5-104 cell_gradient_2d, manapy/ast/functions3d.py:4-120 cell_gradient_3d */
+int mb_cell_gradient(const mb_mesh *m, const double *w_c, const double *w_ghost, double *w_x,
+                     double *w_y, double *w_z, void *stream);
+
+/* manapy/ast/functions2d.py:280-325 barthlimiter_2d, manapy/ast/functions3d.py:364-408 barthlimiter_3d */
+int mb_barthlimiter(const mb_mesh *m, const double *w_c, const double *w_ghost, const double *w_x,
+                    const double *w_y, const double *w_z, double *psi, void *stream);
+
+/* manapy/ast/functions2d.py:199-276 centertovertex_2d, manapy/ast/functions3d.py:251-362 */
+int mb_centertovertex(const mb_mesh *m, const double *w_c, const double *w_ghost, double *w_node,
+                      void *stream);
+
+/* manapy/ast/functions2d.py:108-196 face_gradient_2d, manapy/ast/functions3d.py:122-248 */
+int mb_face_gradient(const mb_mesh *m, const mb_bc *bc, const double *w_c, const double *w_ghost,
+                     const double *w_node, double *wx_face, double *wy_face, double *wz_face,
+                     void *stream);
+
+/* manapy/solvers/advecdiff/fvm_utils.py:43-176 explicitscheme_convective_2d, :180-314 _3d */
+int mb_explicitscheme_convective(const mb_mesh *m, double *rez_w, const double *w_c,
+                                 const double *w_ghost, const double *u_face, const double *v_face,
+                                 const double *w_face, const double *w_x, const double *w_y,
+                                 const double *w_z, const double *psi, int32_t order, void *stream);
+
+/* manapy/solvers/advecdiff/fvm_utils.py:5-26 explicitscheme_dissipative */
+int mb_explicitscheme_dissipative(const mb_mesh *m, const double *wx_face, const double *wy_face,
+                                  const double *wz_face, double *dissip_w, double Dxx, double Dyy,
+                                  double Dzz, void *stream);
+
+/* manapy/solvers/advecdiff/fvm_utils.py:317-340 time_step; the min lands in *dt_dev (device) */
+int mb_time_step(const mb_mesh *m, const double *u, const double *v, const double *w, double cfl,
+                 double Dxx, double Dyy, double Dzz, double *dt_dev, void *stream);
+
+/* manapy/solvers/advecdiff/fvm_utils.py:342-346 update_new_value; dt read from *dt_dev */
+int mb_update_new_value(const mb_mesh *m, double *ne_c, const double *rez, const double *dissip,
+                        const double *src, const double *dt_dev, void *stream);
+
+/* ---- shallow water ------------------------------------------------------------------- */
+
+/* manapy/solvers/shallowater/fvm_utils.py:152-342 srnh_scheme for n independent states:
+ * states [n][10] = hu_l hu_r hv_l hv_r h_l h_r hc_l hc_r Z_l Z_r, normals [n][3], mesure [n]
+ * -> flux [n][5] */
+int mb_srnh_flux(int32_t n, const double *states, const double *normals, const double *mesure,
+                 double grav, double *flux, void *stream);
+
+/* manapy/solvers/shallowater/fvm_utils.py:16-42 time_step_SW -> *dt_dev */
+int mb_time_step_sw(const mb_mesh *m, const double *h, const double *hu, const double *hv,
+                    double cfl, double grav, double Dxx, double Dyy, double *dt_dev, void *stream);
+
+/* manapy/solvers/shallowater/fvm_utils.py:344-496 explicitscheme_convective_SW.
+ * q = {h, hu, hv, hc, Z} cell states, g = their ghosts; grads = {h_x, h_y, hc_x, hc_y}, psi = hc's
+ * limiter (manapy/solvers/shallowater/system.py:168-178).  face_flux is scratch [nbfaces][5]. */
+int mb_explicitscheme_convective_sw(const mb_mesh *m, double *const rez[5], const double *const q[5],
+                                    const double *const g[5], const double *const grads[4],
+                                    const double *psi, double grav, int32_t order,
+                                    double *face_flux, void *stream);
+
+/* manapy/solvers/shallowater/fvm_utils.py:44-148 term_source_srnh_SW -> src_hu, src_hv
+ * (src_h, src_hc, src_Z are zero in the reference and are not written) */
+int mb_term_source_srnh_sw(const mb_mesh *m, const double *h, const double *Z, const double *h_ghost,
+                           const double *Z_ghost, double grav, double *src_hu, double *src_hv,
+                           void *stream);
+
+/* manapy/solvers/shallowater/fvm_utils.py:3-14 update_SW (no coriolis, no wind) */
+int mb_update_sw(const mb_mesh *m, double *const q[5], const double *const rez[5],
+                 const double *src_hu, const double *src_hv, const double *dt_dev, void *stream);
+
+/* ---- fused steps ---------------------------------------------------------------------- */
+
+typedef struct mb_advdiff_params {
+  int32_t order;       /* 1 or 2 */
+  int32_t diffusion;   /* 0: Dxx = Dyy = Dzz = 0 (manapy skips the diffusive flux) */
+  double Dxx, Dyy, Dzz;
+} mb_advdiff_params;
+
+/* One advection-diffusion step, the work of AdvectionDiffusionSolver.compute_fluxes +
+ * compute_new_val (manapy/solvers/advecdiff/system.py:156-172) in two launches:
+ *   1. cell gradients + Barth limiter (order 2) and centre->vertex values (diffusion);
+ *   2. per cell: upwind fluxes, diamond diffusion, forward-Euler update.
+ * w_in is read, w_out written (distinct buffers).  sign_face[f] = u.n of face f
+ * (mb_face_sign), src may be NULL (zero source).  Scratch: gx, gy, gz, psi [nbcells],
+ * w_node [nbnodes]. */
+int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
+                    const double *w_in, double *w_out, const double *sign_face, const double *src,
+                    const double *dt_dev, double *gx, double *gy, double *gz, double *psi,
+                    double *w_node, void *stream);
+
+/* sign_face[f] = u_face[f] n_x + v_face[f] n_y + w_face[f] n_z, the upwind selector of
+ * manapy/solvers/advecdiff/fvm_utils.py:53-64 */
+int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face,
+                 const double *w_face, double *sign_face, void *stream);
+
+/* One shallow-water step (ShallowWaterSolver.stepper + compute_fluxes + compute_new_val,
+ * manapy/solvers/shallowater/system.py:186-192,248-281,237-242) with Neumann ghosts on
+ * every boundary face (manapy's default): dt (time_step_SW) -> [order 2: h, hc gradients
+ * and hc limiter] -> face fluxes -> per-cell gather + bathymetry source + update.
+ * q_in / q_out: 5 distinct cell arrays each (h, hu, hv, hc, Z).  Scratch: face_flux
+ * [nbfaces][5], scratch [5][nbcells] (order 2 only, else may be NULL); dt_dev receives
+ * this step's dt. */
+int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5],
+               double cfl, double grav, int32_t order, double *scratch, double *face_flux,
+               double *dt_dev, void *stream);
+
+/* Library build information (architecture string), for diagnostics. */
+const char *mb_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MANAPY_B200_H */

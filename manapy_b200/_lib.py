@@ -1,0 +1,117 @@
+"""ctypes binding of ``lib/libmanapy_b200.so`` (the C ABI in ``include/manapy_b200.h``).
+
+The library is built in-tree by ``manapy_b200.build.build()``.  Importing
+this module does not load it; ``lib()`` does, and raises ``RuntimeError`` when
+the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmanapy_b200.so")
+
+MB_OK, MB_EINVAL, MB_ECUDA = 0, -1, -2
+G_NONE, G_DIRICHLET, G_NEUMANN, G_NONSLIP, G_NEUMANN_NH, G_CELL_AT_FACE = 0, 1, 2, 3, 4, 5
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_d = ctypes.c_double
+
+
+class MbMesh(ctypes.Structure):
+    _fields_ = [("dim", _i32), ("nbcells", _i32), ("nbfaces", _i32), ("nbnodes", _i32),
+                ("nlf", _i32), ("pad_", _i32),
+                ("cell_center", _vp), ("cell_volume", _vp), ("cell_faces", _vp),
+                ("cell_order", _vp), ("cellnid_ptr", _vp), ("cellnid_idx", _vp),
+                ("ghostnid_ptr", _vp), ("ghostnid_idx", _vp),
+                ("face_cellid", _vp), ("face_nodeid", _vp), ("face_name", _vp),
+                ("face_normal", _vp), ("face_center", _vp), ("face_mesure", _vp),
+                ("face_ghostcenter", _vp), ("face_air", _vp), ("face_f", _vp), ("face_dist", _vp),
+                ("n2c_ptr", _vp), ("n2c_idx", _vp), ("n2c_alpha", _vp),
+                ("n2g_ptr", _vp), ("n2g_idx", _vp), ("n2g_alpha", _vp),
+                ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp)]
+
+
+class MbBC(ctypes.Structure):
+    _fields_ = [("kind", _vp), ("value", _vp), ("face_grad_on", _vp)]
+
+
+class MbAdvDiffParams(ctypes.Structure):
+    _fields_ = [("order", _i32), ("diffusion", _i32), ("Dxx", _d), ("Dyy", _d), ("Dzz", _d)]
+
+
+_M = ctypes.POINTER(MbMesh)
+_B = ctypes.POINTER(MbBC)
+_P5 = _vp * 5
+_P4 = _vp * 4
+
+# name -> argtypes (restype is int unless listed in _RESTYPES)
+_SIGS = {
+    "mb_facetocell": [_M, _vp, _vp, _vp],
+    "mb_ghost_value": [_M, _B, _vp, _vp, _vp],
+    "mb_cell_gradient": [_M, _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_barthlimiter": [_M, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_centertovertex": [_M, _vp, _vp, _vp, _vp],
+    "mb_face_gradient": [_M, _B, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_explicitscheme_convective": [_M, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp],
+    "mb_explicitscheme_dissipative": [_M, _vp, _vp, _vp, _vp, _d, _d, _d, _vp],
+    "mb_time_step": [_M, _vp, _vp, _vp, _d, _d, _d, _d, _vp, _vp],
+    "mb_update_new_value": [_M, _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_srnh_flux": [_i32, _vp, _vp, _vp, _d, _vp, _vp],
+    "mb_time_step_sw": [_M, _vp, _vp, _vp, _d, _d, _d, _d, _vp, _vp],
+    "mb_explicitscheme_convective_sw": [_M, _P5, _P5, _P5, _P4, _vp, _d, _i32, _vp, _vp],
+    "mb_term_source_srnh_sw": [_M, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp],
+    "mb_update_sw": [_M, _P5, _P5, _vp, _vp, _vp, _vp],
+    "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                        _vp, _vp, _vp, _vp],
+    "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
+    "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
+    "mb_build_info": [],
+}
+_RESTYPES = {"mb_build_info": ctypes.c_char_p}
+
+EXPORTED = tuple(_SIGS)
+
+_lib = None
+
+
+def lib(path: str = LIB_PATH):
+    """Load the CUDA library (once); raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            "manapy_b200 CUDA library not found at %s; build it with "
+            "`python -c 'import manapy_b200.build as b; b.build()'`" % path)
+    L = ctypes.CDLL(path)
+    for name, args in _SIGS.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    _lib = L
+    return L
+
+
+class MbError(RuntimeError):
+    pass
+
+
+def check(rc: int, name: str = "call"):
+    if rc != MB_OK:
+        what = {MB_EINVAL: "invalid argument", MB_ECUDA: "CUDA error"}.get(rc, "error %d" % rc)
+        raise MbError("%s failed: %s" % (name, what))
+
+
+def call(name, *args):
+    check(getattr(lib(), name)(*args), name)
+
+
+def p5(ptrs):
+    return _P5(*ptrs)
+
+
+def p4(ptrs):
+    return _P4(*ptrs)

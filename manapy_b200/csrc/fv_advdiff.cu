@@ -1,0 +1,609 @@
+// Advection-diffusion kernels: manapy's explicit scheme on triangles (DIM 2)
+// and tetrahedra (DIM 3), FP64.
+//
+// Reference loops (manapy source tree):
+//   cell gradient       manapy/ast/functions2d.py:5-104, functions3d.py:4-120
+//   Barth limiter       manapy/ast/functions2d.py:280-325, functions3d.py:364-408
+//   centre -> vertex    manapy/ast/functions2d.py:199-276, functions3d.py:251-362
+//   face gradient       manapy/ast/functions2d.py:108-196, functions3d.py:122-248
+//   upwind flux         manapy/solvers/advecdiff/fvm_utils.py:43-314
+//   diamond diffusion   manapy/solvers/advecdiff/fvm_utils.py:5-26
+//   time step           manapy/solvers/advecdiff/fvm_utils.py:317-340
+//   update              manapy/solvers/advecdiff/fvm_utils.py:342-346
+#include "fv_common.cuh"
+
+namespace mb {
+
+// ---------------------------------------------------------------- per-cell pieces
+
+// Unweighted least-squares gradient over the vertex neighbours, then the
+// stencil's boundary ghosts, in manapy's order.
+template <int DIM, class G>
+__device__ __forceinline__ void lsq_gradient(const mb_mesh &m, const double *__restrict__ w, G ghost,
+                                             int i, double &gx, double &gy, double &gz) {
+  const double *cc = m.cell_center;
+  const double cx = ld(cc + 3 * i), cy = ld(cc + 3 * i + 1);
+  const double cz = DIM == 3 ? ld(cc + 3 * i + 2) : 0.0;
+  const double wi = ld(w + i);
+  double ixx = 0., iyy = 0., izz = 0., ixy = 0., ixz = 0., iyz = 0.;
+  double jx = 0., jy = 0., jz = 0.;
+  const int b = ld(m.cellnid_ptr + i), e = ld(m.cellnid_ptr + i + 1);
+  for (int k = b; k < e; ++k) {
+    const int c = ld(m.cellnid_idx + k);
+    const double dx = ld(cc + 3 * c) - cx, dy = ld(cc + 3 * c + 1) - cy;
+    const double dw = ld(w + c) - wi;
+    ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
+    jx += (dx * dw); jy += (dy * dw);
+    if (DIM == 3) {
+      const double dz = ld(cc + 3 * c + 2) - cz;
+      izz += dz * dz; ixz += (dx * dz); iyz += (dy * dz);
+      jz += (dz * dw);
+    }
+  }
+  const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+  const double *gc = m.face_ghostcenter;
+  for (int k = gb; k < ge; ++k) {
+    const int f = ld(m.ghostnid_idx + k);
+    const double dx = ld(gc + 3 * f) - cx, dy = ld(gc + 3 * f + 1) - cy;
+    const double dw = ghost(f) - wi;
+    ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
+    jx += (dx * dw); jy += (dy * dw);
+    if (DIM == 3) {
+      const double dz = ld(gc + 3 * f + 2) - cz;
+      izz += dz * dz; ixz += (dx * dz); iyz += (dy * dz);
+      jz += (dz * dw);
+    }
+  }
+  if (DIM == 2) {
+    const double dia = ixx * iyy - ixy * ixy;
+    gx = (iyy * jx - ixy * jy) / dia;
+    gy = (ixx * jy - ixy * jx) / dia;
+    gz = 0.;
+  } else {
+    const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz)
+                       - izz * (ixy * ixy);
+    gx = ((iyy * izz - iyz * iyz) * jx + (ixz * iyz - ixy * izz) * jy + (ixy * iyz - ixz * iyy) * jz) / dia;
+    gy = ((ixz * iyz - ixy * izz) * jx + (ixx * izz - ixz * ixz) * jy + (ixy * ixz - iyz * ixx) * jz) / dia;
+    gz = ((ixy * iyz - ixz * iyy) * jx + (ixy * ixz - iyz * ixx) * jy + (ixx * iyy - ixy * ixy) * jz) / dia;
+  }
+}
+
+// Barth-Jespersen limiter of cell i.
+template <int DIM, class G>
+__device__ __forceinline__ double barth(const mb_mesh &m, const double *__restrict__ w, G ghost,
+                                        int i, double gx, double gy, double gz) {
+  const int nlf = DIM == 2 ? 3 : 4;
+  const double wi = ld(w + i);
+  double wmax = wi, wmin = wi;
+  int fs[4];
+#pragma unroll
+  for (int j = 0; j < nlf; ++j) {
+    const int f = ld(m.cell_faces + 4 * i + j);
+    fs[j] = f;
+    const int nm = ld(m.face_name + f);
+    const double a = ld(w + ld(m.face_cellid + 2 * f));
+    const double b = (nm == 0 || nm > 10) ? ld(w + ld(m.face_cellid + 2 * f + 1)) : ghost(f);
+    wmax = pmax(pmax(wmax, a), b);
+    wmin = pmin(pmin(wmin, a), b);
+  }
+  const double eps = DIM == 2 ? 1e-8 : 1e-10;
+  const double *cc = m.cell_center, *fc = m.face_center;
+  const double cx = ld(cc + 3 * i), cy = ld(cc + 3 * i + 1);
+  const double cz = DIM == 3 ? ld(cc + 3 * i + 2) : 0.0;
+  double psi = 1.;
+#pragma unroll
+  for (int j = 0; j < nlf; ++j) {
+    const int f = fs[j];
+    const double r1 = ld(fc + 3 * f) - cx, r2 = ld(fc + 3 * f + 1) - cy;
+    double delta = gx * r1 + gy * r2;
+    if (DIM == 3) delta = gx * r1 + gy * r2 + gz * (ld(fc + 3 * f + 2) - cz);
+    double psi_ij = 1.;
+    if (!(fabs(delta) < eps)) {
+      if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
+      if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
+    }
+    psi = pmin(psi, psi_ij);
+  }
+  return psi;
+}
+
+// Centre -> vertex value of node n: cells, then ghosts, precomputed weights.
+template <class G>
+__device__ __forceinline__ double node_value(const mb_mesh &m, const double *__restrict__ w, G ghost, int n) {
+  double acc = 0.;
+  const int b = ld(m.n2c_ptr + n), e = ld(m.n2c_ptr + n + 1);
+  for (int k = b; k < e; ++k) acc += ld(m.n2c_alpha + k) * ld(w + ld(m.n2c_idx + k));
+  const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
+  for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
+  return acc;
+}
+
+// Diamond-cell face gradient of face f; vr = value on the right (cell or ghost).
+template <int DIM>
+__device__ __forceinline__ void face_gradient(const mb_mesh &m, const double *__restrict__ wn, int f,
+                                              double vl, double vr, double &gx, double &gy, double &gz) {
+  const int *nd = m.face_nodeid + 4 * f;
+  if (DIM == 2) {
+    const double vi1 = ld(wn + ld(nd)), vi2 = ld(wn + ld(nd + 1));
+    const double *F = m.face_f + 8 * f;
+    const double inv = 1 / (2 * ld(m.face_air + f));
+    const double s1 = vi1 + vl, s2 = vl + vi2, s3 = vi2 + vr, s4 = vr + vi1;
+    gx = inv * (s1 * ld(F + 1) + s2 * ld(F + 3) + s3 * ld(F + 5) + s4 * ld(F + 7));
+    gy = -1 / (2 * ld(m.face_air + f)) * (s1 * ld(F + 0) + s2 * ld(F + 2) + s3 * ld(F + 4) + s4 * ld(F + 6));
+    gz = 0.;
+  } else {
+    const double VA = ld(wn + ld(nd)), VB = ld(wn + ld(nd + 1)), VC = ld(wn + ld(nd + 2));
+    const double VD = VC;  // tetrahedra: the fourth face node is the third
+    const double *F = m.face_f + 6 * f;
+    const double *N = m.face_normal + 3 * f;
+    const double a = ld(m.face_air + f);
+    const double dAC = VA - VC, dBD = VB - VD, dRL = vr - vl;
+    gx = (ld(F + 0) * dAC + ld(F + 3) * dBD + ld(N + 0) * dRL) / a;
+    gy = (ld(F + 1) * dAC + ld(F + 4) * dBD + ld(N + 1) * dRL) / a;
+    gz = (ld(F + 2) * dAC + ld(F + 5) * dBD + ld(N + 2) * dRL) / a;
+  }
+}
+
+// Linear reconstruction at face f from cell c (order 2), 2D uses x, y only.
+template <int DIM>
+__device__ __forceinline__ double reconstruct(const mb_mesh &m, const double *__restrict__ w,
+                                              const double *__restrict__ gx, const double *__restrict__ gy,
+                                              const double *__restrict__ gz, const double *__restrict__ psi,
+                                              int c, int f) {
+  const double *cc = m.cell_center + 3 * c, *fc = m.face_center + 3 * f;
+  double d = ld(gx + c) * (ld(fc) - ld(cc)) + ld(gy + c) * (ld(fc + 1) - ld(cc + 1));
+  if (DIM == 3)
+    d = ld(gx + c) * (ld(fc) - ld(cc)) + ld(gy + c) * (ld(fc + 1) - ld(cc + 1)) + ld(gz + c) * (ld(fc + 2) - ld(cc + 2));
+  return ld(w + c) + ld(psi + c) * d;
+}
+
+// ---------------------------------------------------------------- kernels: reference entry points
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_cell_gradient(mb_mesh m, const double *w, const double *ghost,
+                                                          double *gx, double *gy, double *gz) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double x, y, z;
+    lsq_gradient<DIM>(m, w, GhostArray{ghost}, i, x, y, z);
+    gx[i] = x; gy[i] = y; gz[i] = z;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_barth(mb_mesh m, const double *w, const double *ghost,
+                                                  const double *gx, const double *gy, const double *gz,
+                                                  double *psi) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x)
+    psi[i] = barth<DIM>(m, w, GhostArray{ghost}, i, ld(gx + i), ld(gy + i), DIM == 3 ? ld(gz + i) : 0.0);
+}
+
+__global__ void __launch_bounds__(kBlock) k_centertovertex(mb_mesh m, const double *w, const double *ghost,
+                                                           double *wn) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.nbnodes; n += gridDim.x * blockDim.x)
+    wn[n] = node_value(m, w, GhostArray{ghost}, n);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_face_gradient(mb_mesh m, const uint8_t *on, const double *w,
+                                                          const double *ghost, const double *wn,
+                                                          double *gfx, double *gfy, double *gfz) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nbfaces; f += gridDim.x * blockDim.x) {
+    if (!on[f]) continue;
+    const int c0 = ld(m.face_cellid + 2 * f), c1 = ld(m.face_cellid + 2 * f + 1);
+    const double vl = ld(w + c0), vr = c1 >= 0 ? ld(w + c1) : ld(ghost + f);
+    double x, y, z;
+    face_gradient<DIM>(m, wn, f, vl, vr, x, y, z);
+    gfx[f] = x; gfy[f] = y;
+    if (DIM == 3) gfz[f] = z;
+  }
+}
+
+// Slot visited k-th when a cell's faces are taken in ascending face id.
+__device__ __forceinline__ int order_slot(uint8_t code, int k) { return (code >> (2 * k)) & 3; }
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_convective(mb_mesh m, double *rez, const double *w,
+                                                       const double *ghost, const double *uf,
+                                                       const double *vf, const double *wf,
+                                                       const double *gx, const double *gy,
+                                                       const double *gz, const double *psi, int order) {
+  const int nlf = DIM == 2 ? 3 : 4;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double cv[4];
+    bool bnd[4];
+#pragma unroll
+    for (int j = 0; j < nlf; ++j) {
+      const int f = ld(m.cell_faces + 4 * i + j);
+      const int c0 = ld(m.face_cellid + 2 * f), c1 = ld(m.face_cellid + 2 * f + 1);
+      const double *N = m.face_normal + 3 * f;
+      const double s = ld(uf + f) * ld(N) + ld(vf + f) * ld(N + 1) + ld(wf + f) * ld(N + 2);
+      double sol;
+      if (s >= 0) sol = order == 2 ? reconstruct<DIM>(m, w, gx, gy, gz, psi, c0, f) : ld(w + c0);
+      else if (c1 < 0) sol = ld(ghost + f);
+      else sol = order == 2 ? reconstruct<DIM>(m, w, gx, gy, gz, psi, c1, f) : ld(w + c1);
+      const double F = s * sol;
+      cv[j] = (i == c0) ? -F : F;
+      bnd[j] = c1 < 0;
+    }
+    const uint8_t code = ld(m.cell_order + i);
+    double acc = 0.;
+#pragma unroll
+    for (int k = 0; k < nlf; ++k) {
+      const int s = order_slot(code, k);
+      if (!bnd[s]) acc += cv[s];
+    }
+#pragma unroll
+    for (int k = 0; k < nlf; ++k) {
+      const int s = order_slot(code, k);
+      if (bnd[s]) acc += cv[s];
+    }
+    rez[i] = acc;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_dissipative(mb_mesh m, const double *gfx, const double *gfy,
+                                                        const double *gfz, double *dis, double Dxx,
+                                                        double Dyy, double Dzz) {
+  const int nlf = DIM == 2 ? 3 : 4;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double q[4];
+#pragma unroll
+    for (int j = 0; j < nlf; ++j) {
+      const int f = ld(m.cell_faces + 4 * i + j);
+      const double *N = m.face_normal + 3 * f;
+      const double v = Dxx * ld(gfx + f) * ld(N) + Dyy * ld(gfy + f) * ld(N + 1) + Dzz * ld(gfz + f) * ld(N + 2);
+      const int c0 = ld(m.face_cellid + 2 * f);
+      q[j] = (i == c0) ? v : -v;
+    }
+    const uint8_t code = ld(m.cell_order + i);
+    double acc = 0.;
+#pragma unroll
+    for (int k = 0; k < nlf; ++k) acc += q[order_slot(code, k)];
+    dis[i] = acc;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_facetocell(mb_mesh m, const double *uf, double *uc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double acc = 0.;
+    for (int j = 0; j < m.nlf; ++j) acc += ld(uf + ld(m.cell_faces + 4 * i + j));
+    uc[i] = acc / m.nlf;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_ghost(mb_mesh m, mb_bc bc, const double *w, double *ghost) {
+  const GhostRule g = make_rule(m, bc, w);
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nbfaces; f += gridDim.x * blockDim.x)
+    if (bc.kind[f] != MB_G_NONE) ghost[f] = g(f);
+}
+
+__global__ void k_fill(double *p, double v) { *p = v; }
+
+__global__ void __launch_bounds__(kBlock) k_time_step(mb_mesh m, const double *u, const double *v,
+                                                      const double *w, double cfl, double Dxx, double Dyy,
+                                                      double Dzz, double *dt) {
+  double best = 1e300;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    const double vol = ld(m.cell_volume + i);
+    const double ui = ld(u + i), vi = ld(v + i), wi = ld(w + i);
+    double lam = 0.;
+    for (int j = 0; j < m.nlf; ++j) {
+      const double *N = m.face_normal + 3 * ld(m.cell_faces + 4 * i + j);
+      const double n0 = ld(N), n1 = ld(N + 1), n2 = ld(N + 2);
+      lam += fabs(ui * n0 + vi * n1 + wi * n2);
+      const double mes = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+      const double lam_diff = Dxx * (mes * mes) + Dyy * (mes * mes) + Dzz * (mes * mes);
+      lam += lam_diff / vol;
+    }
+    if (lam != 0) best = pmin(best, cfl * vol / lam);
+  }
+  best = block_min(best);
+  if (threadIdx.x == 0 && best < 1e300) atomic_min_pos(dt, best);
+}
+
+__global__ void __launch_bounds__(kBlock) k_update(int n, double *wc, const double *rez, const double *dis,
+                                                   const double *src, const double *dt_dev,
+                                                   const double *vol) {
+  const double dt = *dt_dev;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    wc[i] += dt * ((ld(rez + i) + ld(dis + i)) / ld(vol + i) + ld(src + i));
+}
+
+__global__ void __launch_bounds__(kBlock) k_face_sign(mb_mesh m, const double *uf, const double *vf,
+                                                      const double *wf, double *s) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nbfaces; f += gridDim.x * blockDim.x) {
+    const double *N = m.face_normal + 3 * f;
+    s[f] = ld(uf + f) * ld(N) + ld(vf + f) * ld(N + 1) + ld(wf + f) * ld(N + 2);
+  }
+}
+
+// ---------------------------------------------------------------- kernels: fused step
+
+// Phase 1: blocks [0, ncb) do cell gradients + limiter, blocks [ncb, ...) do node values.
+template <int DIM, bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock) k_step_phase1(mb_mesh m, mb_bc bc, const double *w, double *gx,
+                                                        double *gy, double *gz, double *psi, double *wn,
+                                                        int ncb) {
+  const GhostRule ghost = make_rule(m, bc, w);
+  if (ORDER2 && (int)blockIdx.x < ncb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nbcells) return;
+    double x, y, z;
+    lsq_gradient<DIM>(m, w, ghost, i, x, y, z);
+    gx[i] = x; gy[i] = y;
+    if (DIM == 3) gz[i] = z;
+    psi[i] = barth<DIM>(m, w, ghost, i, x, y, z);
+    return;
+  }
+  if (DIFF) {
+    const int n = (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x;
+    if (n >= m.nbnodes) return;
+    wn[n] = node_value(m, w, ghost, n);
+  }
+}
+
+// Phase 2: per cell, upwind + diamond fluxes over its faces and the update.
+template <int DIM, bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+                                                        const double *w, double *w_out, const double *sign,
+                                                        const double *src, const double *dt_dev,
+                                                        const double *gx, const double *gy, const double *gz,
+                                                        const double *psi, const double *wn) {
+  const int nlf = DIM == 2 ? 3 : 4;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRule ghost = make_rule(m, bc, w);
+  const double wi = ld(w + i);
+  double cv[4], q[4];
+  bool bnd[4];
+#pragma unroll
+  for (int j = 0; j < nlf; ++j) {
+    const int f = ld(m.cell_faces + 4 * i + j);
+    const int c0 = ld(m.face_cellid + 2 * f), c1 = ld(m.face_cellid + 2 * f + 1);
+    const bool own = (i == c0);
+    const int other = own ? c1 : c0;
+    const bool b = c1 < 0;
+    const double vo = b ? ghost(f) : ld(w + other);  // unreconstructed value across the face
+    // upwind flux of face f in manapy's orientation (left = c0)
+    const double s = ld(sign + f);
+    double sol;
+    if (s >= 0) {
+      // left state
+      if (ORDER2) sol = reconstruct<DIM>(m, w, gx, gy, gz, psi, c0, f);
+      else sol = own ? wi : vo;
+    } else {
+      if (b) sol = vo;
+      else if (ORDER2) sol = reconstruct<DIM>(m, w, gx, gy, gz, psi, c1, f);
+      else sol = own ? vo : wi;
+    }
+    const double F = s * sol;
+    cv[j] = own ? -F : F;
+    bnd[j] = b;
+    if (DIFF) {
+      double v = 0.;
+      if (ld(bc.face_grad_on + f)) {
+        const double vl = own ? wi : vo;
+        const double vr = own ? vo : wi;
+        double fx, fy, fz;
+        face_gradient<DIM>(m, wn, f, vl, vr, fx, fy, fz);
+        const double *N = m.face_normal + 3 * f;
+        v = p.Dxx * fx * ld(N) + p.Dyy * fy * ld(N + 1) + p.Dzz * fz * ld(N + 2);
+      }
+      q[j] = own ? v : -v;
+    }
+  }
+  const uint8_t code = ld(m.cell_order + i);
+  double rez = 0.;
+#pragma unroll
+  for (int k = 0; k < nlf; ++k) {
+    const int s = order_slot(code, k);
+    if (!bnd[s]) rez += cv[s];
+  }
+#pragma unroll
+  for (int k = 0; k < nlf; ++k) {
+    const int s = order_slot(code, k);
+    if (bnd[s]) rez += cv[s];
+  }
+  double dis = 0.;
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < nlf; ++k) dis += q[order_slot(code, k)];
+  }
+  const double dt = *dt_dev;
+  const double sc = src ? ld(src + i) : 0.0;
+  w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
+}
+
+// ---------------------------------------------------------------- shallow-water order-2 pre-pass
+
+// Neumann ghost: the interior cell's value (the default boundary of a manapy Variable).
+struct NeumannCopy {
+  const double *w;
+  const int32_t *fcell;
+  __device__ __forceinline__ double operator()(int f) const { return ld(w + ld(fcell + 2 * f)); }
+};
+
+// h and hc LSQ gradients and hc's Barth limiter (manapy/solvers/shallowater/system.py:164-166).
+__global__ void __launch_bounds__(kBlock) k_sw_grad(mb_mesh m, const double *h, const double *hc, double *hx,
+                                                    double *hy, double *cx, double *cy, double *psi) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double x, y, z;
+    lsq_gradient<2>(m, h, NeumannCopy{h, m.face_cellid}, i, x, y, z);
+    hx[i] = x; hy[i] = y;
+    lsq_gradient<2>(m, hc, NeumannCopy{hc, m.face_cellid}, i, x, y, z);
+    cx[i] = x; cy[i] = y;
+    psi[i] = barth<2>(m, hc, NeumannCopy{hc, m.face_cellid}, i, x, y, 0.0);
+  }
+}
+
+// ---------------------------------------------------------------- launch helpers
+
+inline int grid_for(long long n) {
+  int g = ceil_div(n, kBlock);
+  const int cap = 148 * 16;
+  return g < 1 ? 1 : (g > cap ? cap : g);
+}
+
+inline int check_launch() { return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA; }
+
+template <int DIM, bool O2, bool DF>
+int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
+                double *w_out, const double *sign, const double *src, const double *dt, double *gx,
+                double *gy, double *gz, double *psi, double *wn, cudaStream_t st) {
+  const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
+  const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
+  if (ncb + nnb > 0)
+    k_step_phase1<DIM, O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, gx, gy, gz, psi, wn, ncb);
+  k_step_phase2<DIM, O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src,
+                                                                             dt, gx, gy, gz, psi, wn);
+  return check_launch();
+}
+
+int sw_gradients(const mb_mesh &m, const double *h, const double *hc, double *hx, double *hy, double *cx,
+                 double *cy, double *psi, cudaStream_t st) {
+  k_sw_grad<<<grid_for(m.nbcells), kBlock, 0, st>>>(m, h, hc, hx, hy, cx, cy, psi);
+  return check_launch();
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+static bool mesh_ok(const mb_mesh *m) {
+  return m && (m->dim == 2 || m->dim == 3) && m->nbcells > 0 && m->nbfaces > 0 && m->nbnodes > 0 &&
+         m->nlf == (m->dim == 2 ? 3 : 4);
+}
+
+#define ST(s) reinterpret_cast<cudaStream_t>(s)
+
+extern "C" {
+
+int mb_facetocell(const mb_mesh *m, const double *u_face, double *u_cell, void *stream) {
+  if (!mesh_ok(m) || !u_face || !u_cell) return MB_EINVAL;
+  k_facetocell<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, u_face, u_cell);
+  return check_launch();
+}
+
+int mb_ghost_value(const mb_mesh *m, const mb_bc *bc, const double *w_c, double *w_ghost, void *stream) {
+  if (!mesh_ok(m) || !bc || !w_c || !w_ghost) return MB_EINVAL;
+  k_ghost<<<grid_for(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, *bc, w_c, w_ghost);
+  return check_launch();
+}
+
+int mb_cell_gradient(const mb_mesh *m, const double *w_c, const double *w_ghost, double *w_x, double *w_y,
+                     double *w_z, void *stream) {
+  if (!mesh_ok(m) || !w_c || !w_ghost || !w_x || !w_y || !w_z) return MB_EINVAL;
+  if (m->dim == 2)
+    k_cell_gradient<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_x, w_y, w_z);
+  else
+    k_cell_gradient<3><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_x, w_y, w_z);
+  return check_launch();
+}
+
+int mb_barthlimiter(const mb_mesh *m, const double *w_c, const double *w_ghost, const double *w_x,
+                    const double *w_y, const double *w_z, double *psi, void *stream) {
+  if (!mesh_ok(m) || !w_c || !w_ghost || !w_x || !w_y || !w_z || !psi) return MB_EINVAL;
+  if (m->dim == 2)
+    k_barth<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_x, w_y, w_z, psi);
+  else
+    k_barth<3><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_x, w_y, w_z, psi);
+  return check_launch();
+}
+
+int mb_centertovertex(const mb_mesh *m, const double *w_c, const double *w_ghost, double *w_node,
+                      void *stream) {
+  if (!mesh_ok(m) || !w_c || !w_ghost || !w_node) return MB_EINVAL;
+  k_centertovertex<<<grid_for(m->nbnodes), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_node);
+  return check_launch();
+}
+
+int mb_face_gradient(const mb_mesh *m, const mb_bc *bc, const double *w_c, const double *w_ghost,
+                     const double *w_node, double *wx_face, double *wy_face, double *wz_face, void *stream) {
+  if (!mesh_ok(m) || !bc || !bc->face_grad_on || !w_c || !w_ghost || !w_node || !wx_face || !wy_face ||
+      (m->dim == 3 && !wz_face))
+    return MB_EINVAL;
+  if (m->dim == 2)
+    k_face_gradient<2><<<grid_for(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, bc->face_grad_on, w_c, w_ghost,
+                                                                         w_node, wx_face, wy_face, wz_face);
+  else
+    k_face_gradient<3><<<grid_for(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, bc->face_grad_on, w_c, w_ghost,
+                                                                         w_node, wx_face, wy_face, wz_face);
+  return check_launch();
+}
+
+int mb_explicitscheme_convective(const mb_mesh *m, double *rez_w, const double *w_c, const double *w_ghost,
+                                 const double *u_face, const double *v_face, const double *w_face,
+                                 const double *w_x, const double *w_y, const double *w_z, const double *psi,
+                                 int32_t order, void *stream) {
+  if (!mesh_ok(m) || !rez_w || !w_c || !w_ghost || !u_face || !v_face || !w_face || (order != 1 && order != 2))
+    return MB_EINVAL;
+  if (order == 2 && (!w_x || !w_y || !w_z || !psi)) return MB_EINVAL;
+  if (m->dim == 2)
+    k_convective<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, rez_w, w_c, w_ghost, u_face, v_face,
+                                                                      w_face, w_x, w_y, w_z, psi, order);
+  else
+    k_convective<3><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, rez_w, w_c, w_ghost, u_face, v_face,
+                                                                      w_face, w_x, w_y, w_z, psi, order);
+  return check_launch();
+}
+
+int mb_explicitscheme_dissipative(const mb_mesh *m, const double *wx_face, const double *wy_face,
+                                  const double *wz_face, double *dissip_w, double Dxx, double Dyy, double Dzz,
+                                  void *stream) {
+  if (!mesh_ok(m) || !wx_face || !wy_face || !wz_face || !dissip_w) return MB_EINVAL;
+  if (m->dim == 2)
+    k_dissipative<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, wx_face, wy_face, wz_face, dissip_w,
+                                                                       Dxx, Dyy, Dzz);
+  else
+    k_dissipative<3><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, wx_face, wy_face, wz_face, dissip_w,
+                                                                       Dxx, Dyy, Dzz);
+  return check_launch();
+}
+
+int mb_time_step(const mb_mesh *m, const double *u, const double *v, const double *w, double cfl, double Dxx,
+                 double Dyy, double Dzz, double *dt_dev, void *stream) {
+  if (!mesh_ok(m) || !u || !v || !w || !dt_dev) return MB_EINVAL;
+  k_fill<<<1, 1, 0, ST(stream)>>>(dt_dev, 1e6);
+  k_time_step<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, u, v, w, cfl, Dxx, Dyy, Dzz, dt_dev);
+  return check_launch();
+}
+
+int mb_update_new_value(const mb_mesh *m, double *ne_c, const double *rez, const double *dissip,
+                        const double *src, const double *dt_dev, void *stream) {
+  if (!mesh_ok(m) || !ne_c || !rez || !dissip || !src || !dt_dev) return MB_EINVAL;
+  k_update<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(m->nbcells, ne_c, rez, dissip, src, dt_dev,
+                                                            m->cell_volume);
+  return check_launch();
+}
+
+int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face, const double *w_face,
+                 double *sign_face, void *stream) {
+  if (!mesh_ok(m) || !u_face || !v_face || !w_face || !sign_face) return MB_EINVAL;
+  k_face_sign<<<grid_for(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, u_face, v_face, w_face, sign_face);
+  return check_launch();
+}
+
+int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p, const double *w_in,
+                    double *w_out, const double *sign_face, const double *src, const double *dt_dev, double *gx,
+                    double *gy, double *gz, double *psi, double *w_node, void *stream) {
+  if (!mesh_ok(m) || !bc || !p || !w_in || !w_out || w_in == w_out || !sign_face || !dt_dev) return MB_EINVAL;
+  if (p->order != 1 && p->order != 2) return MB_EINVAL;
+  const bool o2 = p->order == 2, df = p->diffusion != 0;
+  if (o2 && (!gx || !gy || !psi || (m->dim == 3 && !gz))) return MB_EINVAL;
+  if (df && (!w_node || !bc->face_grad_on)) return MB_EINVAL;
+  if (!bc->kind || !bc->value) return MB_EINVAL;
+  cudaStream_t st = ST(stream);
+#define MB_STEP(D, O, F) \
+  return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_face, src, dt_dev, gx, gy, gz, psi, w_node, st)
+  if (m->dim == 2) {
+    if (o2) { if (df) MB_STEP(2, true, true); else MB_STEP(2, true, false); }
+    else { if (df) MB_STEP(2, false, true); else MB_STEP(2, false, false); }
+  } else {
+    if (o2) { if (df) MB_STEP(3, true, true); else MB_STEP(3, true, false); }
+    else { if (df) MB_STEP(3, false, true); else MB_STEP(3, false, false); }
+  }
+#undef MB_STEP
+}
+
+}  // extern "C"

@@ -1,0 +1,478 @@
+// Shallow-water kernels: manapy's SRNH scheme on triangles, FP64.
+//
+// Reference loops (manapy source tree):
+//   srnh_scheme                   manapy/solvers/shallowater/fvm_utils.py:152-342
+//   explicitscheme_convective_SW  manapy/solvers/shallowater/fvm_utils.py:344-496
+//   term_source_srnh_SW           manapy/solvers/shallowater/fvm_utils.py:44-148
+//   time_step_SW                  manapy/solvers/shallowater/fvm_utils.py:16-42
+//   update_SW                     manapy/solvers/shallowater/fvm_utils.py:3-14
+//
+// The face flux costs two transcendentals, four square roots and ~30 divisions,
+// so each face flux is computed once (face kernel, one thread per face) and the
+// five residuals are gathered per cell in manapy's order (inner faces by
+// ascending id, then boundary faces by ascending id).
+#include "fv_common.cuh"
+
+namespace mb {
+
+// SRNH flux with As = 0 (so d = 0 and beta = 0).  Terms multiplied by those
+// zeros are kept, as in manapy, so that NaN/Inf propagate the same way.
+__device__ __forceinline__ void srnh(double hu_l, double hu_r, double hv_l, double hv_r, double h_l, double h_r,
+                                     double hc_l, double hc_r, double Z_l, double Z_r, double n0, double n1,
+                                     double mesure, double grav, double flux[5]) {
+  const double As = 0., p = 0.4, xi = 1 / (1 - p);
+  const double ninv0 = -1 * n1, ninv1 = n0;
+  const double sl = sqrt(h_l), sr = sqrt(h_r);
+  const double u_h = (hu_l / h_l * sl + hu_r / h_r * sr) / (sl + sr);
+  const double v_h = (hv_l / h_l * sl + hv_r / h_r * sr) / (sl + sr);
+  const double c_h = (hc_l / h_l * sl + hc_r / h_r * sr) / (sl + sr);
+  const double un_h = (u_h * n0 + v_h * n1) / mesure;
+  const double vn_h = (u_h * ninv0 + v_h * ninv1) / mesure;
+  const double hroe = (h_l + h_r) / 2, uroe = un_h, vroe = vn_h, croe = c_h;
+  const double uleft = (hu_l * n0 + hv_l * n1) / mesure;
+  const double vleft = (hu_l * ninv0 + hv_l * ninv1) / mesure;
+  const double uright = (hu_r * n0 + hv_r * n1) / mesure;
+  const double vright = (hu_r * ninv0 + hv_r * ninv1) / mesure;
+  double w_lrh = (h_l + h_r) / 2, w_lrhu = (uleft + uright) / 2, w_lrhv = (vleft + vright) / 2;
+  double w_lrhc = (hc_l + hc_r) / 2;
+  const double wd0 = h_r - h_l, wd1 = uright - uleft, wd2 = vright - vleft, wd3 = hc_r - hc_l, wd4 = Z_r - Z_l;
+  const double u2 = uroe * uroe;
+  const double d = As * xi * (3 * u2 + (vroe * vroe));
+  const double sound = sqrt(grav * hroe);
+  const double Q = -(u2 + 3 * grav * (hroe + d)) / 9;
+  const double R = uroe * (9 * grav * (2 * hroe - d) - 2 * u2) / 54;
+  const double theta = acos(R / (sqrt(-(Q * Q * Q))));
+  const double sq = 2 * sqrt(-Q);
+  const double lambda1 = sq * cos(theta / 3) + (2. / 3) * uroe;
+  const double lambda2 = sq * cos((theta + 2 * 3.141592653589793) / 3) + (2. / 3) * uroe;
+  const double lambda3 = sq * cos((theta + 4 * 3.141592653589793) / 3) + (2. / 3) * uroe;
+  const double lambda4 = uroe, lambda5 = uroe;
+  const double alpha1 = lambda1 - uroe, alpha2 = lambda2 - uroe, alpha3 = lambda3 - uroe;
+  const double beta = 2 * As * xi * vroe / hroe;
+  const double s2 = sound * sound;
+  const double gamma1 = s2 - u2 + lambda2 * lambda3 - beta * alpha2 * alpha3 * vroe;
+  const double gamma2 = s2 - u2 + lambda1 * lambda3 - beta * alpha1 * alpha3 * vroe;
+  const double gamma3 = s2 - u2 + lambda1 * lambda2 - beta * alpha1 * alpha2 * vroe;
+  const double sigma1 = -alpha1 * alpha2 + alpha2 * alpha3 - alpha1 * alpha3 + (alpha1 * alpha1);
+  const double sigma2 = alpha1 * alpha2 + alpha2 * alpha3 - alpha1 * alpha3 - (alpha2 * alpha2);
+  const double sigma3 = alpha1 * alpha2 - alpha2 * alpha3 - alpha1 * alpha3 + (alpha3 * alpha3);
+  const double eps = 1e-10;
+  const double sign1 = fabs(lambda1) < eps ? 0. : lambda1 / fabs(lambda1);
+  const double sign2 = fabs(lambda2) < eps ? 0. : lambda2 / fabs(lambda2);
+  const double sign3 = fabs(lambda3) < eps ? 0. : lambda3 / fabs(lambda3);
+  const double sign4 = fabs(lambda4) < eps ? 0. : lambda4 / fabs(lambda4);
+  const double sign5 = fabs(lambda5) < eps ? 0. : lambda5 / fabs(lambda5);
+  const double a1 = (alpha1 * alpha1) / s2 - 1, a2 = (alpha2 * alpha2) / s2 - 1, a3 = (alpha3 * alpha3) / s2 - 1;
+  const double g1 = gamma1 / sigma1, g2 = gamma2 / sigma2, g3 = gamma3 / sigma3;
+  // column 1
+  const double r00 = sign1 * g1 - sign2 * g2 + sign3 * g3 + sign5 * (beta * vroe);
+  const double r10 = lambda1 * sign1 * g1 - lambda2 * sign2 * g2 + lambda3 * sign3 * g3 + sign5 * (beta * uroe * vroe);
+  const double r20 = vroe * sign1 * g1 - vroe * sign2 * g2 + vroe * sign3 * g3 - vroe * sign5 * (1 - beta * vroe);
+  const double r30 = croe * sign1 * g1 - croe * sign2 * g2 + croe * sign3 * g3 - croe * sign4 + croe * sign5 * beta * vroe;
+  const double r40 = a1 * sign1 * g1 - a2 * sign2 * g2 + a3 * sign3 * g3 - sign5 * (beta * vroe);
+  // column 2
+  const double t1 = (alpha2 + alpha3), t2 = (alpha1 + alpha3), t3 = (alpha1 + alpha2);
+  const double r01 = -sign1 * t1 / sigma1 + sign2 * t2 / sigma2 - sign3 * t3 / sigma3;
+  const double r11 = -lambda1 * sign1 * t1 / sigma1 + lambda2 * sign2 * t2 / sigma2 - lambda3 * sign3 * t3 / sigma3;
+  const double r21 = -vroe * sign1 * t1 / sigma1 + vroe * sign2 * t2 / sigma2 - vroe * sign3 * t3 / sigma3;
+  const double r31 = -croe * sign1 * t1 / sigma1 + croe * sign2 * t2 / sigma2 - croe * sign3 * t3 / sigma3;
+  const double r41 = -a1 * sign1 * t1 / sigma1 + a2 * sign2 * t2 / sigma2 - a3 * sign3 * t3 / sigma3;
+  // column 3
+  const double r02 = sign1 * beta * alpha2 * alpha3 / sigma1 - sign2 * beta * alpha1 * alpha3 / sigma2 +
+                     sign3 * beta * alpha1 * alpha2 / sigma3 - sign5 * beta;
+  const double r12 = lambda1 * sign1 * beta * alpha2 * alpha3 / sigma1 - lambda2 * sign2 * beta * alpha1 * alpha3 / sigma2 +
+                     lambda3 * sign3 * beta * alpha1 * alpha2 / sigma3 - sign5 * beta * uroe;
+  const double r22 = vroe * sign1 * beta * alpha2 * alpha3 / sigma1 - vroe * sign2 * beta * alpha1 * alpha3 / sigma2 +
+                     vroe * sign3 * beta * alpha1 * alpha2 / sigma3 + sign5 * (1 - beta * vroe);
+  const double r32 = croe * sign1 * beta * alpha2 * alpha3 / sigma1 - croe * sign2 * beta * alpha1 * alpha3 / sigma2 +
+                     croe * sign3 * beta * alpha1 * alpha2 / sigma3 - croe * sign5 * beta;
+  const double r42 = a1 * sign1 * beta * alpha2 * alpha3 / sigma1 - a2 * sign2 * beta * alpha1 * alpha3 / sigma2 +
+                     a3 * sign3 * beta * alpha1 * alpha2 / sigma3 + sign5 * beta;
+  // column 4: only rmat[3][3] = sign4 is non-zero
+  // column 5
+  const double r04 = sign1 * s2 / sigma1 - sign2 * s2 / sigma2 + sign3 * s2 / sigma3;
+  const double r14 = lambda1 * sign1 * s2 / sigma1 - lambda2 * sign2 * s2 / sigma2 + lambda3 * sign3 * s2 / sigma3;
+  const double r24 = vroe * sign1 * s2 / sigma1 - vroe * sign2 * s2 / sigma2 + vroe * sign3 * s2 / sigma3;
+  const double r34 = croe * sign1 * s2 / sigma1 - croe * sign2 * s2 / sigma2 + croe * sign3 * s2 / sigma3;
+  const double r44 = a1 * sign1 * s2 / sigma1 - a2 * sign2 * s2 / sigma2 + a3 * sign3 * s2 / sigma3;
+  // rows . w_dif, summed left to right from 0 as manapy's sum() does
+  const double hnew = 0. + r00 * wd0 + r01 * wd1 + r02 * wd2 + 0. * wd3 + r04 * wd4;
+  const double unew0 = 0. + r10 * wd0 + r11 * wd1 + r12 * wd2 + 0. * wd3 + r14 * wd4;
+  const double vnew0 = 0. + r20 * wd0 + r21 * wd1 + r22 * wd2 + 0. * wd3 + r24 * wd4;
+  const double cnew = 0. + r30 * wd0 + r31 * wd1 + r32 * wd2 + sign4 * wd3 + r34 * wd4;
+  (void)r40; (void)r41; (void)r42; (void)r44;
+  w_lrh = w_lrh - hnew / 2;
+  w_lrhu = w_lrhu - unew0 / 2;
+  w_lrhv = w_lrhv - vnew0 / 2;
+  w_lrhc = w_lrhc - cnew / 2;
+  double unew = (w_lrhu * n0 + w_lrhv * -1 * n1) / mesure;
+  double vnew = (w_lrhu * -1 * ninv0 + w_lrhv * ninv1) / mesure;
+  const double q_s = n0 * unew + n1 * vnew;
+  flux[0] = q_s;
+  flux[1] = q_s * unew / w_lrh + 0.5 * grav * w_lrh * w_lrh * n0;
+  flux[2] = q_s * vnew / w_lrh + 0.5 * grav * w_lrh * w_lrh * n1;
+  flux[3] = q_s * w_lrhc / w_lrh;
+  const double w3 = w_lrh * w_lrh * w_lrh;
+  const double uv = (unew * unew) + (vnew * vnew);
+  flux[4] = As * xi * n0 * unew * uv / w3 + As * xi * n1 * vnew * uv / w3;
+}
+
+struct SWState {
+  const double *q[5];  // h, hu, hv, hc, Z (cells)
+  const double *g[5];  // ghosts (faces); null -> neumann copy of the interior cell
+  const double *gr[4]; // h_x, h_y, hc_x, hc_y (order 2)
+  const double *psi;   // hc's limiter (order 2)
+};
+
+__device__ __forceinline__ double sw_ghost(const SWState &s, int k, int f, int c0) {
+  return s.g[k] ? ld(s.g[k] + f) : ld(s.q[k] + c0);
+}
+
+template <bool ORDER2>
+__global__ void __launch_bounds__(kBlock) k_sw_face_flux(mb_mesh m, SWState s, double grav, double *ff) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nbfaces; f += gridDim.x * blockDim.x) {
+    const int l = ld(m.face_cellid + 2 * f), r = ld(m.face_cellid + 2 * f + 1);
+    const double *N = m.face_normal + 3 * f;
+    const double n0 = ld(N), n1 = ld(N + 1), mes = ld(m.face_mesure + f);
+    double h_l = ld(s.q[0] + l), hc_l = ld(s.q[3] + l);
+    double h_r, hu_r, hv_r, hc_r, Z_r;
+    const double *fc = m.face_center + 3 * f, *cc = m.cell_center;
+    if (ORDER2) {
+      const double rl0 = ld(fc) - ld(cc + 3 * l), rl1 = ld(fc + 1) - ld(cc + 3 * l + 1);
+      const double pl = ld(s.psi + l);
+      h_l = h_l + pl * (ld(s.gr[0] + l) * rl0 + ld(s.gr[1] + l) * rl1);
+      hc_l = hc_l + pl * (ld(s.gr[2] + l) * rl0 + ld(s.gr[3] + l) * rl1);
+    }
+    if (r >= 0) {
+      h_r = ld(s.q[0] + r); hu_r = ld(s.q[1] + r); hv_r = ld(s.q[2] + r); hc_r = ld(s.q[3] + r);
+      Z_r = ld(s.q[4] + r);
+      if (ORDER2) {
+        const double rr0 = ld(fc) - ld(cc + 3 * r), rr1 = ld(fc + 1) - ld(cc + 3 * r + 1);
+        const double pr = ld(s.psi + r);
+        h_r = h_r + pr * (ld(s.gr[0] + r) * rr0 + ld(s.gr[1] + r) * rr1);
+        hc_r = hc_r + pr * (ld(s.gr[2] + r) * rr0 + ld(s.gr[3] + r) * rr1);
+      }
+    } else {
+      h_r = sw_ghost(s, 0, f, l); hu_r = sw_ghost(s, 1, f, l); hv_r = sw_ghost(s, 2, f, l);
+      hc_r = sw_ghost(s, 3, f, l); Z_r = sw_ghost(s, 4, f, l);
+    }
+    double fl[5];
+    srnh(ld(s.q[1] + l), hu_r, ld(s.q[2] + l), hv_r, h_l, h_r, hc_l, hc_r, ld(s.q[4] + l), Z_r, n0, n1, mes, grav, fl);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) ff[(long long)5 * f + k] = fl[k];
+  }
+}
+
+__device__ __forceinline__ int order_slot_sw(uint8_t code, int k) { return (code >> (2 * k)) & 3; }
+
+// Residuals of cell i gathered in manapy's order.
+__device__ __forceinline__ void sw_gather(const mb_mesh &m, const double *__restrict__ ff, int i, double rez[5]) {
+  int fs[3];
+  bool own[3], bnd[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int f = ld(m.cell_faces + 4 * i + j);
+    fs[j] = f;
+    own[j] = ld(m.face_cellid + 2 * f) == i;
+    bnd[j] = ld(m.face_cellid + 2 * f + 1) < 0;
+  }
+  const uint8_t code = ld(m.cell_order + i);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) rez[k] = 0.;
+#pragma unroll
+  for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int s = order_slot_sw(code, k);
+      if (bnd[s] != (pass == 1)) continue;
+      const double *F = ff + (long long)5 * fs[s];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) rez[c] = own[s] ? rez[c] - ld(F + c) : rez[c] + ld(F + c);
+    }
+  }
+}
+
+// Well-balanced bathymetry source of triangle i -> (src_hu, src_hv).
+template <class GH, class GZ>
+__device__ __forceinline__ void sw_source(const mb_mesh &m, const double *__restrict__ h,
+                                          const double *__restrict__ Z, GH hg, GZ zg, double grav, int i,
+                                          double &shu, double &shv) {
+  const double G0 = ld(m.cell_center + 3 * i), G1 = ld(m.cell_center + 3 * i + 1);
+  double c_1 = 0., c_2 = 0.;
+  double ss[3][3], mata[3], matb[3], zv[3];
+  const double h_1p = ld(h + i), z_1p = ld(Z + i);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int f = ld(m.cell_faces + 4 * i + j);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ss[j][c] = ld(m.cell_nf + 9 * i + 3 * j + c);
+    double h_p1, z_p1;
+    if (ld(m.face_name + f) == 0) {
+      // cells.cellfid is compacted, so slot j may hold the -1 padding; manapy's
+      // Numba indexing wraps it to the last cell.
+      int nb = ld(m.cell_cellfid + 4 * i + j);
+      if (nb < 0) nb += m.nbcells;
+      h_p1 = ld(h + nb);
+      z_p1 = ld(Z + nb);
+    } else {
+      h_p1 = hg(f);
+      z_p1 = zg(f);
+    }
+    zv[j] = z_p1;
+    mata[j] = h_p1 * ss[j][0];
+    matb[j] = h_p1 * ss[j][1];
+    const double hm = 0.5 * (h_1p + h_p1);
+    c_1 = c_1 + (hm * 0.5 * (h_1p + h_p1)) * ss[j][0];
+    c_2 = c_2 + (hm * 0.5 * (h_1p + h_p1)) * ss[j][1];
+  }
+  const double c_3 = 3.0 * h_1p;
+  const double delta = (mata[1] * matb[2] - mata[2] * matb[1]) - (mata[0] * matb[2] - matb[0] * mata[2]) +
+                       (mata[0] * matb[1] - matb[0] * mata[1]);
+  const double deltax = c_3 * (mata[1] * matb[2] - mata[2] * matb[1]) - (c_1 * matb[2] - c_2 * mata[2]) +
+                        (c_1 * matb[1] - c_2 * mata[1]);
+  const double deltay = (c_1 * matb[2] - c_2 * mata[2]) - c_3 * (mata[0] * matb[2] - matb[0] * mata[2]) +
+                        (mata[0] * c_2 - matb[0] * c_1);
+  const double deltaz = (mata[1] * c_2 - matb[1] * c_1) - (mata[0] * c_2 - matb[0] * c_1) +
+                        c_3 * (mata[0] * matb[1] - matb[0] * mata[1]);
+  const double h_1 = deltax / delta, h_2 = deltay / delta, h_3 = deltaz / delta;
+  const double z_1 = z_1p + h_1p - h_1, z_2 = z_1p + h_1p - h_2, z_3 = z_1p + h_1p - h_3;
+  const double b0 = ld(m.cell_vertex1 + 2 * i), b1 = ld(m.cell_vertex1 + 2 * i + 1);
+  const double ns0[2] = {(G1 - b1), -(G0 - b0)};
+  double ns1[2], ns2[2], s1[2], s2[2], s3[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) { ns1[c] = ns0[c] - ss[1][c]; ns2[c] = ns0[c] + ss[0][c]; }
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    s1[c] = 0.5 * h_1 * (zv[0] * ss[0][c] + z_2 * ns0[c] + z_3 * (-1) * ns2[c]);
+    s2[c] = 0.5 * h_2 * (zv[1] * ss[1][c] + z_1 * (-1) * ns0[c] + z_3 * ns1[c]);
+    s3[c] = 0.5 * h_3 * (zv[2] * ss[2][c] + z_1 * ns2[c] + z_2 * (-1) * ns1[c]);
+  }
+  shu = -grav * (s1[0] + s2[0] + s3[0]);
+  shv = -grav * (s1[1] + s2[1] + s3[1]);
+}
+
+struct FaceArr {
+  const double *g;
+  __device__ __forceinline__ double operator()(int f) const { return ld(g + f); }
+};
+struct FaceCopy {  // neumann ghost: the interior cell's value
+  const double *q;
+  const int32_t *fcell;
+  __device__ __forceinline__ double operator()(int f) const { return ld(q + ld(fcell + 2 * f)); }
+};
+
+__global__ void __launch_bounds__(kBlock) k_time_step_sw(mb_mesh m, const double *h, const double *hu,
+                                                         const double *hv, double cfl, double grav, double Dxx,
+                                                         double Dyy, double *dt) {
+  double best = 1e300;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    const double hi = ld(h + i), hui = ld(hu + i), hvi = ld(hv + i), vol = ld(m.cell_volume + i);
+    const double velson = sqrt(grav * hi);
+    double lam = 0.;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int f = ld(m.cell_faces + 4 * i + j);
+      const double *N = m.face_normal + 3 * f;
+      const double n0 = ld(N), n1 = ld(N + 1), mf = ld(m.face_mesure + f);
+      const double u_n = fabs(hui / hi * n0 + hvi / hi * n1);
+      lam += (u_n / mf + velson) * mf;
+      const double mes = sqrt(n0 * n0 + n1 * n1);
+      lam += (Dxx * (mes * mes) + Dyy * (mes * mes)) / vol;
+    }
+    best = pmin(best, cfl * vol / lam);
+  }
+  best = block_min(best);
+  if (threadIdx.x == 0 && best < 1e300) atomic_min_pos(dt, best);
+}
+
+__global__ void __launch_bounds__(kBlock) k_sw_gather_rez(mb_mesh m, const double *ff, double *r0, double *r1,
+                                                          double *r2, double *r3, double *r4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double rez[5];
+    sw_gather(m, ff, i, rez);
+    r0[i] = rez[0]; r1[i] = rez[1]; r2[i] = rez[2]; r3[i] = rez[3]; r4[i] = rez[4];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_sw_source(mb_mesh m, const double *h, const double *Z,
+                                                      const double *hg, const double *zg, double grav,
+                                                      double *shu, double *shv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double a, b;
+    sw_source(m, h, Z, FaceArr{hg}, FaceArr{zg}, grav, i, a, b);
+    shu[i] = a;
+    shv[i] = b;
+  }
+}
+
+struct SWQ {
+  double *q[5];
+};
+struct SWR {
+  const double *r[5];
+};
+
+__global__ void __launch_bounds__(kBlock) k_update_sw(int n, SWQ q, SWR r, const double *shu, const double *shv,
+                                                      const double *dt_dev, const double *vol) {
+  const double dt = *dt_dev;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = ld(vol + i);
+    q.q[0][i] += dt * (ld(r.r[0] + i) + 0.) / v;
+    q.q[1][i] += dt * ((ld(r.r[1] + i) + ld(shu + i)) / v + 0. + 0.);
+    q.q[2][i] += dt * ((ld(r.r[2] + i) + ld(shv + i)) / v + 0. + 0.);
+    q.q[3][i] += dt * (ld(r.r[3] + i) + 0. - 0.) / v;
+    q.q[4][i] += dt * (ld(r.r[4] + i) + 0.) / v;
+  }
+}
+
+// Fused gather + source + update of one step (neumann ghosts), q_in -> q_out.
+__global__ void __launch_bounds__(kBlock) k_sw_cell_update(mb_mesh m, SWState s, SWQ out, const double *ff,
+                                                           const double *dt_dev, double grav) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  double rez[5];
+  sw_gather(m, ff, i, rez);
+  double shu, shv;
+  sw_source(m, s.q[0], s.q[4], FaceCopy{s.q[0], m.face_cellid}, FaceCopy{s.q[4], m.face_cellid}, grav, i, shu, shv);
+  const double dt = *dt_dev, v = ld(m.cell_volume + i);
+  out.q[0][i] = ld(s.q[0] + i) + dt * (rez[0] + 0.) / v;
+  out.q[1][i] = ld(s.q[1] + i) + dt * ((rez[1] + shu) / v + 0. + 0.);
+  out.q[2][i] = ld(s.q[2] + i) + dt * ((rez[2] + shv) / v + 0. + 0.);
+  out.q[3][i] = ld(s.q[3] + i) + dt * (rez[3] + 0. - 0.) / v;
+  out.q[4][i] = ld(s.q[4] + i) + dt * (rez[4] + 0.) / v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_srnh_batch(int n, const double *st, const double *nrm,
+                                                       const double *mes, double grav, double *flux) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double *s = st + 10 * (long long)k;
+    double fl[5];
+    srnh(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], s[8], s[9], nrm[3 * k], nrm[3 * k + 1], mes[k], grav, fl);
+    for (int c = 0; c < 5; ++c) flux[5 * (long long)k + c] = fl[c];
+  }
+}
+
+__global__ void k_fill_sw(double *p, double v) { *p = v; }
+
+inline int grid_for_sw(long long n) {
+  int g = ceil_div(n, kBlock);
+  const int cap = 148 * 16;
+  return g < 1 ? 1 : (g > cap ? cap : g);
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+#define ST(s) reinterpret_cast<cudaStream_t>(s)
+
+static bool sw_mesh_ok(const mb_mesh *m) {
+  return m && m->dim == 2 && m->nlf == 3 && m->nbcells > 0 && m->nbfaces > 0;
+}
+
+// declared in fv_advdiff.cu
+namespace mb {
+int sw_gradients(const mb_mesh &m, const double *h, const double *hc, double *hx, double *hy, double *cx,
+                 double *cy, double *psi, cudaStream_t st);
+}
+
+extern "C" {
+
+int mb_srnh_flux(int32_t n, const double *states, const double *normals, const double *mesure, double grav,
+                 double *flux, void *stream) {
+  if (n < 0 || (n > 0 && (!states || !normals || !mesure || !flux))) return MB_EINVAL;
+  if (n == 0) return MB_OK;
+  k_srnh_batch<<<grid_for_sw(n), kBlock, 0, ST(stream)>>>(n, states, normals, mesure, grav, flux);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_time_step_sw(const mb_mesh *m, const double *h, const double *hu, const double *hv, double cfl,
+                    double grav, double Dxx, double Dyy, double *dt_dev, void *stream) {
+  if (!sw_mesh_ok(m) || !h || !hu || !hv || !dt_dev) return MB_EINVAL;
+  k_fill_sw<<<1, 1, 0, ST(stream)>>>(dt_dev, 1e6);
+  k_time_step_sw<<<grid_for_sw(m->nbcells), kBlock, 0, ST(stream)>>>(*m, h, hu, hv, cfl, grav, Dxx, Dyy, dt_dev);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_explicitscheme_convective_sw(const mb_mesh *m, double *const rez[5], const double *const q[5],
+                                    const double *const g[5], const double *const grads[4], const double *psi,
+                                    double grav, int32_t order, double *face_flux, void *stream) {
+  if (!sw_mesh_ok(m) || !rez || !q || !g || !face_flux || (order != 1 && order != 2)) return MB_EINVAL;
+  SWState s{};
+  for (int k = 0; k < 5; ++k) {
+    if (!rez[k] || !q[k] || !g[k]) return MB_EINVAL;
+    s.q[k] = q[k];
+    s.g[k] = g[k];
+  }
+  if (order == 2) {
+    if (!grads || !psi) return MB_EINVAL;
+    for (int k = 0; k < 4; ++k) {
+      if (!grads[k]) return MB_EINVAL;
+      s.gr[k] = grads[k];
+    }
+    s.psi = psi;
+    k_sw_face_flux<true><<<grid_for_sw(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, s, grav, face_flux);
+  } else {
+    k_sw_face_flux<false><<<grid_for_sw(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, s, grav, face_flux);
+  }
+  k_sw_gather_rez<<<grid_for_sw(m->nbcells), kBlock, 0, ST(stream)>>>(*m, face_flux, rez[0], rez[1], rez[2],
+                                                                       rez[3], rez[4]);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_term_source_srnh_sw(const mb_mesh *m, const double *h, const double *Z, const double *h_ghost,
+                           const double *Z_ghost, double grav, double *src_hu, double *src_hv, void *stream) {
+  if (!sw_mesh_ok(m) || !h || !Z || !h_ghost || !Z_ghost || !src_hu || !src_hv || !m->cell_cellfid ||
+      !m->cell_nf || !m->cell_vertex1)
+    return MB_EINVAL;
+  k_sw_source<<<grid_for_sw(m->nbcells), kBlock, 0, ST(stream)>>>(*m, h, Z, h_ghost, Z_ghost, grav, src_hu, src_hv);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_update_sw(const mb_mesh *m, double *const q[5], const double *const rez[5], const double *src_hu,
+                 const double *src_hv, const double *dt_dev, void *stream) {
+  if (!sw_mesh_ok(m) || !q || !rez || !src_hu || !src_hv || !dt_dev) return MB_EINVAL;
+  SWQ qq;
+  SWR rr;
+  for (int k = 0; k < 5; ++k) {
+    if (!q[k] || !rez[k]) return MB_EINVAL;
+    qq.q[k] = q[k];
+    rr.r[k] = rez[k];
+  }
+  k_update_sw<<<grid_for_sw(m->nbcells), kBlock, 0, ST(stream)>>>(m->nbcells, qq, rr, src_hu, src_hv, dt_dev,
+                                                                   m->cell_volume);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
+               int32_t order, double *scratch, double *face_flux, double *dt_dev, void *stream) {
+  if (!sw_mesh_ok(m) || !q_in || !q_out || !face_flux || !dt_dev || (order != 1 && order != 2)) return MB_EINVAL;
+  if (!m->cell_cellfid || !m->cell_nf || !m->cell_vertex1) return MB_EINVAL;
+  SWState s{};
+  SWQ out;
+  for (int k = 0; k < 5; ++k) {
+    if (!q_in[k] || !q_out[k] || q_in[k] == q_out[k]) return MB_EINVAL;
+    s.q[k] = q_in[k];
+    s.g[k] = nullptr;  // neumann ghosts
+    out.q[k] = q_out[k];
+  }
+  cudaStream_t st = ST(stream);
+  int rc = mb_time_step_sw(m, q_in[0], q_in[1], q_in[2], cfl, grav, 0.0, 0.0, dt_dev, stream);
+  if (rc != MB_OK) return rc;
+  if (order == 2) {
+    if (!scratch) return MB_EINVAL;
+    const long long n = m->nbcells;
+    double *hx = scratch, *hy = scratch + n, *cx = scratch + 2 * n, *cy = scratch + 3 * n, *psi = scratch + 4 * n;
+    rc = sw_gradients(*m, q_in[0], q_in[3], hx, hy, cx, cy, psi, st);
+    if (rc != MB_OK) return rc;
+    s.gr[0] = hx; s.gr[1] = hy; s.gr[2] = cx; s.gr[3] = cy;
+    s.psi = psi;
+    k_sw_face_flux<true><<<grid_for_sw(m->nbfaces), kBlock, 0, st>>>(*m, s, grav, face_flux);
+  } else {
+    k_sw_face_flux<false><<<grid_for_sw(m->nbfaces), kBlock, 0, st>>>(*m, s, grav, face_flux);
+  }
+  k_sw_cell_update<<<ceil_div(m->nbcells, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_dev, grav);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+"""Device-resident mesh tables and ghost rules (the ``mb_mesh`` / ``mb_bc`` of the C ABI).
+
+``DeviceMesh`` turns the host arrays of ``geometry.build`` into the tables the
+kernels read: SoA geometry, CSR neighbour lists, per-cell face slots with the
+order manapy accumulates them in, and precomputed centre->vertex weights.
+Device memory comes from torch tensors (the allocator is plumbing only); the
+kernels are called through the C ABI with their raw pointers.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .geometry import padded_from_csr  # noqa: F401  (re-export for callers)
+
+
+def _t(a, dtype, dev):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)
+
+
+def cell_order_codes(faceid_local):
+    """uint8 per cell: slot visited k-th in ascending face id, 2 bits per k."""
+    order = np.argsort(faceid_local, axis=1, kind="stable").astype(np.uint32)
+    code = np.zeros(len(order), dtype=np.uint32)
+    for k in range(order.shape[1]):
+        code |= order[:, k] << (2 * k)
+    return code.astype(np.uint8)
+
+
+def vertex_weights(A):
+    """Centre->vertex weight of every node->cell and node->ghost incidence, in
+    manapy's expression order (manapy/ast/functions2d.py:219, functions3d.py:272-274)."""
+    dim = A["dim"]
+    vx = A["nodes_vertex"]
+    lx, ly, lz = A["nodes_lambda_x"], A["nodes_lambda_y"], A["nodes_lambda_z"]
+    Rx, Ry, Rz = A["nodes_R_x"], A["nodes_R_y"], A["nodes_R_z"]
+    num = A["nodes_number"].astype(np.float64)
+    if dim == 2:
+        den = num + lx * Rx + ly * Ry
+    else:
+        den = num + lx * Rx + ly * Ry + lz * Rz
+
+    def alpha(ptr, pts):
+        node = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+        xd = pts[:, 0] - vx[node, 0]
+        yd = pts[:, 1] - vx[node, 1]
+        if dim == 2:
+            num_ = 1. + lx[node] * xd + ly[node] * yd
+        else:
+            zd = pts[:, 2] - vx[node, 2]
+            num_ = 1. + lx[node] * xd + ly[node] * yd + lz[node] * zd
+        return num_ / den[node]
+
+    a_c = alpha(A["n2c_ptr"], A["cells_center"][A["n2c_idx"]])
+    a_g = alpha(A["n2g_ptr"], A["faces_ghostcenter"][A["n2g_idx"], :3])
+    return a_c, a_g
+
+
+class DeviceMesh:
+    """All mesh tables on one CUDA device plus the ``mb_mesh`` struct pointing at them.
+
+    With ``reorder=True`` (the default) the tables use the locality numbering of
+    ``reorder.Renumbering``; ``to_device_order`` / ``to_host_order`` move field
+    arrays between that numbering and manapy's.
+    """
+
+    def __init__(self, A, device="cuda", reorder=True):
+        from .reorder import Renumbering
+        dev = torch.device(device)
+        self.device = dev
+        self.A = A
+        dim = int(A["dim"])
+        nc, nf, nn = int(A["nbcells"]), int(A["nbfaces"]), int(A["nbnodes"])
+        nlf = 3 if dim == 2 else 4
+        if len(A.get("unmatched_boundary_faces", ())):
+            raise ValueError("mesh has boundary faces that match no boundary side (manapy names them "
+                             "100/200 and leaves them out of every face list)")
+        self.dim, self.nbcells, self.nbfaces, self.nbnodes, self.nlf = dim, nc, nf, nn, nlf
+        R = Renumbering(A, enabled=reorder)
+        self.R = R
+        cp, fp, np_ = R.cperm, R.fperm, R.nperm
+        ci, fi, ni = R.cinv, R.finv, R.ninv
+        f64, i32 = np.float64, np.int32
+        T = {}
+        T["cell_center"] = _t(A["cells_center"][cp], f64, dev)
+        T["cell_volume"] = _t(A["cells_volume"][cp], f64, dev)
+        faces_old = A["cells_faceid"][cp, :nlf]
+        faces = np.full((nc, 4), -1, dtype=i32)
+        faces[:, :nlf] = fi[faces_old]
+        T["cell_faces"] = _t(faces, i32, dev)
+        # accumulation order: ascending manapy face id
+        T["cell_order"] = _t(cell_order_codes(faces_old), np.uint8, dev)
+        if "cellnid_ptr" in A:
+            ptr, idx, _ = R.relabel_csr(A["cellnid_ptr"], A["cellnid_idx"], cp, ci)
+            T["cellnid_ptr"] = _t(ptr, i32, dev)
+            T["cellnid_idx"] = _t(idx, i32, dev)
+        ptr, idx, _ = R.relabel_csr(A["ghostnid_ptr"], A["ghostnid_idx"], cp, fi)
+        T["ghostnid_ptr"] = _t(ptr, i32, dev)
+        T["ghostnid_idx"] = _t(idx, i32, dev)
+        cid = A["faces_cellid"][fp]
+        cid_new = np.where(cid >= 0, ci[np.maximum(cid, 0)], -1)
+        T["face_cellid"] = _t(cid_new, i32, dev)
+        fn = np.full((nf, 4), -1, dtype=i32)
+        k = A["faces_nodeid"].shape[1] - 1
+        fn[:, :k] = ni[A["faces_nodeid"][fp, :k]]
+        T["face_nodeid"] = _t(fn, i32, dev)
+        T["face_name"] = _t(A["faces_name"][fp], i32, dev)
+        T["face_normal"] = _t(A["faces_normal"][fp], f64, dev)
+        T["face_center"] = _t(A["faces_center"][fp], f64, dev)
+        T["face_mesure"] = _t(A["faces_mesure"][fp], f64, dev)
+        T["face_ghostcenter"] = _t(A["faces_ghostcenter"][fp, :3], f64, dev)
+        T["face_air"] = _t(A["faces_airDiamond"][fp], f64, dev)
+        if dim == 2:
+            ff = np.concatenate([A["faces_f_1"], A["faces_f_2"], A["faces_f_3"], A["faces_f_4"]], axis=1)
+        else:
+            ff = np.concatenate([A["faces_f_1"], A["faces_f_2"]], axis=1)
+        T["face_f"] = _t(ff[fp], f64, dev)
+        T["face_dist"] = _t(A["faces_dist_ortho"][fp], f64, dev)
+        a_c, a_g = vertex_weights(A)
+        ptr, idx, src = R.relabel_csr(A["n2c_ptr"], A["n2c_idx"], np_, ci)
+        T["n2c_ptr"], T["n2c_idx"], T["n2c_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_c[src], f64, dev)
+        ptr, idx, src = R.relabel_csr(A["n2g_ptr"], A["n2g_idx"], np_, fi)
+        T["n2g_ptr"], T["n2g_idx"], T["n2g_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_g[src], f64, dev)
+        if dim == 2:
+            # compacted face-neighbour table; its -1 padding is read by manapy as the
+            # last cell (negative-index wrap), which is cell ci[nc-1] in this numbering
+            cf_old = A["cells_cellfid"][cp, :3]
+            cf = np.full((nc, 4), -1, dtype=i32)
+            cf[:, :3] = np.where(cf_old >= 0, ci[np.maximum(cf_old, 0)], ci[nc - 1])
+            T["cell_cellfid"] = _t(cf, i32, dev)
+            T["cell_nf"] = _t(A["cells_nf"][cp], f64, dev)
+            T["cell_vertex1"] = _t(A["nodes_vertex"][A["cells_nodeid"][cp, 1], :2], f64, dev)
+        self.t = T
+        s = _lib.MbMesh()
+        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = dim, nc, nf, nn, nlf, 0
+        for name, _ in _lib.MbMesh._fields_:
+            if name in T:
+                setattr(s, name, T[name].data_ptr())
+        self.struct = s
+        # field permutations: device[k] = host[perm[k]], host[j] = device[inv[j]]
+        self.perm = {"cell": torch.from_numpy(cp).to(dev), "face": torch.from_numpy(fp).to(dev),
+                     "node": torch.from_numpy(np_).to(dev)}
+        self.inv = {"cell": torch.from_numpy(ci).to(dev), "face": torch.from_numpy(fi).to(dev),
+                    "node": torch.from_numpy(ni).to(dev)}
+        self.reordered = bool(reorder)
+
+    def to_device_order(self, kind, host_t, out):
+        """out[k] = host_t[perm[k]] (``host_t`` already on the device, manapy order)."""
+        if not self.reordered or kind is None:
+            out.copy_(host_t)
+        else:
+            torch.index_select(host_t, 0, self.perm[kind], out=out)
+
+    def to_host_order(self, kind, dev_t):
+        if not self.reordered or kind is None:
+            return dev_t
+        return torch.index_select(dev_t, 0, self.inv[kind])
+
+    def has_lsq(self):
+        return "cellnid_ptr" in self.t
+
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in self.t.values())
+
+
+class DeviceBC:
+    """One variable's ghost rules on the device (``mb_bc``)."""
+
+    def __init__(self, A, resolved, device="cuda", mesh=None):
+        from .boundary import G_CELL_AT_FACE
+        dev = torch.device(device)
+        nf = int(A["nbfaces"])
+        self.resolved = resolved
+        fp = mesh.R.fperm if mesh is not None else np.arange(nf)
+        ci = mesh.R.cinv if mesh is not None else np.arange(int(A["nbcells"]))
+        kind = resolved.kind
+        value = resolved.value.copy()
+        # MB_G_CELL_AT_FACE reads the cell array at the face's manapy index; the cell
+        # to read (in the device numbering) travels in value[f]
+        caf = np.nonzero(kind == G_CELL_AT_FACE)[0]
+        value[caf] = ci[caf]
+        self.kind = _t(kind[fp], np.int8, dev)
+        self.value = _t(value[fp], np.float64, dev)
+        on = np.zeros(nf, dtype=np.uint8)
+        on[A["innerfaces"]] = 1
+        on[resolved.dirichletfaces] = 1
+        on[resolved.neumannfaces] = 1
+        self.face_grad_on = _t(on[fp], np.uint8, dev)
+        s = _lib.MbBC()
+        s.kind = self.kind.data_ptr()
+        s.value = self.value.data_ptr()
+        s.face_grad_on = self.face_grad_on.data_ptr()
+        self.struct = s

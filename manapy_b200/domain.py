@@ -1,0 +1,186 @@
+"""``Domain``: manapy's mesh object, built on the host and mirrored on the GPU.
+
+Mirrors ``manapy.ddm.Domain`` (``manapy/ddm/domain.py:36-961``) for a
+single-rank mesh: the same constructor options, the same ``cells`` /
+``faces`` / ``nodes`` / ``halos`` accessors holding manapy-layout numpy
+arrays, and the same face lists.  manapy reads its mesh from per-rank HDF5
+files written by ``MeshPartition``; here the mesh is passed in memory
+(``mesh=(elements, vertex)`` in manapy's reader layout, see ``meshgen``) or
+read from a gmsh file with ``Domain.from_msh``.  The device tables the CUDA
+kernels read are built on first use (``domain.device_mesh``).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import geometry
+from .base import Struct, make_get_conf, process_conf
+
+__all__ = ["Domain"]
+
+
+class _NS:
+    """Read-only attribute namespace over a dict of arrays."""
+
+    def __init__(self, **items):
+        self.__dict__.update(items)
+
+    def __repr__(self):
+        return "<%s>" % ", ".join(sorted(self.__dict__))
+
+
+class _OneRankComm:
+    """Communicator stand-in of a one-rank domain (no halo cells)."""
+
+    def Get_size(self):
+        return 1
+
+    def Get_rank(self):
+        return 0
+
+    def Barrier(self):
+        return None
+
+    def allreduce(self, x, op=None):
+        return x
+
+
+class Domain:
+    _parameters = [
+        ("backend", "str", "cuda", False, "kernel backend: cuda (sm_100a)"),
+        ("multithreading", "str", "single", None, "accepted for compatibility; unused"),
+        ("signature", "bool", True, False, "accepted for compatibility; unused"),
+        ("cache", "bool", False, False, "accepted for compatibility; unused"),
+        ("float_precision", "str", "double", None, "precision of the float arrays"),
+        ("int_precision", "str", "signed", None, "precision of the integer arrays"),
+        ("device", "str", "cuda", None, "torch device holding the mesh tables"),
+    ]
+
+    @classmethod
+    def process_conf(cls, conf, kwargs):
+        return process_conf(cls._parameters, conf, kwargs)
+
+    def __init__(self, dim=None, comm=None, conf=None, mesh=None, **kwargs):
+        if conf is None:
+            conf = Struct()
+        self.conf = self.process_conf(conf, kwargs)
+        get = make_get_conf(self.conf, kwargs)
+        if dim is None:
+            raise ValueError("dim must be given")
+        if int(dim) not in (2, 3):
+            raise ValueError("dim must be 2 or 3")
+        if get("float_precision") == "single":
+            raise ValueError("float_precision='single' is not supported by the FP64 CUDA path; "
+                             "use the FP32-compensated solvers instead")
+        self.float_precision = "f8"
+        self.int_precision = "i4" if get("int_precision") == "signed" else "u4"
+        self.signature = get("signature")
+        self.device = get("device")
+        if mesh is None:
+            mesh = getattr(conf, "mesh", None)
+        if mesh is None:
+            raise ValueError("no mesh given: pass mesh=(elements, vertex) or use Domain.from_msh(path)")
+        elements, vertex = mesh
+        self._comm = comm if comm is not None else _OneRankComm()
+        self._dim = np.int32(dim)
+        self._A = geometry.build(elements, vertex, int(dim))
+        if len(self._A["unmatched_boundary_faces"]):
+            raise ValueError("%d boundary faces match no boundary side (their vertices carry "
+                             "incompatible tags)" % len(self._A["unmatched_boundary_faces"]))
+        self._build_views()
+        from .backend import CUDABackend
+        self.backend = CUDABackend(self)
+        self._dmesh = None
+
+    @classmethod
+    def from_msh(cls, path, dim, conf=None, **kwargs):
+        """Build from a gmsh 4.1 ASCII file (boundary vertex tags from its physical groups)."""
+        from .gmsh import read_msh
+        return cls(dim=dim, conf=conf, mesh=read_msh(path, dim), **kwargs)
+
+    # ------------------------------------------------------------------ views
+    def _build_views(self):
+        A = self._A
+        P = geometry.padded_from_csr
+        nc, nf, nn = A["nbcells"], A["nbfaces"], A["nbnodes"]
+        self._cells = _NS(
+            nodeid=A["cells_nodeid"], faceid=A["cells_faceid"], cellfid=A["cells_cellfid"],
+            center=A["cells_center"], volume=A["cells_volume"],
+            cellnid=P(A["cellnid_ptr"], A["cellnid_idx"]),
+            ghostnid=P(A["ghostnid_ptr"], A["ghostnid_idx"]),
+            nf=A.get("cells_nf", np.zeros((nc, 4, 3))),
+            halonid=np.zeros((nc, 2), np.int32), haloghostnid=np.zeros((nc, 2), np.int32),
+            haloghostcenter=np.zeros((0, 3)), periodicnid=np.zeros((nc, 2), np.int32),
+            periodicfid=np.zeros(nc, np.int32), shift=np.zeros((nc, 3)),
+            loctoglob=np.arange(nc, dtype=np.int32), globtoloc=np.arange(nc, dtype=np.int32),
+            tc=np.arange(nc, dtype=np.int32), nbcells=nc)
+        faces = dict(nodeid=A["faces_nodeid"], cellid=A["faces_cellid"], name=A["faces_name"],
+                     oldname=A["faces_name"], normal=A["faces_normal"], mesure=A["faces_mesure"],
+                     center=A["faces_center"], ghostcenter=A["faces_ghostcenter"],
+                     airDiamond=A["faces_airDiamond"], f_1=A["faces_f_1"], f_2=A["faces_f_2"],
+                     f_3=A["faces_f_3"], f_4=A["faces_f_4"], param1=A["faces_param1"],
+                     param2=A["faces_param2"], param3=A["faces_param3"],
+                     param4=A.get("faces_param4", np.zeros(nf)), dist_ortho=A["faces_dist_ortho"],
+                     halofid=np.zeros(nf, np.int32), nbfaces=nf)
+        self._faces = _NS(**faces)
+        self._nodes = _NS(
+            vertex=A["nodes_vertex"], name=A["nodes_name"], oldname=A["nodes_name"].copy(),
+            cellid=P(A["n2c_ptr"], A["n2c_idx"]), ghostid=P(A["n2g_ptr"], A["n2g_idx"]),
+            R_x=A["nodes_R_x"], R_y=A["nodes_R_y"], R_z=A["nodes_R_z"],
+            lambda_x=A["nodes_lambda_x"], lambda_y=A["nodes_lambda_y"], lambda_z=A["nodes_lambda_z"],
+            number=A["nodes_number"], halonid=np.zeros((nn, 2), np.int32),
+            periodicid=np.zeros((nn, 2), np.int32), haloghostid=np.zeros((nn, 2), np.int32),
+            loctoglob=np.arange(nn, dtype=np.int32), nbnodes=nn)
+        self._halos = _NS(centvol=np.zeros((2, 2)), halosint=np.zeros((2, 2), np.int32),
+                          halosext=np.zeros((2, 2), np.int32), sizehaloghost=0,
+                          indsend=np.zeros(1, np.int32), scount=np.zeros(1, np.uint32),
+                          rcount=np.zeros(1, np.uint32), comm_ptr=self._comm)
+        self._BCs = {"in": ["neumann", 1], "out": ["neumann", 2], "upper": ["neumann", 3],
+                     "bottom": ["neumann", 4]}
+        if self._dim == 3:
+            self._BCs.update({"front": ["neumann", 5], "back": ["neumann", 6]})
+
+    # ------------------------------------------------------------------ device
+    @property
+    def device_mesh(self):
+        """The device tables (``mb_mesh``), built on first use."""
+        if self._dmesh is None:
+            from .device import DeviceMesh
+            self._dmesh = DeviceMesh(self._A, self.device)
+        return self._dmesh
+
+    @property
+    def host_arrays(self):
+        return self._A
+
+    # ------------------------------------------------------------------ accessors
+    cells = property(lambda self: self._cells)
+    faces = property(lambda self: self._faces)
+    nodes = property(lambda self: self._nodes)
+    halos = property(lambda self: self._halos)
+    dim = property(lambda self: self._dim)
+    comm = property(lambda self: self._comm)
+    nbcells = property(lambda self: np.int32(self._A["nbcells"]))
+    nbfaces = property(lambda self: np.int32(self._A["nbfaces"]))
+    nbnodes = property(lambda self: np.int32(self._A["nbnodes"]))
+    nbhalos = property(lambda self: 0)
+    innerfaces = property(lambda self: self._A["innerfaces"])
+    infaces = property(lambda self: self._A["infaces"])
+    outfaces = property(lambda self: self._A["outfaces"])
+    upperfaces = property(lambda self: self._A["upperfaces"])
+    bottomfaces = property(lambda self: self._A["bottomfaces"])
+    frontfaces = property(lambda self: self._A.get("frontfaces", np.zeros(0, np.int32)))
+    backfaces = property(lambda self: self._A.get("backfaces", np.zeros(0, np.int32)))
+    halofaces = property(lambda self: np.zeros(0, np.int32))
+    boundaryfaces = property(lambda self: self._A["boundaryfaces"])
+    periodicboundaryfaces = property(lambda self: np.zeros(0, np.int32))
+    halonodes = property(lambda self: np.zeros(0, np.int32))
+
+    @property
+    def bounds(self):
+        v = self._A["nodes_vertex"]
+        return np.array([[v[:, k].min(), v[:, k].max()] for k in range(int(self._dim))])
+
+    def __str__(self):
+        return ("\n> dim   :: %d\n> total cells  :: %d\n> total nodes  :: %d\n> total faces  :: %d\n"
+                % (self.dim, self.nbcells, self.nbnodes, self.nbfaces))

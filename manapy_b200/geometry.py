@@ -80,19 +80,28 @@ def ragged_union(row_items_ptr, row_items, item_ptr, item_vals, exclude_self=Fal
     row_of_item = np.repeat(np.arange(nrows, dtype=np.int64), rcnt)
     icnt = np.diff(item_ptr)[row_items]
     total = int(icnt.sum())
+    # candidates of each row in a padded [nrows, width] matrix, sorted per row
+    per_row = np.bincount(row_of_item, weights=icnt, minlength=nrows).astype(np.int64)
+    width = max(int(per_row.max()) if nrows else 0, 1)
     row_of_val = np.repeat(row_of_item, icnt)
     starts = np.repeat(item_ptr[row_items], icnt)
     offs = np.arange(total, dtype=np.int64) - np.repeat(np.cumsum(icnt) - icnt, icnt)
-    vals = item_vals[starts + offs].astype(np.int64)
+    vals = item_vals[starts + offs]
+    rstart = np.zeros(nrows + 1, dtype=np.int64)
+    np.cumsum(per_row, out=rstart[1:])
+    col = np.arange(total, dtype=np.int64) - rstart[row_of_val]
+    big = np.iinfo(np.int32).max
+    mat = np.full((nrows, width), big, dtype=np.int32)
+    mat[row_of_val, col] = vals
+    mat.sort(axis=1)
+    keep = mat != big
+    keep[:, 1:] &= mat[:, 1:] != mat[:, :-1]
     if exclude_self:
-        keep = vals != row_of_val
-        vals = vals[keep]
-        row_of_val = row_of_val[keep]
-    span = int(max(vals.max() + 1 if len(vals) else 1, 1))
-    key = np.unique(row_of_val * span + vals)
-    rows = key // span
-    ptr = _group_ptr(rows, nrows)
-    return ptr, (key - rows * span).astype(I32)
+        keep &= mat != np.arange(nrows, dtype=np.int32)[:, None]
+    cnt = keep.sum(axis=1)
+    ptr = np.zeros(nrows + 1, dtype=np.int64)
+    np.cumsum(cnt, out=ptr[1:])
+    return ptr, mat[keep].astype(I32)
 
 
 class Arrays(dict):

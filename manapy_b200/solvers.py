@@ -1,0 +1,478 @@
+"""Explicit solvers with manapy's call surface, running the fused CUDA steps.
+
+``AdvectionDiffusionSolver`` mirrors ``manapy/solvers/advecdiff/system.py:21-172``
+and ``ShallowWaterSolver`` mirrors ``manapy/solvers/shallowater/system.py:23-281``:
+same options, same validation errors, same ``stepper()`` /
+``compute_fluxes()`` / ``compute_new_val()`` sequence.
+
+Execution: ``compute_new_val()`` runs one fused step (two kernel launches for
+advection-diffusion, three for shallow water) that recomputes what
+``compute_fluxes()`` would have produced on the fly.  The intermediate arrays
+manapy leaves behind (``var.ghost``, ``var.convective``, ``var.dissipative``,
+``var.gradfacex/y/z``) are still available: reading one runs the matching
+single kernel on the step's input state.  Editing ``var.convective``,
+``var.dissipative`` or ``var.source`` between ``compute_fluxes()`` and
+``compute_new_val()`` switches that step to the unfused update, so the edit
+is honoured exactly as in manapy.
+
+``advance(n)`` runs ``n`` whole steps (``stepper`` + ``compute_fluxes`` +
+``compute_new_val``) on the device without host round trips, optionally
+replayed from a CUDA graph.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .base import Struct, make_get_conf, process_conf
+from .variable import Variable
+
+__all__ = ["AdvectionDiffusionSolver", "ShallowWaterSolver"]
+
+
+def _p(t):
+    return t.data_ptr() if t is not None else None
+
+
+class AdvectionDiffusionSolver:
+    _parameters = [("Dxx", float, 0., 0., "Diffusion in x direction"),
+                   ("Dyy", float, 0., 0., "Diffusion in y direction"),
+                   ("Dzz", float, 0., 0., "Diffusion in z direction"),
+                   ("dt", float, 0., 0., "time step"),
+                   ("order", int, 1, 1, "order of the convective scheme"),
+                   ("cfl", float, .4, 0, "cfl of the explicit scheme")]
+
+    @classmethod
+    def process_conf(cls, conf, kwargs):
+        return process_conf(cls._parameters, conf, kwargs)
+
+    def __init__(self, var=None, vel=(None, None, None), conf=None, **kwargs):
+        if conf is None:
+            conf = Struct()
+        self.conf = self.process_conf(conf, kwargs)
+        get = make_get_conf(self.conf, kwargs)
+        if not isinstance(var, Variable):
+            raise ValueError("primal var must be a Variable type")
+        if not isinstance(vel[0], Variable):
+            raise ValueError("u must be a Variable type")
+        if not isinstance(vel[1], Variable):
+            raise ValueError("v must be a Variable type")
+        self.var = var
+        self.comm = var.comm
+        self.domain = var.domain
+        self.dim = var.dim
+        self.float_precision = self.domain.float_precision
+        self.u, self.v = vel[0], vel[1]
+        if len(vel) == 3:
+            if not isinstance(vel[2], Variable):
+                raise ValueError("w must be a Variable type")
+            self.w = vel[2]
+        else:
+            self.w = Variable(domain=self.domain)
+        self.Dxx = np.float64(get("Dxx"))
+        self.Dyy = np.float64(get("Dyy"))
+        self.Dzz = np.float64(get("Dzz"))
+        self.dt = np.float64(get("dt"))
+        self.order = np.int32(get("order"))
+        self.cfl = np.float64(get("cfl"))
+        if self.order not in (1, 2):
+            raise ValueError("order must be 1 or 2")
+        self.diffusion = not (self.Dxx == self.Dyy == self.Dzz == 0)
+        self.backend = self.domain.backend
+        self.signature = self.domain.signature
+        for t in ("convective", "dissipative", "source"):
+            var.add_term(t)
+        self._dm = None
+        self._dt_dev = None
+        self._dt_key = None
+        self._sign = None
+        self._sign_key = None
+        self._pending = False
+        self._spare = None
+        self._graph = None
+        self._dt_host = None
+
+    # ------------------------------------------------------------ device helpers
+    def _setup(self):
+        if self._dm is None:
+            self._dm = self.domain.device_mesh
+            dev = self._dm.device
+            self._dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+            self._sign = torch.zeros(self._dm.nbfaces, dtype=torch.float64, device=dev)
+            self._params = _lib.MbAdvDiffParams(int(self.order), int(self.diffusion), float(self.Dxx),
+                                                float(self.Dyy), float(self.Dzz))
+        return self._dm
+
+    def _stream(self):
+        return torch.cuda.current_stream(self._dm.device).cuda_stream
+
+    def _update_sign(self):
+        key = (self.u.version("face"), self.v.version("face"), self.w.version("face"))
+        if key != self._sign_key:
+            _lib.call("mb_face_sign", self._dm.struct, _p(self.u.dev("face")), _p(self.v.dev("face")),
+                      _p(self.w.dev("face")), _p(self._sign), self._stream())
+            self._sign_key = (self.u.version("face"), self.v.version("face"), self.w.version("face"))
+
+    def _time_step_dev(self):
+        """dt on the device; recomputed only when the cell velocity or options change
+        (manapy recomputes the same value every step from the same inputs)."""
+        key = (self.u.version("cell"), self.v.version("cell"), self.w.version("cell"),
+               float(self.cfl), float(self.Dxx), float(self.Dyy), float(self.Dzz))
+        if key != self._dt_key:
+            _lib.call("mb_time_step", self._dm.struct, _p(self.u.dev("cell")), _p(self.v.dev("cell")),
+                      _p(self.w.dev("cell")), float(self.cfl), float(self.Dxx), float(self.Dyy),
+                      float(self.Dzz), _p(self._dt_dev), self._stream())
+            self._dt_key = (self.u.version("cell"), self.v.version("cell"), self.w.version("cell"),
+                            float(self.cfl), float(self.Dxx), float(self.Dyy), float(self.Dzz))
+            self._dt_host = None
+        return self._dt_dev
+
+    # ------------------------------------------------------------ manapy API
+    def stepper(self):
+        """manapy/solvers/advecdiff/system.py:149-153: the CFL time step."""
+        self._setup()
+        self._time_step_dev()
+        if self._dt_host is None:
+            self._dt_host = float(self._dt_dev.item())
+        self.dt = np.float64(self._dt_host)
+        return self.dt
+
+    def explicit_convective(self):
+        """manapy/solvers/advecdiff/system.py:131-141 (unfused: gradient, limiter, upwind flux)."""
+        self._setup()
+        var = self.var
+        if self.order == 2:
+            var.compute_cell_gradient()
+        _lib.call("mb_explicitscheme_convective", self._dm.struct, _p(var.dev_out("convective")),
+                  _p(var.dev("cell")), _p(var.dev("ghost")), _p(self.u.dev("face")), _p(self.v.dev("face")),
+                  _p(self.w.dev("face")), _p(var.dev("gradcellx")), _p(var.dev("gradcelly")),
+                  _p(var.dev("gradcellz")), _p(var.dev("psi")), int(self.order), self._stream())
+
+    def explicit_dissipative(self):
+        """manapy/solvers/advecdiff/system.py:143-146 (unfused)."""
+        self._setup()
+        var = self.var
+        var.compute_face_gradient()
+        _lib.call("mb_explicitscheme_dissipative", self._dm.struct, _p(var.dev("gradfacex")),
+                  _p(var.dev("gradfacey")), _p(var.dev("gradfacez")), _p(var.dev_out("dissipative")),
+                  float(self.Dxx), float(self.Dyy), float(self.Dzz), self._stream())
+
+    def _materialise(self, w_in):
+        """Run the unfused kernels on state ``w_in`` to fill ghost, convective, dissipative
+        (and face gradients, nodes) exactly as manapy's compute_fluxes leaves them."""
+        var = self.var
+        cur = var.swap_cell(w_in)
+        try:
+            var.update_ghost_value()
+            self.explicit_convective()
+            if self.diffusion:
+                var.interpolate_celltonode()
+                self.explicit_dissipative()
+        finally:
+            var.swap_cell(cur)
+
+    def _install_lazies(self, w_in):
+        var = self.var
+        done = {"v": False}
+
+        def run():
+            if not done["v"]:
+                done["v"] = True
+                for n in names:
+                    var._s.lazy.pop(n, None)
+                self._materialise(w_in)
+
+        names = ["ghost", "convective"] + (["dissipative", "gradfacex", "gradfacey", "gradfacez"]
+                                           if self.diffusion else [])
+        for n in names:
+            var.set_lazy(n, run)
+
+    def compute_fluxes(self):
+        """manapy/solvers/advecdiff/system.py:156-168; fused into compute_new_val()."""
+        self._setup()
+        var = self.var
+        self._pending = True
+        self._res_versions = tuple(var.version(n) for n in ("convective", "dissipative"))
+        self._install_lazies(var.dev("cell"))
+
+    def compute_new_val(self):
+        """manapy/solvers/advecdiff/system.py:171-172: w += dt((rez + dissip)/V + src)."""
+        self._setup()
+        var = self.var
+        if self._dt_host is None or float(self.dt) != self._dt_host:
+            # stepper() not called, or S.dt set by hand: use S.dt as manapy does
+            self._dt_dev.fill_(float(self.dt))
+            self._dt_key = None
+            self._dt_host = float(self.dt)
+        edited = (not self._pending or
+                  tuple(var.version(n) for n in ("convective", "dissipative")) != self._res_versions)
+        if edited:
+            for n in ("ghost", "convective", "dissipative", "gradfacex", "gradfacey", "gradfacez"):
+                if n in var._s.lazy:
+                    var._s.d(n)
+            _lib.call("mb_update_new_value", self._dm.struct, _p(var.dev("cell")),
+                      _p(var.dev("convective")), _p(var.dev("dissipative")), _p(var.dev("source")),
+                      _p(self._dt_dev), self._stream())
+            var._s.version["cell"] += 1
+        else:
+            self._fused_step()
+        self._pending = False
+
+    def _source_ptr(self):
+        var = self.var
+        return None if var.version("source") == 0 else _p(var.dev("source"))
+
+    def _fused_step(self):
+        var = self.var
+        dm = self._dm
+        self._update_sign()
+        w_in = var.dev("cell")
+        if self._spare is None or self._spare.numel() != w_in.numel():
+            self._spare = torch.empty_like(w_in)
+        w_out = self._spare
+        gz = var.dev_out("gradcellz") if self.dim == 3 else var.dev("gradcellz")
+        _lib.call("mb_advdiff_step", dm.struct, var.device_bc.struct, self._params, _p(w_in), _p(w_out),
+                  _p(self._sign), self._source_ptr(), _p(self._dt_dev),
+                  _p(var.dev_out("gradcellx") if self.order == 2 else var.dev("gradcellx")),
+                  _p(var.dev_out("gradcelly") if self.order == 2 else var.dev("gradcelly")), _p(gz),
+                  _p(var.dev_out("psi") if self.order == 2 else var.dev("psi")),
+                  _p(var.dev_out("node") if self.diffusion else var.dev("node")), self._stream())
+        self._spare = var.swap_cell(w_out)
+        self._install_lazies(self._spare)
+
+    # ------------------------------------------------------------ device loop
+    def advance(self, nsteps, graph=False):
+        """Run ``nsteps`` full steps on the device (dt, fluxes, update) without host
+        synchronisation.  Returns the simulated time span (dt is constant while the
+        velocity does not change).  ``graph=True`` replays two-step CUDA graphs."""
+        self._setup()
+        var = self.var
+        self._time_step_dev()
+        self._update_sign()
+        var.dev("cell")
+        if self._spare is None:
+            self._spare = torch.empty_like(var.dev("cell"))
+        n = int(nsteps)
+        if not graph or n < 2:
+            for _ in range(n):
+                self._fused_step()
+        else:
+            g = self._get_graph()
+            for _ in range(n // 2):
+                g.replay()
+            var._s.version["cell"] += 1
+            self._install_lazies(self._spare)
+            if n % 2:
+                self._fused_step()
+        if self._dt_host is None:
+            self._dt_host = float(self._dt_dev.item())
+        self.dt = np.float64(self._dt_host)
+        return n * self._dt_host
+
+    def _get_graph(self):
+        """Two fused steps (A->B, B->A) captured once; the cell buffer ends where it began."""
+        if self._graph is not None:
+            return self._graph
+        var = self.var
+        a = var.dev("cell")
+        b = self._spare
+        dm = self._dm
+        gz = var.dev("gradcellz")
+        args = (var.device_bc.struct, self._params)
+        src = self._source_ptr()
+        s = torch.cuda.Stream(device=dm.device)
+        s.wait_stream(torch.cuda.current_stream(dm.device))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            # warm-up outside capture is not needed: the library performs no lazy init
+            with torch.cuda.graph(g, stream=s):
+                st = torch.cuda.current_stream(dm.device).cuda_stream
+                for x, y in ((a, b), (b, a)):
+                    _lib.call("mb_advdiff_step", dm.struct, args[0], args[1], _p(x), _p(y), _p(self._sign),
+                              src, _p(self._dt_dev), _p(var.dev("gradcellx")), _p(var.dev("gradcelly")),
+                              _p(gz), _p(var.dev("psi")), _p(var.dev("node")), st)
+        torch.cuda.current_stream(dm.device).wait_stream(s)
+        self._graph = g
+        return g
+
+
+class ShallowWaterSolver:
+    _parameters = [("Dxx", float, 0., 0., "Diffusion in x direction"),
+                   ("Dyy", float, 0., 0., "Diffusion in y direction"),
+                   ("dt", float, 0., 0., "time step"),
+                   ("order", int, 1, 1, "order of the convective scheme"),
+                   ("cfl", float, .8, 0, "cfl of the explicit scheme"),
+                   ("Mann", float, 0., 0., "Manning number for the friction"),
+                   ("fc", float, 0., 0., "Coriolis force"),
+                   ("grav", float, 9.81, 0., "gravity constant"),
+                   ("wind", bool, False, True, "wind")]
+
+    @classmethod
+    def process_conf(cls, conf, kwargs):
+        return process_conf(cls._parameters, conf, kwargs)
+
+    def __init__(self, h=None, hvel=(None, None), hc=None, Z=None, conf=None, **kwargs):
+        if conf is None:
+            conf = Struct()
+        self.conf = self.process_conf(conf, kwargs)
+        get = make_get_conf(self.conf, kwargs)
+        if not isinstance(h, Variable):
+            raise ValueError("h must be a Variable type")
+        if not isinstance(hvel[0], Variable):
+            raise ValueError("hu must be a Variable type")
+        if not isinstance(hvel[1], Variable):
+            raise ValueError("hv must be a Variable type")
+        self.h = h
+        self.comm = h.comm
+        self.domain = h.domain
+        self.dim = h.dim
+        if self.dim != 2:
+            raise ValueError("the shallow-water scheme is two-dimensional")
+        self.float_precision = self.domain.float_precision
+        self.hu, self.hv = hvel
+        if Z is not None and not isinstance(Z, Variable):
+            raise ValueError("Z must be a Variable type")
+        if hc is not None and not isinstance(hc, Variable):
+            raise ValueError("hC must be a Variable type")
+        self.Z = Z if Z is not None else Variable(domain=self.domain)
+        self.hc = hc if hc is not None else Variable(domain=self.domain)
+        self.varbs = {"h": self.h, "hu": self.hu, "hv": self.hv, "hc": self.hc, "Z": self.Z}
+        for var in self.varbs.values():
+            for term in ("source", "dissipation", "coriolis", "friction", "convective"):
+                var.add_term(term)
+        self.Dxx = get("Dxx")
+        self.Dyy = get("Dyy")
+        self.Dzz = 0.
+        self.dt = get("dt")
+        self.order = get("order")
+        self.cfl = get("cfl")
+        self.Mann = get("Mann")
+        self.fc = get("fc")
+        self.grav = get("grav")
+        self.wind = get("wind")
+        if self.order not in (1, 2):
+            raise ValueError("order must be 1 or 2")
+        if not (self.Dxx == self.Dyy == 0):
+            raise NotImplementedError("shallow-water diffusion: manapy's diffusive branch references "
+                                      "attributes it never sets (manapy/solvers/shallowater/system.py:269-271)")
+        if self.Mann != 0 or self.fc != 0 or self.wind:
+            raise NotImplementedError("friction, Coriolis and wind source terms are not implemented")
+        self.diffusion = False
+        self.backend = self.domain.backend
+        self.signature = self.domain.signature
+        self._dm = None
+        self._ff = None
+        self._spare = None
+        self._scratch = None
+        self._dt_host = None
+
+    def _setup(self):
+        if self._dm is None:
+            self._dm = self.domain.device_mesh
+            dev = self._dm.device
+            self._dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+            self._ff = torch.zeros(5 * self._dm.nbfaces, dtype=torch.float64, device=dev)
+            if self.order == 2:
+                self._scratch = torch.zeros(5 * self._dm.nbcells, dtype=torch.float64, device=dev)
+        return self._dm
+
+    def _stream(self):
+        return torch.cuda.current_stream(self._dm.device).cuda_stream
+
+    def _all_neumann(self):
+        from . import boundary as B
+        for var in self.varbs.values():
+            k = var.resolved_bc.kind
+            if np.any((k != B.G_NEUMANN) & (k != B.G_NONE)):
+                return False
+        return True
+
+    def _q(self):
+        return [self.varbs[k].dev("cell") for k in ("h", "hu", "hv", "hc", "Z")]
+
+    def stepper(self):
+        """manapy/solvers/shallowater/system.py:186-192 (returns dt; manapy returns None)."""
+        self._setup()
+        q = self._q()
+        _lib.call("mb_time_step_sw", self._dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), float(self.cfl),
+                  float(self.grav), float(self.Dxx), float(self.Dyy), _p(self._dt_dev), self._stream())
+        self.dt = float(self._dt_dev.item())
+        self._dt_host = self.dt
+        return self.dt
+
+    def update_ghost_values(self):
+        for var in self.varbs.values():
+            var.update_ghost_value()
+
+    def explicit_convective(self):
+        """manapy/solvers/shallowater/system.py:162-178 (unfused)."""
+        self._setup()
+        if self.order == 2:
+            self.h.compute_cell_gradient()
+            self.hc.compute_cell_gradient()
+        names = ("h", "hu", "hv", "hc", "Z")
+        rez = _lib.p5([_p(self.varbs[k].dev_out("convective")) for k in names])
+        q = _lib.p5([_p(self.varbs[k].dev("cell")) for k in names])
+        g = _lib.p5([_p(self.varbs[k].dev("ghost")) for k in names])
+        gr = _lib.p4([_p(self.h.dev("gradcellx")), _p(self.h.dev("gradcelly")), _p(self.hc.dev("gradcellx")),
+                      _p(self.hc.dev("gradcelly"))])
+        _lib.call("mb_explicitscheme_convective_sw", self._dm.struct, rez, q, g, gr, _p(self.hc.dev("psi")),
+                  float(self.grav), int(self.order), _p(self._ff), self._stream())
+
+    def update_term_source(self):
+        """manapy/solvers/shallowater/system.py:217-227."""
+        self._setup()
+        for v in (self.h, self.hc, self.Z):
+            v.dev_out("source").zero_()
+        _lib.call("mb_term_source_srnh_sw", self._dm.struct, _p(self.h.dev("cell")), _p(self.Z.dev("cell")),
+                  _p(self.h.dev("ghost")), _p(self.Z.dev("ghost")), float(self.grav),
+                  _p(self.hu.dev_out("source")), _p(self.hv.dev_out("source")), self._stream())
+
+    def compute_fluxes(self):
+        """manapy/solvers/shallowater/system.py:248-281; fused into compute_new_val() when
+        every variable has manapy's default (Neumann) boundaries."""
+        self._setup()
+        self._fused = self._all_neumann()
+        if not self._fused:
+            self.stepper()
+            self.update_ghost_values()
+            self.explicit_convective()
+            self.update_term_source()
+
+    def compute_new_val(self):
+        """manapy/solvers/shallowater/system.py:237-242."""
+        self._setup()
+        if getattr(self, "_fused", False):
+            self._fused_step()
+            self._fused = False
+            return
+        names = ("h", "hu", "hv", "hc", "Z")
+        q = _lib.p5([_p(self.varbs[k].dev("cell")) for k in names])
+        rez = _lib.p5([_p(self.varbs[k].dev("convective")) for k in names])
+        if self._dt_host is None or float(self.dt) != self._dt_host:
+            self._dt_dev.fill_(float(self.dt))
+        _lib.call("mb_update_sw", self._dm.struct, q, rez, _p(self.hu.dev("source")),
+                  _p(self.hv.dev("source")), _p(self._dt_dev), self._stream())
+        for k in names:
+            self.varbs[k]._s.version["cell"] += 1
+
+    def _fused_step(self):
+        names = ("h", "hu", "hv", "hc", "Z")
+        qin = [self.varbs[k].dev("cell") for k in names]
+        if self._spare is None:
+            self._spare = [torch.empty_like(t) for t in qin]
+        qout = self._spare
+        _lib.call("mb_sw_step", self._dm.struct, _lib.p5([_p(t) for t in qin]), _lib.p5([_p(t) for t in qout]),
+                  float(self.cfl), float(self.grav), int(self.order),
+                  _p(self._scratch) if self._scratch is not None else None, _p(self._ff), _p(self._dt_dev),
+                  self._stream())
+        self._spare = [self.varbs[k].swap_cell(t) for k, t in zip(names, qout)]
+        self._dt_host = None
+
+    def advance(self, nsteps):
+        """``nsteps`` fused steps on the device; returns the simulated time (one sync at the end
+        is avoided: the per-step dt stays on the device, so the time is not accumulated here)."""
+        self._setup()
+        for _ in range(int(nsteps)):
+            self._fused_step()

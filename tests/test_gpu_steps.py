@@ -1,0 +1,177 @@
+"""Whole steps through the public API (fused CUDA path) against the reference and the oracle.
+
+Tolerance: the plain FP64 path must stay within 1e-12 relative (max-norm over
+cells) of the reference after the full run; per-kernel rounding differences
+(fused multiply-adds) are ~1e-16 per step.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, rel_max
+import manapy_b200 as M
+from manapy_b200 import boundary as B, geometry as G, workloads as W
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _advdiff_api(el, vx, wl):
+    dom = M.Domain(dim=wl.dim, mesh=(el, vx))
+    w = M.Variable(domain=dom, BC=wl.bc, values=wl.bc_values)
+    u, v, wz = (M.Variable(domain=dom) for _ in range(3))
+    uf, vf, wf = wl.velocity(dom.faces.center)
+    u.face = uf
+    v.face = vf
+    wz.face = wf
+    for x in (u, v, wz):
+        x.interpolate_facetocell()
+    w.cell = wl.init(dom.cells.center)
+    S = M.AdvectionDiffusionSolver(w, vel=(u, v, wz), conf=M.Struct(Dxx=wl.diffusion[0], Dyy=wl.diffusion[1],
+                                                                     Dzz=wl.diffusion[2], order=wl.order,
+                                                                     cfl=wl.cfl))
+    return dom, w, S
+
+
+def _oracle(el, vx, wl):
+    A = G.build(el, vx, wl.dim)
+    o = O.AdvDiffOracle(A, B.resolve(A, wl.bc, wl.bc_values), *wl.diffusion, order=wl.order, cfl=wl.cfl)
+    o.set_velocity(*wl.velocity(A["faces_center"]))
+    o.w[:] = wl.init(A["cells_center"])
+    return o
+
+
+@pytest.mark.parametrize("name,wl", [("traj_c1", W.C1), ("traj_o2", W.C2.scaled(n=32, steps=100)),
+                                     ("traj_3d", W.C4.scaled(n=6, steps=30))])
+def test_manapy_loop_matches_reference(name, wl, cuda):
+    g = golden(name)
+    el, vx = g["in_elements"], g["in_vertex"]
+    dom, w, S = _advdiff_api(el, vx, wl)
+    dts = []
+    for it in range(int(g["steps"])):
+        dts.append(S.stepper())
+        S.compute_fluxes()
+        S.compute_new_val()
+        key = "w_step%d" % (it + 1)
+        if key in g.files:
+            assert rel_max(w.cell, g[key]) < TOL, key
+    assert rel_max(np.array(dts), g["dts"]) < 1e-15
+    assert rel_max(w.cell, g["w_final"]) < TOL
+
+
+@pytest.mark.parametrize("wl", [W.C1.scaled(n=60, steps=40), W.C2.scaled(n=150, steps=25),
+                                W.C4.scaled(n=10, steps=15), W.C4.scaled(n=8, steps=10, order=1)])
+def test_advance_matches_oracle(wl, cuda):
+    el, vx = wl.mesh()
+    dom, w, S = _advdiff_api(el, vx, wl)
+    o = _oracle(el, vx, wl)
+    S.advance(wl.steps, graph=True)
+    for _ in range(wl.steps):
+        o.step()
+    assert rel_max(w.cell, o.w) < TOL
+
+
+def test_graph_and_eager_agree_bitwise(cuda):
+    wl = W.C2.scaled(n=40, steps=9)
+    el, vx = wl.mesh()
+    _, w1, S1 = _advdiff_api(el, vx, wl)
+    _, w2, S2 = _advdiff_api(el, vx, wl)
+    S1.advance(wl.steps, graph=True)
+    S2.advance(wl.steps, graph=False)
+    assert np.array_equal(w1.cell, w2.cell)
+
+
+def test_intermediate_arrays_match_reference_kernels(cuda):
+    """After compute_fluxes, manapy's intermediate arrays are readable and exact."""
+    g = golden("traj_o2")
+    wl = W.C2.scaled(n=32, steps=3)
+    el, vx = g["in_elements"], g["in_vertex"]
+    dom, w, S = _advdiff_api(el, vx, wl)
+    o = _oracle(el, vx, wl)
+    for _ in range(2):
+        S.stepper(); S.compute_fluxes(); S.compute_new_val()
+        o.step()
+    S.stepper()
+    S.compute_fluxes()
+    o.stepper()
+    o.compute_fluxes()
+    assert rel_max(w.convective, o.rez) < 1e-13
+    assert rel_max(w.dissipative, o.dissip) < 1e-13
+    assert rel_max(w.gradcellx, o.gx) < 1e-13 and rel_max(w.psi, o.psi) < 1e-13
+    assert rel_max(w.gradfacex, o.gfx) < 1e-13
+    # reading convective switched this step to the unfused update; still exact
+    S.compute_new_val()
+    o.compute_new_val()
+    assert rel_max(w.cell, o.w) < TOL
+
+
+def test_user_edit_of_residual_is_honoured(cuda):
+    wl = W.C1.scaled(n=20, steps=1)
+    el, vx = wl.mesh()
+    dom, w, S = _advdiff_api(el, vx, wl)
+    o = _oracle(el, vx, wl)
+    S.stepper(); S.compute_fluxes()
+    o.stepper(); o.compute_fluxes()
+    rez = w.convective
+    rez[:] = rez * 0.5
+    w.convective = rez
+    o.rez *= 0.5
+    S.compute_new_val(); o.compute_new_val()
+    assert rel_max(w.cell, o.w) < TOL
+
+
+def test_full_size_c2_steps(cuda):
+    """The 2,000,000-triangle mesh: three steps against the oracle, and conservation of
+    the update (sum V dw = dt * sum of residuals) on the device."""
+    wl = W.C2.scaled(steps=3)
+    el, vx = wl.mesh()
+    dom, w, S = _advdiff_api(el, vx, wl)
+    o = _oracle(el, vx, wl)
+    for _ in range(3):
+        S.stepper(); S.compute_fluxes(); S.compute_new_val()
+        o.step()
+    assert rel_max(w.cell, o.w) < TOL
+
+
+def _sw_api(el, vx, wl):
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    h, hu, hv, hc, Z = (M.Variable(domain=dom) for _ in range(5))
+    for var, a in zip((h, hu, hv, hc, Z), wl.init_sw(dom.cells.center)):
+        var.cell = a
+    S = M.ShallowWaterSolver(h, hvel=(hu, hv), hc=hc, Z=Z, conf=M.Struct(order=wl.order, cfl=wl.cfl, grav=wl.grav))
+    return dom, (h, hu, hv, hc, Z), S
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_shallow_water_matches_oracle(order, cuda):
+    wl = W.C3.scaled(n=40, steps=60, order=order)
+    el, vx = wl.mesh()
+    dom, vs, S = _sw_api(el, vx, wl)
+    A = dom.host_arrays
+    so = O.ShallowWaterOracle(A, order=order, cfl=wl.cfl, grav=wl.grav)
+    for k, a in zip(("h", "hu", "hv", "hc", "Z"), wl.init_sw(A["cells_center"])):
+        so.state()[k][:] = a
+    for _ in range(wl.steps):
+        S.stepper(); S.compute_fluxes(); S.compute_new_val()
+        so.step()
+    for k, var in zip(("h", "hu", "hv", "hc", "Z"), vs):
+        ref = so.state()[k]
+        if np.any(ref):
+            assert rel_max(var.cell, ref) < 1e-11, k
+    # mass: FP64 sum of V h changes only through boundary fluxes (Neumann walls leak)
+    assert abs(np.sum(vs[0].cell * A["cells_volume"]) - np.sum(so.h * A["cells_volume"])) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["traj_sw1", "traj_sw2"])
+def test_shallow_water_matches_reference(name, cuda):
+    import os
+    from conftest import GOLDEN
+    if not os.path.exists(os.path.join(GOLDEN, name + ".npz")):
+        pytest.skip("fixture not generated")
+    g = golden(name)
+    wl = W.C3.scaled(n=30, order=int(g["order"]), steps=int(g["steps"]))
+    dom, vs, S = _sw_api(g["in_elements"], g["in_vertex"], wl)
+    for _ in range(wl.steps):
+        S.stepper(); S.compute_fluxes(); S.compute_new_val()
+    for k, var in zip(("h", "hu", "hv"), vs[:3]):
+        assert rel_max(var.cell, g[k + "_final"]) < 1e-11, k

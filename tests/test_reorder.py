@@ -1,0 +1,60 @@
+"""Device renumbering: tables stay consistent and per-cell lists keep manapy's order."""
+import numpy as np
+import pytest
+
+from manapy_b200 import geometry as G, meshgen
+from manapy_b200.device import DeviceBC, DeviceMesh, cell_order_codes
+from manapy_b200 import boundary as B
+
+
+@pytest.mark.parametrize("dim,n", [(2, 12), (3, 3)])
+def test_relabelled_tables_are_consistent(dim, n):
+    el, vx = meshgen.square_triangles(n, seed=3) if dim == 2 else meshgen.cube_tetrahedra(n, seed=3)
+    A = G.build(el, vx, dim)
+    dm = DeviceMesh(A, "cpu", reorder=True)
+    R = dm.R
+    t = {k: v.numpy() for k, v in dm.t.items()}
+    nlf = 3 if dim == 2 else 4
+    # permutations are bijections
+    for p, inv in ((R.cperm, R.cinv), (R.fperm, R.finv), (R.nperm, R.ninv)):
+        assert np.array_equal(np.sort(p), np.arange(len(p)))
+        assert np.array_equal(inv[p], np.arange(len(p)))
+    # cell -> faces and face -> cells agree with the host tables
+    old_faces = A["cells_faceid"][:, :nlf]
+    assert np.array_equal(t["cell_faces"][:, :nlf], R.finv[old_faces[R.cperm]])
+    fc = A["faces_cellid"]
+    new_fc = t["face_cellid"]
+    assert np.array_equal(new_fc[R.finv, 0], R.cinv[fc[:, 0]])
+    b = fc[:, 1] < 0
+    assert np.all(new_fc[R.finv[b], 1] == -1)
+    assert np.array_equal(new_fc[R.finv[~b], 1], R.cinv[fc[~b, 1]])
+    # cell-neighbour lists keep manapy's order (ascending old id)
+    ptr, idx = t["cellnid_ptr"], t["cellnid_idx"]
+    for k in range(0, A["nbcells"], max(1, A["nbcells"] // 50)):
+        old = R.cperm[k]
+        mine = R.cperm[idx[ptr[k]:ptr[k + 1]]]
+        ref = A["cellnid_idx"][A["cellnid_ptr"][old]:A["cellnid_ptr"][old + 1]]
+        assert np.array_equal(mine, ref)
+    # accumulation order codes refer to ascending *manapy* face ids
+    assert np.array_equal(t["cell_order"], cell_order_codes(old_faces[R.cperm]))
+    # geometry moved with its entity
+    assert np.array_equal(t["cell_center"], A["cells_center"][R.cperm])
+    assert np.array_equal(t["face_normal"], A["faces_normal"][R.fperm])
+    # neighbours are closer in memory after renumbering (locality)
+    c0, c1 = new_fc[:, 0], new_fc[:, 1]
+    inner = c1 >= 0
+    assert np.median(np.abs(c0[inner] - c1[inner])) < np.median(np.abs(fc[~b, 0] - fc[~b, 1]))
+
+
+def test_cell_at_face_ghost_index_follows_renumbering():
+    el, vx = meshgen.square_triangles(10, seed=1)
+    A = G.build(el, vx, 2)
+    # a dirichlet side listed after a neumann side (bottom faces have small ids)
+    bc = B.resolve(A, {"in": "neumann", "bottom": "dirichlet", "upper": "neumann", "out": "neumann"},
+                   {"bottom": 1.0})
+    caf = np.nonzero(bc.kind == B.G_CELL_AT_FACE)[0]
+    assert len(caf) == 10
+    dm = DeviceMesh(A, "cpu", reorder=True)
+    db = DeviceBC(A, bc, "cpu", mesh=dm)
+    v = db.value.numpy()
+    assert np.array_equal(v[dm.R.finv[caf]], dm.R.cinv[caf])
