@@ -241,6 +241,13 @@ class AdvectionDiffusionSolver:
         self._spare = var.swap_cell(w_out)
         self._install_lazies(self._spare)
 
+    def launches_per_step(self):
+        """Kernel launches of one fused step."""
+        return 1 + int(self.order == 2 or bool(self.diffusion))
+
+    def release_graphs(self):
+        self._graph = None
+
     # ------------------------------------------------------------ device loop
     def advance(self, nsteps, graph=False):
         """Run ``nsteps`` full steps on the device (dt, fluxes, update) without host
@@ -470,9 +477,16 @@ class ShallowWaterSolver:
         self._spare = [self.varbs[k].swap_cell(t) for k, t in zip(names, qout)]
         self._dt_host = None
 
+    def launches_per_step(self):
+        """Kernel launches of one fused step: dt init + dt min, [gradients], face fluxes, cells."""
+        return 4 + int(self.order == 2)
+
+    def release_graphs(self):
+        return None
+
     def advance(self, nsteps):
-        """``nsteps`` fused steps on the device; returns the simulated time (one sync at the end
-        is avoided: the per-step dt stays on the device, so the time is not accumulated here)."""
+        """``nsteps`` fused steps on the device, without host synchronisation (each step's dt
+        stays on the device)."""
         self._setup()
         for _ in range(int(nsteps)):
             self._fused_step()

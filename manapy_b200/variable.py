@@ -49,7 +49,10 @@ class _Store:
         self.kind[name] = kind if n else None
 
     def _upload(self, name, arr):
-        src = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float64)).to(self.device)
+        if isinstance(arr, torch.Tensor):  # e.g. pinned host memory: asynchronous copy
+            src = arr.to(device=self.device, dtype=torch.float64, non_blocking=True)
+        else:
+            src = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float64)).to(self.device)
         if self.kind[name] is None:
             self.dev[name].copy_(src)
         else:
@@ -84,6 +87,11 @@ class _Store:
 
     def set(self, name, value):
         t = self.w(name)
+        if isinstance(value, torch.Tensor):
+            if value.numel() != t.numel():
+                raise ValueError("%s expects %d values, got %d" % (name, t.numel(), value.numel()))
+            self._upload(name, value.reshape(-1))
+            return
         v = np.asarray(value, dtype=np.float64)
         if v.ndim == 0:
             t.fill_(float(v))

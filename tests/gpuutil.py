@@ -42,5 +42,5 @@ def mesh(A, reorder=False):
     return DeviceMesh(A, "cuda", reorder=reorder)
 
 
-def bc(A, resolved):
-    return DeviceBC(A, resolved, "cuda")
+def bc(A, resolved, mesh=None):
+    return DeviceBC(A, resolved, "cuda", mesh=mesh)

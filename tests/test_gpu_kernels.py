@@ -27,31 +27,44 @@ def _case(name, dim):
 def _random_case(dim, n, seed):
     el, vx = (meshgen.square_triangles(n, seed=seed) if dim == 2 else meshgen.cube_tetrahedra(n, seed=seed))
     A = G.build(el, vx, dim)
-    sides = ("in", "out", "bottom", "upper") + (("front", "back") if dim == 3 else ())
-    kinds = ("dirichlet", "neumann", "nonslip", "dirichlet", "neumann", "dirichlet")
+    # dirichlet sides first: manapy's value array is the cell array after a neumann side
+    sides = ("in", "upper", "back", "out", "bottom", "front") if dim == 3 else ("in", "upper", "out", "bottom")
+    kinds = ("dirichlet", "dirichlet", "dirichlet", "neumann", "nonslip", "neumann") if dim == 3 else \
+        ("dirichlet", "dirichlet", "neumann", "nonslip")
     bcs = dict(zip(sides, kinds))
     vals = {s: (lambda x, y, z: 0.3 + x - 2 * y) for s, k in bcs.items() if k == "dirichlet"}
     return A, B.resolve(A, bcs, vals)
 
 
-def _check_all(A, resolved, w, uf, vf, wf, D, cuda):
+def _check_all(A, resolved, w, uf, vf, wf, D, cuda, reorder=False):
     import gpuutil as U
     m = O.Mesh(A)
-    dm = U.mesh(A)
-    db = U.bc(A, resolved)
+    dm = U.mesh(A, reorder=reorder)
+    db = U.bc(A, resolved, dm if reorder else None)
+    R = dm.R
     st = U.stream()
     M = dm.struct
+    # device arrays live in the mesh's numbering: permute in, permute back out
+    Tc = lambda a: U.T(np.asarray(a)[R.cperm])  # noqa: E731
+    Tf = lambda a: U.T(np.asarray(a)[R.fperm])  # noqa: E731
+    Tn = lambda a: U.T(np.asarray(a)[R.nperm])  # noqa: E731
+    Hc = lambda t: U.H(t)[R.cinv]  # noqa: E731
+    Hf = lambda t: U.H(t)[R.finv]  # noqa: E731
+    Hn = lambda t: U.H(t)[R.ninv]  # noqa: E731
     # ghost
     ghost_o = np.zeros(m.nf)
     O.ghost_update(m, resolved, w, ghost_o)
-    wd, gd = U.T(w), U.Z(m.nf)
+    wd, gd = Tc(w), U.Z(m.nf)
     U.call("mb_ghost_value", M, db.struct, U.P(wd), U.P(gd), st)
-    assert rel_max(U.H(gd), ghost_o) == 0
+    got = Hf(gd)
+    bf = A["boundaryfaces"]
+    assert rel_max(got[bf], ghost_o[bf]) == 0
+    gd = Tf(ghost_o)
     # facetocell
     uc_o = O.facetocell(m, uf)
     ucd = U.Z(m.nc)
-    U.call("mb_facetocell", M, U.P(U.T(uf)), U.P(ucd), st)
-    assert rel_max(U.H(ucd), uc_o) <= 1e-15
+    U.call("mb_facetocell", M, U.P(Tf(uf)), U.P(ucd), st)
+    assert rel_max(Hc(ucd), uc_o) <= 1e-15
     # gradient + limiter
     gx, gy, gz, psi = (np.zeros(m.nc) for _ in range(4))
     O.cell_gradient(m, w, ghost_o, gx, gy, gz)
@@ -59,55 +72,64 @@ def _check_all(A, resolved, w, uf, vf, wf, D, cuda):
     gxd, gyd, gzd, psid = (U.Z(m.nc) for _ in range(4))
     U.call("mb_cell_gradient", M, U.P(wd), U.P(gd), U.P(gxd), U.P(gyd), U.P(gzd), st)
     U.call("mb_barthlimiter", M, U.P(wd), U.P(gd), U.P(gxd), U.P(gyd), U.P(gzd), U.P(psid), st)
-    assert rel_max(U.H(gxd), gx) < TOL and rel_max(U.H(gyd), gy) < TOL
+    assert rel_max(Hc(gxd), gx) < TOL and rel_max(Hc(gyd), gy) < TOL
     if m.dim == 3:
-        assert rel_max(U.H(gzd), gz) < TOL
-    # the limiter is evaluated on the oracle's gradients to isolate it
+        assert rel_max(Hc(gzd), gz) < TOL
+    # the limiter on the oracle's gradients, to isolate it
     psid2 = U.Z(m.nc)
-    U.call("mb_barthlimiter", M, U.P(wd), U.P(gd), U.P(U.T(gx)), U.P(U.T(gy)), U.P(U.T(gz)), U.P(psid2), st)
-    assert rel_max(U.H(psid2), psi) < TOL
+    gxt, gyt, gzt = Tc(gx), Tc(gy), Tc(gz)
+    U.call("mb_barthlimiter", M, U.P(wd), U.P(gd), U.P(gxt), U.P(gyt), U.P(gzt), U.P(psid2), st)
+    assert rel_max(Hc(psid2), psi) < TOL
     # centre -> vertex
     node = np.zeros(m.nn)
     O.centertovertex(m, w, ghost_o, node)
     nd = U.Z(m.nn)
     U.call("mb_centertovertex", M, U.P(wd), U.P(gd), U.P(nd), st)
-    assert rel_max(U.H(nd), node) < TOL
+    assert rel_max(Hn(nd), node) < TOL
     # face gradient
     fx, fy, fz = (np.zeros(m.nf) for _ in range(3))
     O.face_gradient(m, w, ghost_o, node, fx, fy, fz, resolved.dirichletfaces, resolved.neumannfaces)
     fxd, fyd, fzd = (U.Z(m.nf) for _ in range(3))
-    U.call("mb_face_gradient", M, db.struct, U.P(wd), U.P(gd), U.P(U.T(node)), U.P(fxd), U.P(fyd), U.P(fzd), st)
-    assert rel_max(U.H(fxd), fx) < TOL and rel_max(U.H(fyd), fy) < TOL
+    nodet = Tn(node)
+    U.call("mb_face_gradient", M, db.struct, U.P(wd), U.P(gd), U.P(nodet), U.P(fxd), U.P(fyd), U.P(fzd), st)
+    assert rel_max(Hf(fxd), fx) < TOL and rel_max(Hf(fyd), fy) < TOL
     if m.dim == 3:
-        assert rel_max(U.H(fzd), fz) < TOL
+        assert rel_max(Hf(fzd), fz) < TOL
     # convective, orders 1 and 2, on the oracle's gradients
+    uft, vft, wft = Tf(uf), Tf(vf), Tf(wf)
+    gxt, gyt, gzt, psit = Tc(gx), Tc(gy), Tc(gz), Tc(psi)
     for order in (1, 2):
         rez = np.zeros(m.nc)
         O.convective(m, rez, w, ghost_o, uf, vf, wf, gx, gy, gz, psi, order)
         rd = U.Z(m.nc)
-        U.call("mb_explicitscheme_convective", M, U.P(rd), U.P(wd), U.P(gd), U.P(U.T(uf)), U.P(U.T(vf)),
-               U.P(U.T(wf)), U.P(U.T(gx)), U.P(U.T(gy)), U.P(U.T(gz)), U.P(U.T(psi)), order, st)
-        assert rel_max(U.H(rd), rez) < TOL, order
+        U.call("mb_explicitscheme_convective", M, U.P(rd), U.P(wd), U.P(gd), U.P(uft), U.P(vft), U.P(wft),
+               U.P(gxt), U.P(gyt), U.P(gzt), U.P(psit), order, st)
+        assert rel_max(Hc(rd), rez) < TOL, order
+        gxt, gyt, gzt, psit = Tc(gx), Tc(gy), Tc(gz), Tc(psi)
+        uft, vft, wft = Tf(uf), Tf(vf), Tf(wf)
     # dissipative
     dis = np.zeros(m.nc)
     O.dissipative(m, fx, fy, fz, dis, *D)
     dd = U.Z(m.nc)
-    U.call("mb_explicitscheme_dissipative", M, U.P(U.T(fx)), U.P(U.T(fy)), U.P(U.T(fz)), U.P(dd), *D, st)
-    assert rel_max(U.H(dd), dis) < TOL
+    fxt, fyt, fzt = Tf(fx), Tf(fy), Tf(fz)
+    U.call("mb_explicitscheme_dissipative", M, U.P(fxt), U.P(fyt), U.P(fzt), U.P(dd), *D, st)
+    assert rel_max(Hc(dd), dis) < TOL
     # time step
     vc = O.facetocell(m, vf)
     wc = O.facetocell(m, wf)
     dt_o = O.time_step(m, uc_o, vc, wc, 0.8, *D)
     dtd = U.Z(1)
-    U.call("mb_time_step", M, U.P(U.T(uc_o)), U.P(U.T(vc)), U.P(U.T(wc)), 0.8, *D, U.P(dtd), st)
+    a, b, c = Tc(uc_o), Tc(vc), Tc(wc)
+    U.call("mb_time_step", M, U.P(a), U.P(b), U.P(c), 0.8, *D, U.P(dtd), st)
     assert rel_max(U.H(dtd)[0], dt_o) < 1e-15
     # update
     src = np.linspace(-1, 1, m.nc) * 1e-3
     w2 = w.copy()
     O.update_new_value(m, w2, rez, dis, src, dt_o)
-    w2d = U.T(w)
-    U.call("mb_update_new_value", M, U.P(w2d), U.P(U.T(rez)), U.P(U.T(dis)), U.P(U.T(src)), U.P(U.T([dt_o])), st)
-    assert rel_max(U.H(w2d), w2) < 1e-14
+    w2d = Tc(w)
+    r_t, d_t, s_t, dt_t = Tc(rez), Tc(dis), Tc(src), U.T([dt_o])
+    U.call("mb_update_new_value", M, U.P(w2d), U.P(r_t), U.P(d_t), U.P(s_t), U.P(dt_t), st)
+    assert rel_max(Hc(w2d), w2) < 1e-14
     return ghost_o, gx, gy, gz, psi, node, fx, fy, fz
 
 
@@ -121,15 +143,16 @@ def test_kernels_on_golden_inputs(name, dim, cuda):
     assert rel_max(gx, g["gradx"]) < 1e-14 and rel_max(node, g["w_node"]) < 1e-13
 
 
+@pytest.mark.parametrize("reorder", [False, True])
 @pytest.mark.parametrize("dim,n", [(2, 40), (3, 6)])
-def test_kernels_on_random_fields(dim, n, cuda):
+def test_kernels_on_random_fields(dim, n, reorder, cuda):
     A, resolved = _random_case(dim, n, seed=7 + dim)
     rng = np.random.default_rng(5)
     w = rng.standard_normal(A["nbcells"])
     uf, vf, wf = (rng.uniform(-1, 1, A["nbfaces"]) for _ in range(3))
     if dim == 2:
         wf = np.zeros(A["nbfaces"])
-    _check_all(A, resolved, w, uf, vf, wf, (2e-3, 1e-3, 5e-4 if dim == 3 else 0.0), cuda)
+    _check_all(A, resolved, w, uf, vf, wf, (2e-3, 1e-3, 5e-4 if dim == 3 else 0.0), cuda, reorder=reorder)
 
 
 def test_srnh_flux_batch(cuda):
