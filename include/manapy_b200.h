@@ -31,6 +31,7 @@ extern "C" {
 #define MB_OK 0
 #define MB_EINVAL (-1)   /* bad argument (null pointer, bad size, bad dim) */
 #define MB_ECUDA (-2)    /* a CUDA launch or call failed */
+#define MB_ETOOBIG (-3)  /* the mesh needs more scratch than mb_advdiff_step_noalloc holds */
 
 /* Ghost rule of a boundary face (manapy/boundary/bc_utils.py:45-68). */
 #define MB_G_NONE 0
@@ -200,6 +201,26 @@ int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face,
 int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5],
                double cfl, double grav, int32_t order, double *scratch, double *face_flux,
                double *dt_dev, void *stream);
+
+/* Same step as mb_advdiff_step, for callers that cannot allocate device memory.
+ *
+ * No counterpart in the reference: manapy allocates its work arrays with numpy.
+ * This variant is for code that may not call cudaMalloc at all -- a plugin whose
+ * host application owns every device allocation through its own pool, a service
+ * that reserves its device-memory budget up front, or a loop where a cudaMalloc
+ * (which can synchronise the device) is not acceptable.  Its scratch
+ * (4*nbcells + nbnodes doubles) lives in a fixed array inside the library,
+ * MB_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), which every GPU that loads the
+ * library keeps reserved until the process exits; larger meshes get MB_ETOOBIG.
+ * The first call on each device looks up that array's device address, so make
+ * it before any stream capture.  All calls share the one array: calls that may
+ * overlap on the GPU (different streams, or host threads) race with each other
+ * and must be serialised by the caller.  Nothing in the array needs clearing
+ * between calls.  Arguments as for mb_advdiff_step, without the scratch. */
+#define MB_NOALLOC_SCRATCH_DOUBLES (2 * 1024 * 1024)
+int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
+                            const double *w_in, double *w_out, const double *sign_face,
+                            const double *src, const double *dt_dev, void *stream);
 
 /* Library build information (architecture string), for diagnostics. */
 const char *mb_build_info(void);

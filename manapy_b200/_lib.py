@@ -12,7 +12,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libmanapy_b200.so")
 
-MB_OK, MB_EINVAL, MB_ECUDA = 0, -1, -2
+MB_OK, MB_EINVAL, MB_ECUDA, MB_ETOOBIG = 0, -1, -2, -3
+NOALLOC_SCRATCH_DOUBLES = 2 * 1024 * 1024
 G_NONE, G_DIRICHLET, G_NEUMANN, G_NONSLIP, G_NEUMANN_NH, G_CELL_AT_FACE = 0, 1, 2, 3, 4, 5
 
 _vp = ctypes.c_void_p
@@ -67,6 +68,7 @@ _SIGS = {
     "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                         _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
+    "mb_advdiff_step_noalloc": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
     "mb_build_info": [],
 }
@@ -101,7 +103,8 @@ class MbError(RuntimeError):
 
 def check(rc: int, name: str = "call"):
     if rc != MB_OK:
-        what = {MB_EINVAL: "invalid argument", MB_ECUDA: "CUDA error"}.get(rc, "error %d" % rc)
+        what = {MB_EINVAL: "invalid argument", MB_ECUDA: "CUDA error",
+                MB_ETOOBIG: "mesh too large for the built-in scratch"}.get(rc, "error %d" % rc)
         raise MbError("%s failed: %s" % (name, what))
 
 

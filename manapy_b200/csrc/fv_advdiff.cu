@@ -607,3 +607,53 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- no-allocation variant
+//
+// mb_advdiff_step needs 4*nbcells + nbnodes doubles of scratch that the caller
+// allocates.  Some callers cannot allocate device memory at all: a plugin that
+// lives inside a host application owning every device allocation through its
+// own pool, a service that reserves its whole device-memory budget up front,
+// or a loop that must not call cudaMalloc because that call can synchronise the
+// device.  For them the scratch below is a fixed array in the library's own
+// device image, reserved on every GPU that loads the library until the process
+// exits.
+#include <mutex>
+
+namespace {
+
+static __device__ __align__(256) double g_noalloc_scratch[MB_NOALLOC_SCRATCH_DOUBLES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_base[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
+                                       const double *w_in, double *w_out, const double *sign_face,
+                                       const double *src, const double *dt_dev, void *stream) {
+  if (!mesh_ok(m) || !bc || !p) return MB_EINVAL;
+  const long long need = 4LL * m->nbcells + m->nbnodes;
+  if (need > (long long)MB_NOALLOC_SCRATCH_DOUBLES) return MB_ETOOBIG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MB_ECUDA;
+  if (dev < 0 || dev >= kMaxDevices) return MB_EINVAL;
+  double *base = nullptr;
+  {
+    // first call on this device: look up where the array lives on it (host code
+    // cannot use the symbol itself as a device address)
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+      void *ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return MB_ECUDA;
+      g_noalloc_base[dev] = static_cast<double *>(ptr);
+    }
+    base = g_noalloc_base[dev];
+  }
+  // Every slice is written by the first launch of the step before the second
+  // launch reads it, so nothing has to be cleared between calls.
+  const long long n = m->nbcells;
+  return mb_advdiff_step(m, bc, p, w_in, w_out, sign_face, src, dt_dev, base, base + n, base + 2 * n,
+                         base + 3 * n, base + 4 * n, stream);
+}
