@@ -81,6 +81,29 @@ typedef struct mb_mesh {
   const int32_t *cell_cellfid;
   const double *cell_nf;
   const double *cell_vertex1;
+  /* compact cell-centred tables read by the fused step (2D; NULL selects the
+   * face tables above):
+   *   cell_vtx   [nbcells][4] vertices in manapy's local order (cells.nodeid);
+   *   cell_nbr   [nbcells][4] cell across local face j (faces (v_j, v_j+1)), or
+   *              -1-f for boundary face f;
+   *   cell_flags [nbcells] bit j: the cell is faces.cellid[f][0]; bit 3+j:
+   *              faces.nodeid[f][0] is v_j+1 (else v_j); bit 6+j: the stored
+   *              normal is -(y_a - y_b, x_b - x_a), a = faces.nodeid[f][0];
+   *   node_coord [nbnodes][2] vertex coordinates; cell_xy [nbcells][2] centres. */
+  const int32_t *cell_vtx;
+  const int32_t *cell_nbr;
+  const uint32_t *cell_flags;
+  const double *node_coord;
+  const double *cell_xy;
+  /* the same neighbour lists as cellnid_* and n2c_*, stored SELL-32: rows are taken
+   * in groups of 32 (one warp); group g occupies idx[ptr[g] .. ptr[g+1]) as
+   * [len_g][32] (entry k of row 32g+l at ptr[g] + 32k + l); lsq rows are padded
+   * with -1, n2c rows with their first cell and weight 0 */
+  const int32_t *lsq_sell_ptr;
+  const int32_t *lsq_sell_idx;
+  const int32_t *n2c_sell_ptr;
+  const int32_t *n2c_sell_idx;
+  const double *n2c_sell_alpha;
 } mb_mesh;
 
 typedef struct mb_bc {
@@ -178,13 +201,19 @@ typedef struct mb_advdiff_params {
  * compute_new_val (manapy/solvers/advecdiff/system.py:156-172) in two launches:
  *   1. cell gradients + Barth limiter (order 2) and centre->vertex values (diffusion);
  *   2. per cell: upwind fluxes, diamond diffusion, forward-Euler update.
- * w_in is read, w_out written (distinct buffers).  sign_face[f] = u.n of face f
- * (mb_face_sign), src may be NULL (zero source).  Scratch: gx, gy, gz, psi [nbcells],
- * w_node [nbnodes]. */
+ * w_in is read, w_out written (distinct buffers).  sign_cf[4*i+j] = u.n of the j-th
+ * local face of cell i in manapy's face orientation (mb_cell_face_sign); src may be
+ * NULL (zero source).  Scratch: cell_scratch [4*nbcells] (order 2), node_scratch
+ * [nbnodes] (diffusion); NULL where not needed. */
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
-                    const double *w_in, double *w_out, const double *sign_face, const double *src,
-                    const double *dt_dev, double *gx, double *gy, double *gz, double *psi,
-                    double *w_node, void *stream);
+                    const double *w_in, double *w_out, const double *sign_cf, const double *src,
+                    const double *dt_dev, double *cell_scratch, double *node_scratch, void *stream);
+
+/* sign_cf[4*i+j] = u_face[f] n_x + v_face[f] n_y + w_face[f] n_z for the j-th local face f
+ * of cell i (zero for unused slots): the upwind selector of
+ * manapy/solvers/advecdiff/fvm_utils.py:53-64 laid out per cell for mb_advdiff_step */
+int mb_cell_face_sign(const mb_mesh *m, const double *u_face, const double *v_face,
+                      const double *w_face, double *sign_cf, void *stream);
 
 /* sign_face[f] = u_face[f] n_x + v_face[f] n_y + w_face[f] n_z, the upwind selector of
  * manapy/solvers/advecdiff/fvm_utils.py:53-64 */
@@ -219,7 +248,7 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
  * between calls.  Arguments as for mb_advdiff_step, without the scratch. */
 #define MB_NOALLOC_SCRATCH_DOUBLES (2 * 1024 * 1024)
 int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
-                            const double *w_in, double *w_out, const double *sign_face,
+                            const double *w_in, double *w_out, const double *sign_cf,
                             const double *src, const double *dt_dev, void *stream);
 
 /* Library build information (architecture string), for diagnostics. */

@@ -10,7 +10,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libmanapy_b200.so")
+# MANAPY_B200_LIB selects another build of the same library (A/B comparisons of build options)
+LIB_PATH = os.environ.get("MANAPY_B200_LIB") or os.path.join(HERE, "lib", "libmanapy_b200.so")
 
 MB_OK, MB_EINVAL, MB_ECUDA, MB_ETOOBIG = 0, -1, -2, -3
 NOALLOC_SCRATCH_DOUBLES = 2 * 1024 * 1024
@@ -32,7 +33,10 @@ class MbMesh(ctypes.Structure):
                 ("face_ghostcenter", _vp), ("face_air", _vp), ("face_f", _vp), ("face_dist", _vp),
                 ("n2c_ptr", _vp), ("n2c_idx", _vp), ("n2c_alpha", _vp),
                 ("n2g_ptr", _vp), ("n2g_idx", _vp), ("n2g_alpha", _vp),
-                ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp)]
+                ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp),
+                ("cell_vtx", _vp), ("cell_nbr", _vp), ("cell_flags", _vp), ("node_coord", _vp), ("cell_xy", _vp),
+                ("lsq_sell_ptr", _vp), ("lsq_sell_idx", _vp), ("n2c_sell_ptr", _vp), ("n2c_sell_idx", _vp),
+                ("n2c_sell_alpha", _vp)]
 
 
 class MbBC(ctypes.Structure):
@@ -65,9 +69,9 @@ _SIGS = {
     "mb_explicitscheme_convective_sw": [_M, _P5, _P5, _P5, _P4, _vp, _d, _i32, _vp, _vp],
     "mb_term_source_srnh_sw": [_M, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp],
     "mb_update_sw": [_M, _P5, _P5, _vp, _vp, _vp, _vp],
-    "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                        _vp, _vp, _vp, _vp],
+    "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
+    "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_advdiff_step_noalloc": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
     "mb_build_info": [],

@@ -310,6 +310,21 @@ __global__ void __launch_bounds__(kBlock) k_update(int n, double *wc, const doub
     wc[i] += dt * ((ld(rez + i) + ld(dis + i)) / ld(vol + i) + ld(src + i));
 }
 
+__global__ void __launch_bounds__(kBlock) k_cell_face_sign(mb_mesh m, const double *uf, const double *vf,
+                                                           const double *wf, double *s) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    for (int j = 0; j < 4; ++j) {
+      double v = 0.;
+      if (j < m.nlf) {
+        const int f = ld(m.cell_faces + 4 * i + j);
+        const double *N = m.face_normal + 3 * f;
+        v = ld(uf + f) * ld(N) + ld(vf + f) * ld(N + 1) + ld(wf + f) * ld(N + 2);
+      }
+      s[4 * i + j] = v;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kBlock) k_face_sign(mb_mesh m, const double *uf, const double *vf,
                                                       const double *wf, double *s) {
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nbfaces; f += gridDim.x * blockDim.x) {
@@ -366,7 +381,7 @@ __global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_
     const bool b = c1 < 0;
     const double vo = b ? ghost(f) : ld(w + other);  // unreconstructed value across the face
     // upwind flux of face f in manapy's orientation (left = c0)
-    const double s = ld(sign + f);
+    const double s = ld(sign + 4 * i + j);
     double sol;
     if (s >= 0) {
       // left state
@@ -415,6 +430,233 @@ __global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_
   w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
 }
 
+// ---------------------------------------------------------------- fused step, compact 2D layout
+//
+// Per cell: its three vertices (manapy's local order), the neighbour across
+// each local face (or -1-f for boundary face f), three orientation bits per
+// face and the upwind sign u.n of each face.  Face normals, centres, diamond
+// vectors and areas are recomputed from the vertex coordinates with manapy's
+// expressions: the subtractions are exact, so normals and face centres are the
+// same numbers manapy stores.
+//
+// Neighbour lists (LSQ stencil, node -> cells) are stored SELL-32: for each
+// group of 32 consecutive rows (one warp), entry k of every row sits in one
+// 128-byte segment, so a warp reads its k-th neighbours with one coalesced
+// load; rows are padded with -1 to the group's longest row.  Entries keep
+// manapy's order.
+//
+// Phase 1 writes a packed record {w, gx, gy, psi} per cell, so phase 2 fetches
+// everything it needs from a neighbour with two 16-byte loads.
+
+__device__ __forceinline__ int4 ld4(const int32_t *p) { return __ldg(reinterpret_cast<const int4 *>(p)); }
+__device__ __forceinline__ double2 ldd2(const double *p) { return __ldg(reinterpret_cast<const double2 *>(p)); }
+__device__ __forceinline__ int comp(const int4 v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
+template <class T>
+__device__ __forceinline__ T pick3(T a, T b, T c, int k) { return k == 0 ? a : (k == 1 ? b : c); }
+
+// flags of the compact 2D layout
+__device__ __forceinline__ bool f2_own(uint32_t fl, int j) { return (fl >> j) & 1u; }
+__device__ __forceinline__ bool f2_rev(uint32_t fl, int j) { return (fl >> (3 + j)) & 1u; }
+__device__ __forceinline__ bool f2_flip(uint32_t fl, int j) { return (fl >> (6 + j)) & 1u; }
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+                                                      double *__restrict__ rec, double *__restrict__ wn, int ncb) {
+  const GhostRule ghost = make_rule(m, bc, w);
+  const int lane = threadIdx.x & 31;
+  if (ORDER2 && (int)blockIdx.x < ncb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nbcells) return;
+    const double2 c = ldd2(m.cell_xy + 2 * i);
+    const double wi = ld(w + i);
+    // least-squares gradient: vertex neighbours (SELL-32), then stencil ghosts
+    // every row of the warp runs to the group length (a uniform trip count keeps
+    // several gathers in flight); a padding entry points at the cell itself,
+    // whose terms are exact zeros
+    double ixx = 0., iyy = 0., ixy = 0., jx = 0., jy = 0.;
+    const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
+#pragma unroll 4
+    for (int k = sb + lane; k < se; k += 32) {
+      int cc = ld(m.lsq_sell_idx + k);
+      cc = cc < 0 ? i : cc;
+      const double2 pc = ldd2(m.cell_xy + 2 * cc);
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dw = ld(w + cc) - wi;
+      ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
+      jx += (dx * dw); jy += (dy * dw);
+    }
+    const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+    for (int k = gb; k < ge; ++k) {
+      const int f = ld(m.ghostnid_idx + k);
+      const double dx = ld(m.face_ghostcenter + 3 * f) - c.x, dy = ld(m.face_ghostcenter + 3 * f + 1) - c.y;
+      const double dw = ghost(f) - wi;
+      ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
+      jx += (dx * dw); jy += (dy * dw);
+    }
+    const double dia = ixx * iyy - ixy * ixy;
+    const double x = (iyy * jx - ixy * jy) / dia;
+    const double y = (ixx * jy - ixy * jx) / dia;
+    // Barth limiter over the three faces
+    const int4 vt = ld4(m.cell_vtx + 4 * i);
+    const int4 nb = ld4(m.cell_nbr + 4 * i);
+    const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
+                  P2 = ldd2(m.node_coord + 2 * vt.z);
+    double wmax = wi, wmin = wi;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int o = comp(nb, j);
+      const double b = o < 0 ? ghost(-1 - o) : ld(w + o);
+      wmax = pmax(wmax, b);
+      wmin = pmin(wmin, b);
+    }
+    double ps = 1.;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double2 a = j == 0 ? P0 : (j == 1 ? P1 : P2), b = j == 0 ? P1 : (j == 1 ? P2 : P0);
+      const double r1 = 0.5 * (a.x + b.x) - c.x, r2 = 0.5 * (a.y + b.y) - c.y;
+      const double delta = x * r1 + y * r2;
+      double psi_ij = 1.;
+      if (!(fabs(delta) < 1e-8)) {
+        if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
+        if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
+      }
+      ps = pmin(ps, psi_ij);
+    }
+    reinterpret_cast<double2 *>(rec)[2 * i] = make_double2(wi, x);
+    reinterpret_cast<double2 *>(rec)[2 * i + 1] = make_double2(y, ps);
+    return;
+  }
+  if (DIFF) {
+    const int n = (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x;
+    if (n >= m.nbnodes) return;
+    double acc = 0.;
+    const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
+#pragma unroll 4
+    for (int k = sb + lane; k < se; k += 32) {
+      // padding repeats the row's first cell with weight 0: an exact zero term
+      const int cc = ld(m.n2c_sell_idx + k);
+      acc += ld(m.n2c_sell_alpha + k) * ld(w + cc);
+    }
+    const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
+    for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
+    wn[n] = acc;
+  }
+}
+
+#ifndef MB_P2_MIN_BLOCKS
+#define MB_P2_MIN_BLOCKS 3
+#endif
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+                                                         const double *__restrict__ w, double *__restrict__ w_out,
+                                                         const double *__restrict__ sign,
+                                                         const double *__restrict__ src,
+                                                         const double *__restrict__ dt_dev,
+                                                         const double *__restrict__ rec,
+                                                         const double *__restrict__ wn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRule ghost = make_rule(m, bc, w);
+  const int4 vt = ld4(m.cell_vtx + 4 * i);
+  const int4 nb = ld4(m.cell_nbr + 4 * i);
+  const uint32_t fl = ld(m.cell_flags + i);
+  const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
+                P2 = ldd2(m.node_coord + 2 * vt.z);
+  const double2 ci = ldd2(m.cell_xy + 2 * i);
+  const double2 s01 = ldd2(sign + 4 * i);
+  const double s2 = ld(sign + 4 * i + 2);
+  double wi, gxi = 0., gyi = 0., psii = 0.;
+  if (ORDER2) {
+    const double2 r0 = ldd2(rec + 4 * i), r1 = ldd2(rec + 4 * i + 2);
+    wi = r0.x; gxi = r0.y; gyi = r1.x; psii = r1.y;
+  } else {
+    wi = ld(w + i);
+  }
+  double cv[3], q[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int o = comp(nb, j);
+    const bool b = o < 0;
+    const int f = -1 - o;
+    const bool own = f2_own(fl, j);
+    const bool rev = f2_rev(fl, j);
+    const double2 Pj = j == 0 ? P0 : (j == 1 ? P1 : P2), Pk = j == 0 ? P1 : (j == 1 ? P2 : P0);
+    const double2 Xa = rev ? Pk : Pj;   // faces.nodeid[f][0]
+    const double2 Xb = rev ? Pj : Pk;   // faces.nodeid[f][1]
+    const double fcx = 0.5 * (Xa.x + Xb.x), fcy = 0.5 * (Xa.y + Xb.y);
+    double vo, gxo = 0., gyo = 0., pso = 0.;
+    double2 co;
+    if (b) {
+      vo = ghost(f);
+      co = make_double2(ld(m.face_ghostcenter + 3 * f), ld(m.face_ghostcenter + 3 * f + 1));
+    } else {
+      if (ORDER2) {
+        const double2 r0 = ldd2(rec + 4 * o), r1 = ldd2(rec + 4 * o + 2);
+        vo = r0.x; gxo = r0.y; gyo = r1.x; pso = r1.y;
+      } else {
+        vo = ld(w + o);
+      }
+      co = ldd2(m.cell_xy + 2 * o);
+    }
+    // upwind flux of the face in manapy's orientation (left = faces.cellid[f][0])
+    const double s = j == 0 ? s01.x : (j == 1 ? s01.y : s2);
+    const bool take_me = (s >= 0) == own;
+    double sol;
+    if (take_me) {
+      sol = ORDER2 ? wi + psii * (gxi * (fcx - ci.x) + gyi * (fcy - ci.y)) : wi;
+    } else if (b) {
+      sol = vo;  // boundary ghost, never reconstructed
+    } else {
+      sol = ORDER2 ? vo + pso * (gxo * (fcx - co.x) + gyo * (fcy - co.y)) : vo;
+    }
+    const double F = s * sol;
+    cv[j] = own ? -F : F;
+    if (DIFF) {
+      double v = 0.;
+      if (!b || ld(bc.face_grad_on + f)) {
+        const double2 v1 = own ? ci : co, v2 = own ? co : ci;   // centres of cellid[f][0], [1]
+        const double vl = own ? wi : vo, vr = own ? vo : wi;
+        const double f1x = v1.x - Xa.x, f1y = v1.y - Xa.y;
+        const double f2x = Xb.x - v1.x, f2y = Xb.y - v1.y;
+        const double f3x = v2.x - Xb.x, f3y = v2.y - Xb.y;
+        const double f4x = Xa.x - v2.x, f4y = Xa.y - v2.y;
+        const double air = 0.5 * ((Xb.x - Xa.x) * (v2.y - v1.y) + (v1.x - v2.x) * (Xb.y - Xa.y));
+        const int ia = rev ? comp(vt, (j + 1) % 3) : comp(vt, j);
+        const int ib = rev ? comp(vt, j) : comp(vt, (j + 1) % 3);
+        const double vi1 = ld(wn + ia), vi2 = ld(wn + ib);
+        const double t1 = vi1 + vl, t2 = vl + vi2, t3 = vi2 + vr, t4 = vr + vi1;
+        const double fgx = 1 / (2 * air) * (t1 * f1y + t2 * f2y + t3 * f3y + t4 * f4y);
+        const double fgy = -1 / (2 * air) * (t1 * f1x + t2 * f2x + t3 * f3x + t4 * f4x);
+        double n0 = Xa.y - Xb.y, n1 = Xb.x - Xa.x;
+        if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
+        v = p.Dxx * fgx * n0 + p.Dyy * fgy * n1;
+      }
+      q[j] = own ? v : -v;
+    }
+  }
+  // manapy's accumulation order, with register selects instead of indexed arrays
+  const uint8_t code = ld(m.cell_order + i);
+  double rez = 0.;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick3(nb.x, nb.y, nb.z, sl) >= 0) rez += pick3(cv[0], cv[1], cv[2], sl);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick3(nb.x, nb.y, nb.z, sl) < 0) rez += pick3(cv[0], cv[1], cv[2], sl);
+  }
+  double dis = 0.;
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dis += pick3(q[0], q[1], q[2], order_slot(code, k));
+  }
+  const double dt = *dt_dev;
+  const double sc = src ? ld(src + i) : 0.0;
+  w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
+}
+
 // ---------------------------------------------------------------- shallow-water order-2 pre-pass
 
 // Neumann ghost: the interior cell's value (the default boundary of a manapy Variable).
@@ -447,12 +689,27 @@ inline int grid_for(long long n) {
 
 inline int check_launch() { return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA; }
 
+inline bool compact_2d(const mb_mesh &m) {
+  return m.dim == 2 && m.cell_vtx && m.cell_nbr && m.cell_flags && m.node_coord && m.cell_xy && m.lsq_sell_ptr &&
+         m.lsq_sell_idx && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
+}
+
+// cell scratch: [4][nbcells] planes gx, gy, gz, psi (face-table path) or [nbcells][4]
+// records {w, gx, gy, psi} (compact 2D path); node scratch: [nbnodes]
 template <int DIM, bool O2, bool DF>
 int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
-                double *w_out, const double *sign, const double *src, const double *dt, double *gx,
-                double *gy, double *gz, double *psi, double *wn, cudaStream_t st) {
+                double *w_out, const double *sign, const double *src, const double *dt, double *cs,
+                double *wn, cudaStream_t st) {
   const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
+  if (DIM == 2 && compact_2d(m)) {
+    if (ncb + nnb > 0) k_f2_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+    k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs,
+                                                                        wn);
+    return check_launch();
+  }
+  const long long n = m.nbcells;
+  double *gx = cs, *gy = cs + n, *gz = cs + 2 * n, *psi = cs + 3 * n;
   if (ncb + nnb > 0)
     k_step_phase1<DIM, O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, gx, gy, gz, psi, wn, ncb);
   k_step_phase2<DIM, O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src,
@@ -584,18 +841,25 @@ int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face, c
   return check_launch();
 }
 
+int mb_cell_face_sign(const mb_mesh *m, const double *u_face, const double *v_face, const double *w_face,
+                      double *sign_cf, void *stream) {
+  if (!mesh_ok(m) || !u_face || !v_face || !w_face || !sign_cf) return MB_EINVAL;
+  k_cell_face_sign<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, u_face, v_face, w_face, sign_cf);
+  return check_launch();
+}
+
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p, const double *w_in,
-                    double *w_out, const double *sign_face, const double *src, const double *dt_dev, double *gx,
-                    double *gy, double *gz, double *psi, double *w_node, void *stream) {
-  if (!mesh_ok(m) || !bc || !p || !w_in || !w_out || w_in == w_out || !sign_face || !dt_dev) return MB_EINVAL;
+                    double *w_out, const double *sign_cf, const double *src, const double *dt_dev,
+                    double *cell_scratch, double *node_scratch, void *stream) {
+  if (!mesh_ok(m) || !bc || !p || !w_in || !w_out || w_in == w_out || !sign_cf || !dt_dev) return MB_EINVAL;
   if (p->order != 1 && p->order != 2) return MB_EINVAL;
   const bool o2 = p->order == 2, df = p->diffusion != 0;
-  if (o2 && (!gx || !gy || !psi || (m->dim == 3 && !gz))) return MB_EINVAL;
-  if (df && (!w_node || !bc->face_grad_on)) return MB_EINVAL;
+  if (o2 && !cell_scratch) return MB_EINVAL;
+  if (df && (!node_scratch || !bc->face_grad_on)) return MB_EINVAL;
   if (!bc->kind || !bc->value) return MB_EINVAL;
   cudaStream_t st = ST(stream);
 #define MB_STEP(D, O, F) \
-  return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_face, src, dt_dev, gx, gy, gz, psi, w_node, st)
+  return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, st)
   if (m->dim == 2) {
     if (o2) { if (df) MB_STEP(2, true, true); else MB_STEP(2, true, false); }
     else { if (df) MB_STEP(2, false, true); else MB_STEP(2, false, false); }
@@ -631,7 +895,7 @@ double *g_noalloc_base[kMaxDevices] = {};
 }  // namespace
 
 extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
-                                       const double *w_in, double *w_out, const double *sign_face,
+                                       const double *w_in, double *w_out, const double *sign_cf,
                                        const double *src, const double *dt_dev, void *stream) {
   if (!mesh_ok(m) || !bc || !p) return MB_EINVAL;
   const long long need = 4LL * m->nbcells + m->nbnodes;
@@ -653,7 +917,5 @@ extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const 
   }
   // Every slice is written by the first launch of the step before the second
   // launch reads it, so nothing has to be cleared between calls.
-  const long long n = m->nbcells;
-  return mb_advdiff_step(m, bc, p, w_in, w_out, sign_face, src, dt_dev, base, base + n, base + 2 * n,
-                         base + 3 * n, base + 4 * n, stream);
+  return mb_advdiff_step(m, bc, p, w_in, w_out, sign_cf, src, dt_dev, base, base + 4LL * m->nbcells, stream);
 }

@@ -28,6 +28,42 @@ def cell_order_codes(faceid_local):
     return code.astype(np.uint8)
 
 
+def sell32(ptr, idx, vals=None, fill=-1):
+    """SELL-32 layout of a CSR table: rows in groups of 32, each group stored
+    [longest row][32] so entry k of the 32 rows is contiguous.  Padding is -1,
+    or each row's first entry with ``fill="first"`` (padding values are 0).
+    Returns (group_ptr, idx_sell, vals_sell)."""
+    ptr = np.asarray(ptr, dtype=np.int64)
+    n = len(ptr) - 1
+    ng = (n + 31) // 32
+    cnt = np.zeros(ng * 32, dtype=np.int64)
+    cnt[:n] = np.diff(ptr)
+    glen = cnt.reshape(ng, 32).max(axis=1)
+    gptr = np.zeros(ng + 1, dtype=np.int64)
+    np.cumsum(glen * 32, out=gptr[1:])
+    row = np.repeat(np.arange(n), np.diff(ptr))
+    k = np.arange(len(idx)) - np.repeat(ptr[:-1], np.diff(ptr))
+    dest = gptr[row // 32] + k * 32 + (row % 32)
+    if fill != "first":
+        out = np.full(int(gptr[-1]), fill, dtype=np.int32)
+    else:
+        # pad each row with its own first entry (callers give such entries a zero weight)
+        first = np.zeros(ng * 32, dtype=np.int64)
+        nz = np.diff(ptr) > 0
+        first[:n][nz] = np.asarray(idx)[ptr[:-1][nz]]
+        slot = np.arange(int(gptr[-1]))
+        g = np.searchsorted(gptr, slot, side="right") - 1
+        out = first[g * 32 + (slot - gptr[g]) % 32].astype(np.int32)
+    out[dest] = idx
+    outv = None
+    if vals is not None:
+        outv = np.zeros(int(gptr[-1]), dtype=np.float64)
+        outv[dest] = vals
+    if gptr[-1] >= 2 ** 31:
+        raise ValueError("neighbour table too large for 32-bit offsets")
+    return gptr.astype(np.int32), out, outv
+
+
 def vertex_weights(A):
     """Centre->vertex weight of every node->cell and node->ghost incidence, in
     manapy's expression order (manapy/ast/functions2d.py:219, functions3d.py:272-274)."""
@@ -95,6 +131,8 @@ class DeviceMesh:
             ptr, idx, _ = R.relabel_csr(A["cellnid_ptr"], A["cellnid_idx"], cp, ci)
             T["cellnid_ptr"] = _t(ptr, i32, dev)
             T["cellnid_idx"] = _t(idx, i32, dev)
+            gp, gi, _ = sell32(ptr, idx)
+            T["lsq_sell_ptr"], T["lsq_sell_idx"] = _t(gp, i32, dev), _t(gi, i32, dev)
         ptr, idx, _ = R.relabel_csr(A["ghostnid_ptr"], A["ghostnid_idx"], cp, fi)
         T["ghostnid_ptr"] = _t(ptr, i32, dev)
         T["ghostnid_idx"] = _t(idx, i32, dev)
@@ -120,6 +158,8 @@ class DeviceMesh:
         a_c, a_g = vertex_weights(A)
         ptr, idx, src = R.relabel_csr(A["n2c_ptr"], A["n2c_idx"], np_, ci)
         T["n2c_ptr"], T["n2c_idx"], T["n2c_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_c[src], f64, dev)
+        gp, gi, gv = sell32(ptr, idx, a_c[src], fill="first")
+        T["n2c_sell_ptr"], T["n2c_sell_idx"], T["n2c_sell_alpha"] = _t(gp, i32, dev), _t(gi, i32, dev), _t(gv, f64, dev)
         ptr, idx, src = R.relabel_csr(A["n2g_ptr"], A["n2g_idx"], np_, fi)
         T["n2g_ptr"], T["n2g_idx"], T["n2g_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_g[src], f64, dev)
         if dim == 2:
@@ -131,6 +171,8 @@ class DeviceMesh:
             T["cell_cellfid"] = _t(cf, i32, dev)
             T["cell_nf"] = _t(A["cells_nf"][cp], f64, dev)
             T["cell_vertex1"] = _t(A["nodes_vertex"][A["cells_nodeid"][cp, 1], :2], f64, dev)
+        if dim == 2:
+            self._compact_2d(A, T, dev)
         self.t = T
         s = _lib.MbMesh()
         s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = dim, nc, nf, nn, nlf, 0
@@ -144,6 +186,47 @@ class DeviceMesh:
         self.inv = {"cell": torch.from_numpy(ci).to(dev), "face": torch.from_numpy(fi).to(dev),
                     "node": torch.from_numpy(ni).to(dev)}
         self.reordered = bool(reorder)
+
+    def _compact_2d(self, A, T, dev):
+        """Cell-centred tables of the fused 2D step (see ``mb_mesh`` in the C header)."""
+        R = self.R
+        cp, ci, fi, ni, np_ = R.cperm, R.cinv, R.finv, R.ninv, R.nperm
+        nc = self.nbcells
+        nodes = A["cells_nodeid"][cp, :3].astype(np.int64)          # manapy's local vertex order
+        faces = A["cells_faceid"][cp, :3].astype(np.int64)          # local face j = (v_j, v_j+1)
+        fcid = A["faces_cellid"]
+        c0 = fcid[faces, 0]
+        c1 = fcid[faces, 1]
+        own = c0 == cp[:, None]
+        other = np.where(own, c1, c0)
+        bnd = c1 < 0
+        nbr = np.where(bnd, -1 - fi[faces], ci[np.maximum(other, 0)])
+        fa = A["faces_nodeid"][faces, 0]                            # faces.nodeid[f][0]
+        v_next = np.roll(nodes, -1, axis=1)
+        rev = fa == v_next
+        assert np.all(rev | (fa == nodes)), "face nodes do not match the cell's local faces"
+        X = A["nodes_vertex"]
+        a = np.where(rev, v_next, nodes)
+        b = np.where(rev, nodes, v_next)
+        n0 = X[a, 1] - X[b, 1]
+        n1 = X[b, 0] - X[a, 0]
+        stored = A["faces_normal"][faces]
+        flip = (stored[..., 0] != n0) | (stored[..., 1] != n1)
+        assert np.array_equal(np.where(flip, -1 * n0, n0), stored[..., 0]) and \
+            np.array_equal(np.where(flip, -1 * n1, n1), stored[..., 1]), "normals are not vertex differences"
+        flags = np.zeros(nc, dtype=np.uint32)
+        for j in range(3):
+            flags |= (own[:, j].astype(np.uint32) << j) | (rev[:, j].astype(np.uint32) << (3 + j)) \
+                | (flip[:, j].astype(np.uint32) << (6 + j))
+        vtx = np.zeros((nc, 4), dtype=np.int32)
+        vtx[:, :3] = ni[nodes]
+        nb4 = np.full((nc, 4), -1, dtype=np.int32)
+        nb4[:, :3] = nbr
+        T["cell_vtx"] = _t(vtx, np.int32, dev)
+        T["cell_nbr"] = _t(nb4, np.int32, dev)
+        T["cell_flags"] = _t(flags.view(np.int32), np.int32, dev)
+        T["node_coord"] = _t(X[np_, :2], np.float64, dev)
+        T["cell_xy"] = _t(A["cells_center"][cp, :2], np.float64, dev)
 
     def to_device_order(self, kind, host_t, out):
         """out[k] = host_t[perm[k]] (``host_t`` already on the device, manapy order)."""

@@ -99,7 +99,7 @@ class AdvectionDiffusionSolver:
             self._dm = self.domain.device_mesh
             dev = self._dm.device
             self._dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
-            self._sign = torch.zeros(self._dm.nbfaces, dtype=torch.float64, device=dev)
+            self._sign = torch.zeros(4 * self._dm.nbcells, dtype=torch.float64, device=dev)
             self._params = _lib.MbAdvDiffParams(int(self.order), int(self.diffusion), float(self.Dxx),
                                                 float(self.Dyy), float(self.Dzz))
         return self._dm
@@ -110,7 +110,7 @@ class AdvectionDiffusionSolver:
     def _update_sign(self):
         key = (self.u.version("face"), self.v.version("face"), self.w.version("face"))
         if key != self._sign_key:
-            _lib.call("mb_face_sign", self._dm.struct, _p(self.u.dev("face")), _p(self.v.dev("face")),
+            _lib.call("mb_cell_face_sign", self._dm.struct, _p(self.u.dev("face")), _p(self.v.dev("face")),
                       _p(self.w.dev("face")), _p(self._sign), self._stream())
             self._sign_key = (self.u.version("face"), self.v.version("face"), self.w.version("face"))
 
@@ -183,8 +183,11 @@ class AdvectionDiffusionSolver:
                     var._s.lazy.pop(n, None)
                 self._materialise(w_in)
 
-        names = ["ghost", "convective"] + (["dissipative", "gradfacex", "gradfacey", "gradfacez"]
-                                           if self.diffusion else [])
+        names = ["ghost", "convective"]
+        if self.order == 2:
+            names += ["gradcellx", "gradcelly", "gradcellz", "psi"]
+        if self.diffusion:
+            names += ["node", "dissipative", "gradfacex", "gradfacey", "gradfacez"]
         for n in names:
             var.set_lazy(n, run)
 
@@ -223,6 +226,13 @@ class AdvectionDiffusionSolver:
         var = self.var
         return None if var.version("source") == 0 else _p(var.dev("source"))
 
+    def _scratch(self):
+        dm = self._dm
+        if getattr(self, "_cs", None) is None:
+            self._cs = torch.empty(4 * dm.nbcells, dtype=torch.float64, device=dm.device)
+            self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
+        return self._cs, self._ns
+
     def _fused_step(self):
         var = self.var
         dm = self._dm
@@ -231,13 +241,9 @@ class AdvectionDiffusionSolver:
         if self._spare is None or self._spare.numel() != w_in.numel():
             self._spare = torch.empty_like(w_in)
         w_out = self._spare
-        gz = var.dev_out("gradcellz") if self.dim == 3 else var.dev("gradcellz")
+        cs, ns = self._scratch()
         _lib.call("mb_advdiff_step", dm.struct, var.device_bc.struct, self._params, _p(w_in), _p(w_out),
-                  _p(self._sign), self._source_ptr(), _p(self._dt_dev),
-                  _p(var.dev_out("gradcellx") if self.order == 2 else var.dev("gradcellx")),
-                  _p(var.dev_out("gradcelly") if self.order == 2 else var.dev("gradcelly")), _p(gz),
-                  _p(var.dev_out("psi") if self.order == 2 else var.dev("psi")),
-                  _p(var.dev_out("node") if self.diffusion else var.dev("node")), self._stream())
+                  _p(self._sign), self._source_ptr(), _p(self._dt_dev), _p(cs), _p(ns), self._stream())
         self._spare = var.swap_cell(w_out)
         self._install_lazies(self._spare)
 
@@ -285,7 +291,7 @@ class AdvectionDiffusionSolver:
         a = var.dev("cell")
         b = self._spare
         dm = self._dm
-        gz = var.dev("gradcellz")
+        cs, ns = self._scratch()
         args = (var.device_bc.struct, self._params)
         src = self._source_ptr()
         s = torch.cuda.Stream(device=dm.device)
@@ -297,8 +303,7 @@ class AdvectionDiffusionSolver:
                 st = torch.cuda.current_stream(dm.device).cuda_stream
                 for x, y in ((a, b), (b, a)):
                     _lib.call("mb_advdiff_step", dm.struct, args[0], args[1], _p(x), _p(y), _p(self._sign),
-                              src, _p(self._dt_dev), _p(var.dev("gradcellx")), _p(var.dev("gradcelly")),
-                              _p(gz), _p(var.dev("psi")), _p(var.dev("node")), st)
+                              src, _p(self._dt_dev), _p(cs), _p(ns), st)
         torch.cuda.current_stream(dm.device).wait_stream(s)
         self._graph = g
         return g

@@ -58,3 +58,27 @@ def test_cell_at_face_ghost_index_follows_renumbering():
     db = DeviceBC(A, bc, "cpu", mesh=dm)
     v = db.value.numpy()
     assert np.array_equal(v[dm.R.finv[caf]], dm.R.cinv[caf])
+
+
+def test_sell32_layout_round_trips():
+    from manapy_b200.device import sell32
+    rng = np.random.default_rng(0)
+    cnt = rng.integers(0, 20, size=77)
+    ptr = np.zeros(78, dtype=np.int64)
+    np.cumsum(cnt, out=ptr[1:])
+    idx = rng.integers(0, 1000, size=int(ptr[-1]))
+    vals = rng.standard_normal(int(ptr[-1]))
+    for fill in (-1, "first"):
+        gp, gi, gv = sell32(ptr, idx, vals, fill=fill)
+        for r in range(77):
+            g, l = divmod(r, 32)
+            length = (gp[g + 1] - gp[g]) // 32
+            row = gi[gp[g] + 32 * np.arange(length) + l]
+            rv = gv[gp[g] + 32 * np.arange(length) + l]
+            assert np.array_equal(row[:cnt[r]], idx[ptr[r]:ptr[r + 1]])
+            assert np.array_equal(rv[:cnt[r]], vals[ptr[r]:ptr[r + 1]])
+            assert np.all(rv[cnt[r]:] == 0)
+            if fill == -1:
+                assert np.all(row[cnt[r]:] == -1)
+            elif cnt[r]:
+                assert np.all(row[cnt[r]:] == idx[ptr[r]])

@@ -28,9 +28,9 @@ def _setup(wl):
     R = dm.R
     uf, vf, wf = wl.velocity(A["faces_center"])
     st = U.stream()
-    sign = U.Z(A["nbfaces"])
+    sign = U.Z(4 * A["nbcells"])
     u_, v_, w_ = U.T(uf[R.fperm]), U.T(vf[R.fperm]), U.T(wf[R.fperm])
-    U.call("mb_face_sign", dm.struct, U.P(u_), U.P(v_), U.P(w_), U.P(sign), st)
+    U.call("mb_cell_face_sign", dm.struct, U.P(u_), U.P(v_), U.P(w_), U.P(sign), st)
     uc, vc, wc = U.Z(A["nbcells"]), U.Z(A["nbcells"]), U.Z(A["nbcells"])
     for src, dst in ((u_, uc), (v_, vc), (w_, wc)):
         U.call("mb_facetocell", dm.struct, U.P(src), U.P(dst), st)
@@ -44,9 +44,9 @@ def _setup(wl):
 def _regular(U, A, dm, db, prm, sign, dt, w_in, st):
     nc, nn = A["nbcells"], A["nbnodes"]
     out = U.Z(nc)
-    scratch = [U.Z(nc) for _ in range(4)] + [U.Z(nn)]
+    cell_scratch, node_scratch = U.Z(4 * nc), U.Z(nn)
     U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w_in), U.P(out), U.P(sign), None, U.P(dt),
-           *[U.P(t) for t in scratch], st)
+           U.P(cell_scratch), U.P(node_scratch), st)
     return out
 
 
