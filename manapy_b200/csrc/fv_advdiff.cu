@@ -454,13 +454,75 @@ __device__ __forceinline__ int comp(const int4 v, int j) { return j == 0 ? v.x :
 template <class T>
 __device__ __forceinline__ T pick3(T a, T b, T c, int k) { return k == 0 ? a : (k == 1 ? b : c); }
 
+// L2 eviction-priority hints (per instruction; no device state is changed).
+// Phase 1 writes its outputs with evict_last so they are still in L2 when
+// phase 2 reads them; tables read once per step are loaded with evict_first.
+#ifndef MB_L2_HINTS
+#define MB_L2_HINTS 1
+#endif
+__device__ __forceinline__ uint64_t l2_keep() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_stream() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void st2_keep(double *a, double x, double y, uint64_t pol) {
+#if MB_L2_HINTS
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(x), "d"(y), "l"(pol) : "memory");
+#else
+  *reinterpret_cast<double2 *>(a) = make_double2(x, y);
+#endif
+}
+__device__ __forceinline__ void st1_keep(double *a, double x, uint64_t pol) {
+#if MB_L2_HINTS
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(x), "l"(pol) : "memory");
+#else
+  *a = x;
+#endif
+}
+__device__ __forceinline__ int ld1_stream(const int32_t *a, uint64_t pol) {
+#if MB_L2_HINTS
+  int v;
+  asm volatile("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+#else
+  return __ldg(a);
+#endif
+}
+__device__ __forceinline__ double2 ldd2_stream(const double *a, uint64_t pol) {
+#if MB_L2_HINTS
+  double2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+  return v;
+#else
+  return __ldg(reinterpret_cast<const double2 *>(a));
+#endif
+}
+__device__ __forceinline__ double ldd_stream(const double *a, uint64_t pol) {
+#if MB_L2_HINTS
+  double v;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+#else
+  return __ldg(a);
+#endif
+}
+
 // flags of the compact 2D layout
 __device__ __forceinline__ bool f2_own(uint32_t fl, int j) { return (fl >> j) & 1u; }
 __device__ __forceinline__ bool f2_rev(uint32_t fl, int j) { return (fl >> (3 + j)) & 1u; }
 __device__ __forceinline__ bool f2_flip(uint32_t fl, int j) { return (fl >> (6 + j)) & 1u; }
 
+#ifndef MB_P1_MIN_BLOCKS
+#define MB_P1_MIN_BLOCKS 6
+#endif
+
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+__global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                       double *__restrict__ rec, double *__restrict__ wn, int ncb) {
   const GhostRule ghost = make_rule(m, bc, w);
   const int lane = threadIdx.x & 31;
@@ -475,9 +537,29 @@ __global__ void __launch_bounds__(kBlock) k_f2_phase1(mb_mesh m, mb_bc bc, const
     // whose terms are exact zeros
     double ixx = 0., iyy = 0., ixy = 0., jx = 0., jy = 0.;
     const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
-#pragma unroll 4
-    for (int k = sb + lane; k < se; k += 32) {
-      int cc = ld(m.lsq_sell_idx + k);
+    const int L = (se - sb) >> 5;
+    const int32_t *ix = m.lsq_sell_idx + sb + lane;
+    const uint64_t pst = l2_stream();
+    int k = 0;
+    // batches of four: four index loads, then eight gathers in flight, then the
+    // four terms accumulated in manapy's order
+    for (; k + 4 <= L; k += 4) {
+      int cc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { cc[u] = ld1_stream(ix + 32 * (k + u), pst); cc[u] = cc[u] < 0 ? i : cc[u]; }
+      double2 pc[4];
+      double wc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { pc[u] = ldd2(m.cell_xy + 2 * cc[u]); wc[u] = ld(w + cc[u]); }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double dx = pc[u].x - c.x, dy = pc[u].y - c.y, dw = wc[u] - wi;
+        ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
+        jx += (dx * dw); jy += (dy * dw);
+      }
+    }
+    for (; k < L; ++k) {
+      int cc = ld1_stream(ix + 32 * k, pst);
       cc = cc < 0 ? i : cc;
       const double2 pc = ldd2(m.cell_xy + 2 * cc);
       const double dx = pc.x - c.x, dy = pc.y - c.y, dw = ld(w + cc) - wi;
@@ -521,8 +603,9 @@ __global__ void __launch_bounds__(kBlock) k_f2_phase1(mb_mesh m, mb_bc bc, const
       }
       ps = pmin(ps, psi_ij);
     }
-    reinterpret_cast<double2 *>(rec)[2 * i] = make_double2(wi, x);
-    reinterpret_cast<double2 *>(rec)[2 * i + 1] = make_double2(y, ps);
+    const uint64_t keep = l2_keep();
+    st2_keep(rec + 4 * i, wi, x, keep);
+    st2_keep(rec + 4 * i + 2, y, ps, keep);
     return;
   }
   if (DIFF) {
@@ -530,15 +613,16 @@ __global__ void __launch_bounds__(kBlock) k_f2_phase1(mb_mesh m, mb_bc bc, const
     if (n >= m.nbnodes) return;
     double acc = 0.;
     const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
+    const uint64_t pst = l2_stream();
 #pragma unroll 4
     for (int k = sb + lane; k < se; k += 32) {
       // padding repeats the row's first cell with weight 0: an exact zero term
-      const int cc = ld(m.n2c_sell_idx + k);
-      acc += ld(m.n2c_sell_alpha + k) * ld(w + cc);
+      const int cc = ld1_stream(m.n2c_sell_idx + k, pst);
+      acc += ldd_stream(m.n2c_sell_alpha + k, pst) * ld(w + cc);
     }
     const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
     for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
-    wn[n] = acc;
+    st1_keep(wn + n, acc, l2_keep());
   }
 }
 
@@ -563,8 +647,9 @@ __global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh 
   const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
                 P2 = ldd2(m.node_coord + 2 * vt.z);
   const double2 ci = ldd2(m.cell_xy + 2 * i);
-  const double2 s01 = ldd2(sign + 4 * i);
-  const double s2 = ld(sign + 4 * i + 2);
+  const uint64_t pst = l2_stream();
+  const double2 s01 = ldd2_stream(sign + 4 * i, pst);
+  const double s2 = ldd_stream(sign + 4 * i + 2, pst);
   double wi, gxi = 0., gyi = 0., psii = 0.;
   if (ORDER2) {
     const double2 r0 = ldd2(rec + 4 * i), r1 = ldd2(rec + 4 * i + 2);
