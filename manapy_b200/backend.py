@@ -25,6 +25,17 @@ class CUDABackend:
         self.float_precision = "float64"
         self.int_precision = "int32" if int_precision == "signed" else "uint32"
 
+    @classmethod
+    def for_manapy_domain(cls, manapy_domain, device="cuda"):
+        """Backend for a domain built by manapy itself: the device tables are rebuilt
+        from its element and vertex arrays (the same arrays manapy derives its
+        geometry from), so kernel arguments taken from that domain line up."""
+        from .domain import Domain
+        nodeid = manapy_domain.cells.nodeid
+        vertex = manapy_domain.nodes.vertex
+        dom = Domain(dim=int(manapy_domain.dim), mesh=(nodeid, vertex), device=device)
+        return cls(dom)
+
     def compile(self, func, signature=False, forcedbackend=None, outer=False):
         name = getattr(func, "__name__", None)
         impl = plugin.KERNELS.get(name)
