@@ -88,7 +88,8 @@ typedef struct mb_mesh {
    *              -1-f for boundary face f;
    *   cell_flags [nbcells] bit j: the cell is faces.cellid[f][0]; bit 3+j:
    *              faces.nodeid[f][0] is v_j+1 (else v_j); bit 6+j: the stored
-   *              normal is -(y_a - y_b, x_b - x_a), a = faces.nodeid[f][0];
+   *              normal is -(y_a - y_b, x_b - x_a), a = faces.nodeid[f][0]; bit 9+j:
+ *              cells.nf (outward normal) of face j is minus the face normal;
    *   node_coord [nbnodes][2] vertex coordinates; cell_xy [nbcells][2] centres. */
   const int32_t *cell_vtx;
   const int32_t *cell_nbr;
@@ -220,16 +221,19 @@ int mb_cell_face_sign(const mb_mesh *m, const double *u_face, const double *v_fa
 int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face,
                  const double *w_face, double *sign_face, void *stream);
 
-/* One shallow-water step (ShallowWaterSolver.stepper + compute_fluxes + compute_new_val,
- * manapy/solvers/shallowater/system.py:186-192,248-281,237-242) with Neumann ghosts on
- * every boundary face (manapy's default): dt (time_step_SW) -> [order 2: h, hc gradients
- * and hc limiter] -> face fluxes -> per-cell gather + bathymetry source + update.
- * q_in / q_out: 5 distinct cell arrays each (h, hu, hv, hc, Z).  Scratch: face_flux
- * [nbfaces][5], scratch [5][nbcells] (order 2 only, else may be NULL); dt_dev receives
- * this step's dt. */
+/* One shallow-water step (ShallowWaterSolver.compute_fluxes + compute_new_val,
+ * manapy/solvers/shallowater/system.py:248-281,237-242) with Neumann ghosts on every
+ * boundary face (manapy's default), in two launches: [order 2: h, hc gradients and hc
+ * limiter] face fluxes, then per cell the residual gather, bathymetry source and update.
+ * The update uses *dt_cur (from mb_time_step_sw, or the previous step's dt_next); the
+ * second launch also evaluates time_step_SW on the updated state into *dt_next (the next
+ * step's dt), unless dt_next is NULL.  q_in / q_out: 5 cell arrays each (h, hu, hv, hc, Z);
+ * q_out[k] != q_in[k] except Z (the bed does not change and may be shared).  Scratch:
+ * face_flux [nbfaces][4], scratch [5][nbcells] (order 2 only, else NULL).  Needs the
+ * compact 2D tables of mb_mesh. */
 int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5],
                double cfl, double grav, int32_t order, double *scratch, double *face_flux,
-               double *dt_dev, void *stream);
+               const double *dt_cur, double *dt_next, void *stream);
 
 /* Same step as mb_advdiff_step, for callers that cannot allocate device memory.
  *

@@ -73,7 +73,7 @@ _SIGS = {
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_advdiff_step_noalloc": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp],
-    "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
+    "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],
     "mb_build_info": [],
 }
 _RESTYPES = {"mb_build_info": ctypes.c_char_p}

@@ -214,10 +214,15 @@ class DeviceMesh:
         flip = (stored[..., 0] != n0) | (stored[..., 1] != n1)
         assert np.array_equal(np.where(flip, -1 * n0, n0), stored[..., 0]) and \
             np.array_equal(np.where(flip, -1 * n1, n1), stored[..., 1]), "normals are not vertex differences"
+        # cells.nf: the outward normal table of the bathymetry source (+- the face normal)
+        nf_tab = A["cells_nf"][cp]
+        nfneg = (nf_tab[..., 0] != stored[..., 0]) | (nf_tab[..., 1] != stored[..., 1])
+        assert np.array_equal(np.where(nfneg, -1 * stored[..., 0], stored[..., 0]), nf_tab[..., 0]), \
+            "cells.nf is not +- the face normal"
         flags = np.zeros(nc, dtype=np.uint32)
         for j in range(3):
             flags |= (own[:, j].astype(np.uint32) << j) | (rev[:, j].astype(np.uint32) << (3 + j)) \
-                | (flip[:, j].astype(np.uint32) << (6 + j))
+                | (flip[:, j].astype(np.uint32) << (6 + j)) | (nfneg[:, j].astype(np.uint32) << (9 + j))
         vtx = np.zeros((nc, 4), dtype=np.int32)
         vtx[:, :3] = ni[nodes]
         nb4 = np.full((nc, 4), -1, dtype=np.int32)

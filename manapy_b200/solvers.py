@@ -378,12 +378,16 @@ class ShallowWaterSolver:
         self._spare = None
         self._scratch = None
         self._dt_host = None
+        self._fused = False
 
     def _setup(self):
         if self._dm is None:
             self._dm = self.domain.device_mesh
             dev = self._dm.device
-            self._dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+            # dt double buffer: slot _cur holds the dt of the current state when _dt_key matches
+            self._dt_buf = torch.zeros(2, dtype=torch.float64, device=dev)
+            self._cur = 0
+            self._dt_key = None
             self._ff = torch.zeros(5 * self._dm.nbfaces, dtype=torch.float64, device=dev)
             if self.order == 2:
                 self._scratch = torch.zeros(5 * self._dm.nbcells, dtype=torch.float64, device=dev)
@@ -403,14 +407,27 @@ class ShallowWaterSolver:
     def _q(self):
         return [self.varbs[k].dev("cell") for k in ("h", "hu", "hv", "hc", "Z")]
 
+    def _state_key(self):
+        return tuple(self.varbs[k].version("cell") for k in ("h", "hu", "hv"))
+
+    def _dt_slot(self):
+        """Device slot holding the dt of the current state (computed if stale)."""
+        slot = self._dt_buf[self._cur:self._cur + 1]
+        if self._dt_key != self._state_key():
+            q = self._q()
+            _lib.call("mb_time_step_sw", self._dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), float(self.cfl),
+                      float(self.grav), float(self.Dxx), float(self.Dyy), _p(slot), self._stream())
+            self._dt_key = self._state_key()
+            self._dt_host = None
+        return slot
+
     def stepper(self):
         """manapy/solvers/shallowater/system.py:186-192 (returns dt; manapy returns None)."""
         self._setup()
-        q = self._q()
-        _lib.call("mb_time_step_sw", self._dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), float(self.cfl),
-                  float(self.grav), float(self.Dxx), float(self.Dyy), _p(self._dt_dev), self._stream())
-        self.dt = float(self._dt_dev.item())
-        self._dt_host = self.dt
+        slot = self._dt_slot()
+        if self._dt_host is None:
+            self._dt_host = float(slot.item())
+        self.dt = self._dt_host
         return self.dt
 
     def update_ghost_values(self):
@@ -451,6 +468,16 @@ class ShallowWaterSolver:
             self.update_ghost_values()
             self.explicit_convective()
             self.update_term_source()
+        else:
+            self.stepper()  # manapy evaluates the CFL step inside compute_fluxes
+
+    def _use_dt(self):
+        """The dt slot this step uses: the current state's dt, or S.dt if set by hand."""
+        slot = self._dt_slot()
+        if self._dt_host is not None and float(self.dt) != self._dt_host:
+            slot.fill_(float(self.dt))
+            self._dt_host = float(self.dt)
+        return slot
 
     def compute_new_val(self):
         """manapy/solvers/shallowater/system.py:237-242."""
@@ -462,29 +489,34 @@ class ShallowWaterSolver:
         names = ("h", "hu", "hv", "hc", "Z")
         q = _lib.p5([_p(self.varbs[k].dev("cell")) for k in names])
         rez = _lib.p5([_p(self.varbs[k].dev("convective")) for k in names])
-        if self._dt_host is None or float(self.dt) != self._dt_host:
-            self._dt_dev.fill_(float(self.dt))
+        dt = torch.tensor([float(self.dt)], dtype=torch.float64, device=self._dm.device)
         _lib.call("mb_update_sw", self._dm.struct, q, rez, _p(self.hu.dev("source")),
-                  _p(self.hv.dev("source")), _p(self._dt_dev), self._stream())
+                  _p(self.hv.dev("source")), _p(dt), self._stream())
         for k in names:
             self.varbs[k]._s.version["cell"] += 1
+        self._dt_key = None
 
     def _fused_step(self):
-        names = ("h", "hu", "hv", "hc", "Z")
+        names = ("h", "hu", "hv", "hc")
         qin = [self.varbs[k].dev("cell") for k in names]
+        z = self.Z.dev("cell")
         if self._spare is None:
             self._spare = [torch.empty_like(t) for t in qin]
         qout = self._spare
-        _lib.call("mb_sw_step", self._dm.struct, _lib.p5([_p(t) for t in qin]), _lib.p5([_p(t) for t in qout]),
-                  float(self.cfl), float(self.grav), int(self.order),
-                  _p(self._scratch) if self._scratch is not None else None, _p(self._ff), _p(self._dt_dev),
+        cur = self._use_dt()
+        nxt = self._dt_buf[1 - self._cur:2 - self._cur]
+        _lib.call("mb_sw_step", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
+                  _lib.p5([_p(t) for t in qout] + [_p(z)]), float(self.cfl), float(self.grav), int(self.order),
+                  _p(self._scratch) if self._scratch is not None else None, _p(self._ff), _p(cur), _p(nxt),
                   self._stream())
         self._spare = [self.varbs[k].swap_cell(t) for k, t in zip(names, qout)]
+        self._cur = 1 - self._cur
+        self._dt_key = self._state_key()
         self._dt_host = None
 
     def launches_per_step(self):
-        """Kernel launches of one fused step: dt init + dt min, [gradients], face fluxes, cells."""
-        return 4 + int(self.order == 2)
+        """Kernel launches of one fused step: face fluxes, cells (+ next dt), [gradients]."""
+        return 2 + int(self.order == 2)
 
     def release_graphs(self):
         return None
@@ -493,5 +525,7 @@ class ShallowWaterSolver:
         """``nsteps`` fused steps on the device, without host synchronisation (each step's dt
         stays on the device)."""
         self._setup()
+        if not self._all_neumann():
+            raise NotImplementedError("advance() runs the fused step, which needs Neumann boundaries")
         for _ in range(int(nsteps)):
             self._fused_step()

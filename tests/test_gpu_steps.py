@@ -142,9 +142,9 @@ def _sw_api(el, vx, wl):
     return dom, (h, hu, hv, hc, Z), S
 
 
-@pytest.mark.parametrize("order", [1, 2])
-def test_shallow_water_matches_oracle(order, cuda):
-    wl = W.C3.scaled(n=40, steps=60, order=order)
+@pytest.mark.parametrize("order,n,steps", [(1, 40, 60), (2, 40, 60), (1, 120, 150)])
+def test_shallow_water_matches_oracle(order, n, steps, cuda):
+    wl = W.C3.scaled(n=n, steps=steps, order=order)
     el, vx = wl.mesh()
     dom, vs, S = _sw_api(el, vx, wl)
     A = dom.host_arrays
@@ -157,7 +157,7 @@ def test_shallow_water_matches_oracle(order, cuda):
     for k, var in zip(("h", "hu", "hv", "hc", "Z"), vs):
         ref = so.state()[k]
         if np.any(ref):
-            assert rel_max(var.cell, ref) < 1e-11, k
+            assert rel_max(var.cell, ref) < TOL, k
     # mass: FP64 sum of V h changes only through boundary fluxes (Neumann walls leak)
     assert abs(np.sum(vs[0].cell * A["cells_volume"]) - np.sum(so.h * A["cells_volume"])) < 1e-12
 
@@ -174,4 +174,4 @@ def test_shallow_water_matches_reference(name, cuda):
     for _ in range(wl.steps):
         S.stepper(); S.compute_fluxes(); S.compute_new_val()
     for k, var in zip(("h", "hu", "hv"), vs[:3]):
-        assert rel_max(var.cell, g[k + "_final"]) < 1e-11, k
+        assert rel_max(var.cell, g[k + "_final"]) < TOL, k
