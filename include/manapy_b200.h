@@ -90,7 +90,11 @@ typedef struct mb_mesh {
    *              faces.nodeid[f][0] is v_j+1 (else v_j); bit 6+j: the stored
    *              normal is -(y_a - y_b, x_b - x_a), a = faces.nodeid[f][0]; bit 9+j:
  *              cells.nf (outward normal) of face j is minus the face normal;
-   *   node_coord [nbnodes][2] vertex coordinates; cell_xy [nbcells][2] centres. */
+   *   node_coord [nbnodes][2] vertex coordinates; cell_xy [nbcells][2] centres.
+   * 3D (tetrahedra): cell_nbr / cell_vtx as above with local faces (v0,v1,v2),
+   * (v2,v3,v0), (v0,v1,v3), (v3,v1,v2); cell_flags has 6 bits per face j at bit 6j:
+   * own, 3-bit permutation to manapy's descending face-node order, orientation
+   * swap, normal flip; node_coord and cell_xy are [n][4] (x, y, z, unused). */
   const int32_t *cell_vtx;
   const int32_t *cell_nbr;
   const uint32_t *cell_flags;
@@ -204,8 +208,8 @@ typedef struct mb_advdiff_params {
  *   2. per cell: upwind fluxes, diamond diffusion, forward-Euler update.
  * w_in is read, w_out written (distinct buffers).  sign_cf[4*i+j] = u.n of the j-th
  * local face of cell i in manapy's face orientation (mb_cell_face_sign); src may be
- * NULL (zero source).  Scratch: cell_scratch [4*nbcells] (order 2), node_scratch
- * [nbnodes] (diffusion); NULL where not needed. */
+ * NULL (zero source).  Scratch: cell_scratch [4*nbcells] in 2D, [6*nbcells] in 3D
+ * (order 2), node_scratch [nbnodes] (diffusion); NULL where not needed. */
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
                     const double *dt_dev, double *cell_scratch, double *node_scratch, void *stream);
@@ -242,7 +246,8 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
  * host application owns every device allocation through its own pool, a service
  * that reserves its device-memory budget up front, or a loop where a cudaMalloc
  * (which can synchronise the device) is not acceptable.  Its scratch
- * (4*nbcells + nbnodes doubles) lives in a fixed array inside the library,
+ * (4*nbcells + nbnodes doubles in 2D, 6*nbcells + nbnodes in 3D) lives in a fixed
+ * array inside the library,
  * MB_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), which every GPU that loads the
  * library keeps reserved until the process exits; larger meshes get MB_ETOOBIG.
  * The first call on each device looks up that array's device address, so make

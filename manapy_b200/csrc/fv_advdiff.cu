@@ -742,6 +742,247 @@ __global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh 
   w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
 }
 
+// ---------------------------------------------------------------- fused step, compact 3D layout
+//
+// Tetrahedra.  Local face j of a cell is (v0,v1,v2), (v2,v3,v0), (v0,v1,v3),
+// (v3,v1,v2) (manapy/ddm/ddm_utils3d.py:785-791).  cell_flags holds six bits per
+// face at bit 6j: bit 0 the cell is faces.cellid[f][0]; bits 1-3 the permutation
+// taking the local face's vertices to manapy's descending node order (which fixes
+// the face centre and the stored normal); bit 4 manapy's orientation swap of the
+// last two nodes (the order of the diamond vectors); bit 5 the stored normal is
+// minus 0.5 (v_d1 - v_d0) x (v_d2 - v_d0).  Node coordinates and cell centres
+// are stored [n][4]; the phase-1 record is {w, gx, gy, gz, psi, -} per cell.
+
+__device__ __constant__ int8_t kTetFace[4][3] = {{0, 1, 2}, {2, 3, 0}, {0, 1, 3}, {3, 1, 2}};
+__device__ __constant__ int8_t kPerm3[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
+struct D3 {
+  double x, y, z;
+};
+__device__ __forceinline__ D3 d3(double x, double y, double z) { return D3{x, y, z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return d3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return d3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return d3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+  return d3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 ld3(const double *p) {  // [n][4] rows
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p + 2));
+  return d3(a.x, a.y, b.x);
+}
+__device__ __forceinline__ D3 pick4(const D3 *P, int k) { return k == 0 ? P[0] : (k == 1 ? P[1] : (k == 2 ? P[2] : P[3])); }
+template <class T>
+__device__ __forceinline__ T pick4v(T a, T b, T c, T d, int k) { return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d)); }
+
+// manapy's descending-order vertices of local face j: (d0, d1, d2), as local vertex indices
+__device__ __forceinline__ void face_desc(uint32_t fl, int j, int &d0, int &d1, int &d2) {
+  const int code = (fl >> (6 * j + 1)) & 7u;
+  d0 = kTetFace[j][kPerm3[code][0]];
+  d1 = kTetFace[j][kPerm3[code][1]];
+  d2 = kTetFace[j][kPerm3[code][2]];
+}
+
+#ifndef MB_P1_3D_MIN_BLOCKS
+#define MB_P1_3D_MIN_BLOCKS 3
+#endif
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+                                                                        double *__restrict__ rec,
+                                                                        double *__restrict__ wn, int ncb) {
+  const GhostRule ghost = make_rule(m, bc, w);
+  const int lane = threadIdx.x & 31;
+  if (ORDER2 && (int)blockIdx.x < ncb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nbcells) return;
+    const D3 c = ld3(m.cell_xy + 4 * i);
+    const double wi = ld(w + i);
+    double ixx = 0., iyy = 0., izz = 0., ixy = 0., ixz = 0., iyz = 0., jx = 0., jy = 0., jz = 0.;
+    const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
+    const int L = (se - sb) >> 5;
+    const int32_t *ix = m.lsq_sell_idx + sb + lane;
+    for (int k = 0; k < L; ++k) {
+      int cc = ld(ix + 32 * k);
+      cc = cc < 0 ? i : cc;
+      const D3 pc = ld3(m.cell_xy + 4 * cc);
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z, dw = ld(w + cc) - wi;
+      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+      ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+      jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
+    }
+    const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+    for (int k = gb; k < ge; ++k) {
+      const int f = ld(m.ghostnid_idx + k);
+      const double *gc = m.face_ghostcenter + 3 * f;
+      const double dx = ld(gc) - c.x, dy = ld(gc + 1) - c.y, dz = ld(gc + 2) - c.z;
+      const double dw = ghost(f) - wi;
+      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+      ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+      jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
+    }
+    const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) - izz * (ixy * ixy);
+    const double gx = ((iyy * izz - iyz * iyz) * jx + (ixz * iyz - ixy * izz) * jy + (ixy * iyz - ixz * iyy) * jz) / dia;
+    const double gy = ((ixz * iyz - ixy * izz) * jx + (ixx * izz - ixz * ixz) * jy + (ixy * ixz - iyz * ixx) * jz) / dia;
+    const double gz = ((ixy * iyz - ixz * iyy) * jx + (ixy * ixz - iyz * ixx) * jy + (ixx * iyy - ixy * ixy) * jz) / dia;
+    // Barth limiter over the four faces
+    const int4 vt = ld4(m.cell_vtx + 4 * i);
+    const int4 nb = ld4(m.cell_nbr + 4 * i);
+    const uint32_t fl = ld(m.cell_flags + i);
+    const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
+                     ld3(m.node_coord + 4 * vt.w)};
+    double wmax = wi, wmin = wi;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int o = comp(nb, j);
+      const double b = o < 0 ? ghost(-1 - o) : ld(w + o);
+      wmax = pmax(wmax, b);
+      wmin = pmin(wmin, b);
+    }
+    double ps = 1.;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int d0, d1, d2;
+      face_desc(fl, j, d0, d1, d2);
+      const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
+      const double delta = gx * (fc.x - c.x) + gy * (fc.y - c.y) + gz * (fc.z - c.z);
+      double psi_ij = 1.;
+      if (!(fabs(delta) < 1e-10)) {
+        if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
+        if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
+      }
+      ps = pmin(ps, psi_ij);
+    }
+    double2 *r2 = reinterpret_cast<double2 *>(rec + 6 * (long long)i);
+    r2[0] = make_double2(wi, gx);
+    r2[1] = make_double2(gy, gz);
+    r2[2] = make_double2(ps, 0.);
+    return;
+  }
+  if (DIFF) {
+    const int n = (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x;
+    if (n >= m.nbnodes) return;
+    double acc = 0.;
+    const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
+    for (int k = sb + lane; k < se; k += 32) acc += ld(m.n2c_sell_alpha + k) * ld(w + ld(m.n2c_sell_idx + k));
+    const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
+    for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
+    wn[n] = acc;
+  }
+}
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, 2) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+                                                         const double *__restrict__ w, double *__restrict__ w_out,
+                                                         const double *__restrict__ sign,
+                                                         const double *__restrict__ src,
+                                                         const double *__restrict__ dt_dev,
+                                                         const double *__restrict__ rec,
+                                                         const double *__restrict__ wn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRule ghost = make_rule(m, bc, w);
+  const int4 vt = ld4(m.cell_vtx + 4 * i);
+  const int4 nb = ld4(m.cell_nbr + 4 * i);
+  const uint32_t fl = ld(m.cell_flags + i);
+  const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
+                   ld3(m.node_coord + 4 * vt.w)};
+  const D3 ci = ld3(m.cell_xy + 4 * i);
+  const double2 sa = ldd2(sign + 4 * i), sb = ldd2(sign + 4 * i + 2);
+  double wi, gxi = 0., gyi = 0., gzi = 0., psii = 0.;
+  if (ORDER2) {
+    const double2 *r = reinterpret_cast<const double2 *>(rec + 6 * (long long)i);
+    const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
+    wi = a.x; gxi = a.y; gyi = b.x; gzi = b.y; psii = c.x;
+  } else {
+    wi = ld(w + i);
+  }
+  double cv[4], q[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int o = comp(nb, j);
+    const bool b = o < 0;
+    const int f = -1 - o;
+    const bool own = (fl >> (6 * j)) & 1u;
+    int d0, d1, d2;
+    face_desc(fl, j, d0, d1, d2);
+    const D3 V0 = pick4(P, d0), V1 = pick4(P, d1), V2 = pick4(P, d2);
+    const D3 fc = (1. / 3) * ((V0 + V1) + V2);
+    double vo, gxo = 0., gyo = 0., gzo = 0., pso = 0.;
+    D3 co;
+    if (b) {
+      vo = ghost(f);
+      co = d3(ld(m.face_ghostcenter + 3 * f), ld(m.face_ghostcenter + 3 * f + 1), ld(m.face_ghostcenter + 3 * f + 2));
+    } else {
+      if (ORDER2) {
+        const double2 *r = reinterpret_cast<const double2 *>(rec + 6 * (long long)o);
+        const double2 a = __ldg(r), bb = __ldg(r + 1), c = __ldg(r + 2);
+        vo = a.x; gxo = a.y; gyo = bb.x; gzo = bb.y; pso = c.x;
+      } else {
+        vo = ld(w + o);
+      }
+      co = ld3(m.cell_xy + 4 * o);
+    }
+    const double s = pick4v(sa.x, sa.y, sb.x, sb.y, j);
+    const bool take_me = (s >= 0) == own;
+    double sol;
+    if (take_me) {
+      sol = ORDER2 ? wi + psii * (gxi * (fc.x - ci.x) + gyi * (fc.y - ci.y) + gzi * (fc.z - ci.z)) : wi;
+    } else if (b) {
+      sol = vo;
+    } else {
+      sol = ORDER2 ? vo + pso * (gxo * (fc.x - co.x) + gyo * (fc.y - co.y) + gzo * (fc.z - co.z)) : vo;
+    }
+    const double F = s * sol;
+    cv[j] = own ? -F : F;
+    if (DIFF) {
+      double v = 0.;
+      if (!b || ld(bc.face_grad_on + f)) {
+        const D3 Nd = 0.5 * cross(V1 - V0, V2 - V0);
+        const D3 N = ((fl >> (6 * j + 5)) & 1u) ? (-1.0) * Nd : Nd;
+        const bool swp = (fl >> (6 * j + 4)) & 1u;
+        const int i1 = d0, i2 = swp ? d2 : d1, i3 = swp ? d1 : d2;   // faces.nodeid order
+        const D3 Q2 = pick4(P, i2), Q3 = pick4(P, i3), Q1 = pick4(P, i1);
+        const D3 v1 = own ? ci : co, v2 = own ? co : ci;
+        const D3 s1 = v2 - Q2, s2 = Q3 - Q2, s3 = v1 - Q2;
+        const D3 f1 = 0.5 * cross(s1, s2) + 0.5 * cross(s2, s3);
+        const D3 s4 = v2 - Q3, s5 = Q1 - Q3, s6 = v1 - Q3;
+        const D3 f2 = 0.5 * cross(s4, s5) + 0.5 * cross(s5, s6);
+        const double air = dot(N, v2 - v1);
+        const int gi1 = comp(vt, i1), gi2 = comp(vt, i2), gi3 = comp(vt, i3);
+        const double VA = ld(wn + gi1), VB = ld(wn + gi2), VC = ld(wn + gi3), VD = VC;
+        const double VL = own ? wi : vo, VR = own ? vo : wi;
+        const double dAC = VA - VC, dBD = VB - VD, dRL = VR - VL;
+        const double fgx = (f1.x * dAC + f2.x * dBD + N.x * dRL) / air;
+        const double fgy = (f1.y * dAC + f2.y * dBD + N.y * dRL) / air;
+        const double fgz = (f1.z * dAC + f2.z * dBD + N.z * dRL) / air;
+        v = p.Dxx * fgx * N.x + p.Dyy * fgy * N.y + p.Dzz * fgz * N.z;
+      }
+      q[j] = own ? v : -v;
+    }
+  }
+  const uint8_t code = ld(m.cell_order + i);
+  double rez = 0.;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick4v(nb.x, nb.y, nb.z, nb.w, sl) >= 0) rez += pick4v(cv[0], cv[1], cv[2], cv[3], sl);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick4v(nb.x, nb.y, nb.z, nb.w, sl) < 0) rez += pick4v(cv[0], cv[1], cv[2], cv[3], sl);
+  }
+  double dis = 0.;
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dis += pick4v(q[0], q[1], q[2], q[3], order_slot(code, k));
+  }
+  const double dt = *dt_dev;
+  const double sc = src ? ld(src + i) : 0.0;
+  w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
+}
+
 // ---------------------------------------------------------------- shallow-water order-2 pre-pass
 
 // Neumann ghost: the interior cell's value (the default boundary of a manapy Variable).
@@ -774,8 +1015,8 @@ inline int grid_for(long long n) {
 
 inline int check_launch() { return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA; }
 
-inline bool compact_2d(const mb_mesh &m) {
-  return m.dim == 2 && m.cell_vtx && m.cell_nbr && m.cell_flags && m.node_coord && m.cell_xy && m.lsq_sell_ptr &&
+inline bool compact_tables(const mb_mesh &m) {
+  return m.cell_vtx && m.cell_nbr && m.cell_flags && m.node_coord && m.cell_xy && m.lsq_sell_ptr &&
          m.lsq_sell_idx && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
 }
 
@@ -787,10 +1028,16 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
                 double *wn, cudaStream_t st) {
   const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
-  if (DIM == 2 && compact_2d(m)) {
-    if (ncb + nnb > 0) k_f2_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
-    k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs,
-                                                                        wn);
+  if (compact_tables(m)) {
+    if (DIM == 2) {
+      if (ncb + nnb > 0) k_f2_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+      k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt,
+                                                                          cs, wn);
+    } else {
+      if (ncb + nnb > 0) k_f3_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+      k_f3_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt,
+                                                                          cs, wn);
+    }
     return check_launch();
   }
   const long long n = m.nbcells;
@@ -983,7 +1230,8 @@ extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const 
                                        const double *w_in, double *w_out, const double *sign_cf,
                                        const double *src, const double *dt_dev, void *stream) {
   if (!mesh_ok(m) || !bc || !p) return MB_EINVAL;
-  const long long need = 4LL * m->nbcells + m->nbnodes;
+  const long long per_cell = m->dim == 2 ? 4 : 6;
+  const long long need = per_cell * m->nbcells + m->nbnodes;
   if (need > (long long)MB_NOALLOC_SCRATCH_DOUBLES) return MB_ETOOBIG;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return MB_ECUDA;
@@ -1002,5 +1250,5 @@ extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const 
   }
   // Every slice is written by the first launch of the step before the second
   // launch reads it, so nothing has to be cleared between calls.
-  return mb_advdiff_step(m, bc, p, w_in, w_out, sign_cf, src, dt_dev, base, base + 4LL * m->nbcells, stream);
+  return mb_advdiff_step(m, bc, p, w_in, w_out, sign_cf, src, dt_dev, base, base + per_cell * m->nbcells, stream);
 }

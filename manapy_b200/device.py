@@ -173,6 +173,8 @@ class DeviceMesh:
             T["cell_vertex1"] = _t(A["nodes_vertex"][A["cells_nodeid"][cp, 1], :2], f64, dev)
         if dim == 2:
             self._compact_2d(A, T, dev)
+        else:
+            self._compact_3d(A, T, dev)
         self.t = T
         s = _lib.MbMesh()
         s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = dim, nc, nf, nn, nlf, 0
@@ -232,6 +234,67 @@ class DeviceMesh:
         T["cell_flags"] = _t(flags.view(np.int32), np.int32, dev)
         T["node_coord"] = _t(X[np_, :2], np.float64, dev)
         T["cell_xy"] = _t(A["cells_center"][cp, :2], np.float64, dev)
+
+    # local faces of a tetrahedron (manapy/ddm/ddm_utils3d.py:785-791) and the six
+    # permutations of three items, in the order the kernels decode them
+    TET_FACES = np.array([[0, 1, 2], [2, 3, 0], [0, 1, 3], [3, 1, 2]])
+    PERM3 = np.array([[0, 1, 2], [0, 2, 1], [1, 0, 2], [1, 2, 0], [2, 0, 1], [2, 1, 0]])
+
+    def _compact_3d(self, A, T, dev):
+        """Cell-centred tables of the fused 3D step (see ``mb_mesh`` in the C header)."""
+        R = self.R
+        cp, ci, fi, ni, np_ = R.cperm, R.cinv, R.finv, R.ninv, R.nperm
+        nc = self.nbcells
+        nodes = A["cells_nodeid"][cp, :4].astype(np.int64)
+        faces = A["cells_faceid"][cp, :4].astype(np.int64)
+        fcid = A["faces_cellid"]
+        c0 = fcid[faces, 0]
+        c1 = fcid[faces, 1]
+        own = c0 == cp[:, None]
+        other = np.where(own, c1, c0)
+        bnd = c1 < 0
+        nbr = np.where(bnd, -1 - fi[faces], ci[np.maximum(other, 0)])
+        X = A["nodes_vertex"][:, :3]
+        stored = A["faces_normal"][faces]                          # [nc, 4, 3]
+        fnodes = A["faces_nodeid"][faces][..., :3]                 # oriented order
+        flags = np.zeros(nc, dtype=np.uint32)
+        for j in range(4):
+            loc = nodes[:, self.TET_FACES[j]]                       # [nc, 3] original node ids
+            order = np.argsort(-loc, axis=1, kind="stable")         # descending original id
+            code = self._perm_codes(order)
+            desc = np.take_along_axis(loc, order, axis=1)
+            ori = fnodes[:, j]
+            swap = (ori[:, 1] == desc[:, 2]) & (ori[:, 2] == desc[:, 1])
+            assert np.all(ori[:, 0] == desc[:, 0]) and np.all(swap | ((ori[:, 1] == desc[:, 1]) & (ori[:, 2] == desc[:, 2]))), \
+                "face nodes are not the descending order of the cell's local face"
+            V0, V1, V2 = X[desc[:, 0]], X[desc[:, 1]], X[desc[:, 2]]
+            u = V1 - V0
+            v = V2 - V0
+            Nd = 0.5 * np.stack([u[:, 1] * v[:, 2] - u[:, 2] * v[:, 1], u[:, 2] * v[:, 0] - u[:, 0] * v[:, 2],
+                                 u[:, 0] * v[:, 1] - u[:, 1] * v[:, 0]], axis=1)
+            st = stored[:, j]
+            flip = np.any(st != Nd, axis=1)
+            assert np.array_equal(np.where(flip[:, None], -1 * Nd, Nd), st), "normals are not vertex cross products"
+            flags |= (own[:, j].astype(np.uint32) << (6 * j)) | (code << (6 * j + 1)) \
+                | (swap.astype(np.uint32) << (6 * j + 4)) | (flip.astype(np.uint32) << (6 * j + 5))
+        T["cell_vtx"] = _t(ni[nodes], np.int32, dev)
+        T["cell_nbr"] = _t(nbr, np.int32, dev)
+        T["cell_flags"] = _t(flags.view(np.int32), np.int32, dev)
+        nc4 = np.zeros((len(np_), 4))
+        nc4[:, :3] = X[np_]
+        T["node_coord"] = _t(nc4, np.float64, dev)
+        cc4 = np.zeros((nc, 4))
+        cc4[:, :3] = A["cells_center"][cp]
+        T["cell_xy"] = _t(cc4, np.float64, dev)
+
+    @classmethod
+    def _perm_codes(cls, order):
+        """Index in PERM3 of each row of ``order`` (a permutation of 0, 1, 2)."""
+        key = order[:, 0] * 9 + order[:, 1] * 3 + order[:, 2]
+        table = np.zeros(27, dtype=np.uint32)
+        for k, p in enumerate(cls.PERM3):
+            table[p[0] * 9 + p[1] * 3 + p[2]] = k
+        return table[key]
 
     def to_device_order(self, kind, host_t, out):
         """out[k] = host_t[perm[k]] (``host_t`` already on the device, manapy order)."""

@@ -229,7 +229,7 @@ class AdvectionDiffusionSolver:
     def _scratch(self):
         dm = self._dm
         if getattr(self, "_cs", None) is None:
-            self._cs = torch.empty(4 * dm.nbcells, dtype=torch.float64, device=dm.device)
+            self._cs = torch.empty((4 if dm.dim == 2 else 6) * dm.nbcells, dtype=torch.float64, device=dm.device)
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
 

@@ -44,7 +44,7 @@ def _setup(wl):
 def _regular(U, A, dm, db, prm, sign, dt, w_in, st):
     nc, nn = A["nbcells"], A["nbnodes"]
     out = U.Z(nc)
-    cell_scratch, node_scratch = U.Z(4 * nc), U.Z(nn)
+    cell_scratch, node_scratch = U.Z((4 if A["dim"] == 2 else 6) * nc), U.Z(nn)
     U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w_in), U.P(out), U.P(sign), None, U.P(dt),
            U.P(cell_scratch), U.P(node_scratch), st)
     return out
