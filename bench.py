@@ -48,6 +48,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-steps", type=int, default=5, help="oracle steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32c", action="store_true", help="skip the FP32-compensated measurement")
+    ap.add_argument("--serve", action="store_true", help="continuous-batching serving run instead of one workload")
+    ap.add_argument("--requests", type=int, default=300, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (requests/s)")
+    ap.add_argument("--serial-sample", type=int, default=60, help="serving: requests timed serially in FP64")
+    ap.add_argument("--workers", type=int, default=None, help="serving: mesh-preparation processes")
     ap.add_argument("--n", type=int, default=None, help="mesh resolution override (small profiling cases)")
     return ap.parse_args()
 
@@ -199,6 +205,70 @@ def cpu_baseline(dom, wl, steps):
                       % (steps, wl.cells)}
 
 
+def run_fp32c(wl, dom, w64, vel, K, Wm, world):
+    """The FP32-compensated step on the same mesh and initial state: device-timed
+    throughput, and its L2 / Linf error against the FP64 state after the same steps."""
+    import torch
+    import manapy_b200 as M
+    ref = w64.cell.copy()          # FP64 state after Wm + K steps
+    w = M.Variable(domain=dom, BC=wl.bc, values=wl.bc_values)
+    w.cell = wl.init(dom.cells.center)
+    S = M.AdvectionDiffusionSolver(w, vel=vel, conf=M.Struct(
+        Dxx=wl.diffusion[0], Dyy=wl.diffusion[1], Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl,
+        precision="fp32c"))
+    S.advance(Wm, graph=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    S.advance(K, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    got = w.cell
+    l2 = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    linf = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+    S.release_graphs()
+    return {"value": world * wl.cells * K / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / K,
+            "dtype": "f32 state + compensated sums, f64 geometry and dt",
+            "l2_rel_err_vs_fp64": l2, "linf_rel_err_vs_fp64": linf, "steps_compared": Wm + K}
+
+
+def run_fp32c_sw(wl, dom, vs64, S64, K, Wm, world):
+    """FP32-compensated shallow water on the same mesh and initial state: throughput, L2 /
+    Linf error of h, hu, hv against the FP64 state after the same steps, FP64 mass drift."""
+    import torch
+    import manapy_b200 as M
+    ref = [v.cell.copy() for v in vs64[:3]]
+    m64 = S64.mass()
+    vs = [M.Variable(domain=dom) for _ in range(5)]
+    for var, a in zip(vs, wl.init_sw(dom.cells.center)):
+        var.cell = a
+    S = M.ShallowWaterSolver(vs[0], hvel=(vs[1], vs[2]), hc=vs[3], Z=vs[4],
+                             conf=M.Struct(order=wl.order, cfl=wl.cfl, grav=wl.grav, precision="fp32c"))
+    m0 = S.mass()
+    S.advance(Wm)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    S.advance(K)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    out = {"value": world * wl.cells * K / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / K,
+           "dtype": "f32 state and fluxes + compensated sums, f64 geometry, source and dt",
+           "steps_compared": Wm + K}
+    for name, r, v in zip(("h", "hu", "hv"), ref, vs[:3]):
+        got = v.cell
+        out["l2_rel_err_vs_fp64_" + name] = float(np.linalg.norm(got - r) / np.linalg.norm(r))
+        out["linf_rel_err_vs_fp64_" + name] = float(np.max(np.abs(got - r)) / np.max(np.abs(r)))
+    out["mass_fp64_sum"] = {"start": m0, "fp32c_end": S.mass(), "fp64_end": m64}
+    return out
+
+
 def run_ours(args):
     import torch
     from manapy_b200 import workloads as W
@@ -237,6 +307,12 @@ def run_ours(args):
     value = world * wl.cells * K / (ms_max / 1e3)
     ms_step = ms_max / K
     launches_per_step = S.launches_per_step()
+    fp32c = None
+    if not args.no_fp32c:
+        if wl.kind == "advdiff":
+            fp32c = run_fp32c(wl, dom, w, vel, K, Wm, world)
+        elif wl.order == 1:
+            fp32c = run_fp32c_sw(wl, dom, vs, S, K, Wm, world)
 
     # end to end through the public API, manapy's driver loop
     E = max(args.e2e_steps, 1)
@@ -296,6 +372,9 @@ def run_ours(args):
         "clocks": ck,
         "gpu_launches": launches_per_step * K,
     }
+    if fp32c is not None:
+        fp32c["vs_fp64"] = fp32c["value"] / value
+        line["fp32c"] = fp32c
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(dom, wl, args.cpu_steps)
     if rank == 0:
@@ -306,7 +385,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def _ref_worker(wk, steps, warmup, q):
+def _ref_worker(wk, steps, warmup, start, out):
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -326,12 +405,11 @@ def _ref_worker(wk, steps, warmup, q):
             o.state()[k][:] = a
     for _ in range(warmup):
         o.step()
-    q.put(("ready", 0.0))
-    go = q.get()  # noqa: F841
+    start.wait()  # every process starts its timed steps together
     t0 = time.perf_counter()
     for _ in range(steps):
         o.step()
-    q.put(("done", time.perf_counter() - t0))
+    out.put(time.perf_counter() - t0)
 
 
 def run_reference(args):
@@ -350,22 +428,19 @@ def run_reference(args):
         mem_gb = 32
     per = max(wl.cells / 2e6 * 4.0, 0.05)
     procs_n = max(1, min(cores, int(mem_gb * 0.5 / per), 32))
-    # each timed step of every process is one full oracle step; bound the sample
-    steps = max(1, min(args.steps, 3))
+    # each timed step of every process is one full oracle step; bound the sample to about
+    # 2e7 cell-updates per process (10-20 s of serial work)
+    steps = max(2, min(args.steps, int(2e7 // wl.cells)))
     warm = 1
-    qs, ps = [], []
-    for _ in range(procs_n):
-        q = ctx.Queue()
-        p = ctx.Process(target=_ref_worker, args=(args.workload, steps, warm, q))
+    start = ctx.Barrier(procs_n + 1)
+    out = ctx.Queue()
+    ps = [ctx.Process(target=_ref_worker, args=(args.workload, steps, warm, start, out), daemon=True)
+          for _ in range(procs_n)]
+    for p in ps:
         p.start()
-        qs.append(q)
-        ps.append(p)
-    for q in qs:
-        assert q.get()[0] == "ready"
+    start.wait()
     t0 = time.perf_counter()
-    for q in qs:
-        q.put("go")
-    times = [q.get()[1] for q in qs]
+    times = [out.get() for _ in ps]
     wall = time.perf_counter() - t0
     for p in ps:
         p.join()
@@ -373,7 +448,8 @@ def run_reference(args):
     line = {
         "metric": "cell-updates/s (FP64 explicit FV step, %s)" % wl.name, "impl": "reference",
         "value": value, "unit": "cell-updates/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * max(times) / steps,
+        "steps": steps, "steps_requested": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * max(times) / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded jittered mesh of the workload, manapy's initial state",
         "config": {"workload": wl.name, "cells": wl.cells, "order": wl.order, "kind": wl.kind},
@@ -386,8 +462,87 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """Seeded request stream through the continuous-batching server (FP32-compensated,
+    batched kernels, graph-replayed steps); beside it, serial plain-FP64 solves of a sample
+    of the same requests through the public API, one after another."""
+    import torch
+    import manapy_b200 as M
+    from manapy_b200 import serving as SV
+    torch.cuda.set_device(0)
+    reqs = SV.make_requests(args.requests, args.rate, seed=2024)
+    total_cu = sum(r.cells * r.steps for r in reqs)
+    srv = SV.BatchServer(workers=args.workers)
+    # warm-up: compile paths, worker start-up
+    SV.BatchServer(workers=0).serve(SV.make_requests(4, 0.0, seed=1, cells=(2e3, 2e4), steps=(20, 40)))
+    t0 = time.perf_counter()
+    recs = srv.serve(reqs)
+    wall = time.perf_counter() - t0
+    lat = np.array([r["latency"] for r in recs])
+    # serial plain FP64: host preparation excluded (done beforehand), device solve timed per request
+    sample = reqs[:max(1, min(args.serial_sample, len(reqs)))]
+    service = []
+    from manapy_b200 import meshgen
+    for r in sample:
+        el, vx = meshgen.square_triangles(r.n, seed=r.seed)
+        dom = M.Domain(dim=2, mesh=(el, vx))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        if r.kind == "advdiff":
+            w = M.Variable(domain=dom, BC={k: "dirichlet" for k in SV.SIDES}, values={k: 0.0 for k in SV.SIDES})
+            u, v = M.Variable(domain=dom), M.Variable(domain=dom)
+            u.face = np.full(dom.nbfaces, r.ux)
+            v.face = np.full(dom.nbfaces, r.uy)
+            u.cell = np.full(dom.nbcells, r.ux)
+            v.cell = np.full(dom.nbcells, r.uy)
+            w.cell = SV.initial_state(r, dom.cells.center)[0]
+            S = M.AdvectionDiffusionSolver(w, vel=(u, v), conf=M.Struct(Dxx=r.D, Dyy=r.D, order=2, cfl=0.8))
+            S.advance(r.steps, graph=True)
+            _ = w.cell
+        else:
+            vs = [M.Variable(domain=dom) for _ in range(5)]
+            for var, a in zip(vs, SV.initial_state(r, dom.cells.center)):
+                var.cell = a
+            S = M.ShallowWaterSolver(vs[0], hvel=(vs[1], vs[2]), hc=vs[3], Z=vs[4],
+                                     conf=M.Struct(order=1, cfl=0.5, grav=9.81))
+            S.advance(r.steps)
+            _ = vs[0].cell
+        torch.cuda.synchronize()
+        service.append(time.perf_counter() - t1)
+    service = np.array(service)
+    cu_sample = sum(r.cells * r.steps for r in sample)
+    serial_rate = cu_sample / service.sum()
+    # FIFO single-server queue over the same arrivals with the measured service times
+    # (the sample's times, cycled over the stream in order)
+    tq, slat = 0.0, []
+    for k, r in enumerate(reqs):
+        svc = service[k] if k < len(service) else service[k % len(service)] * (
+            (r.cells * r.steps) / max(sample[k % len(service)].cells * sample[k % len(service)].steps, 1))
+        tq = max(tq, r.arrival) + svc
+        slat.append(tq - r.arrival)
+    slat = np.array(slat)
+    line = {
+        "metric": "served p50/p99 latency at sustained throughput (continuous batching, FP32-compensated)",
+        "value": total_cu / wall, "unit": "cell-updates/s", "n_gpus": 1, "higher_is_better": True,
+        "dtype": "f32 state + compensated sums, f64 geometry and dt", "data": "synthetic seeded request stream",
+        "config": {"workload": "C5-serving", "requests": len(reqs), "rate_per_s": args.rate,
+                   "cells": "log-uniform 2e3-5e5", "steps": "uniform 100-2000", "mix": "70% adv-diff o2, 30% SW o1"},
+        "serving": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                    "mean_s": float(lat.mean()), "makespan_s": wall, "requests_per_s": len(reqs) / wall,
+                    "cell_updates": total_cu},
+        "serial_fp64": {"value": serial_rate, "unit": "cell-updates/s", "sample": len(sample),
+                        "p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
+                        "note": "device solves through the public API, one request at a time; host mesh "
+                                "preparation excluded; FIFO latencies over the same arrivals"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.serve:
+        run_serving(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

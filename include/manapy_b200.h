@@ -109,6 +109,10 @@ typedef struct mb_mesh {
   const int32_t *n2c_sell_ptr;
   const int32_t *n2c_sell_idx;
   const double *n2c_sell_alpha;
+  /* n2c_sell_alpha rounded to FP32 (read by the FP32-compensated step only) */
+  const float *n2c_sell_alpha_f32;
+  /* [nbfaces][4] = {n_x, n_y, 1/mesure, 0} rounded to FP32 (FP32-compensated shallow water, 2D) */
+  const float *face_nm_f32;
 } mb_mesh;
 
 typedef struct mb_bc {
@@ -214,6 +218,18 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
                     const double *dt_dev, double *cell_scratch, double *node_scratch, void *stream);
 
+/* FP32-compensated twin of mb_advdiff_step (no counterpart in manapy, whose single
+ * precision mode is FP32 throughout, manapy/backends/cpu/backend.py:46-49): the same
+ * two launches with FP32 state (w_in, w_out), FP32 u.n (sign_cf, [4*nbcells]), FP32
+ * source (src, may be NULL), FP32 phase-1 records and node values, FP32 fluxes summed
+ * per cell with compensated (Neumaier) summation; coordinates, every geometric
+ * coefficient and dt stay FP64.  Scratch: cell_scratch [4*nbcells] floats in 2D,
+ * [5*nbcells] in 3D (order 2), node_scratch [nbnodes] floats (diffusion).  Needs the
+ * compact tables of mb_mesh, n2c_sell_alpha_f32 included. */
+int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
+                         const float *w_in, float *w_out, const float *sign_cf, const float *src,
+                         const double *dt_dev, float *cell_scratch, float *node_scratch, void *stream);
+
 /* sign_cf[4*i+j] = u_face[f] n_x + v_face[f] n_y + w_face[f] n_z for the j-th local face f
  * of cell i (zero for unused slots): the upwind selector of
  * manapy/solvers/advecdiff/fvm_utils.py:53-64 laid out per cell for mb_advdiff_step */
@@ -238,6 +254,70 @@ int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face,
 int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5],
                double cfl, double grav, int32_t order, double *scratch, double *face_flux,
                const double *dt_cur, double *dt_next, void *stream);
+
+/* FP32-compensated twin of mb_sw_step (no counterpart in manapy), first order, Neumann
+ * ghosts: FP32 state (q_in, q_out: h, hu, hv, hc, Z), FP32 SRNH flux arithmetic and face
+ * fluxes (face_flux [nbfaces][4] floats), residuals summed per cell with compensated
+ * (Neumaier) summation; normals come from face_nm_f32; the bathymetry source, dt_cur and
+ * dt_next (time_step_SW of the updated state) are FP64. */
+int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5], double cfl,
+                    double grav, int32_t order, float *face_flux, const double *dt_cur, double *dt_next,
+                    void *stream);
+
+/* ---- batches of independent triangle meshes (serving) ----------------------------------
+ *
+ * No counterpart in manapy (one mesh per process).  Many meshes advance in the same
+ * launches: the caller lays out one item per mesh in device memory and, per launch, a
+ * map from block to item (each item owns a contiguous block range, so no block spans two
+ * meshes).  A device step counter (*clock, incremented by the last launch of every step)
+ * selects each item's ping-pong buffer -- the input of global step t is w[(t - start_step)
+ * & 1] -- and items outside [start_step, end_step) do nothing, so one captured CUDA graph
+ * of a step serves while items are admitted and retired between replays (the caller
+ * rewrites items and maps only between steps). */
+typedef struct mb_advdiff_item {
+  mb_mesh m;                /* the mesh's tables (compact 2D tables required) */
+  mb_bc bc;
+  mb_advdiff_params p;
+  float *w[2];              /* ping-pong FP32 state */
+  const float *sign_cf;     /* [4*nbcells] FP32 u.n per cell face */
+  const float *src;         /* NULL: no source */
+  const double *dt_dev;     /* the item's dt */
+  float *cell_scratch;      /* [4*nbcells] (order 2) */
+  float *node_scratch;      /* [nbnodes] (diffusion) */
+  int32_t start_step;       /* first global step the item runs */
+  int32_t end_step;         /* first global step it does not run */
+  int32_t p1_begin;         /* first block of the item in the phase-1 launch */
+  int32_t p1_cell_blocks;   /* its phase-1 blocks [p1_begin, p1_begin + this) do cells, the rest nodes */
+  int32_t p2_begin;         /* first block of the item in the phase-2 launch */
+  int32_t pad_;
+} mb_advdiff_item;
+
+/* One FP32-compensated advection-diffusion step of every active item (the step of
+ * mb_advdiff_step_f32c per mesh), order and diffusion common to the batch; then *clock += 1.
+ * p1_map [p1_blocks], p2_map [p2_blocks]: item of each block (p1 unused when order 1 without
+ * diffusion). */
+int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const int32_t *p1_map, int32_t p1_blocks,
+                               const int32_t *p2_map, int32_t p2_blocks, int32_t order, int32_t diffusion,
+                               int32_t *clock, void *stream);
+
+/* A shallow-water mesh of a batch (first order, Neumann ghosts, FP32-compensated). */
+typedef struct mb_sw_item {
+  mb_mesh m;                /* compact 2D tables and face_nm_f32 required */
+  float *q[2][4];           /* ping-pong FP32 h, hu, hv, hc; step t reads q[(t - start_step) & 1] */
+  const float *Z;           /* bed, FP32 */
+  float *face_flux;         /* [nbfaces][4] scratch */
+  double *dt;               /* [2]: step t uses dt[(t - start_step) & 1] and writes the next step's dt
+                               into the other slot; dt[0] must hold the first step's dt */
+  double cfl, grav;
+  int32_t start_step, end_step;
+  int32_t f_begin;          /* first block of the item in the face launch */
+  int32_t c_begin;          /* first block of the item in the cell launch */
+} mb_sw_item;
+
+/* One FP32-compensated shallow-water step (mb_sw_step_f32c per mesh) of every active item;
+ * then *clock += 1.  face_map [face_blocks], cell_map [cell_blocks]: item of each block. */
+int mb_sw_batch_step_f32c(const mb_sw_item *items, const int32_t *face_map, int32_t face_blocks,
+                          const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream);
 
 /* Same step as mb_advdiff_step, for callers that cannot allocate device memory.
  *

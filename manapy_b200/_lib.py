@@ -36,7 +36,7 @@ class MbMesh(ctypes.Structure):
                 ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp),
                 ("cell_vtx", _vp), ("cell_nbr", _vp), ("cell_flags", _vp), ("node_coord", _vp), ("cell_xy", _vp),
                 ("lsq_sell_ptr", _vp), ("lsq_sell_idx", _vp), ("n2c_sell_ptr", _vp), ("n2c_sell_idx", _vp),
-                ("n2c_sell_alpha", _vp)]
+                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp)]
 
 
 class MbBC(ctypes.Structure):
@@ -45,6 +45,19 @@ class MbBC(ctypes.Structure):
 
 class MbAdvDiffParams(ctypes.Structure):
     _fields_ = [("order", _i32), ("diffusion", _i32), ("Dxx", _d), ("Dyy", _d), ("Dzz", _d)]
+
+
+class MbAdvDiffItem(ctypes.Structure):
+    _fields_ = [("m", MbMesh), ("bc", MbBC), ("p", MbAdvDiffParams), ("w", _vp * 2), ("sign_cf", _vp),
+                ("src", _vp), ("dt_dev", _vp), ("cell_scratch", _vp), ("node_scratch", _vp),
+                ("start_step", _i32), ("end_step", _i32), ("p1_begin", _i32), ("p1_cell_blocks", _i32),
+                ("p2_begin", _i32), ("pad_", _i32)]
+
+
+class MbSwItem(ctypes.Structure):
+    _fields_ = [("m", MbMesh), ("q", (_vp * 4) * 2), ("Z", _vp), ("face_flux", _vp), ("dt", _vp),
+                ("cfl", _d), ("grav", _d), ("start_step", _i32), ("end_step", _i32), ("f_begin", _i32),
+                ("c_begin", _i32)]
 
 
 _M = ctypes.POINTER(MbMesh)
@@ -73,6 +86,10 @@ _SIGS = {
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_advdiff_step_noalloc": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_advdiff_step_f32c": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_sw_step_f32c": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
+    "mb_advdiff_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
+    "mb_sw_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],
     "mb_build_info": [],
 }

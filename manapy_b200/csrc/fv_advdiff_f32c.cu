@@ -1,0 +1,619 @@
+// FP32-compensated advection-diffusion step on the compact cell-centred tables.
+//
+// Same scheme and the same per-cell gathers as the FP64 fused step
+// (manapy/solvers/advecdiff/system.py:156-172: ghost values, LSQ gradient +
+// Barth limiter, centre->vertex values, upwind and diamond fluxes, forward
+// Euler), with the precision split:
+//   FP32  cell state, phase-1 records {w, grad, psi}, node values, u.n,
+//         centre->vertex weights, every flux and the per-cell residual, whose
+//         face terms are summed with Neumaier's compensated summation;
+//   FP64  vertex and centre coordinates, every geometric quantity derived from
+//         them (face centres, normals, diamond vectors and areas, LSQ moment
+//         matrices, 1/volume) until it is multiplied by a state value, and dt.
+// Geometric coefficients are formed in FP64 and rounded once to FP32, so the
+// FP32 arithmetic only ever sees state x coefficient products.
+#include "fv_compact.cuh"
+
+namespace mb {
+
+// Ghost value of boundary face f for an FP32 state (the rules of GhostRule).
+struct GhostRuleF {
+  const int8_t *kind;
+  const double *value;
+  const double *dist;
+  const int32_t *face_cellid;
+  const float *w;
+  __device__ __forceinline__ float operator()(int f) const {
+    const int k = kind[f];
+    if (k == MB_G_DIRICHLET) return (float)ld(value + f);
+    const float wc = ld(w + ld(face_cellid + 2 * f));
+    if (k == MB_G_NEUMANN) return wc;
+    if (k == MB_G_NONSLIP) return -1.f * wc;
+    if (k == MB_G_NEUMANN_NH) return (float)((double)wc + ld(value + f) * ld(dist + f));
+    if (k == MB_G_CELL_AT_FACE) return ld(w + (long long)ld(value + f));
+    return 0.f;
+  }
+};
+
+__device__ __forceinline__ GhostRuleF make_rule_f(const mb_mesh &m, const mb_bc &bc, const float *w) {
+  return GhostRuleF{bc.kind, bc.value, m.face_dist, m.face_cellid, w};
+}
+
+__device__ __forceinline__ float fminp(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float fmaxp(float a, float b) { return b > a ? b : a; }
+
+// Neumaier's compensated sum (the error of every addition is carried in c).
+struct CompSum {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    const float t = s + x;
+    c += fabsf(s) >= fabsf(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ float value() const { return s + c; }
+};
+
+__device__ __forceinline__ float4 ldf4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void st4_keep(float *a, float4 v, uint64_t pol) {
+#if MB_L2_HINTS
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w), "l"(pol)
+               : "memory");
+#else
+  *reinterpret_cast<float4 *>(a) = v;
+#endif
+}
+__device__ __forceinline__ void st1f_keep(float *a, float x, uint64_t pol) {
+#if MB_L2_HINTS
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(x), "l"(pol) : "memory");
+#else
+  *a = x;
+#endif
+}
+__device__ __forceinline__ float ldf_stream(const float *a, uint64_t pol) {
+#if MB_L2_HINTS
+  float v;
+  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+#else
+  return __ldg(a);
+#endif
+}
+
+// centre->vertex value of node n (phase 1, node blocks): FP32 weights, FP32 sum
+__device__ __forceinline__ void node_value_f32(const mb_mesh &m, const GhostRuleF &ghost, const float *__restrict__ w,
+                                               float *__restrict__ wn, int n, int lane) {
+  if (n >= m.nbnodes) return;
+  float acc = 0.f;
+  const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
+  const uint64_t pst = l2_stream();
+#pragma unroll 4
+  for (int k = sb + lane; k < se; k += 32) {
+    const int cc = ld1_stream(m.n2c_sell_idx + k, pst);
+    acc = fmaf(ldf_stream(m.n2c_sell_alpha_f32 + k, pst), ld(w + cc), acc);
+  }
+  const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
+  for (int k = gb; k < ge; ++k) acc = fmaf((float)ld(m.n2g_alpha + k), ghost(ld(m.n2g_idx + k)), acc);
+  st1f_keep(wn + n, acc, l2_keep());
+}
+
+// ---------------------------------------------------------------- triangles
+
+#ifndef MB_P1C_MIN_BLOCKS
+#define MB_P1C_MIN_BLOCKS 6
+#endif
+#ifndef MB_P2C_MIN_BLOCKS
+#define MB_P2C_MIN_BLOCKS 3
+#endif
+
+// phase 1 of block `bid` of one mesh: blocks [0, ncb) gradient + limiter records,
+// the rest centre->vertex node values
+template <bool ORDER2, bool DIFF>
+__device__ __forceinline__ void f2c_phase1(const mb_mesh &m, const mb_bc &bc, const float *__restrict__ w,
+                                           float *__restrict__ rec, float *__restrict__ wn, int ncb, int bid) {
+  const GhostRuleF ghost = make_rule_f(m, bc, w);
+  const int lane = threadIdx.x & 31;
+  if (ORDER2 && bid < ncb) {
+    const int i = bid * blockDim.x + threadIdx.x;
+    if (i >= m.nbcells) return;
+    const double2 c = ldd2(m.cell_xy + 2 * i);
+    const float wi = ld(w + i);
+    // LSQ: moment matrix in FP64 (geometry), right-hand side in FP32
+    double ixx = 0., iyy = 0., ixy = 0.;
+    float jx = 0.f, jy = 0.f;
+    const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
+    const int L = (se - sb) >> 5;
+    const int32_t *ix = m.lsq_sell_idx + sb + lane;
+    const uint64_t pst = l2_stream();
+    int k = 0;
+    for (; k + 4 <= L; k += 4) {
+      int cc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { cc[u] = ld1_stream(ix + 32 * (k + u), pst); cc[u] = cc[u] < 0 ? i : cc[u]; }
+      double2 pc[4];
+      float wc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { pc[u] = ldd2(m.cell_xy + 2 * cc[u]); wc[u] = ld(w + cc[u]); }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double dx = pc[u].x - c.x, dy = pc[u].y - c.y;
+        const float dw = wc[u] - wi;
+        ixx += dx * dx; iyy += dy * dy; ixy += dx * dy;
+        jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy);
+      }
+    }
+    for (; k < L; ++k) {
+      int cc = ld1_stream(ix + 32 * k, pst);
+      cc = cc < 0 ? i : cc;
+      const double2 pc = ldd2(m.cell_xy + 2 * cc);
+      const double dx = pc.x - c.x, dy = pc.y - c.y;
+      const float dw = ld(w + cc) - wi;
+      ixx += dx * dx; iyy += dy * dy; ixy += dx * dy;
+      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy);
+    }
+    const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+    for (int k = gb; k < ge; ++k) {
+      const int f = ld(m.ghostnid_idx + k);
+      const double dx = ld(m.face_ghostcenter + 3 * f) - c.x, dy = ld(m.face_ghostcenter + 3 * f + 1) - c.y;
+      const float dw = ghost(f) - wi;
+      ixx += dx * dx; iyy += dy * dy; ixy += dx * dy;
+      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy);
+    }
+    const double rdia = 1. / (ixx * iyy - ixy * ixy);
+    const float a = (float)(iyy * rdia), b = (float)(ixy * rdia), e = (float)(ixx * rdia);
+    const float x = a * jx - b * jy;
+    const float y = e * jy - b * jx;
+    // Barth limiter over the three faces
+    const int4 vt = ld4(m.cell_vtx + 4 * i);
+    const int4 nb = ld4(m.cell_nbr + 4 * i);
+    const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
+                  P2 = ldd2(m.node_coord + 2 * vt.z);
+    float wmax = wi, wmin = wi;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int o = comp(nb, j);
+      const float bv = o < 0 ? ghost(-1 - o) : ld(w + o);
+      wmax = fmaxp(wmax, bv);
+      wmin = fminp(wmin, bv);
+    }
+    float ps = 1.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double2 pa = j == 0 ? P0 : (j == 1 ? P1 : P2), pb = j == 0 ? P1 : (j == 1 ? P2 : P0);
+      const float r1 = (float)(0.5 * (pa.x + pb.x) - c.x), r2 = (float)(0.5 * (pa.y + pb.y) - c.y);
+      const float delta = x * r1 + y * r2;
+      float psi_ij = 1.f;
+      if (!(fabsf(delta) < 1e-8f)) {
+        if (delta > 0.f) psi_ij = fminp(1.f, (wmax - wi) / delta);
+        if (delta < 0.f) psi_ij = fminp(1.f, (wmin - wi) / delta);
+      }
+      ps = fminp(ps, psi_ij);
+    }
+    st4_keep(rec + 4 * (long long)i, make_float4(wi, x, y, ps), l2_keep());
+    return;
+  }
+  if (DIFF) node_value_f32(m, ghost, w, wn, (bid - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x, lane);
+}
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P1C_MIN_BLOCKS)
+    k_f2c_phase1(mb_mesh m, mb_bc bc, const float *__restrict__ w, float *__restrict__ rec, float *__restrict__ wn,
+                 int ncb) {
+  f2c_phase1<ORDER2, DIFF>(m, bc, w, rec, wn, ncb, blockIdx.x);
+}
+
+// phase 2 of block `bid` of one mesh: fluxes and update of its cells
+template <bool ORDER2, bool DIFF>
+__device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p,
+                                           const float *__restrict__ w, float *__restrict__ w_out,
+                                           const float *__restrict__ sign, const float *__restrict__ src,
+                                           const double *__restrict__ dt_dev, const float *__restrict__ rec,
+                                           const float *__restrict__ wn, int bid) {
+  const int i = bid * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRuleF ghost = make_rule_f(m, bc, w);
+  const int4 vt = ld4(m.cell_vtx + 4 * i);
+  const int4 nb = ld4(m.cell_nbr + 4 * i);
+  const uint32_t fl = ld(m.cell_flags + i);
+  const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
+                P2 = ldd2(m.node_coord + 2 * vt.z);
+  const double2 ci = ldd2(m.cell_xy + 2 * i);
+  const float4 s4 = ldf4(sign + 4 * (long long)i);
+  float wi, gxi = 0.f, gyi = 0.f, psii = 0.f;
+  if (ORDER2) {
+    const float4 r = ldf4(rec + 4 * (long long)i);
+    wi = r.x; gxi = r.y; gyi = r.z; psii = r.w;
+  } else {
+    wi = ld(w + i);
+  }
+  float cv[3], q[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int o = comp(nb, j);
+    const bool b = o < 0;
+    const int f = -1 - o;
+    const bool own = f2_own(fl, j);
+    const bool rev = f2_rev(fl, j);
+    const double2 Pj = j == 0 ? P0 : (j == 1 ? P1 : P2), Pk = j == 0 ? P1 : (j == 1 ? P2 : P0);
+    const double2 Xa = rev ? Pk : Pj;
+    const double2 Xb = rev ? Pj : Pk;
+    const double fcx = 0.5 * (Xa.x + Xb.x), fcy = 0.5 * (Xa.y + Xb.y);
+    float vo, gxo = 0.f, gyo = 0.f, pso = 0.f;
+    double2 co;
+    if (b) {
+      vo = ghost(f);
+      co = make_double2(ld(m.face_ghostcenter + 3 * f), ld(m.face_ghostcenter + 3 * f + 1));
+    } else {
+      if (ORDER2) {
+        const float4 r = ldf4(rec + 4 * (long long)o);
+        vo = r.x; gxo = r.y; gyo = r.z; pso = r.w;
+      } else {
+        vo = ld(w + o);
+      }
+      co = ldd2(m.cell_xy + 2 * o);
+    }
+    const float s = j == 0 ? s4.x : (j == 1 ? s4.y : s4.z);
+    const bool take_me = (s >= 0.f) == own;
+    float sol;
+    if (take_me) {
+      sol = ORDER2 ? wi + psii * (gxi * (float)(fcx - ci.x) + gyi * (float)(fcy - ci.y)) : wi;
+    } else if (b) {
+      sol = vo;
+    } else {
+      sol = ORDER2 ? vo + pso * (gxo * (float)(fcx - co.x) + gyo * (float)(fcy - co.y)) : vo;
+    }
+    const float F = s * sol;
+    cv[j] = own ? -F : F;
+    if (DIFF) {
+      float v = 0.f;
+      if (!b || ld(bc.face_grad_on + f)) {
+        const double2 v1 = own ? ci : co, v2 = own ? co : ci;
+        const float vl = own ? wi : vo, vr = own ? vo : wi;
+        const double f1x = v1.x - Xa.x, f1y = v1.y - Xa.y;
+        const double f2x = Xb.x - v1.x, f2y = Xb.y - v1.y;
+        const double f3x = v2.x - Xb.x, f3y = v2.y - Xb.y;
+        const double f4x = Xa.x - v2.x, f4y = Xa.y - v2.y;
+        const double air = 0.5 * ((Xb.x - Xa.x) * (v2.y - v1.y) + (v1.x - v2.x) * (Xb.y - Xa.y));
+        double n0 = Xa.y - Xb.y, n1 = Xb.x - Xa.x;
+        if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
+        // Dxx n0 gx + Dyy n1 gy = sum_k t_k c_k with FP64-formed coefficients c_k
+        const double gxk = p.Dxx * n0 / (2 * air), gyk = p.Dyy * n1 / (2 * air);
+        const float c1 = (float)(gxk * f1y - gyk * f1x), c2 = (float)(gxk * f2y - gyk * f2x);
+        const float c3 = (float)(gxk * f3y - gyk * f3x), c4 = (float)(gxk * f4y - gyk * f4x);
+        const int ia = rev ? comp(vt, (j + 1) % 3) : comp(vt, j);
+        const int ib = rev ? comp(vt, j) : comp(vt, (j + 1) % 3);
+        const float vi1 = ld(wn + ia), vi2 = ld(wn + ib);
+        v = (vi1 + vl) * c1 + (vl + vi2) * c2 + (vi2 + vr) * c3 + (vr + vi1) * c4;
+      }
+      q[j] = own ? v : -v;
+    }
+  }
+  // manapy's order: inner faces, boundary faces, then the diffusive terms
+  const uint8_t code = ld(m.cell_order + i);
+  CompSum res;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick3(nb.x, nb.y, nb.z, sl) >= 0) res.add(pick3(cv[0], cv[1], cv[2], sl));
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick3(nb.x, nb.y, nb.z, sl) < 0) res.add(pick3(cv[0], cv[1], cv[2], sl));
+  }
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) res.add(pick3(q[0], q[1], q[2], order_slot(code, k)));
+  }
+  const double dt = *dt_dev;
+  float inc = (float)(dt / ld(m.cell_volume + i)) * res.value();
+  if (src) inc = fmaf((float)dt, ld(src + i), inc);
+  w_out[i] = wi + inc;
+}
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P2C_MIN_BLOCKS)
+    k_f2c_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p, const float *__restrict__ w, float *__restrict__ w_out,
+                 const float *__restrict__ sign, const float *__restrict__ src, const double *__restrict__ dt_dev,
+                 const float *__restrict__ rec, const float *__restrict__ wn) {
+  f2c_phase2<ORDER2, DIFF>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x);
+}
+
+// ---------------------------------------------------------------- batches of triangle meshes
+//
+// Many independent meshes advance in the same two launches: block b of a launch
+// belongs to item map[b] (blocks never straddle two meshes), which runs the
+// single-mesh block body on its own tables.  A device step counter (the batch
+// clock) selects each item's ping-pong buffer and skips items outside their
+// [start_step, end_step) window, so a captured graph of the step stays valid
+// while items come and go between replays.
+
+__device__ __forceinline__ bool item_active(int t, int start, int end) { return t >= start && t < end; }
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P1C_MIN_BLOCKS)
+    k_f2c_batch_phase1(const mb_advdiff_item *__restrict__ items, const int32_t *__restrict__ map,
+                       const int32_t *__restrict__ clock) {
+  const mb_advdiff_item &it = items[map[blockIdx.x]];
+  const int t = *clock;
+  if (!item_active(t, it.start_step, it.end_step)) return;
+  const float *w = it.w[(t - it.start_step) & 1];
+  f2c_phase1<ORDER2, DIFF>(it.m, it.bc, w, it.cell_scratch, it.node_scratch, it.p1_cell_blocks,
+                           (int)blockIdx.x - it.p1_begin);
+}
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P2C_MIN_BLOCKS)
+    k_f2c_batch_phase2(const mb_advdiff_item *__restrict__ items, const int32_t *__restrict__ map,
+                       const int32_t *__restrict__ clock) {
+  const mb_advdiff_item &it = items[map[blockIdx.x]];
+  const int t = *clock;
+  if (!item_active(t, it.start_step, it.end_step)) return;
+  const int par = (t - it.start_step) & 1;
+  f2c_phase2<ORDER2, DIFF>(it.m, it.bc, it.p, it.w[par], it.w[par ^ 1], it.sign_cf, it.src, it.dt_dev,
+                           it.cell_scratch, it.node_scratch, (int)blockIdx.x - it.p2_begin);
+}
+
+__global__ void k_clock_tick(int32_t *clock) { *clock += 1; }
+
+// ---------------------------------------------------------------- tetrahedra
+
+#ifndef MB_P1C_3D_MIN_BLOCKS
+#define MB_P1C_3D_MIN_BLOCKS 3
+#endif
+
+// record layout: float4 {w, gx, gy, gz} at rec[4i], psi at rec[4 nbcells + i]
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P1C_3D_MIN_BLOCKS)
+    k_f3c_phase1(mb_mesh m, mb_bc bc, const float *__restrict__ w, float *__restrict__ rec, float *__restrict__ wn,
+                 int ncb) {
+  const GhostRuleF ghost = make_rule_f(m, bc, w);
+  const int lane = threadIdx.x & 31;
+  if (ORDER2 && (int)blockIdx.x < ncb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nbcells) return;
+    const D3 c = ld3(m.cell_xy + 4 * i);
+    const float wi = ld(w + i);
+    double ixx = 0., iyy = 0., izz = 0., ixy = 0., ixz = 0., iyz = 0.;
+    float jx = 0.f, jy = 0.f, jz = 0.f;
+    const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
+    const int L = (se - sb) >> 5;
+    const int32_t *ix = m.lsq_sell_idx + sb + lane;
+    for (int k = 0; k < L; ++k) {
+      int cc = ld(ix + 32 * k);
+      cc = cc < 0 ? i : cc;
+      const D3 pc = ld3(m.cell_xy + 4 * cc);
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z;
+      const float dw = ld(w + cc) - wi;
+      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+      ixy += dx * dy; ixz += dx * dz; iyz += dy * dz;
+      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy); jz = fmaf((float)dz, dw, jz);
+    }
+    const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+    for (int k = gb; k < ge; ++k) {
+      const int f = ld(m.ghostnid_idx + k);
+      const double *gc = m.face_ghostcenter + 3 * f;
+      const double dx = ld(gc) - c.x, dy = ld(gc + 1) - c.y, dz = ld(gc + 2) - c.z;
+      const float dw = ghost(f) - wi;
+      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+      ixy += dx * dy; ixz += dx * dz; iyz += dy * dz;
+      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy); jz = fmaf((float)dz, dw, jz);
+    }
+    const double rdia = 1. / (ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) -
+                              izz * (ixy * ixy));
+    // inverse moment matrix (symmetric cofactors / determinant), rounded once
+    const float a11 = (float)((iyy * izz - iyz * iyz) * rdia), a12 = (float)((ixz * iyz - ixy * izz) * rdia);
+    const float a13 = (float)((ixy * iyz - ixz * iyy) * rdia), a22 = (float)((ixx * izz - ixz * ixz) * rdia);
+    const float a23 = (float)((ixy * ixz - iyz * ixx) * rdia), a33 = (float)((ixx * iyy - ixy * ixy) * rdia);
+    const float gx = a11 * jx + a12 * jy + a13 * jz;
+    const float gy = a12 * jx + a22 * jy + a23 * jz;
+    const float gz = a13 * jx + a23 * jy + a33 * jz;
+    const int4 vt = ld4(m.cell_vtx + 4 * i);
+    const int4 nb = ld4(m.cell_nbr + 4 * i);
+    const uint32_t fl = ld(m.cell_flags + i);
+    const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
+                     ld3(m.node_coord + 4 * vt.w)};
+    float wmax = wi, wmin = wi;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int o = comp(nb, j);
+      const float bv = o < 0 ? ghost(-1 - o) : ld(w + o);
+      wmax = fmaxp(wmax, bv);
+      wmin = fminp(wmin, bv);
+    }
+    float ps = 1.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int d0, d1, d2;
+      face_desc(fl, j, d0, d1, d2);
+      const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
+      const float delta = gx * (float)(fc.x - c.x) + gy * (float)(fc.y - c.y) + gz * (float)(fc.z - c.z);
+      float psi_ij = 1.f;
+      if (!(fabsf(delta) < 1e-10f)) {
+        if (delta > 0.f) psi_ij = fminp(1.f, (wmax - wi) / delta);
+        if (delta < 0.f) psi_ij = fminp(1.f, (wmin - wi) / delta);
+      }
+      ps = fminp(ps, psi_ij);
+    }
+    const uint64_t keep = l2_keep();
+    st4_keep(rec + 4 * (long long)i, make_float4(wi, gx, gy, gz), keep);
+    st1f_keep(rec + 4 * (long long)m.nbcells + i, ps, keep);
+    return;
+  }
+  if (DIFF) node_value_f32(m, ghost, w, wn, (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x, lane);
+}
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, 2)
+    k_f3c_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p, const float *__restrict__ w, float *__restrict__ w_out,
+                 const float *__restrict__ sign, const float *__restrict__ src, const double *__restrict__ dt_dev,
+                 const float *__restrict__ rec, const float *__restrict__ wn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRuleF ghost = make_rule_f(m, bc, w);
+  const int4 vt = ld4(m.cell_vtx + 4 * i);
+  const int4 nb = ld4(m.cell_nbr + 4 * i);
+  const uint32_t fl = ld(m.cell_flags + i);
+  const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
+                   ld3(m.node_coord + 4 * vt.w)};
+  const D3 ci = ld3(m.cell_xy + 4 * i);
+  const float4 s4 = ldf4(sign + 4 * (long long)i);
+  const long long nc = m.nbcells;
+  float wi, gxi = 0.f, gyi = 0.f, gzi = 0.f, psii = 0.f;
+  if (ORDER2) {
+    const float4 r = ldf4(rec + 4 * (long long)i);
+    wi = r.x; gxi = r.y; gyi = r.z; gzi = r.w;
+    psii = ld(rec + 4 * nc + i);
+  } else {
+    wi = ld(w + i);
+  }
+  float cv[4], q[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int o = comp(nb, j);
+    const bool b = o < 0;
+    const int f = -1 - o;
+    const bool own = (fl >> (6 * j)) & 1u;
+    int d0, d1, d2;
+    face_desc(fl, j, d0, d1, d2);
+    const D3 V0 = pick4(P, d0), V1 = pick4(P, d1), V2 = pick4(P, d2);
+    const D3 fc = (1. / 3) * ((V0 + V1) + V2);
+    float vo, gxo = 0.f, gyo = 0.f, gzo = 0.f, pso = 0.f;
+    D3 co;
+    if (b) {
+      vo = ghost(f);
+      co = d3(ld(m.face_ghostcenter + 3 * f), ld(m.face_ghostcenter + 3 * f + 1), ld(m.face_ghostcenter + 3 * f + 2));
+    } else {
+      if (ORDER2) {
+        const float4 r = ldf4(rec + 4 * (long long)o);
+        vo = r.x; gxo = r.y; gyo = r.z; gzo = r.w;
+        pso = ld(rec + 4 * nc + o);
+      } else {
+        vo = ld(w + o);
+      }
+      co = ld3(m.cell_xy + 4 * o);
+    }
+    const float s = pick4v(s4.x, s4.y, s4.z, s4.w, j);
+    const bool take_me = (s >= 0.f) == own;
+    float sol;
+    if (take_me) {
+      sol = ORDER2 ? wi + psii * (gxi * (float)(fc.x - ci.x) + gyi * (float)(fc.y - ci.y) + gzi * (float)(fc.z - ci.z))
+                   : wi;
+    } else if (b) {
+      sol = vo;
+    } else {
+      sol = ORDER2 ? vo + pso * (gxo * (float)(fc.x - co.x) + gyo * (float)(fc.y - co.y) + gzo * (float)(fc.z - co.z))
+                   : vo;
+    }
+    const float F = s * sol;
+    cv[j] = own ? -F : F;
+    if (DIFF) {
+      float v = 0.f;
+      if (!b || ld(bc.face_grad_on + f)) {
+        const D3 Nd = 0.5 * cross(V1 - V0, V2 - V0);
+        const D3 N = ((fl >> (6 * j + 5)) & 1u) ? (-1.0) * Nd : Nd;
+        const bool swp = (fl >> (6 * j + 4)) & 1u;
+        const int i1 = d0, i2 = swp ? d2 : d1, i3 = swp ? d1 : d2;
+        const D3 Q2 = pick4(P, i2), Q3 = pick4(P, i3), Q1 = pick4(P, i1);
+        const D3 v1 = own ? ci : co, v2 = own ? co : ci;
+        const D3 s1 = v2 - Q2, s2 = Q3 - Q2, s3 = v1 - Q2;
+        const D3 f1 = 0.5 * cross(s1, s2) + 0.5 * cross(s2, s3);
+        const D3 s4v = v2 - Q3, s5 = Q1 - Q3, s6 = v1 - Q3;
+        const D3 f2 = 0.5 * cross(s4v, s5) + 0.5 * cross(s5, s6);
+        const double rair = 1. / dot(N, v2 - v1);
+        // sum_d D_d g_d N_d = ca (V_A - V_C) + cb (V_B - V_D) + cr (V_R - V_L)
+        const D3 DN = d3(p.Dxx * N.x, p.Dyy * N.y, p.Dzz * N.z);
+        const float ca = (float)(dot(DN, f1) * rair), cb = (float)(dot(DN, f2) * rair),
+                    cr = (float)(dot(DN, N) * rair);
+        const float VA = ld(wn + comp(vt, i1)), VB = ld(wn + comp(vt, i2)), VC = ld(wn + comp(vt, i3));
+        const float VL = own ? wi : vo, VR = own ? vo : wi;
+        v = ca * (VA - VC) + cb * (VB - VC) + cr * (VR - VL);
+      }
+      q[j] = own ? v : -v;
+    }
+  }
+  const uint8_t code = ld(m.cell_order + i);
+  CompSum res;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick4v(nb.x, nb.y, nb.z, nb.w, sl) >= 0) res.add(pick4v(cv[0], cv[1], cv[2], cv[3], sl));
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int sl = order_slot(code, k);
+    if (pick4v(nb.x, nb.y, nb.z, nb.w, sl) < 0) res.add(pick4v(cv[0], cv[1], cv[2], cv[3], sl));
+  }
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) res.add(pick4v(q[0], q[1], q[2], q[3], order_slot(code, k)));
+  }
+  const double dt = *dt_dev;
+  float inc = (float)(dt / ld(m.cell_volume + i)) * res.value();
+  if (src) inc = fmaf((float)dt, ld(src + i), inc);
+  w_out[i] = wi + inc;
+}
+
+template <bool O2, bool DF>
+int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const float *w_in, float *w_out,
+                     const float *sign, const float *src, const double *dt, float *cs, float *wn, cudaStream_t st) {
+  const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
+  const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
+  if (m.dim == 2) {
+    if (ncb + nnb > 0) k_f2c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+    k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn);
+  } else {
+    if (ncb + nnb > 0) k_f3c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+    k_f3c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn);
+  }
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
+                                    const float *w_in, float *w_out, const float *sign_cf, const float *src,
+                                    const double *dt_dev, float *cell_scratch, float *node_scratch, void *stream) {
+  if (!m || !bc || !p || !w_in || !w_out || !sign_cf || !dt_dev || w_in == w_out) return MB_EINVAL;
+  if (m->dim != 2 && m->dim != 3) return MB_EINVAL;
+  if (!(m->cell_vtx && m->cell_nbr && m->cell_flags && m->node_coord && m->cell_xy && m->lsq_sell_ptr &&
+        m->lsq_sell_idx && m->n2c_sell_ptr && m->n2c_sell_idx && m->n2c_sell_alpha_f32))
+    return MB_EINVAL;
+  const bool o2 = p->order == 2, df = p->diffusion != 0;
+  if (p->order != 1 && !o2) return MB_EINVAL;
+  if ((o2 && !cell_scratch) || (df && !node_scratch) || (df && !bc->face_grad_on)) return MB_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (o2 && df) return launch_step_f32c<true, true>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch,
+                                                    node_scratch, st);
+  if (o2) return launch_step_f32c<true, false>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch,
+                                               node_scratch, st);
+  if (df) return launch_step_f32c<false, true>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch,
+                                               node_scratch, st);
+  return launch_step_f32c<false, false>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch,
+                                        st);
+}
+
+extern "C" int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const int32_t *p1_map, int32_t p1_blocks,
+                                          const int32_t *p2_map, int32_t p2_blocks, int32_t order,
+                                          int32_t diffusion, int32_t *clock, void *stream) {
+  if (!items || !p2_map || !clock || p2_blocks <= 0 || p1_blocks < 0 || (order != 1 && order != 2)) return MB_EINVAL;
+  const bool o2 = order == 2, df = diffusion != 0;
+  if ((o2 || df) && (!p1_map || p1_blocks <= 0)) return MB_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (o2 && df) {
+    k_f2c_batch_phase1<true, true><<<p1_blocks, kBlock, 0, st>>>(items, p1_map, clock);
+    k_f2c_batch_phase2<true, true><<<p2_blocks, kBlock, 0, st>>>(items, p2_map, clock);
+  } else if (o2) {
+    k_f2c_batch_phase1<true, false><<<p1_blocks, kBlock, 0, st>>>(items, p1_map, clock);
+    k_f2c_batch_phase2<true, false><<<p2_blocks, kBlock, 0, st>>>(items, p2_map, clock);
+  } else if (df) {
+    k_f2c_batch_phase1<false, true><<<p1_blocks, kBlock, 0, st>>>(items, p1_map, clock);
+    k_f2c_batch_phase2<false, true><<<p2_blocks, kBlock, 0, st>>>(items, p2_map, clock);
+  } else {
+    k_f2c_batch_phase2<false, false><<<p2_blocks, kBlock, 0, st>>>(items, p2_map, clock);
+  }
+  k_clock_tick<<<1, 1, 0, st>>>(clock);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}

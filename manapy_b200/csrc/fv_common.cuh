@@ -23,6 +23,9 @@ __host__ __device__ inline int ceil_div(long long a, int b) { return (int)((a + 
 __device__ __forceinline__ double pmin(double a, double b) { return b < a ? b : a; }
 __device__ __forceinline__ double pmax(double a, double b) { return b > a ? b : a; }
 
+// Slot of a cell's local face visited k-th in manapy's accumulation order (2 bits per k).
+__device__ __forceinline__ int order_slot(uint8_t code, int k) { return (code >> (2 * k)) & 3; }
+
 // Read-only loads through the non-coherent path.
 template <class T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }

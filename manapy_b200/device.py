@@ -16,7 +16,18 @@ from .geometry import padded_from_csr  # noqa: F401  (re-export for callers)
 
 
 def _t(a, dtype, dev):
-    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)
+    """A table as a contiguous array of ``dtype``: numpy when ``dev`` is None (built on the
+    host for a later upload), else a tensor on ``dev``."""
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a if dev is None else torch.from_numpy(a).to(dev)
+
+
+def _upload(a, dev, stream):
+    t = torch.from_numpy(a)
+    if stream is None:
+        return t.to(dev)
+    with torch.cuda.stream(stream):
+        return t.pin_memory().to(dev, non_blocking=True)
 
 
 def cell_order_codes(faceid_local):
@@ -102,8 +113,10 @@ class DeviceMesh:
     """
 
     def __init__(self, A, device="cuda", reorder=True):
+        """``device=None`` builds the tables as numpy arrays on the host (``upload`` moves
+        them to a device later, e.g. after building in a worker process)."""
         from .reorder import Renumbering
-        dev = torch.device(device)
+        dev = torch.device(device) if device is not None else None
         self.device = dev
         self.A = A
         dim = int(A["dim"])
@@ -147,6 +160,11 @@ class DeviceMesh:
         T["face_normal"] = _t(A["faces_normal"][fp], f64, dev)
         T["face_center"] = _t(A["faces_center"][fp], f64, dev)
         T["face_mesure"] = _t(A["faces_mesure"][fp], f64, dev)
+        if dim == 2:
+            nm = np.zeros((nf, 4))
+            nm[:, :2] = A["faces_normal"][fp, :2]
+            nm[:, 2] = 1.0 / A["faces_mesure"][fp]
+            T["face_nm_f32"] = _t(nm, np.float32, dev)
         T["face_ghostcenter"] = _t(A["faces_ghostcenter"][fp, :3], f64, dev)
         T["face_air"] = _t(A["faces_airDiamond"][fp], f64, dev)
         if dim == 2:
@@ -160,6 +178,7 @@ class DeviceMesh:
         T["n2c_ptr"], T["n2c_idx"], T["n2c_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_c[src], f64, dev)
         gp, gi, gv = sell32(ptr, idx, a_c[src], fill="first")
         T["n2c_sell_ptr"], T["n2c_sell_idx"], T["n2c_sell_alpha"] = _t(gp, i32, dev), _t(gi, i32, dev), _t(gv, f64, dev)
+        T["n2c_sell_alpha_f32"] = _t(gv, np.float32, dev)
         ptr, idx, src = R.relabel_csr(A["n2g_ptr"], A["n2g_idx"], np_, fi)
         T["n2g_ptr"], T["n2g_idx"], T["n2g_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_g[src], f64, dev)
         if dim == 2:
@@ -176,18 +195,38 @@ class DeviceMesh:
         else:
             self._compact_3d(A, T, dev)
         self.t = T
-        s = _lib.MbMesh()
-        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = dim, nc, nf, nn, nlf, 0
-        for name, _ in _lib.MbMesh._fields_:
-            if name in T:
-                setattr(s, name, T[name].data_ptr())
-        self.struct = s
         # field permutations: device[k] = host[perm[k]], host[j] = device[inv[j]]
-        self.perm = {"cell": torch.from_numpy(cp).to(dev), "face": torch.from_numpy(fp).to(dev),
-                     "node": torch.from_numpy(np_).to(dev)}
-        self.inv = {"cell": torch.from_numpy(ci).to(dev), "face": torch.from_numpy(fi).to(dev),
-                    "node": torch.from_numpy(ni).to(dev)}
+        i64 = np.int64
+        self.perm = {"cell": _t(cp, i64, dev), "face": _t(fp, i64, dev), "node": _t(np_, i64, dev)}
+        self.inv = {"cell": _t(ci, i64, dev), "face": _t(fi, i64, dev), "node": _t(ni, i64, dev)}
         self.reordered = bool(reorder)
+        self.struct = self._make_struct() if dev is not None else None
+
+    def _make_struct(self):
+        s = _lib.MbMesh()
+        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = (self.dim, self.nbcells, self.nbfaces,
+                                                                  self.nbnodes, self.nlf, 0)
+        for name, _ in _lib.MbMesh._fields_:
+            if name in self.t:
+                setattr(s, name, self.t[name].data_ptr())
+        return s
+
+    def upload(self, device, stream=None):
+        """Move host-built tables (``device=None`` at construction) to ``device``; with a
+        CUDA ``stream`` the copies are asynchronous on it.  Drops the host arrays ``A``."""
+        dev = torch.device(device)
+        self.t = {k: _upload(a, dev, stream) for k, a in self.t.items()}
+        self.perm = {k: _upload(a, dev, stream) for k, a in self.perm.items()}
+        self.inv = {k: _upload(a, dev, stream) for k, a in self.inv.items()}
+        self.device = dev
+        self.A = None
+        self.struct = self._make_struct()
+        return self
+
+    def strip(self):
+        """Drop the host arrays ``A`` (before sending host-built tables to another process)."""
+        self.A = None
+        return self
 
     def _compact_2d(self, A, T, dev):
         """Cell-centred tables of the fused 2D step (see ``mb_mesh`` in the C header)."""
@@ -312,7 +351,8 @@ class DeviceMesh:
         return "cellnid_ptr" in self.t
 
     def nbytes(self):
-        return sum(t.numel() * t.element_size() for t in self.t.values())
+        return sum(int(t.nbytes) if isinstance(t, np.ndarray) else t.numel() * t.element_size()
+                   for t in self.t.values())
 
 
 class DeviceBC:
@@ -320,7 +360,7 @@ class DeviceBC:
 
     def __init__(self, A, resolved, device="cuda", mesh=None):
         from .boundary import G_CELL_AT_FACE
-        dev = torch.device(device)
+        dev = torch.device(device) if device is not None else None
         nf = int(A["nbfaces"])
         self.resolved = resolved
         fp = mesh.R.fperm if mesh is not None else np.arange(nf)
@@ -338,8 +378,18 @@ class DeviceBC:
         on[resolved.dirichletfaces] = 1
         on[resolved.neumannfaces] = 1
         self.face_grad_on = _t(on[fp], np.uint8, dev)
+        self.struct = self._make_struct() if dev is not None else None
+
+    def _make_struct(self):
         s = _lib.MbBC()
         s.kind = self.kind.data_ptr()
         s.value = self.value.data_ptr()
         s.face_grad_on = self.face_grad_on.data_ptr()
-        self.struct = s
+        return s
+
+    def upload(self, device, stream=None):
+        dev = torch.device(device)
+        self.kind, self.value, self.face_grad_on = (_upload(a, dev, stream)
+                                                    for a in (self.kind, self.value, self.face_grad_on))
+        self.struct = self._make_struct()
+        return self

@@ -11,6 +11,8 @@ kernels read are built on first use (``domain.device_mesh``).
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from . import geometry
@@ -180,6 +182,40 @@ class Domain:
     def bounds(self):
         v = self._A["nodes_vertex"]
         return np.array([[v[:, k].min(), v[:, k].max()] for k in range(int(self._dim))])
+
+    # ------------------------------------------------------------------ output
+    def _save(self, on, dt, time, niter, miter, variables, values, file_format, path):
+        from . import vtu
+        if values is None:
+            raise ValueError("value must be given")
+        if file_format != "vtu":
+            raise ValueError("only the vtu format is written")
+        n = int(self.nbcells if on == "cell" else self.nbnodes)
+        vals = [v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v) for v in values]
+        assert len(vals[0]) == n, "value size != number of %ss" % on
+        k = 3 if self._dim == 2 else 4
+        cells = self._A["cells_nodeid"][:, :k]
+        points = self._A["nodes_vertex"][:, :3]
+        data = {variables[j]: vals[j] for j in range(len(vals))}
+        print(" **************************** Computing ****************************")
+        print("$$$$$$$$$$$$$$$$$$$$$$$$$$$$ Saving Results $$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$")
+        print("Iteration = ", niter, "time = ", time, "time step = ", dt)
+        print("max" + variables[0] + " =", float(np.max(vals[0])))
+        piece = "visu%d-%d.vtu" % (self._comm.Get_rank(), miter)
+        vtu.write_vtu(os.path.join(path, piece), points, cells,
+                      cell_data=data if on == "cell" else None, point_data=data if on == "node" else None)
+        vtu.write_pvtu(os.path.join(path, "visu%d.pvtu" % miter), [piece], list(variables), on=on)
+
+    def save_on_cell_multi(self, dt=0, time=0, niter=0, miter=0, variables=None, values=None, file_format="vtu",
+                           path="results"):
+        """Cell fields to ``results/visu<rank>-<miter>.vtu`` + ``visu<miter>.pvtu``
+        (``manapy/ddm/domain.py:784-849``); values may be device tensors."""
+        self._save("cell", dt, time, niter, miter, variables, values, file_format, path)
+
+    def save_on_node_multi(self, dt=0, time=0, niter=0, miter=0, variables=None, values=None, file_format="vtu",
+                           path="results"):
+        """Node fields, as ``save_on_cell_multi`` (``manapy/ddm/domain.py:735-782``)."""
+        self._save("node", dt, time, niter, miter, variables, values, file_format, path)
 
     def __str__(self):
         return ("\n> dim   :: %d\n> total cells  :: %d\n> total nodes  :: %d\n> total faces  :: %d\n"

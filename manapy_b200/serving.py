@@ -1,0 +1,409 @@
+"""Continuous-batching server for explicit finite-volume solves (no counterpart in manapy).
+
+Each request is a whole solve on its own mesh: an advection-diffusion run (second
+order, Barth limiter, diamond diffusion, Dirichlet 0 boundaries) or a
+shallow-water dam break (first order, Neumann walls), for a given number of
+steps, in the FP32-compensated precision.  The server keeps every admitted
+request's mesh tables and fields resident on the GPU and advances all of them
+together: per step, one batched launch pair per family (the block -> mesh maps
+of ``mb_advdiff_batch_step_f32c`` / ``mb_sw_batch_step_f32c``) over all active
+meshes, so requests of very different sizes share the device.  Requests that
+arrive while others run are admitted between steps, as soon as a slot and the
+HBM budget allow; finished ones retire between steps and free their memory.
+
+Mesh preparation (generation, geometry, locality numbering, compact tables) is
+host work; it runs in a pool of worker processes that overlaps the GPU.  The
+step loop is replayed from CUDA graphs, re-captured whenever the set of active
+requests changes.
+
+Results are independent of the mix: every request computes exactly what its
+own solve computes alone (no cross-request sums; each dt reduction is an exact
+min over the request's own cells), so a request's result is bit-for-bit the same
+alone and in any batch.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import dataclasses
+import math
+import multiprocessing as mp
+import os
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+
+__all__ = ["Request", "make_requests", "prepare", "BatchServer"]
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    kind: str            # "advdiff" or "sw"
+    n: int               # mesh: n x n squares, 2 n^2 triangles
+    seed: int
+    steps: int
+    arrival: float = 0.0  # seconds after the start of the run
+    ux: float = 0.0
+    uy: float = 0.0
+    D: float = 0.0
+    ratio: float = 2.0    # dam-break height ratio (left / right)
+
+    @property
+    def cells(self):
+        return 2 * self.n * self.n
+
+
+def make_requests(count, rate, seed=0, cells=(2e3, 5e5), frac_advdiff=0.7, steps=(100, 2000)):
+    """Seeded request stream: Poisson arrivals at ``rate`` per second, mesh sizes
+    log-uniform in ``cells``, 70 % advection-diffusion (speed U[0.2, 1.5], random
+    direction, D log-uniform in [1e-4, 1e-2]), 30 % dam breaks (height ratio U[1.2, 3]),
+    steps uniform in ``steps``."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=count)) if rate > 0 else np.zeros(count)
+    out = []
+    for k in range(count):
+        nc = math.exp(rng.uniform(math.log(cells[0]), math.log(cells[1])))
+        n = max(2, int(round(math.sqrt(nc / 2))))
+        kind = "advdiff" if rng.uniform() < frac_advdiff else "sw"
+        st = int(rng.integers(steps[0], steps[1] + 1))
+        r = Request(rid=k, kind=kind, n=n, seed=int(rng.integers(1 << 30)), steps=st, arrival=float(t[k]))
+        if kind == "advdiff":
+            sp, th = rng.uniform(0.2, 1.5), rng.uniform(0, 2 * math.pi)
+            r.ux, r.uy = sp * math.cos(th), sp * math.sin(th)
+            r.D = math.exp(rng.uniform(math.log(1e-4), math.log(1e-2)))
+        else:
+            r.ratio = rng.uniform(1.2, 3.0)
+        out.append(r)
+    return out
+
+
+# ------------------------------------------------------------------ host preparation
+
+SIDES = ("in", "out", "upper", "bottom")
+
+
+def initial_state(req, centers):
+    """Initial cell fields (device numbering is applied by the caller)."""
+    x, y = centers[:, 0], centers[:, 1]
+    if req.kind == "advdiff":
+        return [np.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / 0.01)]
+    h = np.where(x < 0.5, req.ratio, 1.0)
+    Z = 0.1 * np.exp(-((x - 0.7) ** 2 + (y - 0.5) ** 2) / 0.02)
+    zero = np.zeros_like(x)
+    return [h, zero, zero.copy(), zero.copy(), Z]
+
+
+def prepare(req):
+    """Host work of one request (runs in a worker process): mesh, geometry, device tables
+    (as host arrays), boundary rules and the initial state in the device numbering."""
+    from . import boundary as B, geometry as G, meshgen
+    from .device import DeviceBC, DeviceMesh
+    el, vx = meshgen.square_triangles(req.n, seed=req.seed)
+    A = G.build(el, vx, 2)
+    dm = DeviceMesh(A, device=None)
+    bc = None
+    if req.kind == "advdiff":
+        res = B.resolve(A, {s: "dirichlet" for s in SIDES}, {s: 0.0 for s in SIDES})
+        bc = DeviceBC(A, res, device=None, mesh=dm)
+        bc.resolved = None
+    init = [a[dm.R.cperm] for a in initial_state(req, A["cells_center"])]
+    dm.strip()
+    return req, dm, bc, init
+
+
+# ------------------------------------------------------------------ device side
+
+def _p(t):
+    return t.data_ptr() if t is not None else None
+
+
+class _Slot:
+    """One admitted request: its device tables, fields and batch item."""
+
+    def __init__(self, req, dm, bc, init, dev, stream):
+        self.req = req
+        self.dm = dm.upload(dev, stream)
+        self.bc = bc.upload(dev, stream) if bc is not None else None
+        nc, nf = dm.nbcells, dm.nbfaces
+        f32 = torch.float32
+        with torch.cuda.stream(stream):
+            up = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(dev, non_blocking=True) for a in init]
+            if req.kind == "advdiff":
+                self.w = [up[0].float(), torch.empty(nc, dtype=f32, device=dev)]
+                uf = torch.full((nf,), req.ux, dtype=torch.float64, device=dev)
+                vf = torch.full((nf,), req.uy, dtype=torch.float64, device=dev)
+                zf = torch.zeros(nf, dtype=torch.float64, device=dev)
+                sign = torch.empty(4 * nc, dtype=torch.float64, device=dev)
+                st = stream.cuda_stream
+                _lib.call("mb_cell_face_sign", self.dm.struct, _p(uf), _p(vf), _p(zf), _p(sign), st)
+                self.sign = sign.float()
+                uc = torch.full((nc,), req.ux, dtype=torch.float64, device=dev)
+                vc = torch.full((nc,), req.uy, dtype=torch.float64, device=dev)
+                zc = torch.zeros(nc, dtype=torch.float64, device=dev)
+                self.dt = torch.empty(1, dtype=torch.float64, device=dev)
+                _lib.call("mb_time_step", self.dm.struct, _p(uc), _p(vc), _p(zc), 0.8, req.D, req.D, 0.0,
+                          _p(self.dt), st)
+                self.cs = torch.empty(4 * nc, dtype=f32, device=dev)
+                self.ns = torch.empty(dm.nbnodes, dtype=f32, device=dev)
+                self.params = _lib.MbAdvDiffParams(2, 1, req.D, req.D, 0.0)
+            else:
+                q = [up[k].float() for k in range(4)]
+                self.q = [q, [torch.empty(nc, dtype=f32, device=dev) for _ in range(4)]]
+                self.Z = up[4].float()
+                self.ff = torch.empty(4 * nf, dtype=f32, device=dev)
+                self.dt = torch.empty(2, dtype=torch.float64, device=dev)
+                _lib.call("mb_time_step_sw", self.dm.struct, _p(up[0]), _p(up[1]), _p(up[2]), 0.5, 9.81, 0.0, 0.0,
+                          _p(self.dt), stream.cuda_stream)
+            self.ready = torch.cuda.Event()
+            self.ready.record(stream)
+        self._keep = up  # the uploads stay alive until the copies have run
+        self.start = self.end = None
+        self.fam = None
+        self.nbytes = self.dm.nbytes() + sum(t.numel() * t.element_size() for t in self._tensors())
+
+    def _tensors(self):
+        if self.req.kind == "advdiff":
+            return self.w + [self.sign, self.dt, self.cs, self.ns]
+        return self.q[0] + self.q[1] + [self.Z, self.ff, self.dt]
+
+    def blocks(self):
+        nc = self.dm.nbcells
+        cb = -(-nc // 256)
+        if self.req.kind == "advdiff":
+            return cb + -(-self.dm.nbnodes // 256), cb, cb   # phase-1 blocks, of which cells, phase-2
+        return -(-self.dm.nbfaces // 256), cb              # face blocks, cell blocks
+
+    def result(self):
+        """Final state (device tensors, device numbering): [w] or [h, hu, hv]."""
+        par = (self.end - self.start) & 1
+        if self.req.kind == "advdiff":
+            return [self.w[par]]
+        return self.q[par][:3]
+
+
+class BatchServer:
+    """Continuous-batching server on one GPU.
+
+    ``hbm_budget``: bytes of device memory the admitted requests may hold;
+    ``max_active``: slots; ``chunk``: steps per graph replay between admission points;
+    ``workers``: host processes preparing meshes (0: prepare in this process).
+    """
+
+    def __init__(self, device="cuda:0", hbm_budget=40e9, max_active=256, chunk=16, workers=None,
+                 graphs=True):
+        self.dev = torch.device(device)
+        self.budget = float(hbm_budget)
+        self.max_active = int(max_active)
+        self.chunk = int(chunk)
+        self.graphs = bool(graphs)
+        self.workers = (os.cpu_count() or 1) if workers is None else int(workers)
+        self.stream = torch.cuda.Stream(device=self.dev)
+        self.upload_stream = torch.cuda.Stream(device=self.dev)
+        # one step counter per family: [advection-diffusion, shallow water]
+        self.clock = torch.zeros(2, dtype=torch.int32, device=self.dev)
+        self.clock_host = [0, 0]
+        self.active = {}
+        self._graph = None
+        self._tables = None
+        self._old = []
+
+    # -------------------------------------------------------------- batch tables
+    def _build_tables(self):
+        """Item arrays and block maps of the active slots, uploaded on the compute stream."""
+        ad = [s for s in self.active.values() if s.req.kind == "advdiff"]
+        sw = [s for s in self.active.values() if s.req.kind == "sw"]
+        tabs = {}
+        with torch.cuda.stream(self.stream):
+            if ad:
+                items = (_lib.MbAdvDiffItem * len(ad))()
+                p1, p2 = [], []
+                b1 = b2 = 0
+                for k, s in enumerate(ad):
+                    n1, ncb, n2 = s.blocks()
+                    it = items[k]
+                    it.m, it.bc, it.p = s.dm.struct, s.bc.struct, s.params
+                    it.w[0], it.w[1] = _p(s.w[0]), _p(s.w[1])
+                    it.sign_cf, it.src, it.dt_dev = _p(s.sign), None, _p(s.dt)
+                    it.cell_scratch, it.node_scratch = _p(s.cs), _p(s.ns)
+                    it.start_step, it.end_step = s.start, s.end
+                    it.p1_begin, it.p1_cell_blocks, it.p2_begin = b1, ncb, b2
+                    p1.append(np.full(n1, k, np.int32))
+                    p2.append(np.full(n2, k, np.int32))
+                    b1 += n1
+                    b2 += n2
+                tabs["ad"] = (self._dev_bytes(items), self._dev_i32(np.concatenate(p1)), b1,
+                              self._dev_i32(np.concatenate(p2)), b2)
+            if sw:
+                items = (_lib.MbSwItem * len(sw))()
+                fm, cm = [], []
+                bf = bc = 0
+                for k, s in enumerate(sw):
+                    nfb, ncb = s.blocks()
+                    it = items[k]
+                    it.m = s.dm.struct
+                    for par in range(2):
+                        for c in range(4):
+                            it.q[par][c] = _p(s.q[par][c])
+                    it.Z, it.face_flux, it.dt = _p(s.Z), _p(s.ff), _p(s.dt)
+                    it.cfl, it.grav = 0.5, 9.81
+                    it.start_step, it.end_step = s.start, s.end
+                    it.f_begin, it.c_begin = bf, bc
+                    fm.append(np.full(nfb, k, np.int32))
+                    cm.append(np.full(ncb, k, np.int32))
+                    bf += nfb
+                    bc += ncb
+                tabs["sw"] = (self._dev_bytes(items), self._dev_i32(np.concatenate(fm)), bf,
+                              self._dev_i32(np.concatenate(cm)), bc)
+        return tabs
+
+    def _dev_bytes(self, cstruct_array):
+        raw = np.frombuffer(bytes(cstruct_array), dtype=np.uint8)
+        return torch.from_numpy(raw.copy()).pin_memory().to(self.dev, non_blocking=True)
+
+    def _dev_i32(self, a):
+        return torch.from_numpy(a).pin_memory().to(self.dev, non_blocking=True)
+
+    def _launch_step(self, tabs, st):
+        if "ad" in tabs:
+            items, m1, b1, m2, b2 = tabs["ad"]
+            _lib.call("mb_advdiff_batch_step_f32c", _p(items), _p(m1), b1, _p(m2), b2, 2, 1, _p(self.clock[0:1]),
+                      st)
+        if "sw" in tabs:
+            items, m1, b1, m2, b2 = tabs["sw"]
+            _lib.call("mb_sw_batch_step_f32c", _p(items), _p(m1), b1, _p(m2), b2, _p(self.clock[1:2]), st)
+
+    def _run_chunk(self, nsteps):
+        """``nsteps`` batch steps on the compute stream (each family ticks its own clock)."""
+        tabs = self._tables
+        if self.graphs and nsteps == self.chunk:
+            if self._graph is None:
+                # captured without the device-wide synchronisation of torch.cuda.graph()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.stream(self.stream):
+                    g.capture_begin()
+                    try:
+                        for _ in range(nsteps):
+                            self._launch_step(tabs, self.stream.cuda_stream)
+                    finally:
+                        g.capture_end()
+                self._graph = g
+            with torch.cuda.stream(self.stream):
+                self._graph.replay()
+        else:
+            for _ in range(nsteps):
+                self._launch_step(tabs, self.stream.cuda_stream)
+
+    # -------------------------------------------------------------- serving loop
+    def serve(self, requests, keep_results=False, log=None):
+        """Run ``requests`` (their ``arrival`` times are honoured) to completion.  Returns a
+        list of per-request records: arrival, admission, completion, latency (seconds from
+        arrival to the result on the host), cells, steps, and the result arrays if asked."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        pool = None
+        if self.workers > 0:
+            pool = cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn"))
+        futures = {}
+        prepared = []          # (req, dm, bc, init), in arrival order
+        nxt = 0
+        done = []
+        pending_done = []      # (event, slots)
+        t0 = time.perf_counter()
+        used = 0.0
+        try:
+            while len(done) < len(reqs):
+                now = time.perf_counter() - t0
+                # hand arrived requests to the preparation pool
+                while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                    r = reqs[nxt]
+                    if pool is not None:
+                        futures[r.rid] = pool.submit(prepare, r)
+                    else:
+                        prepared.append(prepare(r))
+                    nxt += 1
+                for rid in [k for k, f in futures.items() if f.done()]:
+                    prepared.append(futures.pop(rid).result())
+                prepared.sort(key=lambda x: x[0].arrival)
+                # admission (between steps): FIFO while a slot and the budget allow
+                changed = False
+                while prepared and len(self.active) < self.max_active:
+                    req, dm, bc, init = prepared[0]
+                    est = dm.nbytes() + 48.0 * dm.nbcells + 16.0 * dm.nbfaces
+                    if used + est > self.budget and self.active:
+                        break
+                    prepared.pop(0)
+                    slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream)
+                    self.stream.wait_event(slot.ready)
+                    slot.admitted = time.perf_counter() - t0
+                    slot.fam = 0 if req.kind == "advdiff" else 1
+                    slot.start = self.clock_host[slot.fam]
+                    slot.end = slot.start + req.steps
+                    used += slot.nbytes
+                    self.active[req.rid] = slot
+                    changed = True
+                if changed:
+                    self._retable()
+                if not self.active:
+                    if nxt >= len(reqs) and not futures and not prepared and not pending_done:
+                        break
+                    self._complete(pending_done, done, t0, keep_results, log)
+                    time.sleep(0.002)
+                    continue
+                # advance to the next finishing request or one chunk, whichever is first
+                remaining = min(s.end - self.clock_host[s.fam] for s in self.active.values())
+                nsteps = max(1, min(self.chunk, remaining))
+                self._run_chunk(nsteps)
+                fams = {s.fam for s in self.active.values()}
+                for f in fams:
+                    self.clock_host[f] += nsteps
+                fin = [s for s in self.active.values() if s.end <= self.clock_host[s.fam]]
+                if fin:
+                    for s in fin:
+                        del self.active[s.req.rid]
+                    with torch.cuda.stream(self.stream):
+                        outs = [[t.to("cpu", non_blocking=True) for t in s.result()] for s in fin]
+                    ev = torch.cuda.Event()
+                    ev.record(self.stream)
+                    pending_done.append((ev, fin, outs))
+                    self._retable()
+                used -= self._complete(pending_done, done, t0, keep_results, log)
+            torch.cuda.synchronize(self.dev)
+            used -= self._complete(pending_done, done, t0, keep_results, log)
+        finally:
+            if pool:
+                pool.shutdown(cancel_futures=True)
+        return done
+
+    def _retable(self):
+        """New item tables and block maps for the current active set (the old ones stay
+        alive until later steps have certainly finished with them)."""
+        if self._tables is not None:
+            self._old.append((self._tables, self._graph))
+            self._old = self._old[-8:]
+        self._tables = self._build_tables() if self.active else None
+        self._graph = None
+
+    def _complete(self, pending_done, done, t0, keep_results, log):
+        """Record requests whose results reached the host; returns the bytes they release."""
+        freed = 0
+        still = []
+        for ev, fin, outs in pending_done:
+            if not ev.query():
+                still.append((ev, fin, outs))
+                continue
+            tdone = time.perf_counter() - t0
+            for s, o in zip(fin, outs):
+                rec = {"rid": s.req.rid, "kind": s.req.kind, "cells": s.dm.nbcells, "steps": s.req.steps,
+                       "arrival": s.req.arrival, "admitted": s.admitted, "done": tdone,
+                       "latency": tdone - s.req.arrival}
+                if keep_results:
+                    inv = s.dm.inv["cell"].cpu().numpy()
+                    rec["result"] = [x.numpy()[inv] for x in o]
+                done.append(rec)
+                freed += s.nbytes
+            if log:
+                log(len(done))
+        pending_done[:] = still
+        return freed

@@ -41,7 +41,10 @@ class AdvectionDiffusionSolver:
                    ("Dzz", float, 0., 0., "Diffusion in z direction"),
                    ("dt", float, 0., 0., "time step"),
                    ("order", int, 1, 1, "order of the convective scheme"),
-                   ("cfl", float, .4, 0, "cfl of the explicit scheme")]
+                   ("cfl", float, .4, 0, "cfl of the explicit scheme"),
+                   ("precision", str, "fp64", 0, "fp64 (manapy's arithmetic) or fp32c: FP32 state and "
+                                                 "fluxes with compensated per-cell sums, FP64 geometry and dt "
+                                                 "(no counterpart in manapy)")]
 
     @classmethod
     def process_conf(cls, conf, kwargs):
@@ -78,6 +81,9 @@ class AdvectionDiffusionSolver:
         self.cfl = np.float64(get("cfl"))
         if self.order not in (1, 2):
             raise ValueError("order must be 1 or 2")
+        self.precision = str(get("precision"))
+        if self.precision not in ("fp64", "fp32c"):
+            raise ValueError("precision must be 'fp64' or 'fp32c'")
         self.diffusion = not (self.Dxx == self.Dyy == self.Dzz == 0)
         self.backend = self.domain.backend
         self.signature = self.domain.signature
@@ -92,6 +98,14 @@ class AdvectionDiffusionSolver:
         self._spare = None
         self._graph = None
         self._dt_host = None
+        self._w32 = None       # FP32 ping-pong state of the fp32c mode
+        self._w32_i = 0
+        self._w32_key = None   # var.version("cell") the FP32 state corresponds to
+        self._sign32 = None
+        self._sign32_key = None
+        self._src32 = None
+        self._src32_key = None
+        self._graph_src = None
 
     # ------------------------------------------------------------ device helpers
     def _setup(self):
@@ -173,6 +187,7 @@ class AdvectionDiffusionSolver:
             var.swap_cell(cur)
 
     def _install_lazies(self, w_in):
+        """``w_in``: the step's FP64 input state, or a callable returning it."""
         var = self.var
         done = {"v": False}
 
@@ -181,7 +196,7 @@ class AdvectionDiffusionSolver:
                 done["v"] = True
                 for n in names:
                     var._s.lazy.pop(n, None)
-                self._materialise(w_in)
+                self._materialise(w_in() if callable(w_in) else w_in)
 
         names = ["ghost", "convective"]
         if self.order == 2:
@@ -234,6 +249,8 @@ class AdvectionDiffusionSolver:
         return self._cs, self._ns
 
     def _fused_step(self):
+        if self.precision == "fp32c":
+            return self._fused_step_f32c()
         var = self.var
         dm = self._dm
         self._update_sign()
@@ -246,6 +263,60 @@ class AdvectionDiffusionSolver:
                   _p(self._sign), self._source_ptr(), _p(self._dt_dev), _p(cs), _p(ns), self._stream())
         self._spare = var.swap_cell(w_out)
         self._install_lazies(self._spare)
+
+    # ------------------------------------------------------------ fp32c mode
+    def _f32_state(self):
+        """The FP32 state, reloaded from the cell array when that changed since the last step."""
+        var = self.var
+        dm = self._dm
+        if self._w32 is None:
+            self._w32 = [torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device) for _ in range(2)]
+            nrec = (4 if dm.dim == 2 else 5) * dm.nbcells
+            self._cs32 = torch.empty(nrec, dtype=torch.float32, device=dm.device)
+            self._ns32 = torch.empty(dm.nbnodes, dtype=torch.float32, device=dm.device)
+            self._sign32 = torch.empty(4 * dm.nbcells, dtype=torch.float32, device=dm.device)
+        if var.version("cell") != self._w32_key:
+            self._w32[self._w32_i].copy_(var.dev("cell"))
+            self._w32_key = var.version("cell")
+        return self._w32[self._w32_i]
+
+    def _f32_inputs(self):
+        self._update_sign()
+        if self._sign32_key != self._sign_key:
+            self._sign32.copy_(self._sign)
+            self._sign32_key = self._sign_key
+        var = self.var
+        if var.version("source") == 0:
+            return None
+        if self._src32_key != var.version("source"):
+            self._src32 = var.dev("source").float()
+            self._src32_key = var.version("source")
+        return self._src32
+
+    def _f32_publish(self, w_prev):
+        """Make the FP32 result the variable's cell array (converted on first read)."""
+        var = self.var
+        cur = self._w32[self._w32_i]
+
+        def materialise(buf=cur):
+            var._s.dev["cell"].copy_(buf)
+
+        var._s.lazy.pop("cell", None)  # the previous result, superseded
+        var._s.version["cell"] += 1
+        var.set_lazy("cell", materialise)
+        self._w32_key = var.version("cell")
+        self._install_lazies(lambda buf=w_prev: buf.double())
+
+    def _call_f32c(self, x, y, src, st):
+        _lib.call("mb_advdiff_step_f32c", self._dm.struct, self.var.device_bc.struct, self._params, _p(x), _p(y),
+                  _p(self._sign32), _p(src), _p(self._dt_dev), _p(self._cs32), _p(self._ns32), st)
+
+    def _fused_step_f32c(self):
+        w_in = self._f32_state()
+        src = self._f32_inputs()
+        self._call_f32c(w_in, self._w32[1 - self._w32_i], src, self._stream())
+        self._w32_i = 1 - self._w32_i
+        self._f32_publish(w_in)
 
     def launches_per_step(self):
         """Kernel launches of one fused step."""
@@ -263,10 +334,16 @@ class AdvectionDiffusionSolver:
         var = self.var
         self._time_step_dev()
         self._update_sign()
+        n = int(nsteps)
+        if self.precision == "fp32c":
+            self._advance_f32c(n, graph)
+            if self._dt_host is None:
+                self._dt_host = float(self._dt_dev.item())
+            self.dt = np.float64(self._dt_host)
+            return n * self._dt_host
         var.dev("cell")
         if self._spare is None:
             self._spare = torch.empty_like(var.dev("cell"))
-        n = int(nsteps)
         if not graph or n < 2:
             for _ in range(n):
                 self._fused_step()
@@ -282,6 +359,35 @@ class AdvectionDiffusionSolver:
             self._dt_host = float(self._dt_dev.item())
         self.dt = np.float64(self._dt_host)
         return n * self._dt_host
+
+    def _advance_f32c(self, n, graph):
+        if not graph or n < 2:
+            for _ in range(n):
+                self._fused_step_f32c()
+            return
+        self._f32_state()
+        if self._w32_i != 0:  # the captured pair starts from buffer 0
+            self._fused_step_f32c()
+            n -= 1
+        src = self._f32_inputs()
+        if self._graph is None or self._graph_src != _p(src):
+            a, b = self._w32
+            s = torch.cuda.Stream(device=self._dm.device)
+            s.wait_stream(torch.cuda.current_stream(self._dm.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    st = torch.cuda.current_stream(self._dm.device).cuda_stream
+                    self._call_f32c(a, b, src, st)
+                    self._call_f32c(b, a, src, st)
+            torch.cuda.current_stream(self._dm.device).wait_stream(s)
+            self._graph, self._graph_src = g, _p(src)
+        for _ in range(n // 2):
+            self._graph.replay()
+        if n // 2:
+            self._f32_publish(self._w32[1])
+        if n % 2:
+            self._fused_step_f32c()
 
     def _get_graph(self):
         """Two fused steps (A->B, B->A) captured once; the cell buffer ends where it began."""
@@ -318,7 +424,10 @@ class ShallowWaterSolver:
                    ("Mann", float, 0., 0., "Manning number for the friction"),
                    ("fc", float, 0., 0., "Coriolis force"),
                    ("grav", float, 9.81, 0., "gravity constant"),
-                   ("wind", bool, False, True, "wind")]
+                   ("wind", bool, False, True, "wind"),
+                   ("precision", str, "fp64", 0, "fp64 (manapy's arithmetic) or fp32c: FP32 state and fluxes "
+                                                 "with compensated per-cell sums, FP64 geometry, source and dt "
+                                                 "(first order; no counterpart in manapy)")]
 
     @classmethod
     def process_conf(cls, conf, kwargs):
@@ -370,6 +479,14 @@ class ShallowWaterSolver:
                                       "attributes it never sets (manapy/solvers/shallowater/system.py:269-271)")
         if self.Mann != 0 or self.fc != 0 or self.wind:
             raise NotImplementedError("friction, Coriolis and wind source terms are not implemented")
+        self.precision = str(get("precision"))
+        if self.precision not in ("fp64", "fp32c"):
+            raise ValueError("precision must be 'fp64' or 'fp32c'")
+        if self.precision == "fp32c" and self.order != 1:
+            raise NotImplementedError("the fp32c shallow-water step is first order")
+        self._q32 = None
+        self._q32_key = None
+        self._q32_i = 0
         self.diffusion = False
         self.backend = self.domain.backend
         self.signature = self.domain.signature
@@ -497,6 +614,8 @@ class ShallowWaterSolver:
         self._dt_key = None
 
     def _fused_step(self):
+        if self.precision == "fp32c":
+            return self._fused_step_f32c()
         names = ("h", "hu", "hv", "hc")
         qin = [self.varbs[k].dev("cell") for k in names]
         z = self.Z.dev("cell")
@@ -513,6 +632,57 @@ class ShallowWaterSolver:
         self._cur = 1 - self._cur
         self._dt_key = self._state_key()
         self._dt_host = None
+
+    # ------------------------------------------------------------ fp32c mode
+    _NAMES = ("h", "hu", "hv", "hc", "Z")
+
+    def _keys(self):
+        return tuple(self.varbs[k].version("cell") for k in self._NAMES)
+
+    def _f32_state(self):
+        """[h, hu, hv, hc] (current buffer) and Z in FP32, reloaded when a cell array changed."""
+        dm = self._dm
+        if self._q32 is None:
+            mk = lambda: torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device)  # noqa: E731
+            self._q32 = [[mk() for _ in range(4)], [mk() for _ in range(4)], mk()]
+            self._ff32 = torch.empty(4 * dm.nbfaces, dtype=torch.float32, device=dm.device)
+        if self._keys() != self._q32_key:
+            for t, k in zip(self._q32[self._q32_i] + [self._q32[2]], self._NAMES):
+                t.copy_(self.varbs[k].dev("cell"))
+            self._q32_key = self._keys()
+        return self._q32[self._q32_i], self._q32[2]
+
+    def _fused_step_f32c(self):
+        qin, z = self._f32_state()
+        qout = self._q32[1 - self._q32_i]
+        cur = self._use_dt()
+        nxt = self._dt_buf[1 - self._cur:2 - self._cur]
+        _lib.call("mb_sw_step_f32c", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
+                  _lib.p5([_p(t) for t in qout] + [_p(z)]), float(self.cfl), float(self.grav), int(self.order),
+                  _p(self._ff32), _p(cur), _p(nxt), self._stream())
+        self._q32_i = 1 - self._q32_i
+        for k, buf in zip(self._NAMES[:4], qout):
+            var = self.varbs[k]
+
+            def materialise(var=var, buf=buf):
+                var._s.dev["cell"].copy_(buf)
+
+            var._s.lazy.pop("cell", None)  # the previous result, superseded
+            var._s.version["cell"] += 1
+            var.set_lazy("cell", materialise)
+        self._q32_key = self._keys()
+        self._cur = 1 - self._cur
+        self._dt_key = self._state_key()
+        self._dt_host = None
+
+    def mass(self):
+        """FP64 sum of volume x h over the cells (no counterpart in manapy)."""
+        dm = self._setup()
+        if self.precision == "fp32c" and self._q32 is not None and self._keys() == self._q32_key:
+            h = self._q32[self._q32_i][0].double()
+        else:
+            h = self.h.dev("cell")
+        return float(torch.dot(h, dm.t["cell_volume"]).item())
 
     def launches_per_step(self):
         """Kernel launches of one fused step: face fluxes, cells (+ next dt), [gradients]."""

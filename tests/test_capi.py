@@ -28,3 +28,27 @@ def test_library_exports_header_symbols():
 def test_build_info():
     build.build()
     assert b"sm_100a" in _lib.lib().mb_build_info()
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """ctypes mirrors of mb_mesh, mb_bc, mb_advdiff_params and the batch items have the
+    C compiler's size and field offsets."""
+    import subprocess
+    structs = {"mb_mesh": _lib.MbMesh, "mb_bc": _lib.MbBC, "mb_advdiff_params": _lib.MbAdvDiffParams,
+               "mb_advdiff_item": _lib.MbAdvDiffItem, "mb_sw_item": _lib.MbSwItem}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "manapy_b200.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (name, name))
+        for field, _ in cls._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (name, field, name, field))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                 check=True).stdout.splitlines())
+    for name, cls in structs.items():
+        assert int(got[name]) == ctypes.sizeof(cls), name
+        for field, _ in cls._fields_:
+            assert int(got[name + "." + field]) == getattr(cls, field).offset, (name, field)

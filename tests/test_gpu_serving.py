@@ -1,0 +1,102 @@
+"""Continuous-batching server: every request's result is the same alone and in the mix.
+
+The batched kernels run the single-mesh FP32-compensated block bodies on each
+item's own tables, so a request's result must be bit-for-bit identical whether
+it runs alone, in a mix admitted at once, or in a mix admitted while others run;
+and equal to the single-mesh FP32-compensated solver through the public API.
+Against the FP64 oracle the stated FP32-compensated tolerances apply.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_max
+import manapy_b200 as M
+from manapy_b200 import boundary as B, geometry as G, meshgen
+from manapy_b200.serving import BatchServer, Request, SIDES, initial_state
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix():
+    rs = []
+    k = 0
+    for n, steps in ((12, 30), (25, 47), (8, 64), (31, 20), (17, 51)):
+        rs.append(Request(rid=k, kind="advdiff", n=n, seed=100 + k, steps=steps, ux=0.9 - 0.3 * k,
+                          uy=0.2 + 0.25 * k, D=10 ** (-4 + 0.5 * k)))
+        k += 1
+    for n, steps, ratio in ((14, 33, 1.5), (22, 58, 2.5), (9, 17, 2.0)):
+        rs.append(Request(rid=k, kind="sw", n=n, seed=100 + k, steps=steps, ratio=ratio))
+        k += 1
+    return rs
+
+
+def _by_rid(recs):
+    return {r["rid"]: r for r in recs}
+
+
+def test_alone_and_in_the_mix_are_identical(cuda):
+    reqs = _mix()
+    mixed = _by_rid(BatchServer(workers=0, chunk=8).serve(reqs, keep_results=True))
+    assert sorted(mixed) == [r.rid for r in reqs]
+    for r in reqs:
+        alone = BatchServer(workers=0, chunk=8).serve([r], keep_results=True)[0]
+        for a, b in zip(alone["result"], mixed[r.rid]["result"]):
+            assert np.array_equal(a, b), r
+
+
+def test_staggered_admission_and_worker_pool(cuda):
+    """Requests arriving while others run (prepared by worker processes) give the same results."""
+    reqs = _mix()
+    for k, r in enumerate(reqs):
+        r.arrival = 0.05 * k
+    staggered = _by_rid(BatchServer(workers=2, chunk=4, max_active=3).serve(reqs, keep_results=True))
+    for r in reqs:
+        r.arrival = 0.0
+    at_once = _by_rid(BatchServer(workers=0, chunk=16).serve(reqs, keep_results=True))
+    for r in reqs:
+        for a, b in zip(staggered[r.rid]["result"], at_once[r.rid]["result"]):
+            assert np.array_equal(a, b), r
+        rec = staggered[r.rid]
+        assert rec["done"] >= rec["admitted"] >= 0 and rec["latency"] > 0
+
+
+def test_batched_equals_the_single_mesh_solver_and_the_oracle(cuda):
+    r = Request(rid=0, kind="advdiff", n=20, seed=7, steps=40, ux=0.7, uy=-0.4, D=3e-3)
+    got = BatchServer(workers=0).serve([r], keep_results=True)[0]["result"][0]
+    el, vx = meshgen.square_triangles(r.n, seed=r.seed)
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    w = M.Variable(domain=dom, BC={s: "dirichlet" for s in SIDES}, values={s: 0.0 for s in SIDES})
+    u, v = M.Variable(domain=dom), M.Variable(domain=dom)
+    u.face = np.full(dom.nbfaces, r.ux)
+    v.face = np.full(dom.nbfaces, r.uy)
+    u.cell = np.full(dom.nbcells, r.ux)  # the server's constant cell velocity, exactly
+    v.cell = np.full(dom.nbcells, r.uy)
+    w.cell = initial_state(r, dom.cells.center)[0]
+    S = M.AdvectionDiffusionSolver(w, vel=(u, v), conf=M.Struct(Dxx=r.D, Dyy=r.D, order=2, cfl=0.8,
+                                                                 precision="fp32c"))
+    S.advance(r.steps)
+    assert np.array_equal(got, w.cell)
+    A = G.build(el, vx, 2)
+    o = O.AdvDiffOracle(A, B.resolve(A, {s: "dirichlet" for s in SIDES}, {s: 0.0 for s in SIDES}),
+                        r.D, r.D, 0.0, order=2, cfl=0.8)
+    o.set_velocity(np.full(A["nbfaces"], r.ux), np.full(A["nbfaces"], r.uy), np.zeros(A["nbfaces"]))
+    o.w[:] = initial_state(r, A["cells_center"])[0]
+    for _ in range(r.steps):
+        o.step()
+    assert rel_max(got, o.w) < 1e-5
+
+
+def test_batched_shallow_water_matches_the_single_mesh_step(cuda):
+    r = Request(rid=0, kind="sw", n=16, seed=3, steps=25, ratio=2.2)
+    got = BatchServer(workers=0).serve([r], keep_results=True)[0]["result"]
+    el, vx = meshgen.square_triangles(r.n, seed=r.seed)
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    vs = [M.Variable(domain=dom) for _ in range(5)]
+    for var, a in zip(vs, initial_state(r, dom.cells.center)):
+        var.cell = a
+    S = M.ShallowWaterSolver(vs[0], hvel=(vs[1], vs[2]), hc=vs[3], Z=vs[4],
+                             conf=M.Struct(order=1, cfl=0.5, grav=9.81, precision="fp32c"))
+    S.advance(r.steps)
+    for a, var in zip(got, vs[:3]):
+        assert np.array_equal(a, var.cell)
