@@ -349,10 +349,20 @@ class AdvectionDiffusionSolver:
                 self._fused_step()
         else:
             g = self._get_graph()
+            a, b = self._graph_bufs
+            cur = var.dev("cell")
+            if cur is b:      # after an odd number of steps: one step brings the state back to a
+                self._fused_step()
+                n -= 1
+            elif cur is not a:  # a cell array installed since the capture
+                a.copy_(cur)
+                var.swap_cell(a)
+                self._spare = b
             for _ in range(n // 2):
                 g.replay()
-            var._s.version["cell"] += 1
-            self._install_lazies(self._spare)
+            if n // 2:
+                var._s.version["cell"] += 1
+                self._install_lazies(self._spare)
             if n % 2:
                 self._fused_step()
         if self._dt_host is None:
@@ -370,6 +380,7 @@ class AdvectionDiffusionSolver:
             self._fused_step_f32c()
             n -= 1
         src = self._f32_inputs()
+        self.var.device_bc  # built (and uploaded) before any capture
         if self._graph is None or self._graph_src != _p(src):
             a, b = self._w32
             s = torch.cuda.Stream(device=self._dm.device)
@@ -412,6 +423,7 @@ class AdvectionDiffusionSolver:
                               src, _p(self._dt_dev), _p(cs), _p(ns), st)
         torch.cuda.current_stream(dm.device).wait_stream(s)
         self._graph = g
+        self._graph_bufs = (a, b)
         return g
 
 
