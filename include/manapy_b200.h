@@ -218,17 +218,29 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
                     const double *dt_dev, double *cell_scratch, double *node_scratch, void *stream);
 
+/* The u.n table of the FP32-compensated step from mb_cell_face_sign's FP64 table: per
+ * cell the FP32 u.n of each local face and the cell's signed sum of them (sum over its
+ * faces of -u.n where the cell is faces.cellid[f][0], +u.n elsewhere), formed in FP64:
+ * 2D [nbcells][4] = {s0, s1, s2, sum}; 3D [nbcells][4] then [nbcells] sums (5*nbcells). */
+int mb_cell_face_sign_f32c(const mb_mesh *m, const double *sign_cf, float *sign_f32, void *stream);
+
 /* FP32-compensated twin of mb_advdiff_step (no counterpart in manapy, whose single
  * precision mode is FP32 throughout, manapy/backends/cpu/backend.py:46-49): the same
- * two launches with FP32 state (w_in, w_out), FP32 u.n (sign_cf, [4*nbcells]), FP32
+ * two launches with FP32 state (w_in, w_out), FP32 u.n (sign_cf from mb_cell_face_sign_f32c), FP32
  * source (src, may be NULL), FP32 phase-1 records and node values, FP32 fluxes summed
- * per cell with compensated (Neumaier) summation; coordinates, every geometric
- * coefficient and dt stay FP64.  Scratch: cell_scratch [4*nbcells] floats in 2D,
- * [5*nbcells] in 3D (order 2), node_scratch [nbnodes] floats (diffusion).  Needs the
- * compact tables of mb_mesh, n2c_sell_alpha_f32 included. */
+ * per cell with compensated (Neumaier) summation on differences from the cell's own
+ * value; coordinates, every geometric coefficient and dt stay FP64.  Scratch:
+ * cell_scratch [4*nbcells] floats in 2D, [5*nbcells] in 3D (order 2), node_scratch
+ * [nbnodes] floats (diffusion).  Needs the
+ * compact tables of mb_mesh, n2c_sell_alpha_f32 included.
+ * Compensated state: lo_in / lo_out (FP32 [nbcells], both or neither) carry the rounding
+ * error of the state, w + lo; the update is w_out + lo_out = w_in + (increment + lo_in)
+ * exactly, so the FP32 state loses nothing to rounding from step to step (fluxes still see
+ * the FP32 w).  NULL: plain FP32 state. */
 int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
-                         const float *w_in, float *w_out, const float *sign_cf, const float *src,
-                         const double *dt_dev, float *cell_scratch, float *node_scratch, void *stream);
+                         const float *w_in, float *w_out, const float *lo_in, float *lo_out,
+                         const float *sign_cf, const float *src, const double *dt_dev,
+                         float *cell_scratch, float *node_scratch, void *stream);
 
 /* sign_cf[4*i+j] = u_face[f] n_x + v_face[f] n_y + w_face[f] n_z for the j-th local face f
  * of cell i (zero for unused slots): the upwind selector of
@@ -279,7 +291,8 @@ typedef struct mb_advdiff_item {
   mb_bc bc;
   mb_advdiff_params p;
   float *w[2];              /* ping-pong FP32 state */
-  const float *sign_cf;     /* [4*nbcells] FP32 u.n per cell face */
+  float *lo[2];             /* ping-pong rounding errors of the state (NULL: none) */
+  const float *sign_cf;     /* [4*nbcells] from mb_cell_face_sign_f32c */
   const float *src;         /* NULL: no source */
   const double *dt_dev;     /* the item's dt */
   float *cell_scratch;      /* [4*nbcells] (order 2) */

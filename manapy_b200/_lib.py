@@ -48,7 +48,7 @@ class MbAdvDiffParams(ctypes.Structure):
 
 
 class MbAdvDiffItem(ctypes.Structure):
-    _fields_ = [("m", MbMesh), ("bc", MbBC), ("p", MbAdvDiffParams), ("w", _vp * 2), ("sign_cf", _vp),
+    _fields_ = [("m", MbMesh), ("bc", MbBC), ("p", MbAdvDiffParams), ("w", _vp * 2), ("lo", _vp * 2), ("sign_cf", _vp),
                 ("src", _vp), ("dt_dev", _vp), ("cell_scratch", _vp), ("node_scratch", _vp),
                 ("start_step", _i32), ("end_step", _i32), ("p1_begin", _i32), ("p1_cell_blocks", _i32),
                 ("p2_begin", _i32), ("pad_", _i32)]
@@ -86,7 +86,9 @@ _SIGS = {
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_advdiff_step_noalloc": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp],
-    "mb_advdiff_step_f32c": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "mb_cell_face_sign_f32c": [_M, _vp, _vp, _vp],
+    "mb_advdiff_step_f32c": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                             _vp, _vp],
     "mb_sw_step_f32c": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
     "mb_advdiff_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],

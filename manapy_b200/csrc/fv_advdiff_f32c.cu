@@ -12,6 +12,15 @@
 //         matrices, 1/volume) until it is multiplied by a state value, and dt.
 // Geometric coefficients are formed in FP64 and rounded once to FP32, so the
 // FP32 arithmetic only ever sees state x coefficient products.
+//
+// Difference form.  A cell's face terms nearly cancel (sum of u.n over a cell is the
+// velocity divergence, the diamond coefficients of a face sum to zero), so at fine
+// resolution the residual is a small difference of large terms.  The kernels
+// evaluate every face term on state *differences* from the cell's own value,
+//   sum_j s_j w_j          = sum_j s_j (w_j - w_i) + w_i sum_j s_j,
+//   sum_k c_k t_k          = sum_k a_k (v_k - w_i) + w_i sum_k a_k,
+// with sum_j s_j (the cell's signed u.n sum) and sum_k a_k formed in FP64, so FP32
+// rounding stays relative to the residual instead of to the state.
 #include "fv_compact.cuh"
 
 namespace mb {
@@ -78,6 +87,22 @@ __device__ __forceinline__ float ldf_stream(const float *a, uint64_t pol) {
 #else
   return __ldg(a);
 #endif
+}
+
+// State update with its rounding error carried: (w, lo) + inc -> (w', lo') with
+// w' + lo' = w + (inc + lo) exactly (Knuth's two-sum), so the FP32 state w loses no
+// increment to rounding from step to step; without lo (NULL) a plain FP32 add.
+__device__ __forceinline__ void store_state(float wi, float inc, const float *__restrict__ lo_in,
+                                            float *__restrict__ w_out, float *__restrict__ lo_out, int i) {
+  if (lo_in) {
+    const float a = inc + lo_in[i];
+    const float s = wi + a;
+    const float bv = s - wi;
+    lo_out[i] = (wi - (s - bv)) + (a - bv);
+    w_out[i] = s;
+  } else {
+    w_out[i] = wi + inc;
+  }
 }
 
 // centre->vertex value of node n (phase 1, node blocks): FP32 weights, FP32 sum
@@ -208,7 +233,8 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
                                            const float *__restrict__ w, float *__restrict__ w_out,
                                            const float *__restrict__ sign, const float *__restrict__ src,
                                            const double *__restrict__ dt_dev, const float *__restrict__ rec,
-                                           const float *__restrict__ wn, int bid) {
+                                           const float *__restrict__ wn, const float *__restrict__ lo_in,
+                                           float *__restrict__ lo_out, int bid) {
   const int i = bid * blockDim.x + threadIdx.x;
   if (i >= m.nbcells) return;
   const GhostRuleF ghost = make_rule_f(m, bc, w);
@@ -254,21 +280,21 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
     }
     const float s = j == 0 ? s4.x : (j == 1 ? s4.y : s4.z);
     const bool take_me = (s >= 0.f) == own;
-    float sol;
+    // upwind value minus w_i
+    float dsol;
     if (take_me) {
-      sol = ORDER2 ? wi + psii * (gxi * (float)(fcx - ci.x) + gyi * (float)(fcy - ci.y)) : wi;
+      dsol = ORDER2 ? psii * (gxi * (float)(fcx - ci.x) + gyi * (float)(fcy - ci.y)) : 0.f;
     } else if (b) {
-      sol = vo;
+      dsol = vo - wi;
     } else {
-      sol = ORDER2 ? vo + pso * (gxo * (float)(fcx - co.x) + gyo * (float)(fcy - co.y)) : vo;
+      dsol = ORDER2 ? (vo - wi) + pso * (gxo * (float)(fcx - co.x) + gyo * (float)(fcy - co.y)) : vo - wi;
     }
-    const float F = s * sol;
+    const float F = s * dsol;
     cv[j] = own ? -F : F;
     if (DIFF) {
       float v = 0.f;
       if (!b || ld(bc.face_grad_on + f)) {
         const double2 v1 = own ? ci : co, v2 = own ? co : ci;
-        const float vl = own ? wi : vo, vr = own ? vo : wi;
         const double f1x = v1.x - Xa.x, f1y = v1.y - Xa.y;
         const double f2x = Xb.x - v1.x, f2y = Xb.y - v1.y;
         const double f3x = v2.x - Xb.x, f3y = v2.y - Xb.y;
@@ -276,14 +302,18 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
         const double air = 0.5 * ((Xb.x - Xa.x) * (v2.y - v1.y) + (v1.x - v2.x) * (Xb.y - Xa.y));
         double n0 = Xa.y - Xb.y, n1 = Xb.x - Xa.x;
         if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
-        // Dxx n0 gx + Dyy n1 gy = sum_k t_k c_k with FP64-formed coefficients c_k
+        // Dxx n0 gx + Dyy n1 gy = sum_k c_k t_k, t = (vi1 + vl, vl + vi2, vi2 + vr, vr + vi1);
+        // regrouped per value: a1 vi1 + a2 vi2 + al vl + ar vr
         const double gxk = p.Dxx * n0 / (2 * air), gyk = p.Dyy * n1 / (2 * air);
-        const float c1 = (float)(gxk * f1y - gyk * f1x), c2 = (float)(gxk * f2y - gyk * f2x);
-        const float c3 = (float)(gxk * f3y - gyk * f3x), c4 = (float)(gxk * f4y - gyk * f4x);
+        const double c1 = gxk * f1y - gyk * f1x, c2 = gxk * f2y - gyk * f2x;
+        const double c3 = gxk * f3y - gyk * f3x, c4 = gxk * f4y - gyk * f4x;
+        const double a1 = c1 + c4, a2 = c2 + c3, al = c1 + c2, ar = c3 + c4;
+        const float ao = (float)(own ? ar : al);  // coefficient of the other side's value
+        const float sa = (float)(a1 + a2 + al + ar);
         const int ia = rev ? comp(vt, (j + 1) % 3) : comp(vt, j);
         const int ib = rev ? comp(vt, j) : comp(vt, (j + 1) % 3);
         const float vi1 = ld(wn + ia), vi2 = ld(wn + ib);
-        v = (vi1 + vl) * c1 + (vl + vi2) * c2 + (vi2 + vr) * c3 + (vr + vi1) * c4;
+        v = (float)a1 * (vi1 - wi) + (float)a2 * (vi2 - wi) + ao * (vo - wi) + sa * wi;
       }
       q[j] = own ? v : -v;
     }
@@ -301,6 +331,7 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
     const int sl = order_slot(code, k);
     if (pick3(nb.x, nb.y, nb.z, sl) < 0) res.add(pick3(cv[0], cv[1], cv[2], sl));
   }
+  res.add(wi * s4.w);  // w_i times the cell's signed u.n sum
   if (DIFF) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) res.add(pick3(q[0], q[1], q[2], order_slot(code, k)));
@@ -308,15 +339,16 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
   const double dt = *dt_dev;
   float inc = (float)(dt / ld(m.cell_volume + i)) * res.value();
   if (src) inc = fmaf((float)dt, ld(src + i), inc);
-  w_out[i] = wi + inc;
+  store_state(wi, inc, lo_in, w_out, lo_out, i);
 }
 
 template <bool ORDER2, bool DIFF>
 __global__ void __launch_bounds__(kBlock, MB_P2C_MIN_BLOCKS)
     k_f2c_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p, const float *__restrict__ w, float *__restrict__ w_out,
                  const float *__restrict__ sign, const float *__restrict__ src, const double *__restrict__ dt_dev,
-                 const float *__restrict__ rec, const float *__restrict__ wn) {
-  f2c_phase2<ORDER2, DIFF>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x);
+                 const float *__restrict__ rec, const float *__restrict__ wn, const float *__restrict__ lo_in,
+                 float *__restrict__ lo_out) {
+  f2c_phase2<ORDER2, DIFF>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, lo_in, lo_out, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- batches of triangle meshes
@@ -351,7 +383,8 @@ __global__ void __launch_bounds__(kBlock, MB_P2C_MIN_BLOCKS)
   if (!item_active(t, it.start_step, it.end_step)) return;
   const int par = (t - it.start_step) & 1;
   f2c_phase2<ORDER2, DIFF>(it.m, it.bc, it.p, it.w[par], it.w[par ^ 1], it.sign_cf, it.src, it.dt_dev,
-                           it.cell_scratch, it.node_scratch, (int)blockIdx.x - it.p2_begin);
+                           it.cell_scratch, it.node_scratch, it.lo[par], it.lo[par ^ 1],
+                           (int)blockIdx.x - it.p2_begin);
 }
 
 __global__ void k_clock_tick(int32_t *clock) { *clock += 1; }
@@ -447,7 +480,8 @@ template <bool ORDER2, bool DIFF>
 __global__ void __launch_bounds__(kBlock, 2)
     k_f3c_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p, const float *__restrict__ w, float *__restrict__ w_out,
                  const float *__restrict__ sign, const float *__restrict__ src, const double *__restrict__ dt_dev,
-                 const float *__restrict__ rec, const float *__restrict__ wn) {
+                 const float *__restrict__ rec, const float *__restrict__ wn, const float *__restrict__ lo_in,
+                 float *__restrict__ lo_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.nbcells) return;
   const GhostRuleF ghost = make_rule_f(m, bc, w);
@@ -495,17 +529,18 @@ __global__ void __launch_bounds__(kBlock, 2)
     }
     const float s = pick4v(s4.x, s4.y, s4.z, s4.w, j);
     const bool take_me = (s >= 0.f) == own;
-    float sol;
+    float dsol;  // upwind value minus w_i
     if (take_me) {
-      sol = ORDER2 ? wi + psii * (gxi * (float)(fc.x - ci.x) + gyi * (float)(fc.y - ci.y) + gzi * (float)(fc.z - ci.z))
-                   : wi;
+      dsol = ORDER2 ? psii * (gxi * (float)(fc.x - ci.x) + gyi * (float)(fc.y - ci.y) + gzi * (float)(fc.z - ci.z))
+                    : 0.f;
     } else if (b) {
-      sol = vo;
+      dsol = vo - wi;
     } else {
-      sol = ORDER2 ? vo + pso * (gxo * (float)(fc.x - co.x) + gyo * (float)(fc.y - co.y) + gzo * (float)(fc.z - co.z))
-                   : vo;
+      dsol = ORDER2 ? (vo - wi) + pso * (gxo * (float)(fc.x - co.x) + gyo * (float)(fc.y - co.y) +
+                                         gzo * (float)(fc.z - co.z))
+                    : vo - wi;
     }
-    const float F = s * sol;
+    const float F = s * dsol;
     cv[j] = own ? -F : F;
     if (DIFF) {
       float v = 0.f;
@@ -527,7 +562,7 @@ __global__ void __launch_bounds__(kBlock, 2)
                     cr = (float)(dot(DN, N) * rair);
         const float VA = ld(wn + comp(vt, i1)), VB = ld(wn + comp(vt, i2)), VC = ld(wn + comp(vt, i3));
         const float VL = own ? wi : vo, VR = own ? vo : wi;
-        v = ca * (VA - VC) + cb * (VB - VC) + cr * (VR - VL);
+        v = ca * (VA - VC) + cb * (VB - VC) + cr * (VR - VL);  // already differences
       }
       q[j] = own ? v : -v;
     }
@@ -544,6 +579,7 @@ __global__ void __launch_bounds__(kBlock, 2)
     const int sl = order_slot(code, k);
     if (pick4v(nb.x, nb.y, nb.z, nb.w, sl) < 0) res.add(pick4v(cv[0], cv[1], cv[2], cv[3], sl));
   }
+  res.add(wi * ld(sign + 4 * nc + i));  // w_i times the cell's signed u.n sum
   if (DIFF) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) res.add(pick4v(q[0], q[1], q[2], q[3], order_slot(code, k)));
@@ -551,20 +587,43 @@ __global__ void __launch_bounds__(kBlock, 2)
   const double dt = *dt_dev;
   float inc = (float)(dt / ld(m.cell_volume + i)) * res.value();
   if (src) inc = fmaf((float)dt, ld(src + i), inc);
-  w_out[i] = wi + inc;
+  store_state(wi, inc, lo_in, w_out, lo_out, i);
+}
+
+// FP32 u.n per cell face and, in FP64 then rounded, the cell's signed sum of them
+// (minus for the faces the cell owns, which the residual subtracts)
+__global__ void __launch_bounds__(kBlock) k_sign_f32c(mb_mesh m, const double *__restrict__ s64,
+                                                      float *__restrict__ s32) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const uint32_t fl = ld(m.cell_flags + i);
+  double div = 0.;
+  for (int j = 0; j < m.nlf; ++j) {
+    const double s = ld(s64 + 4 * (long long)i + j);
+    const bool own = m.dim == 2 ? f2_own(fl, j) : ((fl >> (6 * j)) & 1u);
+    div += own ? -s : s;
+    s32[4 * (long long)i + j] = (float)s;
+  }
+  if (m.dim == 2)
+    s32[4 * (long long)i + 3] = (float)div;
+  else
+    s32[4 * (long long)m.nbcells + i] = (float)div;
 }
 
 template <bool O2, bool DF>
 int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const float *w_in, float *w_out,
-                     const float *sign, const float *src, const double *dt, float *cs, float *wn, cudaStream_t st) {
+                     const float *sign, const float *src, const double *dt, float *cs, float *wn, const float *lo_in,
+                     float *lo_out, cudaStream_t st) {
   const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
   if (m.dim == 2) {
     if (ncb + nnb > 0) k_f2c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
-    k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn);
+    k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
+                                                                           lo_in, lo_out);
   } else {
     if (ncb + nnb > 0) k_f3c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
-    k_f3c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn);
+    k_f3c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
+                                                                           lo_in, lo_out);
   }
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }
@@ -574,10 +633,12 @@ int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params 
 using namespace mb;
 
 extern "C" int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
-                                    const float *w_in, float *w_out, const float *sign_cf, const float *src,
-                                    const double *dt_dev, float *cell_scratch, float *node_scratch, void *stream) {
+                                    const float *w_in, float *w_out, const float *lo_in, float *lo_out,
+                                    const float *sign_cf, const float *src, const double *dt_dev, float *cell_scratch,
+                                    float *node_scratch, void *stream) {
   if (!m || !bc || !p || !w_in || !w_out || !sign_cf || !dt_dev || w_in == w_out) return MB_EINVAL;
   if (m->dim != 2 && m->dim != 3) return MB_EINVAL;
+  if ((lo_in == nullptr) != (lo_out == nullptr) || (lo_in && lo_in == lo_out)) return MB_EINVAL;
   if (!(m->cell_vtx && m->cell_nbr && m->cell_flags && m->node_coord && m->cell_xy && m->lsq_sell_ptr &&
         m->lsq_sell_idx && m->n2c_sell_ptr && m->n2c_sell_idx && m->n2c_sell_alpha_f32))
     return MB_EINVAL;
@@ -585,14 +646,14 @@ extern "C" int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_
   if (p->order != 1 && !o2) return MB_EINVAL;
   if ((o2 && !cell_scratch) || (df && !node_scratch) || (df && !bc->face_grad_on)) return MB_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
-  if (o2 && df) return launch_step_f32c<true, true>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch,
-                                                    node_scratch, st);
-  if (o2) return launch_step_f32c<true, false>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch,
-                                               node_scratch, st);
-  if (df) return launch_step_f32c<false, true>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch,
-                                               node_scratch, st);
-  return launch_step_f32c<false, false>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch,
-                                        st);
+#define MB_F32C(O, D) \
+  return launch_step_f32c<O, D>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, lo_in, \
+                                lo_out, st)
+  if (o2 && df) MB_F32C(true, true);
+  if (o2) MB_F32C(true, false);
+  if (df) MB_F32C(false, true);
+  MB_F32C(false, false);
+#undef MB_F32C
 }
 
 extern "C" int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const int32_t *p1_map, int32_t p1_blocks,
@@ -615,5 +676,11 @@ extern "C" int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const in
     k_f2c_batch_phase2<false, false><<<p2_blocks, kBlock, 0, st>>>(items, p2_map, clock);
   }
   k_clock_tick<<<1, 1, 0, st>>>(clock);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+extern "C" int mb_cell_face_sign_f32c(const mb_mesh *m, const double *sign_cf, float *sign_f32, void *stream) {
+  if (!m || !sign_cf || !sign_f32 || !m->cell_flags || (m->dim != 2 && m->dim != 3)) return MB_EINVAL;
+  k_sign_f32c<<<ceil_div(m->nbcells, kBlock), kBlock, 0, (cudaStream_t)stream>>>(*m, sign_cf, sign_f32);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }

@@ -133,13 +133,15 @@ class _Slot:
             up = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(dev, non_blocking=True) for a in init]
             if req.kind == "advdiff":
                 self.w = [up[0].float(), torch.empty(nc, dtype=f32, device=dev)]
+                self.lo = [(up[0] - self.w[0].double()).float(), torch.empty(nc, dtype=f32, device=dev)]
                 uf = torch.full((nf,), req.ux, dtype=torch.float64, device=dev)
                 vf = torch.full((nf,), req.uy, dtype=torch.float64, device=dev)
                 zf = torch.zeros(nf, dtype=torch.float64, device=dev)
                 sign = torch.empty(4 * nc, dtype=torch.float64, device=dev)
                 st = stream.cuda_stream
                 _lib.call("mb_cell_face_sign", self.dm.struct, _p(uf), _p(vf), _p(zf), _p(sign), st)
-                self.sign = sign.float()
+                self.sign = torch.empty(4 * nc, dtype=f32, device=dev)
+                _lib.call("mb_cell_face_sign_f32c", self.dm.struct, _p(sign), _p(self.sign), st)
                 uc = torch.full((nc,), req.ux, dtype=torch.float64, device=dev)
                 vc = torch.full((nc,), req.uy, dtype=torch.float64, device=dev)
                 zc = torch.zeros(nc, dtype=torch.float64, device=dev)
@@ -166,7 +168,7 @@ class _Slot:
 
     def _tensors(self):
         if self.req.kind == "advdiff":
-            return self.w + [self.sign, self.dt, self.cs, self.ns]
+            return self.w + self.lo + [self.sign, self.dt, self.cs, self.ns]
         return self.q[0] + self.q[1] + [self.Z, self.ff, self.dt]
 
     def blocks(self):
@@ -180,7 +182,7 @@ class _Slot:
         """Final state (device tensors, device numbering): [w] or [h, hu, hv]."""
         par = (self.end - self.start) & 1
         if self.req.kind == "advdiff":
-            return [self.w[par]]
+            return [self.w[par].double() + self.lo[par].double()]
         return self.q[par][:3]
 
 
@@ -226,6 +228,7 @@ class BatchServer:
                     it = items[k]
                     it.m, it.bc, it.p = s.dm.struct, s.bc.struct, s.params
                     it.w[0], it.w[1] = _p(s.w[0]), _p(s.w[1])
+                    it.lo[0], it.lo[1] = _p(s.lo[0]), _p(s.lo[1])
                     it.sign_cf, it.src, it.dt_dev = _p(s.sign), None, _p(s.dt)
                     it.cell_scratch, it.node_scratch = _p(s.cs), _p(s.ns)
                     it.start_step, it.end_step = s.start, s.end
@@ -295,6 +298,36 @@ class BatchServer:
         else:
             for _ in range(nsteps):
                 self._launch_step(tabs, self.stream.cuda_stream)
+
+    # -------------------------------------------------------------- resident batch
+    def run_resident(self, requests, steps, warmup=3):
+        """Admit all ``requests`` at once (prepared beforehand), then time ``steps`` batch
+        steps on the device with CUDA events.  Returns (cell-updates per second, seconds)."""
+        if self.workers > 0:
+            with cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn")) as pool:
+                prepared = list(pool.map(prepare, requests))
+        else:
+            prepared = [prepare(r) for r in requests]
+        for req, dm, bc, init in prepared:
+            slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream)
+            self.stream.wait_event(slot.ready)
+            slot.fam = 0 if req.kind == "advdiff" else 1
+            slot.start, slot.end = self.clock_host[slot.fam], 1 << 30
+            slot.admitted = 0.0
+            self.active[req.rid] = slot
+        self._retable()
+        self._run_chunk(warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        for _ in range(steps // self.chunk):
+            self._run_chunk(self.chunk)
+        if steps % self.chunk:
+            self._run_chunk(steps % self.chunk)
+        e1.record(self.stream)
+        torch.cuda.synchronize(self.dev)
+        sec = e0.elapsed_time(e1) / 1e3
+        cu = sum(s.dm.nbcells for s in self.active.values()) * steps
+        return cu / sec, sec
 
     # -------------------------------------------------------------- serving loop
     def serve(self, requests, keep_results=False, log=None):

@@ -271,19 +271,29 @@ class AdvectionDiffusionSolver:
         dm = self._dm
         if self._w32 is None:
             self._w32 = [torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device) for _ in range(2)]
+            # rounding errors of the FP32 state (w + lo carries the state to ~48 bits)
+            self._lo32 = [torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device) for _ in range(2)]
             nrec = (4 if dm.dim == 2 else 5) * dm.nbcells
             self._cs32 = torch.empty(nrec, dtype=torch.float32, device=dm.device)
             self._ns32 = torch.empty(dm.nbnodes, dtype=torch.float32, device=dm.device)
-            self._sign32 = torch.empty(4 * dm.nbcells, dtype=torch.float32, device=dm.device)
+            self._sign32 = torch.empty((4 if dm.dim == 2 else 5) * dm.nbcells, dtype=torch.float32,
+                                       device=dm.device)
         if var.version("cell") != self._w32_key:
-            self._w32[self._w32_i].copy_(var.dev("cell"))
+            w64 = var.dev("cell")
+            hi = self._w32[self._w32_i]
+            hi.copy_(w64)
+            self._lo32[self._w32_i].copy_(w64 - hi.double())
             self._w32_key = var.version("cell")
         return self._w32[self._w32_i]
+
+    def _f64_of(self, k):
+        """FP64 value of FP32 state buffer ``k`` (w + lo)."""
+        return self._w32[k].double() + self._lo32[k].double()
 
     def _f32_inputs(self):
         self._update_sign()
         if self._sign32_key != self._sign_key:
-            self._sign32.copy_(self._sign)
+            _lib.call("mb_cell_face_sign_f32c", self._dm.struct, _p(self._sign), _p(self._sign32), self._stream())
             self._sign32_key = self._sign_key
         var = self.var
         if var.version("source") == 0:
@@ -293,30 +303,35 @@ class AdvectionDiffusionSolver:
             self._src32_key = var.version("source")
         return self._src32
 
-    def _f32_publish(self, w_prev):
-        """Make the FP32 result the variable's cell array (converted on first read)."""
+    def _f32_publish(self, prev):
+        """Make the FP32 result the variable's cell array (converted on first read);
+        ``prev``: the buffer index holding the step's input."""
         var = self.var
-        cur = self._w32[self._w32_i]
+        cur = self._w32_i
 
-        def materialise(buf=cur):
-            var._s.dev["cell"].copy_(buf)
+        def materialise(k=cur):
+            var._s.dev["cell"].copy_(self._f64_of(k))
 
         var._s.lazy.pop("cell", None)  # the previous result, superseded
         var._s.version["cell"] += 1
         var.set_lazy("cell", materialise)
         self._w32_key = var.version("cell")
-        self._install_lazies(lambda buf=w_prev: buf.double())
+        self._install_lazies(lambda k=prev: self._f64_of(k))
 
-    def _call_f32c(self, x, y, src, st):
-        _lib.call("mb_advdiff_step_f32c", self._dm.struct, self.var.device_bc.struct, self._params, _p(x), _p(y),
-                  _p(self._sign32), _p(src), _p(self._dt_dev), _p(self._cs32), _p(self._ns32), st)
+    def _call_f32c(self, k, src, st):
+        """One step from buffer k into buffer 1 - k."""
+        w, lo = self._w32, self._lo32
+        _lib.call("mb_advdiff_step_f32c", self._dm.struct, self.var.device_bc.struct, self._params, _p(w[k]),
+                  _p(w[1 - k]), _p(lo[k]), _p(lo[1 - k]), _p(self._sign32), _p(src), _p(self._dt_dev),
+                  _p(self._cs32), _p(self._ns32), st)
 
     def _fused_step_f32c(self):
-        w_in = self._f32_state()
+        self._f32_state()
         src = self._f32_inputs()
-        self._call_f32c(w_in, self._w32[1 - self._w32_i], src, self._stream())
-        self._w32_i = 1 - self._w32_i
-        self._f32_publish(w_in)
+        k = self._w32_i
+        self._call_f32c(k, src, self._stream())
+        self._w32_i = 1 - k
+        self._f32_publish(k)
 
     def launches_per_step(self):
         """Kernel launches of one fused step."""
@@ -382,21 +397,20 @@ class AdvectionDiffusionSolver:
         src = self._f32_inputs()
         self.var.device_bc  # built (and uploaded) before any capture
         if self._graph is None or self._graph_src != _p(src):
-            a, b = self._w32
             s = torch.cuda.Stream(device=self._dm.device)
             s.wait_stream(torch.cuda.current_stream(self._dm.device))
             g = torch.cuda.CUDAGraph()
             with torch.cuda.stream(s):
                 with torch.cuda.graph(g, stream=s):
                     st = torch.cuda.current_stream(self._dm.device).cuda_stream
-                    self._call_f32c(a, b, src, st)
-                    self._call_f32c(b, a, src, st)
+                    self._call_f32c(0, src, st)
+                    self._call_f32c(1, src, st)
             torch.cuda.current_stream(self._dm.device).wait_stream(s)
             self._graph, self._graph_src = g, _p(src)
         for _ in range(n // 2):
             self._graph.replay()
         if n // 2:
-            self._f32_publish(self._w32[1])
+            self._f32_publish(1)
         if n % 2:
             self._fused_step_f32c()
 

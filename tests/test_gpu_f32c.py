@@ -1,10 +1,11 @@
 """FP32-compensated advection-diffusion step (``precision="fp32c"``) against the FP64 oracle.
 
 Stated tolerances (relative, over all cells, after the whole run):
-L2 = ||w - w_ref||_2 / ||w_ref||_2 <= 2e-6 and Linf = max|w - w_ref| / max|w_ref| <= 1e-5.
-The FP32 state is rounded once per step (half an ulp, 6e-8 relative), so the
-error grows like a random walk over the steps; the compensated face sums keep
-the residual itself at FP32 rounding.
+L2 = ||w - w_ref||_2 / ||w_ref||_2 <= 1e-7 and Linf = max|w - w_ref| / max|w_ref| <= 2e-7.
+The state is FP32 plus its FP32 rounding error (the update is an exact two-sum), so no
+increment is lost from step to step; what remains is FP32 rounding of each step's
+residual, evaluated on differences from the cell's own value with compensated face
+sums (measured: 5e-9 L2 after 1,003 steps of the 2,000,000-cell C2 run).
 """
 import numpy as np
 import pytest
@@ -15,8 +16,8 @@ from manapy_b200 import boundary as B, geometry as G, workloads as W
 import oracle as O
 
 pytestmark = pytest.mark.gpu
-L2_TOL = 2e-6
-LINF_TOL = 1e-5
+L2_TOL = 1e-7
+LINF_TOL = 2e-7
 
 
 def rel_l2(a, b):
