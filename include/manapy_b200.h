@@ -271,10 +271,12 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
  * ghosts: FP32 state (q_in, q_out: h, hu, hv, hc, Z), FP32 SRNH flux arithmetic and face
  * fluxes (face_flux [nbfaces][4] floats), residuals summed per cell with compensated
  * (Neumaier) summation; normals come from face_nm_f32; the bathymetry source, dt_cur and
- * dt_next (time_step_SW of the updated state) are FP64. */
-int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5], double cfl,
-                    double grav, int32_t order, float *face_flux, const double *dt_cur, double *dt_next,
-                    void *stream);
+ * dt_next (time_step_SW of the updated state) are FP64.  lo_in / lo_out (4 FP32 arrays each
+ * for h, hu, hv, hc, or both NULL) carry the rounding error of the state: q_out + lo_out =
+ * q_in + (increment + lo_in) exactly. */
+int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
+                    const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
+                    int32_t order, float *face_flux, const double *dt_cur, double *dt_next, void *stream);
 
 /* ---- batches of independent triangle meshes (serving) ----------------------------------
  *
@@ -317,6 +319,7 @@ int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const int32_t *p1_m
 typedef struct mb_sw_item {
   mb_mesh m;                /* compact 2D tables and face_nm_f32 required */
   float *q[2][4];           /* ping-pong FP32 h, hu, hv, hc; step t reads q[(t - start_step) & 1] */
+  float *lo[2][4];          /* their rounding errors (all NULL: plain FP32 state) */
   const float *Z;           /* bed, FP32 */
   float *face_flux;         /* [nbfaces][4] scratch */
   double *dt;               /* [2]: step t uses dt[(t - start_step) & 1] and writes the next step's dt

@@ -55,7 +55,7 @@ class MbAdvDiffItem(ctypes.Structure):
 
 
 class MbSwItem(ctypes.Structure):
-    _fields_ = [("m", MbMesh), ("q", (_vp * 4) * 2), ("Z", _vp), ("face_flux", _vp), ("dt", _vp),
+    _fields_ = [("m", MbMesh), ("q", (_vp * 4) * 2), ("lo", (_vp * 4) * 2), ("Z", _vp), ("face_flux", _vp), ("dt", _vp),
                 ("cfl", _d), ("grav", _d), ("start_step", _i32), ("end_step", _i32), ("f_begin", _i32),
                 ("c_begin", _i32)]
 
@@ -89,7 +89,7 @@ _SIGS = {
     "mb_cell_face_sign_f32c": [_M, _vp, _vp, _vp],
     "mb_advdiff_step_f32c": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                              _vp, _vp],
-    "mb_sw_step_f32c": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp],
+    "mb_sw_step_f32c": [_M, _P5, _P5, _P4, _P4, _d, _d, _i32, _vp, _vp, _vp, _vp],
     "mb_advdiff_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],

@@ -101,11 +101,27 @@ __device__ __forceinline__ void srnh_f32(float hu_l, float hu_r, float hv_l, flo
 }
 
 struct SWStateF {
-  const float *q[5];  // h, hu, hv, hc, Z
+  const float *q[5];   // h, hu, hv, hc, Z
+  const float *lo[4];  // rounding errors of h, hu, hv, hc (all NULL: plain FP32 state)
 };
 struct SWOutF {
   float *q[5];
+  float *lo[4];
 };
+
+// (q, lo) + inc -> (q', lo') with q' + lo' = q + (inc + lo) exactly (Knuth's two-sum)
+__device__ __forceinline__ float sw_store(float q, float inc, const float *lo_in, float *lo_out, float *q_out, int i) {
+  if (!lo_in) {
+    q_out[i] = q + inc;
+    return q_out[i];
+  }
+  const float a = inc + lo_in[i];
+  const float s = q + a;
+  const float bv = s - q;
+  lo_out[i] = (q - (s - bv)) + (a - bv);
+  q_out[i] = s;
+  return s;
+}
 
 __device__ __forceinline__ void sw2c_face(const mb_mesh &m, const SWStateF &s, float grav, float *ff, double *dt_next,
                                           int f) {
@@ -218,14 +234,10 @@ __device__ __forceinline__ double sw2c_cell_body(const mb_mesh &m, const SWState
   const float shu = (float)(-grav * (s1x + s2x + s3x));
   const float shv = (float)(-grav * (s1y + s2y + s3y));
   const float k = (float)(dt / vol);
-  const float h_n = h_i + k * rez[0].value();
-  const float hu_n = hu_i + k * (rez[1].value() + shu);
-  const float hv_n = hv_i + k * (rez[2].value() + shv);
-  const float hc_n = hc_i + k * rez[3].value();
-  out.q[0][i] = h_n;
-  out.q[1][i] = hu_n;
-  out.q[2][i] = hv_n;
-  out.q[3][i] = hc_n;
+  const float h_n = sw_store(h_i, k * rez[0].value(), s.lo[0], out.lo[0], out.q[0], i);
+  const float hu_n = sw_store(hu_i, k * (rez[1].value() + shu), s.lo[1], out.lo[1], out.q[1], i);
+  const float hv_n = sw_store(hv_i, k * (rez[2].value() + shv), s.lo[2], out.lo[2], out.q[2], i);
+  sw_store(hc_i, k * rez[3].value(), s.lo[3], out.lo[3], out.q[3], i);
   if (out.q[4] != s.q[4]) out.q[4][i] = Z_i;
   if (!want_dt) return 1e300;
   const double hn = h_n, un = hu_n / hn, vn = hv_n / hn;
@@ -260,7 +272,7 @@ __global__ void __launch_bounds__(kBlock) k_sw2c_batch_flux(const mb_sw_item *__
   const int t = *clock;
   if (t < it.start_step || t >= it.end_step) return;
   const int par = (t - it.start_step) & 1;
-  SWStateF s{{it.q[par][0], it.q[par][1], it.q[par][2], it.q[par][3], it.Z}};
+  SWStateF s{{it.q[par][0], it.q[par][1], it.q[par][2], it.q[par][3], it.Z}, {}};
   sw2c_face(it.m, s, (float)it.grav, it.face_flux, it.dt + (par ^ 1),
             ((int)blockIdx.x - it.f_begin) * blockDim.x + threadIdx.x);
 }
@@ -272,8 +284,10 @@ __global__ void __launch_bounds__(kBlock) k_sw2c_batch_cell(const mb_sw_item *__
   const int t = *clock;
   if (t < it.start_step || t >= it.end_step) return;  // uniform over the block
   const int par = (t - it.start_step) & 1;
-  SWStateF s{{it.q[par][0], it.q[par][1], it.q[par][2], it.q[par][3], it.Z}};
-  SWOutF out{{it.q[par ^ 1][0], it.q[par ^ 1][1], it.q[par ^ 1][2], it.q[par ^ 1][3], const_cast<float *>(it.Z)}};
+  SWStateF s{{it.q[par][0], it.q[par][1], it.q[par][2], it.q[par][3], it.Z},
+             {it.lo[par][0], it.lo[par][1], it.lo[par][2], it.lo[par][3]}};
+  SWOutF out{{it.q[par ^ 1][0], it.q[par ^ 1][1], it.q[par ^ 1][2], it.q[par ^ 1][3], const_cast<float *>(it.Z)},
+             {it.lo[par ^ 1][0], it.lo[par ^ 1][1], it.lo[par ^ 1][2], it.lo[par ^ 1][3]}};
   const int i = ((int)blockIdx.x - it.c_begin) * blockDim.x + threadIdx.x;
   double best = 1e300;
   if (i < it.m.nbcells) best = sw2c_cell_body(it.m, s, out, it.face_flux, it.dt[par], true, it.cfl, it.grav, i);
@@ -287,9 +301,9 @@ __global__ void __launch_bounds__(kBlock) k_sw2c_batch_cell(const mb_sw_item *__
 
 using namespace mb;
 
-extern "C" int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5], double cfl,
-                               double grav, int32_t order, float *face_flux, const double *dt_cur, double *dt_next,
-                               void *stream) {
+extern "C" int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
+                               const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
+                               int32_t order, float *face_flux, const double *dt_cur, double *dt_next, void *stream) {
   if (!m || m->dim != 2 || m->nlf != 3 || m->nbcells <= 0 || m->nbfaces <= 0) return MB_EINVAL;
   if (!q_in || !q_out || !face_flux || !dt_cur || dt_next == dt_cur || order != 1) return MB_EINVAL;
   if (!m->cell_cellfid || !m->cell_vtx || !m->cell_nbr || !m->cell_flags || !m->node_coord || !m->cell_xy ||
@@ -301,6 +315,14 @@ extern "C" int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], flo
     if (!q_in[k] || !q_out[k] || (k < 4 && q_in[k] == q_out[k])) return MB_EINVAL;
     s.q[k] = q_in[k];
     out.q[k] = q_out[k];
+  }
+  if ((lo_in == nullptr) != (lo_out == nullptr)) return MB_EINVAL;
+  if (lo_in) {
+    for (int k = 0; k < 4; ++k) {
+      if (!lo_in[k] || !lo_out[k] || lo_in[k] == lo_out[k]) return MB_EINVAL;
+      s.lo[k] = lo_in[k];
+      out.lo[k] = lo_out[k];
+    }
   }
   cudaStream_t st = (cudaStream_t)stream;
   k_sw2c_flux<<<ceil_div(m->nbfaces, kBlock), kBlock, 0, st>>>(*m, s, (float)grav, face_flux, dt_next);

@@ -154,6 +154,8 @@ class _Slot:
             else:
                 q = [up[k].float() for k in range(4)]
                 self.q = [q, [torch.empty(nc, dtype=f32, device=dev) for _ in range(4)]]
+                self.lo = [[(up[k] - q[k].double()).float() for k in range(4)],
+                           [torch.empty(nc, dtype=f32, device=dev) for _ in range(4)]]
                 self.Z = up[4].float()
                 self.ff = torch.empty(4 * nf, dtype=f32, device=dev)
                 self.dt = torch.empty(2, dtype=torch.float64, device=dev)
@@ -169,7 +171,7 @@ class _Slot:
     def _tensors(self):
         if self.req.kind == "advdiff":
             return self.w + self.lo + [self.sign, self.dt, self.cs, self.ns]
-        return self.q[0] + self.q[1] + [self.Z, self.ff, self.dt]
+        return self.q[0] + self.q[1] + self.lo[0] + self.lo[1] + [self.Z, self.ff, self.dt]
 
     def blocks(self):
         nc = self.dm.nbcells
@@ -183,7 +185,7 @@ class _Slot:
         par = (self.end - self.start) & 1
         if self.req.kind == "advdiff":
             return [self.w[par].double() + self.lo[par].double()]
-        return self.q[par][:3]
+        return [self.q[par][c].double() + self.lo[par][c].double() for c in range(3)]
 
 
 class BatchServer:
@@ -250,6 +252,7 @@ class BatchServer:
                     for par in range(2):
                         for c in range(4):
                             it.q[par][c] = _p(s.q[par][c])
+                            it.lo[par][c] = _p(s.lo[par][c])
                     it.Z, it.face_flux, it.dt = _p(s.Z), _p(s.ff), _p(s.dt)
                     it.cfl, it.grav = 0.5, 9.81
                     it.start_step, it.end_step = s.start, s.end

@@ -671,10 +671,16 @@ class ShallowWaterSolver:
         if self._q32 is None:
             mk = lambda: torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device)  # noqa: E731
             self._q32 = [[mk() for _ in range(4)], [mk() for _ in range(4)], mk()]
+            self._lo32 = [[mk() for _ in range(4)], [mk() for _ in range(4)]]  # rounding errors
             self._ff32 = torch.empty(4 * dm.nbfaces, dtype=torch.float32, device=dm.device)
         if self._keys() != self._q32_key:
-            for t, k in zip(self._q32[self._q32_i] + [self._q32[2]], self._NAMES):
-                t.copy_(self.varbs[k].dev("cell"))
+            k = self._q32_i
+            for c, name in enumerate(self._NAMES):
+                w64 = self.varbs[name].dev("cell")
+                t = self._q32[k][c] if c < 4 else self._q32[2]
+                t.copy_(w64)
+                if c < 4:
+                    self._lo32[k][c].copy_(w64 - t.double())
             self._q32_key = self._keys()
         return self._q32[self._q32_i], self._q32[2]
 
@@ -683,15 +689,17 @@ class ShallowWaterSolver:
         qout = self._q32[1 - self._q32_i]
         cur = self._use_dt()
         nxt = self._dt_buf[1 - self._cur:2 - self._cur]
+        k0 = self._q32_i
         _lib.call("mb_sw_step_f32c", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
-                  _lib.p5([_p(t) for t in qout] + [_p(z)]), float(self.cfl), float(self.grav), int(self.order),
+                  _lib.p5([_p(t) for t in qout] + [_p(z)]), _lib.p4([_p(t) for t in self._lo32[k0]]),
+                  _lib.p4([_p(t) for t in self._lo32[1 - k0]]), float(self.cfl), float(self.grav), int(self.order),
                   _p(self._ff32), _p(cur), _p(nxt), self._stream())
-        self._q32_i = 1 - self._q32_i
-        for k, buf in zip(self._NAMES[:4], qout):
+        self._q32_i = 1 - k0
+        for k, buf, lo in zip(self._NAMES[:4], qout, self._lo32[1 - k0]):
             var = self.varbs[k]
 
-            def materialise(var=var, buf=buf):
-                var._s.dev["cell"].copy_(buf)
+            def materialise(var=var, buf=buf, lo=lo):
+                var._s.dev["cell"].copy_(buf.double() + lo.double())
 
             var._s.lazy.pop("cell", None)  # the previous result, superseded
             var._s.version["cell"] += 1
@@ -705,7 +713,7 @@ class ShallowWaterSolver:
         """FP64 sum of volume x h over the cells (no counterpart in manapy)."""
         dm = self._setup()
         if self.precision == "fp32c" and self._q32 is not None and self._keys() == self._q32_key:
-            h = self._q32[self._q32_i][0].double()
+            h = self._q32[self._q32_i][0].double() + self._lo32[self._q32_i][0].double()
         else:
             h = self.h.dev("cell")
         return float(torch.dot(h, dm.t["cell_volume"]).item())
