@@ -33,6 +33,7 @@ def build(verbose=False, force=False):
     if not force and os.path.exists(OUT):
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(s) <= t for s in srcs + hdrs + [os.path.abspath(__file__)]):
+            build_host()
             return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     objdir = os.path.join(HERE, "lib", "obj")
@@ -50,7 +51,26 @@ def build(verbose=False, force=False):
         objs = list(ex.map(compile_one, srcs))
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", OUT + ".tmp", *objs], check=True)
     os.replace(OUT + ".tmp", OUT)
+    build_host(force=force)
     return OUT
+
+
+HOST_OUT = os.path.join(HERE, "lib", "libmanapy_b200_host.so")
+
+
+def build_host(force=False):
+    """The native host mesh builder (``host/*.cpp``, C++17, no GPU code)."""
+    srcs = sorted(glob.glob(os.path.join(HERE, "host", "*.cpp")))
+    if not force and os.path.exists(HOST_OUT):
+        t = os.path.getmtime(HOST_OUT)
+        if all(os.path.getmtime(s) <= t for s in srcs + [os.path.abspath(__file__)]):
+            return HOST_OUT
+    os.makedirs(os.path.dirname(HOST_OUT), exist_ok=True)
+    cxx = shutil.which("g++") or "g++"
+    subprocess.run([cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-o", HOST_OUT + ".tmp", *srcs],
+                   check=True)
+    os.replace(HOST_OUT + ".tmp", HOST_OUT)
+    return HOST_OUT
 
 
 if __name__ == "__main__":

@@ -202,6 +202,33 @@ class DeviceMesh:
         self.reordered = bool(reorder)
         self.struct = self._make_struct() if dev is not None else None
 
+    @classmethod
+    def from_native(cls, elements, vertex, device=None, reorder=True):
+        """The tables of a 2D triangle mesh from the native host builder (``native.tables2d``),
+        bit-identical to ``DeviceMesh(geometry.build(...))``; ``A`` then holds only the
+        manapy-numbered arrays the boundary set-up reads."""
+        from types import SimpleNamespace
+        from . import native
+        T = native.tables2d(elements, vertex, reorder=reorder)
+        self = cls.__new__(cls)
+        nc, nf, nn = len(T["cell_volume"]), len(T["face_name"]), len(T["node_coord"])
+        self.dim, self.nbcells, self.nbfaces, self.nbnodes, self.nlf = 2, nc, nf, nn, 3
+        self.A = {"dim": 2, "nbcells": nc, "nbfaces": nf, "nbnodes": nn}
+        for k in [k for k in T if k.startswith("A.")]:
+            self.A[k[2:]] = T.pop(k)
+        perm = {kind: T.pop("perm_" + kind) for kind in ("cell", "face", "node")}
+        inv = {kind: T.pop("inv_" + kind) for kind in ("cell", "face", "node")}
+        self.R = SimpleNamespace(cperm=perm["cell"], fperm=perm["face"], nperm=perm["node"], cinv=inv["cell"],
+                                 finv=inv["face"], ninv=inv["node"], enabled=bool(reorder))
+        self.reordered = bool(reorder)
+        dev = torch.device(device) if device is not None else None
+        self.device = dev
+        self.t = {k: _t(v, v.dtype, dev) for k, v in T.items()}
+        self.perm = {k: _t(v, np.int64, dev) for k, v in perm.items()}
+        self.inv = {k: _t(v, np.int64, dev) for k, v in inv.items()}
+        self.struct = self._make_struct() if dev is not None else None
+        return self
+
     def _make_struct(self):
         s = _lib.MbMesh()
         s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = (self.dim, self.nbcells, self.nbfaces,

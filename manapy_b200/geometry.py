@@ -314,7 +314,10 @@ def build(elements, vertex, dim, need_cellnid=True):
     A["boundaryfaces"] = np.sort(np.concatenate(lists)).astype(I32)
     A["halofaces"] = np.zeros(0, dtype=I32)
     A["periodicboundaryfaces"] = np.zeros(0, dtype=I32)
-    unmatched = boundary_mask & (name >= 100)
+    # boundary faces that belong to no side: names 100/200 (manapy leaves them out of every
+    # list), and name 0 (all vertices untagged: manapy would treat them as inner faces
+    # reading cell -1)
+    unmatched = boundary_mask & ((name >= 100) | (name == 0))
     A["unmatched_boundary_faces"] = np.nonzero(unmatched)[0].astype(I32)
 
     # ---- ghost centres, ddm_utils2d.py:172-187 / ddm_utils3d.py:96-118

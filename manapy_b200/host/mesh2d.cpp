@@ -1,0 +1,624 @@
+// Native host builder of the device tables of a 2D triangle mesh.
+//
+// One pass from (elements, vertex) -- the layout of manapy's per-rank mesh files
+// (manapy/ddm/pure_ddm.py:21-33) -- to every table the CUDA kernels read, in
+// the locality numbering, without building manapy's Domain arrays first.  It
+// computes the same numbers as the vectorised Python path (geometry.build +
+// DeviceMesh), operation for operation, so its output is bit-identical to it:
+//
+//   cell centres / volumes           manapy/ddm/ddm_utils2d.py:433-452
+//   node -> cells, vertex neighbours ddm_utils2d.py:55-97
+//   faces (unique descending node pairs, numbered in ascending order), cell -> face,
+//   face -> cells, face neighbours   manapy/ddm/domain.py:313-315, ddm_utils2d.py:12-53
+//   face names, normals, areas       ddm_utils2d.py:507-551
+//   outward normals per cell         ddm_utils2d.py:99-120
+//   ghost centres, node -> ghosts    ddm_utils2d.py:163-197, 122-161
+//   centre -> vertex weights         ddm_utils2d.py:608-705, manapy/ast/functions2d.py:219
+//   diamond vectors, areas           ddm_utils2d.py:553-605
+//   orthogonal distances             ddm_utils2d.py:716-744
+//
+// then the Morton / face / node renumbering and the compact, SELL-32 and FP32
+// tables.  Compiled with -ffp-contract=off: every operation rounds as written.
+//
+// C ABI: mbh_build2d() returns a handle holding named tables (dtype, shape, bytes);
+// mbh_count / mbh_info / mbh_data read them; mbh_free releases the handle.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace {
+
+using i32 = int32_t;
+using i64 = int64_t;
+
+struct Table {
+  std::string name;
+  char dtype;  // 'i' int32, 'l' int64, 'd' float64, 'f' float32, 'b' uint8
+  std::vector<i64> shape;
+  std::vector<unsigned char> bytes;
+};
+
+struct Result {
+  std::vector<Table> tables;
+  std::string error;
+  template <class T>
+  void add(const std::string &name, char dt, std::vector<i64> shape, const std::vector<T> &v) {
+    Table t;
+    t.name = name;
+    t.dtype = dt;
+    t.shape = std::move(shape);
+    t.bytes.resize(v.size() * sizeof(T));
+    if (!v.empty()) std::memcpy(t.bytes.data(), v.data(), t.bytes.size());
+    tables.push_back(std::move(t));
+  }
+};
+
+// CSR from (key, value) pairs grouped by key in [0, n), values kept in input order (a
+// stable counting sort, as numpy's stable argsort of the keys)
+void group_csr(const std::vector<i64> &key, const std::vector<i64> &val, i64 n, std::vector<i64> &ptr,
+               std::vector<i64> &idx) {
+  ptr.assign(n + 1, 0);
+  for (i64 k : key) ptr[k + 1]++;
+  for (i64 i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+  idx.resize(key.size());
+  std::vector<i64> pos(ptr.begin(), ptr.end() - 1);
+  for (size_t e = 0; e < key.size(); ++e) idx[pos[key[e]]++] = val[e];
+}
+
+// for each row r: sorted unique union of the lists of its items (CSR), optionally without r
+void ragged_union(i64 nrows, const std::vector<i64> &row_items_ptr, const std::vector<i64> &row_items,
+                  const std::vector<i64> &item_ptr, const std::vector<i64> &item_vals, bool exclude_self,
+                  std::vector<i64> &ptr, std::vector<i64> &idx) {
+  ptr.assign(nrows + 1, 0);
+  idx.clear();
+  std::vector<i64> buf;
+  for (i64 r = 0; r < nrows; ++r) {
+    buf.clear();
+    for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
+      const i64 it = row_items[a];
+      for (i64 b = item_ptr[it]; b < item_ptr[it + 1]; ++b) buf.push_back(item_vals[b]);
+    }
+    std::sort(buf.begin(), buf.end());
+    i64 last = -1;
+    bool have = false;
+    for (i64 v : buf) {
+      if (have && v == last) continue;
+      have = true;
+      last = v;
+      if (exclude_self && v == r) continue;
+      idx.push_back(v);
+    }
+    ptr[r + 1] = (i64)idx.size();
+  }
+}
+
+// SELL-32 of a CSR table (rows in warps of 32, entry k of the 32 rows contiguous);
+// padding: -1, or (fill_first) the row's first entry with value 0
+void sell32(const std::vector<i64> &ptr, const std::vector<i64> &idx, const std::vector<double> *vals,
+            bool fill_first, std::vector<i32> &gptr, std::vector<i32> &out, std::vector<double> &outv) {
+  const i64 n = (i64)ptr.size() - 1;
+  const i64 ng = (n + 31) / 32;
+  gptr.assign(ng + 1, 0);
+  std::vector<i64> g64(ng + 1, 0);
+  for (i64 g = 0; g < ng; ++g) {
+    i64 len = 0;
+    for (i64 r = 32 * g; r < std::min(n, 32 * g + 32); ++r) len = std::max(len, ptr[r + 1] - ptr[r]);
+    g64[g + 1] = g64[g] + 32 * len;
+  }
+  out.assign(g64[ng], -1);
+  outv.assign(vals ? g64[ng] : 0, 0.0);
+  for (i64 g = 0; g < ng; ++g) {
+    const i64 len = (g64[g + 1] - g64[g]) / 32;
+    for (i64 l = 0; l < 32; ++l) {
+      const i64 r = 32 * g + l;
+      const i64 cnt = r < n ? ptr[r + 1] - ptr[r] : 0;
+      const i64 first = (r < n && cnt > 0) ? idx[ptr[r]] : 0;
+      for (i64 k = 0; k < len; ++k) {
+        const i64 d = g64[g] + 32 * k + l;
+        if (k < cnt) {
+          out[d] = (i32)idx[ptr[r] + k];
+          if (vals) outv[d] = (*vals)[ptr[r] + k];
+        } else if (fill_first) {
+          out[d] = (i32)first;
+        }
+      }
+    }
+  }
+  for (i64 g = 0; g <= ng; ++g) gptr[g] = (i32)g64[g];
+}
+
+uint64_t part1by1(uint64_t v) {
+  v &= 0xFFFFFFFFull;
+  v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+  v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+  v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  v = (v | (v << 2)) & 0x3333333333333333ull;
+  v = (v | (v << 1)) & 0x5555555555555555ull;
+  return v;
+}
+
+template <class K>
+std::vector<i64> stable_argsort(const std::vector<K> &key) {
+  std::vector<i64> o(key.size());
+  std::iota(o.begin(), o.end(), 0);
+  std::stable_sort(o.begin(), o.end(), [&](i64 a, i64 b) { return key[a] < key[b]; });
+  return o;
+}
+
+Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder) {
+  auto *res = new Result();
+  for (i64 c = 0; c < nc; ++c)
+    if (el[4 * c + 3] != 3) {
+      res->error = "2D meshes must be all triangles";
+      return res;
+    }
+  auto X = [&](i64 n) { return vx[4 * n]; };
+  auto Y = [&](i64 n) { return vx[4 * n + 1]; };
+  auto Zv = [&](i64 n) { return vx[4 * n + 2]; };
+  auto node = [&](i64 c, int j) { return (i64)el[4 * c + j]; };
+
+  // ---- cell centre and volume
+  std::vector<double> cx(nc), cy(nc), vol(nc);
+  for (i64 c = 0; c < nc; ++c) {
+    const double x1 = X(node(c, 0)), x2 = X(node(c, 1)), x3 = X(node(c, 2));
+    const double y1 = Y(node(c, 0)), y2 = Y(node(c, 1)), y3 = Y(node(c, 2));
+    cx[c] = 1.0 / 3 * (x1 + x2 + x3);
+    cy[c] = 1.0 / 3 * (y1 + y2 + y3);
+    vol[c] = 0.5 * std::fabs((x1 - x2) * (y1 - y3) - (x1 - x3) * (y1 - y2));
+  }
+  // ---- node -> cells, cell -> vertex neighbours
+  std::vector<i64> flat_nodes(3 * nc), flat_cells(3 * nc), c2n_ptr(nc + 1);
+  for (i64 c = 0; c < nc; ++c)
+    for (int j = 0; j < 3; ++j) {
+      flat_nodes[3 * c + j] = node(c, j);
+      flat_cells[3 * c + j] = c;
+    }
+  for (i64 c = 0; c <= nc; ++c) c2n_ptr[c] = 3 * c;
+  std::vector<i64> n2c_ptr, n2c_idx;
+  group_csr(flat_nodes, flat_cells, nn, n2c_ptr, n2c_idx);
+  std::vector<i64> cnid_ptr, cnid_idx;
+  ragged_union(nc, c2n_ptr, flat_nodes, n2c_ptr, n2c_idx, true, cnid_ptr, cnid_idx);
+
+  // ---- faces: descending node pairs, numbered by ascending key
+  static const int LOC[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  std::vector<i64> key(3 * nc), pa(3 * nc), pb(3 * nc);
+  for (i64 c = 0; c < nc; ++c)
+    for (int j = 0; j < 3; ++j) {
+      i64 a = node(c, LOC[j][0]), b = node(c, LOC[j][1]);
+      if (a < b) std::swap(a, b);
+      pa[3 * c + j] = a;
+      pb[3 * c + j] = b;
+      key[3 * c + j] = a * nn + b;
+    }
+  // stable order of the keys (a, b): two counting-sort passes, by b then by a
+  std::vector<i64> ord(3 * nc);
+  {
+    std::vector<i64> tmp(3 * nc), cnt(nn + 1);
+    auto pass = [&](const std::vector<i64> &digit, const std::vector<i64> &in, std::vector<i64> &out) {
+      std::fill(cnt.begin(), cnt.end(), 0);
+      for (i64 e : in) cnt[digit[e] + 1]++;
+      for (i64 d = 0; d < nn; ++d) cnt[d + 1] += cnt[d];
+      for (i64 e : in) out[cnt[digit[e]]++] = e;
+    };
+    std::vector<i64> id(3 * nc);
+    std::iota(id.begin(), id.end(), 0);
+    pass(pb, id, tmp);
+    pass(pa, tmp, ord);
+  }
+  std::vector<i64> inv(3 * nc);
+  std::vector<i64> fa, fb;  // face nodes (descending)
+  std::vector<i64> f0, f1;  // face -> cells
+  for (size_t e = 0; e < ord.size(); ++e) {
+    const i64 o = ord[e];
+    if (e == 0 || key[o] != key[ord[e - 1]]) {
+      fa.push_back(pa[o]);
+      fb.push_back(pb[o]);
+      f0.push_back(o / 3);
+      f1.push_back(-1);
+    } else {
+      if (f1.back() != -1) {
+        res->error = "non-manifold mesh: a face is shared by more than two cells";
+        return res;
+      }
+      f1.back() = o / 3;
+    }
+    inv[o] = (i64)fa.size() - 1;
+  }
+  const i64 nf = (i64)fa.size();
+  // face neighbours, compacted (boundary faces skipped)
+  std::vector<i64> cellfid(3 * nc, -1);
+  for (i64 c = 0; c < nc; ++c) {
+    int k = 0;
+    for (int j = 0; j < 3; ++j) {
+      const i64 f = inv[3 * c + j];
+      if (f1[f] == -1) continue;
+      cellfid[3 * c + k++] = f0[f] == c ? f1[f] : f0[f];
+    }
+  }
+  // ---- names, normals, areas, centres
+  std::vector<i32> namen(nn);
+  for (i64 n = 0; n < nn; ++n) namen[n] = (i32)vx[4 * n + 3];
+  std::vector<i32> name(nf, 0);
+  std::vector<double> nx(nf), ny(nf), nz(nf), mes(nf), fcx(nf), fcy(nf), fcz(nf);
+  for (i64 f = 0; f < nf; ++f) {
+    if (f1[f] == -1) {
+      const i32 a = namen[fa[f]], b = namen[fb[f]];
+      i32 r = 100;
+      for (i32 tag : {44, 33, 4, 3})
+        if ((a == tag && b != 0) || (a != 0 && b == tag)) r = tag;
+      if (a == b) r = a;
+      name[f] = r;
+    }
+    const double n0 = Y(fa[f]) - Y(fb[f]), n1 = X(fb[f]) - X(fa[f]);
+    fcx[f] = 0.5 * (X(fa[f]) + X(fb[f]));
+    fcy[f] = 0.5 * (Y(fa[f]) + Y(fb[f]));
+    fcz[f] = 0.5 * (Zv(fa[f]) + Zv(fb[f]));
+    const double sx = cx[f0[f]] - fcx[f], sy = cy[f0[f]] - fcy[f];
+    const bool flip = (sx * n0 + sy * n1) > 0;
+    nx[f] = flip ? -1 * n0 : n0;
+    ny[f] = flip ? -1 * n1 : n1;
+    nz[f] = flip ? -1 * 0.0 : 0.0;
+    mes[f] = std::sqrt(nx[f] * nx[f] + ny[f] * ny[f]);
+    if (f1[f] == -1 && (name[f] >= 100 || name[f] == 0)) {
+      res->error = "mesh has boundary faces that match no boundary side (manapy names them 100/200 and "
+                   "leaves them out of every face list)";
+      return res;
+    }
+  }
+  // outward normal of each local face (cells.nf)
+  std::vector<double> cnf(9 * nc);
+  for (i64 c = 0; c < nc; ++c)
+    for (int j = 0; j < 3; ++j) {
+      const i64 f = inv[3 * c + j];
+      const double s = (cx[c] - fcx[f]) * nx[f] + (cy[c] - fcy[f]) * ny[f] + (0.0 - fcz[f]) * nz[f];
+      const bool keep = s < 0;
+      cnf[9 * c + 3 * j + 0] = keep ? nx[f] : -1.0 * nx[f];
+      cnf[9 * c + 3 * j + 1] = keep ? ny[f] : -1.0 * ny[f];
+      cnf[9 * c + 3 * j + 2] = keep ? nz[f] : -1.0 * nz[f];
+    }
+  // ---- face lists (manapy numbering)
+  std::vector<i64> lists[5];
+  std::vector<i64> bfaces;
+  for (i64 f = 0; f < nf; ++f) {
+    if (name[f] >= 0 && name[f] <= 4) lists[name[f]].push_back(f);
+    if (name[f] >= 1 && name[f] <= 4) bfaces.push_back(f);
+  }
+  // ---- ghost centres
+  std::vector<double> gc(3 * nf, -1.0);
+  for (i64 f : bfaces) {
+    const double x1x = X(fb[f]), x1y = Y(fb[f]), x2x = X(fa[f]), x2y = Y(fa[f]);
+    const double v1x = cx[f0[f]], v1y = cy[f0[f]];
+    const double gamma = ((v1x - x2x) * (x1x - x2x) + (v1y - x2y) * (x1y - x2y)) /
+                         ((x1x - x2x) * (x1x - x2x) + (x1y - x2y) * (x1y - x2y));
+    const double kk0 = gamma * x1x + (1 - gamma) * x2x, kk1 = gamma * x1y + (1 - gamma) * x2y;
+    gc[3 * f] = 2 * kk0 + (-1 * v1x);
+    gc[3 * f + 1] = 2 * kk1 + (-1 * v1y);
+    gc[3 * f + 2] = gamma;
+  }
+  // node -> boundary faces (ascending face), cell -> stencil ghosts
+  std::vector<i64> gkey, gval;
+  for (i64 f : bfaces) {
+    gkey.push_back(fa[f]);
+    gval.push_back(f);
+    gkey.push_back(fb[f]);
+    gval.push_back(f);
+  }
+  std::vector<i64> n2g_ptr, n2g_idx;
+  group_csr(gkey, gval, nn, n2g_ptr, n2g_idx);
+  std::vector<i64> gnid_ptr, gnid_idx;
+  ragged_union(nc, c2n_ptr, flat_nodes, n2g_ptr, n2g_idx, false, gnid_ptr, gnid_idx);
+  // ---- centre -> vertex weights
+  std::vector<double> lx(nn), ly(nn), Rx(nn), Ry(nn);
+  std::vector<i64> number(nn);
+  for (i64 n = 0; n < nn; ++n) {
+    double xx = 0, yy = 0, xy = 0, sx = 0, sy = 0;
+    auto acc = [&](double px, double py) {
+      const double rx = px - X(n), ry = py - Y(n);
+      xx += rx * rx;
+      yy += ry * ry;
+      xy += rx * ry;
+      sx += rx;
+      sy += ry;
+    };
+    for (i64 a = n2c_ptr[n]; a < n2c_ptr[n + 1]; ++a) acc(cx[n2c_idx[a]], cy[n2c_idx[a]]);
+    for (i64 a = n2g_ptr[n]; a < n2g_ptr[n + 1]; ++a) acc(gc[3 * n2g_idx[a]], gc[3 * n2g_idx[a] + 1]);
+    const double D = xx * yy - xy * xy;
+    lx[n] = (xy * sy - yy * sx) / D;
+    ly[n] = (xy * sx - xx * sy) / D;
+    Rx[n] = sx;
+    Ry[n] = sy;
+    number[n] = (n2c_ptr[n + 1] - n2c_ptr[n]) + (n2g_ptr[n + 1] - n2g_ptr[n]);
+  }
+  auto alpha = [&](i64 n, double px, double py) {
+    const double den = (double)number[n] + lx[n] * Rx[n] + ly[n] * Ry[n];
+    const double xd = px - X(n), yd = py - Y(n);
+    return (1. + lx[n] * xd + ly[n] * yd) / den;
+  };
+  // ---- diamond vectors and areas, orthogonal distances
+  std::vector<double> ff(8 * nf), air(nf), dist(nf, 0.0);
+  auto proj = [&](i64 K, i64 f) {
+    const double vx_ = cx[K] - fcx[f], vy_ = cy[K] - fcy[f];
+    const double s = vx_ * nx[f] + vy_ * ny[f];
+    const double px = cx[K] - s * nx[f], py = cy[K] - s * ny[f];
+    const double z0 = cx[K] - px, z1 = cy[K] - py;
+    return std::sqrt(z0 * z0 + z1 * z1);
+  };
+  for (i64 f = 0; f < nf; ++f) {
+    const bool inner = name[f] == 0;
+    const double v1x = cx[f0[f]], v1y = cy[f0[f]];
+    const double v2x = inner ? cx[f1[f]] : gc[3 * f], v2y = inner ? cy[f1[f]] : gc[3 * f + 1];
+    const double ax = X(fa[f]), ay = Y(fa[f]), bx = X(fb[f]), by = Y(fb[f]);
+    double *F = &ff[8 * f];
+    F[0] = v1x - ax; F[1] = v1y - ay;
+    F[2] = bx - v1x; F[3] = by - v1y;
+    F[4] = v2x - bx; F[5] = v2y - by;
+    F[6] = ax - v2x; F[7] = ay - v2y;
+    air[f] = 0.5 * ((bx - ax) * (v2y - v1y) + (v1x - v2x) * (by - ay));
+    if (inner)
+      dist[f] = proj(f0[f], f) + proj(f1[f], f);
+    else if (name[f] >= 1 && name[f] <= 4)
+      dist[f] = 2 * proj(f0[f], f);
+  }
+
+  // ---- locality numbering
+  std::vector<i64> cperm(nc), fperm(nf), nperm(nn);
+  if (reorder) {
+    double lo0 = cx[0], lo1 = cy[0], hi0 = cx[0], hi1 = cy[0];
+    for (i64 c = 1; c < nc; ++c) {
+      lo0 = std::min(lo0, cx[c]); hi0 = std::max(hi0, cx[c]);
+      lo1 = std::min(lo1, cy[c]); hi1 = std::max(hi1, cy[c]);
+    }
+    const double sp0 = std::max(hi0 - lo0, 1e-300), sp1 = std::max(hi1 - lo1, 1e-300);
+    const double scale = (double)((1 << 20) - 1);
+    std::vector<uint64_t> mk(nc);
+    for (i64 c = 0; c < nc; ++c) {
+      const i64 q0 = (i64)std::floor((cx[c] - lo0) / sp0 * scale), q1 = (i64)std::floor((cy[c] - lo1) / sp1 * scale);
+      mk[c] = part1by1((uint64_t)q0) | (part1by1((uint64_t)q1) << 1);
+    }
+    cperm = stable_argsort(mk);
+  } else {
+    std::iota(cperm.begin(), cperm.end(), 0);
+  }
+  std::vector<i64> cinv(nc);
+  for (i64 k = 0; k < nc; ++k) cinv[cperm[k]] = k;
+  if (reorder) {
+    std::vector<i64> lo(nf), hi(nf);
+    for (i64 f = 0; f < nf; ++f) {
+      const i64 a = cinv[f0[f]], b = f1[f] >= 0 ? cinv[f1[f]] : a;
+      lo[f] = std::min(a, b);
+      hi[f] = std::max(a, b);
+    }
+    std::iota(fperm.begin(), fperm.end(), 0);
+    std::stable_sort(fperm.begin(), fperm.end(),
+                     [&](i64 a, i64 b) { return lo[a] < lo[b] || (lo[a] == lo[b] && hi[a] < hi[b]); });
+    std::vector<i64> first(nn, INT64_MAX);
+    for (i64 n = 0; n < nn; ++n)
+      for (i64 a = n2c_ptr[n]; a < n2c_ptr[n + 1]; ++a) first[n] = std::min(first[n], cinv[n2c_idx[a]]);
+    nperm = stable_argsort(first);
+  } else {
+    std::iota(fperm.begin(), fperm.end(), 0);
+    std::iota(nperm.begin(), nperm.end(), 0);
+  }
+  std::vector<i64> finv(nf), ninv(nn);
+  for (i64 k = 0; k < nf; ++k) finv[fperm[k]] = k;
+  for (i64 k = 0; k < nn; ++k) ninv[nperm[k]] = k;
+
+  // relabelled CSR: rows in `rows` order, values mapped, entry order kept
+  auto relabel = [](const std::vector<i64> &ptr, const std::vector<i64> &idx, const std::vector<i64> &rows,
+                    const std::vector<i64> &vinv, std::vector<i64> &optr, std::vector<i64> &oidx,
+                    std::vector<i64> *src) {
+    optr.assign(rows.size() + 1, 0);
+    oidx.clear();
+    if (src) src->clear();
+    for (size_t r = 0; r < rows.size(); ++r) {
+      for (i64 a = ptr[rows[r]]; a < ptr[rows[r] + 1]; ++a) {
+        oidx.push_back(vinv[idx[a]]);
+        if (src) src->push_back(a);
+      }
+      optr[r + 1] = (i64)oidx.size();
+    }
+  };
+  auto to32 = [](const std::vector<i64> &v) { return std::vector<i32>(v.begin(), v.end()); };
+
+  // ---- device tables
+  {
+    std::vector<double> t(3 * nc);
+    for (i64 k = 0; k < nc; ++k) { t[3 * k] = cx[cperm[k]]; t[3 * k + 1] = cy[cperm[k]]; t[3 * k + 2] = 0.0; }
+    res->add("cell_center", 'd', {nc, 3}, t);
+    std::vector<double> v(nc);
+    for (i64 k = 0; k < nc; ++k) v[k] = vol[cperm[k]];
+    res->add("cell_volume", 'd', {nc}, v);
+  }
+  {
+    std::vector<i32> cf(4 * nc, -1);
+    std::vector<uint8_t> code(nc);
+    for (i64 k = 0; k < nc; ++k) {
+      const i64 c = cperm[k];
+      i64 fo[3];
+      for (int j = 0; j < 3; ++j) { fo[j] = inv[3 * c + j]; cf[4 * k + j] = (i32)finv[fo[j]]; }
+      int o[3] = {0, 1, 2};  // stable order of the three face ids
+      if (fo[o[1]] < fo[o[0]]) std::swap(o[0], o[1]);
+      if (fo[o[2]] < fo[o[1]]) std::swap(o[1], o[2]);
+      if (fo[o[1]] < fo[o[0]]) std::swap(o[0], o[1]);
+      code[k] = (uint8_t)(o[0] | (o[1] << 2) | (o[2] << 4));
+    }
+    res->add("cell_faces", 'i', {nc, 4}, cf);
+    res->add("cell_order", 'b', {nc}, code);
+  }
+  {
+    std::vector<i64> p, ix;
+    relabel(cnid_ptr, cnid_idx, cperm, cinv, p, ix, nullptr);
+    res->add("cellnid_ptr", 'i', {nc + 1}, to32(p));
+    res->add("cellnid_idx", 'i', {(i64)ix.size()}, to32(ix));
+    std::vector<i32> gp, gi;
+    std::vector<double> gv;
+    sell32(p, ix, nullptr, false, gp, gi, gv);
+    res->add("lsq_sell_ptr", 'i', {(i64)gp.size()}, gp);
+    res->add("lsq_sell_idx", 'i', {(i64)gi.size()}, gi);
+    relabel(gnid_ptr, gnid_idx, cperm, finv, p, ix, nullptr);
+    res->add("ghostnid_ptr", 'i', {nc + 1}, to32(p));
+    res->add("ghostnid_idx", 'i', {(i64)ix.size()}, to32(ix));
+  }
+  {
+    std::vector<i32> cid(2 * nf), fn(4 * nf, -1), nm(nf);
+    std::vector<double> nrm(3 * nf), fc(3 * nf), ms(nf), g(3 * nf), a(nf), F(8 * nf), d(nf);
+    std::vector<float> nm32(4 * nf, 0.f);
+    for (i64 k = 0; k < nf; ++k) {
+      const i64 f = fperm[k];
+      cid[2 * k] = (i32)cinv[f0[f]];
+      cid[2 * k + 1] = f1[f] >= 0 ? (i32)cinv[f1[f]] : -1;
+      fn[4 * k] = (i32)ninv[fa[f]];
+      fn[4 * k + 1] = (i32)ninv[fb[f]];
+      nm[k] = name[f];
+      nrm[3 * k] = nx[f]; nrm[3 * k + 1] = ny[f]; nrm[3 * k + 2] = nz[f];
+      fc[3 * k] = fcx[f]; fc[3 * k + 1] = fcy[f]; fc[3 * k + 2] = fcz[f];
+      ms[k] = mes[f];
+      nm32[4 * k] = (float)nx[f];
+      nm32[4 * k + 1] = (float)ny[f];
+      nm32[4 * k + 2] = (float)(1.0 / mes[f]);
+      for (int c = 0; c < 3; ++c) g[3 * k + c] = gc[3 * f + c];
+      a[k] = air[f];
+      for (int c = 0; c < 8; ++c) F[8 * k + c] = ff[8 * f + c];
+      d[k] = dist[f];
+    }
+    res->add("face_cellid", 'i', {nf, 2}, cid);
+    res->add("face_nodeid", 'i', {nf, 4}, fn);
+    res->add("face_name", 'i', {nf}, nm);
+    res->add("face_normal", 'd', {nf, 3}, nrm);
+    res->add("face_center", 'd', {nf, 3}, fc);
+    res->add("face_mesure", 'd', {nf}, ms);
+    res->add("face_nm_f32", 'f', {nf, 4}, nm32);
+    res->add("face_ghostcenter", 'd', {nf, 3}, g);
+    res->add("face_air", 'd', {nf}, a);
+    res->add("face_f", 'd', {nf, 8}, F);
+    res->add("face_dist", 'd', {nf}, d);
+  }
+  {
+    std::vector<i64> p, ix, src;
+    relabel(n2c_ptr, n2c_idx, nperm, cinv, p, ix, &src);
+    std::vector<double> al(ix.size());
+    for (i64 r = 0; r < nn; ++r) {  // row r of the new table is node nperm[r]
+      const i64 n = nperm[r];
+      for (i64 e = p[r]; e < p[r + 1]; ++e) {
+        const i64 c = n2c_idx[src[e]];
+        al[e] = alpha(n, cx[c], cy[c]);
+      }
+    }
+    res->add("n2c_ptr", 'i', {nn + 1}, to32(p));
+    res->add("n2c_idx", 'i', {(i64)ix.size()}, to32(ix));
+    res->add("n2c_alpha", 'd', {(i64)al.size()}, al);
+    std::vector<i32> gp, gi;
+    std::vector<double> gv;
+    sell32(p, ix, &al, true, gp, gi, gv);
+    res->add("n2c_sell_ptr", 'i', {(i64)gp.size()}, gp);
+    res->add("n2c_sell_idx", 'i', {(i64)gi.size()}, gi);
+    res->add("n2c_sell_alpha", 'd', {(i64)gv.size()}, gv);
+    std::vector<float> gv32(gv.begin(), gv.end());
+    res->add("n2c_sell_alpha_f32", 'f', {(i64)gv32.size()}, gv32);
+    relabel(n2g_ptr, n2g_idx, nperm, finv, p, ix, &src);
+    std::vector<double> ag(ix.size());
+    for (i64 r = 0; r < nn; ++r) {
+      const i64 n = nperm[r];
+      for (i64 e = p[r]; e < p[r + 1]; ++e) {
+        const i64 f = n2g_idx[src[e]];
+        ag[e] = alpha(n, gc[3 * f], gc[3 * f + 1]);
+      }
+    }
+    res->add("n2g_ptr", 'i', {nn + 1}, to32(p));
+    res->add("n2g_idx", 'i', {(i64)ix.size()}, to32(ix));
+    res->add("n2g_alpha", 'd', {(i64)ag.size()}, ag);
+  }
+  {
+    std::vector<i32> cf(4 * nc, -1), vtx(4 * nc, 0), nbr(4 * nc, -1);
+    std::vector<uint32_t> flags(nc, 0);
+    std::vector<double> nf_(9 * nc), v1(2 * nc), xy(2 * nc), ncoord(2 * nn);
+    for (i64 k = 0; k < nc; ++k) {
+      const i64 c = cperm[k];
+      for (int j = 0; j < 3; ++j) {
+        const i64 o = cellfid[3 * c + j];
+        cf[4 * k + j] = (i32)(o >= 0 ? cinv[o] : cinv[nc - 1]);
+      }
+      for (int q = 0; q < 9; ++q) nf_[9 * k + q] = cnf[9 * c + q];
+      v1[2 * k] = X(node(c, 1));
+      v1[2 * k + 1] = Y(node(c, 1));
+      xy[2 * k] = cx[c];
+      xy[2 * k + 1] = cy[c];
+      uint32_t fl = 0;
+      for (int j = 0; j < 3; ++j) {
+        vtx[4 * k + j] = (i32)ninv[node(c, j)];
+        const i64 f = inv[3 * c + j];
+        const bool own = f0[f] == c;
+        const i64 other = own ? f1[f] : f0[f];
+        nbr[4 * k + j] = f1[f] < 0 ? (i32)(-1 - finv[f]) : (i32)cinv[other];
+        const i64 vj = node(c, j), vn = node(c, (j + 1) % 3);
+        const bool rev = fa[f] == vn;
+        const i64 a = rev ? vn : vj, b = rev ? vj : vn;
+        const double n0 = Y(a) - Y(b), n1 = X(b) - X(a);
+        const bool flip = nx[f] != n0 || ny[f] != n1;
+        const bool nfneg = cnf[9 * c + 3 * j] != nx[f] || cnf[9 * c + 3 * j + 1] != ny[f];
+        fl |= ((uint32_t)own << j) | ((uint32_t)rev << (3 + j)) | ((uint32_t)flip << (6 + j)) |
+              ((uint32_t)nfneg << (9 + j));
+      }
+      flags[k] = fl;
+    }
+    for (i64 r = 0; r < nn; ++r) { ncoord[2 * r] = X(nperm[r]); ncoord[2 * r + 1] = Y(nperm[r]); }
+    res->add("cell_cellfid", 'i', {nc, 4}, cf);
+    res->add("cell_nf", 'd', {nc, 3, 3}, nf_);
+    res->add("cell_vertex1", 'd', {nc, 2}, v1);
+    res->add("cell_vtx", 'i', {nc, 4}, vtx);
+    res->add("cell_nbr", 'i', {nc, 4}, nbr);
+    res->add("cell_flags", 'i', {nc}, flags);
+    res->add("node_coord", 'd', {nn, 2}, ncoord);
+    res->add("cell_xy", 'd', {nc, 2}, xy);
+  }
+  // permutations and the manapy-numbered arrays the boundary set-up reads
+  res->add("perm_cell", 'l', {nc}, cperm);
+  res->add("perm_face", 'l', {nf}, fperm);
+  res->add("perm_node", 'l', {nn}, nperm);
+  res->add("inv_cell", 'l', {nc}, cinv);
+  res->add("inv_face", 'l', {nf}, finv);
+  res->add("inv_node", 'l', {nn}, ninv);
+  {
+    std::vector<double> fc(3 * nf), cc(3 * nc);
+    for (i64 f = 0; f < nf; ++f) { fc[3 * f] = fcx[f]; fc[3 * f + 1] = fcy[f]; fc[3 * f + 2] = fcz[f]; }
+    for (i64 c = 0; c < nc; ++c) { cc[3 * c] = cx[c]; cc[3 * c + 1] = cy[c]; cc[3 * c + 2] = 0.0; }
+    res->add("A.faces_center", 'd', {nf, 3}, fc);
+    res->add("A.cells_center", 'd', {nc, 3}, cc);
+    static const char *LN[5] = {"A.innerfaces", "A.infaces", "A.outfaces", "A.upperfaces", "A.bottomfaces"};
+    for (int t = 0; t < 5; ++t) res->add(LN[t], 'i', {(i64)lists[t].size()}, to32(lists[t]));
+  }
+  return res;
+}
+
+}  // namespace
+
+extern "C" {
+
+void *mbh_build2d(const int32_t *elements, int64_t nbcells, const double *vertex, int64_t nbnodes, int32_t reorder) {
+  if (!elements || !vertex || nbcells <= 0 || nbnodes <= 0) return nullptr;
+  return build2d(elements, nbcells, vertex, nbnodes, reorder != 0);
+}
+
+const char *mbh_error(void *h) { return h ? static_cast<Result *>(h)->error.c_str() : "null handle"; }
+
+int32_t mbh_count(void *h) { return h ? (int32_t) static_cast<Result *>(h)->tables.size() : 0; }
+
+// name, dtype code and up to 3 dimensions of table k; returns its number of dimensions
+int32_t mbh_info(void *h, int32_t k, const char **name, char *dtype, int64_t shape[3]) {
+  const Table &t = static_cast<Result *>(h)->tables[k];
+  *name = t.name.c_str();
+  *dtype = t.dtype;
+  for (size_t d = 0; d < 3; ++d) shape[d] = d < t.shape.size() ? t.shape[d] : 0;
+  return (int32_t)t.shape.size();
+}
+
+const void *mbh_data(void *h, int32_t k) { return static_cast<Result *>(h)->tables[k].bytes.data(); }
+
+void mbh_free(void *h) { delete static_cast<Result *>(h); }
+
+}  // extern "C"

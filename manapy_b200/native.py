@@ -1,0 +1,74 @@
+"""ctypes binding of the native host mesh builder (``lib/libmanapy_b200_host.so``).
+
+``tables2d(elements, vertex)`` returns every device table of a 2D triangle mesh
+(the ``DeviceMesh`` tables, in the locality numbering), the permutations, and
+the few manapy-numbered arrays the boundary set-up reads, computed in C++
+(``host/mesh2d.cpp``) with the same operations as ``geometry.build`` +
+``DeviceMesh``: the results are bit-identical, 20-50 times faster.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .build import HOST_OUT
+
+_DT = {b"i": np.int32, b"l": np.int64, b"d": np.float64, b"f": np.float32, b"b": np.uint8}
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(HOST_OUT):
+            from .build import build_host
+            build_host()
+        L = ctypes.CDLL(HOST_OUT)
+        L.mbh_build2d.restype = ctypes.c_void_p
+        L.mbh_build2d.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32]
+        L.mbh_error.restype = ctypes.c_char_p
+        L.mbh_error.argtypes = [ctypes.c_void_p]
+        L.mbh_count.restype = ctypes.c_int32
+        L.mbh_count.argtypes = [ctypes.c_void_p]
+        L.mbh_info.restype = ctypes.c_int32
+        L.mbh_info.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_char_p),
+                               ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
+        L.mbh_data.restype = ctypes.c_void_p
+        L.mbh_data.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.mbh_free.argtypes = [ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def tables2d(elements, vertex, reorder=True):
+    """dict name -> numpy array (see ``host/mesh2d.cpp``); raises ValueError on a bad mesh."""
+    el = np.ascontiguousarray(elements, dtype=np.int32)
+    vx = np.ascontiguousarray(vertex, dtype=np.float64)
+    if el.ndim != 2 or el.shape[1] != 4 or vx.ndim != 2 or vx.shape[1] != 4:
+        raise ValueError("expected elements [nc, 4] and vertex [nn, 4]")
+    L = lib()
+    h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)))
+    if not h:
+        raise ValueError("empty mesh")
+    try:
+        err = L.mbh_error(h)
+        if err:
+            raise ValueError(err.decode())
+        out = {}
+        name = ctypes.c_char_p()
+        dt = ctypes.create_string_buffer(1)
+        shape = (ctypes.c_int64 * 3)()
+        for k in range(L.mbh_count(h)):
+            nd = L.mbh_info(h, k, ctypes.byref(name), dt, shape)
+            shp = tuple(shape[d] for d in range(nd))
+            dtype = np.dtype(_DT[dt.raw])
+            n = int(np.prod(shp)) if shp else 0
+            ptr = L.mbh_data(h, k)
+            buf = (ctypes.c_char * (n * dtype.itemsize)).from_address(ptr) if n else b""
+            out[name.value.decode()] = np.frombuffer(buf, dtype=dtype).reshape(shp).copy() if n else \
+                np.zeros(shp, dtype=dtype)
+        return out
+    finally:
+        L.mbh_free(h)

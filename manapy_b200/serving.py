@@ -99,11 +99,11 @@ def initial_state(req, centers):
 def prepare(req):
     """Host work of one request (runs in a worker process): mesh, geometry, device tables
     (as host arrays), boundary rules and the initial state in the device numbering."""
-    from . import boundary as B, geometry as G, meshgen
+    from . import boundary as B, meshgen
     from .device import DeviceBC, DeviceMesh
     el, vx = meshgen.square_triangles(req.n, seed=req.seed)
-    A = G.build(el, vx, 2)
-    dm = DeviceMesh(A, device=None)
+    dm = DeviceMesh.from_native(el, vx)       # the native host builder (C++)
+    A = dm.A
     bc = None
     if req.kind == "advdiff":
         res = B.resolve(A, {s: "dirichlet" for s in SIDES}, {s: 0.0 for s in SIDES})

@@ -1,0 +1,36 @@
+"""The native host builder (C++) reproduces the Python builder's device tables bit for bit."""
+import numpy as np
+import pytest
+
+from manapy_b200 import boundary as B, device as D, geometry as G, meshgen
+from manapy_b200.serving import SIDES
+
+
+@pytest.mark.parametrize("n,seed,reorder", [(7, 0, True), (23, 5, True), (16, 2, False), (40, 9, True)])
+def test_tables_match_the_python_builder(n, seed, reorder):
+    el, vx = meshgen.square_triangles(n, seed=seed)
+    ref = D.DeviceMesh(G.build(el, vx, 2), device=None, reorder=reorder)
+    nat = D.DeviceMesh.from_native(el, vx, reorder=reorder)
+    assert sorted(ref.t) == sorted(nat.t)
+    for k, v in ref.t.items():
+        assert v.dtype == nat.t[k].dtype and v.shape == nat.t[k].shape, k
+        assert v.tobytes() == nat.t[k].tobytes(), k
+    for kind in ("cell", "face", "node"):
+        assert np.array_equal(ref.perm[kind], nat.perm[kind])
+        assert np.array_equal(ref.inv[kind], nat.inv[kind])
+    # boundary rules from the native builder's manapy-numbered arrays
+    A = G.build(el, vx, 2)
+    bc = {s: "dirichlet" for s in SIDES}
+    vals = {s: 1.5 for s in SIDES}
+    b_ref = D.DeviceBC(A, B.resolve(A, bc, vals), device=None, mesh=ref)
+    b_nat = D.DeviceBC(nat.A, B.resolve(nat.A, bc, vals), device=None, mesh=nat)
+    for a in ("kind", "value", "face_grad_on"):
+        assert np.array_equal(getattr(b_ref, a), getattr(b_nat, a)), a
+
+
+def test_rejects_unmatched_boundary_faces():
+    el, vx = meshgen.square_triangles(4, seed=1)
+    vx = vx.copy()
+    vx[:, 3] = 0  # no boundary tags at all
+    with pytest.raises(ValueError, match="match no boundary side"):
+        D.DeviceMesh.from_native(el, vx)
