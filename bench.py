@@ -476,11 +476,13 @@ def run_serving(args):
     reqs = SV.make_requests(args.requests, args.rate, seed=2024)
     total_cu = sum(r.cells * r.steps for r in reqs)
     srv = SV.BatchServer(workers=args.workers)
-    # warm-up: compile paths, worker start-up
-    SV.BatchServer(workers=0).serve(SV.make_requests(4, 0.0, seed=1, cells=(2e3, 2e4), steps=(20, 40)))
+    # warm-up outside the timed run: worker processes started, paths exercised
+    srv.start_pool()
+    srv.serve(SV.make_requests(8, 0.0, seed=1, cells=(2e3, 2e4), steps=(20, 40)))
     t0 = time.perf_counter()
     recs = srv.serve(reqs)
     wall = time.perf_counter() - t0
+    srv.stop_pool()
     lat = np.array([r["latency"] for r in recs])
     # serial plain FP64: host preparation excluded (done beforehand), device solve timed per request
     sample = reqs[:max(1, min(args.serial_sample, len(reqs)))]
@@ -532,7 +534,8 @@ def run_serving(args):
                    "cells": "log-uniform 2e3-5e5", "steps": "uniform 100-2000", "mix": "70% adv-diff o2, 30% SW o1"},
         "serving": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                     "mean_s": float(lat.mean()), "makespan_s": wall, "requests_per_s": len(reqs) / wall,
-                    "cell_updates": total_cu},
+                    "cell_updates": total_cu, "host_seconds": {k: round(v, 3) for k, v in srv.stats.items()},
+                    "workers": srv.workers},
         "serial_fp64": {"value": serial_rate, "unit": "cell-updates/s", "sample": len(sample),
                         "p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
                         "note": "device solves through the public API, one request at a time; host mesh "

@@ -250,6 +250,45 @@ class DeviceMesh:
         self.struct = self._make_struct()
         return self
 
+    # tables the FP32-compensated steps and their set-up kernels read (batched serving)
+    SERVE_TABLES = ("cell_volume", "cell_order", "cell_faces", "cell_vtx", "cell_nbr", "cell_flags", "node_coord",
+                    "cell_xy", "lsq_sell_ptr", "lsq_sell_idx", "n2c_sell_ptr", "n2c_sell_idx", "n2c_sell_alpha_f32",
+                    "ghostnid_ptr", "ghostnid_idx", "face_ghostcenter", "n2g_ptr", "n2g_idx", "n2g_alpha",
+                    "face_cellid", "face_dist", "face_normal", "face_mesure", "face_nm_f32", "cell_cellfid")
+
+    def keep_only(self, names):
+        """Drop every table not in ``names`` (host-built tables, before an upload)."""
+        self.t = {k: v for k, v in self.t.items() if k in names}
+        return self
+
+    def upload_staged(self, device, stream, staging):
+        """Upload host-built tables with one copy: packed (256-byte aligned) into the pinned
+        byte tensor ``staging`` (grown as needed; the caller keeps it unused until the copy on
+        ``stream`` has run), copied to one device buffer, tables as views of it.  The
+        permutations stay on the host."""
+        layout, off = [], 0
+        for k, a in self.t.items():
+            off = (off + 255) // 256 * 256
+            layout.append((k, a, off))
+            off += a.nbytes
+        if staging.numel() < off:
+            raise ValueError("staging buffer too small: %d < %d bytes" % (staging.numel(), off))
+        host = staging.numpy()
+        for k, a, o in layout:
+            host[o:o + a.nbytes] = np.ascontiguousarray(a).reshape(-1).view(np.uint8)
+        dev = torch.device(device)
+        with torch.cuda.stream(stream):
+            buf = torch.empty(off, dtype=torch.uint8, device=dev)
+            buf.copy_(staging[:off], non_blocking=True)
+        tdt = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64,
+               np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8}
+        self.t = {k: buf[o:o + a.nbytes].view(tdt[a.dtype]).view(a.shape) for k, a, o in layout}
+        self._buf = buf
+        self.device = dev
+        self.A = None
+        self.struct = self._make_struct()
+        return off
+
     def strip(self):
         """Drop the host arrays ``A`` (before sending host-built tables to another process)."""
         self.A = None

@@ -155,8 +155,13 @@ def _dot3(a, b):
     return a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1] + a[:, 2] * b[:, 2]
 
 
-def build(elements, vertex, dim, need_cellnid=True):
-    """All ``Domain`` arrays of the explicit step for a single-rank mesh."""
+def build(elements, vertex, dim, need_cellnid=True, halo_rim=False):
+    """All ``Domain`` arrays of the explicit step for a single-rank mesh.
+
+    ``halo_rim=True`` (the submesh of one shard, ``partition.py``): boundary faces that
+    belong to no side are the cut between the shard's halo and the rest of the mesh; they
+    are named 10, manapy's halo-face name, and listed in ``halofaces`` instead of being
+    rejected."""
     elements = np.ascontiguousarray(elements, dtype=I32)
     vertex = np.ascontiguousarray(vertex, dtype=np.float64)
     dim = int(dim)
@@ -318,6 +323,12 @@ def build(elements, vertex, dim, need_cellnid=True):
     # list), and name 0 (all vertices untagged: manapy would treat them as inner faces
     # reading cell -1)
     unmatched = boundary_mask & ((name >= 100) | (name == 0))
+    if halo_rim:
+        name[unmatched] = 10
+        A["faces_name"] = name
+        A["innerfaces"] = where(0)
+        A["halofaces"] = np.nonzero(unmatched)[0].astype(I32)
+        unmatched = np.zeros_like(unmatched)
     A["unmatched_boundary_faces"] = np.nonzero(unmatched)[0].astype(I32)
 
     # ---- ghost centres, ddm_utils2d.py:172-187 / ddm_utils3d.py:96-118

@@ -1,0 +1,148 @@
+"""Spatial sharding of one mesh over ranks (manapy's MPI domain decomposition, rebuilt).
+
+manapy partitions the dual graph with METIS and exchanges a one-layer vertex halo
+before each gradient, limiter and flux evaluation (``manapy/ast/core.py:415-478``,
+``manapy/comms/communication.py:86-145``) plus a dt min-allreduce per step
+(``manapy/solvers/advecdiff/system.py:152``).  Here:
+
+* each rank owns a contiguous range of the cells' Morton order (equal counts);
+* its submesh is the owned cells plus every cell within two vertex-adjacency
+  layers of them (the halo), cells and nodes kept in ascending global order;
+* one exchange per step refreshes the halo values from their owners; the halo is
+  deep enough that an owned cell's update reads only halo cells whose own
+  gradient, limiter and vertex values are complete, so nothing else is
+  exchanged (manapy exchanges four more times per step for order 2);
+* dt is the min over ranks of the min over each rank's cells.
+
+Because the submesh keeps global order, every per-cell list of an owned cell has
+the same members in the same order as on the whole mesh and every number is
+computed by the same operations: an owned cell's result is bit-identical to the
+single-domain result.  The cut faces at the outer edge of the halo are halo faces
+(name 10) with no ghost rule; only outer-halo cells touch them.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import reorder
+
+__all__ = ["partition_cells", "Shard", "build_shards", "HaloExchange"]
+
+
+def partition_cells(center, dim, nparts):
+    """Owner rank of every cell: equal contiguous ranges of the Morton order."""
+    order = reorder.morton_cells(center, dim)
+    nc = len(order)
+    bounds = np.round(np.linspace(0, nc, nparts + 1)).astype(np.int64)
+    owner = np.empty(nc, dtype=np.int32)
+    for r in range(nparts):
+        owner[order[bounds[r]:bounds[r + 1]]] = r
+    return owner
+
+
+def _neighbours(cellnid_ptr, cellnid_idx, mask):
+    rows = np.nonzero(mask)[0]
+    cnt = cellnid_ptr[rows + 1] - cellnid_ptr[rows]
+    starts = np.repeat(cellnid_ptr[rows], cnt)
+    offs = np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    out = np.zeros_like(mask)
+    out[cellnid_idx[starts + offs]] = True
+    return out
+
+
+@dataclasses.dataclass
+class Shard:
+    rank: int
+    cells: np.ndarray      # global ids of the submesh cells, ascending
+    owned: np.ndarray      # bool per submesh cell
+    nodes: np.ndarray      # global ids of the submesh nodes, ascending
+    elements: np.ndarray   # submesh connectivity (local node ids, count column)
+    vertex: np.ndarray     # submesh vertices (global tags kept)
+    send: dict             # peer rank -> local indices of owned cells the peer holds as halo
+    recv: dict             # peer rank -> local indices of halo cells owned by the peer
+
+    @property
+    def nowned(self):
+        return int(self.owned.sum())
+
+
+def build_shards(elements, vertex, dim, nparts, A=None, layers=2):
+    """The ``nparts`` shards of a mesh.  ``A``: its ``geometry.build`` arrays (built if
+    not given; only the cell centres and vertex-neighbour lists are read)."""
+    from . import geometry
+    if A is None:
+        A = geometry.build(elements, vertex, dim)
+    nc = int(A["nbcells"])
+    k = int(elements[0, -1])
+    owner = partition_cells(A["cells_center"], dim, nparts)
+    shards = []
+    for r in range(nparts):
+        own = owner == r
+        cur = own.copy()
+        for _ in range(layers):
+            cur |= _neighbours(A["cellnid_ptr"], A["cellnid_idx"], cur)
+        cells = np.nonzero(cur)[0]
+        nodes = np.unique(elements[cells, :k])
+        local = np.searchsorted(nodes, elements[cells, :k]).astype(np.int32)
+        el = np.empty((len(cells), k + 1), dtype=np.int32)
+        el[:, :k] = local
+        el[:, k] = k
+        shards.append(Shard(rank=r, cells=cells, owned=own[cells], nodes=nodes, elements=el,
+                            vertex=np.ascontiguousarray(vertex[nodes]), send={}, recv={}))
+    # exchange plan: rank r receives its halo cells from their owners, ordered by global id
+    for sh in shards:
+        halo = sh.cells[~sh.owned]
+        for q in np.unique(owner[halo]):
+            g = halo[owner[halo] == q]
+            sh.recv[int(q)] = np.searchsorted(sh.cells, g).astype(np.int64)
+            shards[q].send[sh.rank] = np.searchsorted(shards[q].cells, g).astype(np.int64)
+    assert all(len(s.cells) for s in shards) and nc == sum(s.nowned for s in shards)
+    return shards
+
+
+class HaloExchange:
+    """Refresh the halo entries of a per-rank cell array from their owners.
+
+    Point-to-point sends and receives (``torch.distributed.batch_isend_irecv``) of the
+    packed values, peers in ascending rank order on every rank; with the NCCL backend
+    the buffers stay on the device, with gloo they are staged through host memory.
+    """
+
+    def __init__(self, shard, group=None, device=None):
+        import torch
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.rank = shard.rank
+        self.device = device
+        self.peers = sorted(set(shard.send) | set(shard.recv))
+        to = (lambda a: torch.from_numpy(a).to(device)) if device is not None else torch.from_numpy
+        self.send_idx = {q: to(shard.send.get(q, np.zeros(0, np.int64))) for q in self.peers}
+        self.recv_idx = {q: to(shard.recv.get(q, np.zeros(0, np.int64))) for q in self.peers}
+        backend = dist.get_backend(group)
+        self.stage = backend == "gloo"
+
+    def exchange(self, field):
+        """In place: field[halo] = owners' values (field: 1-D tensor over the submesh cells)."""
+        import torch
+        dist = self.dist
+        ops, recv = [], {}
+        for q in self.peers:
+            s = field.index_select(0, self.send_idx[q])
+            r = torch.empty(len(self.recv_idx[q]), dtype=field.dtype, device=field.device)
+            if self.stage:
+                s, r = s.cpu(), r.cpu()
+            recv[q] = r
+            if len(s):
+                ops.append(dist.P2POp(dist.isend, s, q, group=self.group))
+            if len(r):
+                ops.append(dist.P2POp(dist.irecv, r, q, group=self.group))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        for q in self.peers:
+            if len(recv[q]):
+                field.index_copy_(0, self.recv_idx[q], recv[q].to(field.device))
+        return field

@@ -104,6 +104,7 @@ def prepare(req):
     el, vx = meshgen.square_triangles(req.n, seed=req.seed)
     dm = DeviceMesh.from_native(el, vx)       # the native host builder (C++)
     A = dm.A
+    dm.keep_only(DeviceMesh.SERVE_TABLES)
     bc = None
     if req.kind == "advdiff":
         res = B.resolve(A, {s: "dirichlet" for s in SIDES}, {s: 0.0 for s in SIDES})
@@ -112,6 +113,13 @@ def prepare(req):
     init = [a[dm.R.cperm] for a in initial_state(req, A["cells_center"])]
     dm.strip()
     return req, dm, bc, init
+
+
+def _warm(_):
+    """Worker start-up: load the modules and the native builder."""
+    from . import device, meshgen, native  # noqa: F401
+    native.lib()
+    return os.getpid()
 
 
 # ------------------------------------------------------------------ device side
@@ -123,9 +131,10 @@ def _p(t):
 class _Slot:
     """One admitted request: its device tables, fields and batch item."""
 
-    def __init__(self, req, dm, bc, init, dev, stream):
+    def __init__(self, req, dm, bc, init, dev, stream, staging):
         self.req = req
-        self.dm = dm.upload(dev, stream)
+        dm.upload_staged(dev, stream, staging)
+        self.dm = dm
         self.bc = bc.upload(dev, stream) if bc is not None else None
         nc, nf = dm.nbcells, dm.nbfaces
         f32 = torch.float32
@@ -213,6 +222,38 @@ class BatchServer:
         self._graph = None
         self._tables = None
         self._old = []
+        self._staging = None
+        self._staging_ev = None
+        self.pool = None
+        self.stats = {}
+
+    def start_pool(self):
+        """Start the mesh-preparation worker processes (and load their modules) ahead of a run."""
+        if self.workers > 0 and self.pool is None:
+            self.pool = cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn"))
+            list(self.pool.map(_warm, range(self.workers)))
+        return self
+
+    def stop_pool(self):
+        if self.pool is not None:
+            self.pool.shutdown(cancel_futures=True)
+            self.pool = None
+
+    def _stage(self, nbytes):
+        """The pinned staging buffer of mesh uploads, free for reuse (its last copy has run)."""
+        if self._staging_ev is not None:
+            self._staging_ev.synchronize()
+        if self._staging is None or self._staging.numel() < nbytes:
+            self._staging = torch.empty(int(nbytes * 1.25) + (1 << 20), dtype=torch.uint8, pin_memory=True)
+        return self._staging
+
+    def _admit(self, req, dm, bc, init):
+        need = sum(int(a.nbytes) + 256 for a in dm.t.values())
+        slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream, self._stage(need))
+        self._staging_ev = torch.cuda.Event()
+        self._staging_ev.record(self.upload_stream)
+        self.stream.wait_event(slot.ready)
+        return slot
 
     # -------------------------------------------------------------- batch tables
     def _build_tables(self):
@@ -307,13 +348,15 @@ class BatchServer:
         """Admit all ``requests`` at once (prepared beforehand), then time ``steps`` batch
         steps on the device with CUDA events.  Returns (cell-updates per second, seconds)."""
         if self.workers > 0:
-            with cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn")) as pool:
-                prepared = list(pool.map(prepare, requests))
+            own = self.pool is None
+            self.start_pool()
+            prepared = list(self.pool.map(prepare, requests))
+            if own:
+                self.stop_pool()
         else:
             prepared = [prepare(r) for r in requests]
         for req, dm, bc, init in prepared:
-            slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream)
-            self.stream.wait_event(slot.ready)
+            slot = self._admit(req, dm, bc, init)
             slot.fam = 0 if req.kind == "advdiff" else 1
             slot.start, slot.end = self.clock_host[slot.fam], 1 << 30
             slot.admitted = 0.0
@@ -338,9 +381,12 @@ class BatchServer:
         list of per-request records: arrival, admission, completion, latency (seconds from
         arrival to the result on the host), cells, steps, and the result arrays if asked."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        pool = None
-        if self.workers > 0:
-            pool = cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn"))
+        own_pool = self.workers > 0 and self.pool is None
+        if own_pool:
+            self.start_pool()
+        pool = self.pool if self.workers > 0 else None
+        st = self.stats = {k: 0.0 for k in ("receive", "admit", "retable", "launch", "throttle", "complete", "idle")}
+        inflight = []          # events of the chunks on the device, oldest first
         futures = {}
         prepared = []          # (req, dm, bc, init), in arrival order
         nxt = 0
@@ -359,9 +405,12 @@ class BatchServer:
                     else:
                         prepared.append(prepare(r))
                     nxt += 1
+                ta = time.perf_counter()
                 for rid in [k for k, f in futures.items() if f.done()]:
                     prepared.append(futures.pop(rid).result())
                 prepared.sort(key=lambda x: x[0].arrival)
+                tb = time.perf_counter()
+                st["receive"] += tb - ta
                 # admission (between steps): FIFO while a slot and the budget allow
                 changed = False
                 while prepared and len(self.active) < self.max_active:
@@ -370,8 +419,7 @@ class BatchServer:
                     if used + est > self.budget and self.active:
                         break
                     prepared.pop(0)
-                    slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream)
-                    self.stream.wait_event(slot.ready)
+                    slot = self._admit(req, dm, bc, init)
                     slot.admitted = time.perf_counter() - t0
                     slot.fam = 0 if req.kind == "advdiff" else 1
                     slot.start = self.clock_host[slot.fam]
@@ -379,18 +427,34 @@ class BatchServer:
                     used += slot.nbytes
                     self.active[req.rid] = slot
                     changed = True
+                tc = time.perf_counter()
+                st["admit"] += tc - tb
                 if changed:
                     self._retable()
+                td = time.perf_counter()
+                st["retable"] += td - tc
                 if not self.active:
                     if nxt >= len(reqs) and not futures and not prepared and not pending_done:
                         break
-                    self._complete(pending_done, done, t0, keep_results, log)
+                    used -= self._complete(pending_done, done, t0, keep_results, log)
                     time.sleep(0.002)
+                    st["idle"] += time.perf_counter() - td
                     continue
+                # keep at most two chunks queued on the device, so that admissions and
+                # retirements take effect within about one chunk
+                while len(inflight) >= 2:
+                    inflight.pop(0).synchronize()
+                te = time.perf_counter()
+                st["throttle"] += te - td
                 # advance to the next finishing request or one chunk, whichever is first
                 remaining = min(s.end - self.clock_host[s.fam] for s in self.active.values())
                 nsteps = max(1, min(self.chunk, remaining))
                 self._run_chunk(nsteps)
+                ev_chunk = torch.cuda.Event()
+                ev_chunk.record(self.stream)
+                inflight.append(ev_chunk)
+                tf = time.perf_counter()
+                st["launch"] += tf - te
                 fams = {s.fam for s in self.active.values()}
                 for f in fams:
                     self.clock_host[f] += nsteps
@@ -404,12 +468,14 @@ class BatchServer:
                     ev.record(self.stream)
                     pending_done.append((ev, fin, outs))
                     self._retable()
+                tg = time.perf_counter()
                 used -= self._complete(pending_done, done, t0, keep_results, log)
+                st["complete"] += time.perf_counter() - tg
             torch.cuda.synchronize(self.dev)
             used -= self._complete(pending_done, done, t0, keep_results, log)
         finally:
-            if pool:
-                pool.shutdown(cancel_futures=True)
+            if own_pool:
+                self.stop_pool()
         return done
 
     def _retable(self):
@@ -435,7 +501,7 @@ class BatchServer:
                        "arrival": s.req.arrival, "admitted": s.admitted, "done": tdone,
                        "latency": tdone - s.req.arrival}
                 if keep_results:
-                    inv = s.dm.inv["cell"].cpu().numpy()
+                    inv = np.asarray(s.dm.inv["cell"])
                     rec["result"] = [x.numpy()[inv] for x in o]
                 done.append(rec)
                 freed += s.nbytes
