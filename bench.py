@@ -54,7 +54,7 @@ def parse():
                     help="resident batch of uneven meshes: batched FP32-compensated kernels vs serial FP64 solves")
     ap.add_argument("--meshes", type=int, default=48, help="batched: number of meshes")
     ap.add_argument("--requests", type=int, default=300, help="serving: number of requests")
-    ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (requests/s)")
+    ap.add_argument("--rate", type=float, default=15.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--serial-sample", type=int, default=60, help="serving: requests timed serially in FP64")
     ap.add_argument("--workers", type=int, default=None, help="serving: mesh-preparation processes")
     ap.add_argument("--n", type=int, default=None, help="mesh resolution override (small profiling cases)")

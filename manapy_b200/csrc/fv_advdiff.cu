@@ -450,13 +450,14 @@ __global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_
 #define MB_P1_MIN_BLOCKS 6
 #endif
 
+// block `bid` of phase 1: blocks [0, ncb) gradient + limiter records, the rest node values
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
-                                                      double *__restrict__ rec, double *__restrict__ wn, int ncb) {
+__device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, const double *__restrict__ w,
+                                          double *__restrict__ rec, double *__restrict__ wn, int ncb, int bid) {
   const GhostRule ghost = make_rule(m, bc, w);
   const int lane = threadIdx.x & 31;
-  if (ORDER2 && (int)blockIdx.x < ncb) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ORDER2 && bid < ncb) {
+    const int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.nbcells) return;
     const double2 c = ldd2(m.cell_xy + 2 * i);
     const double wi = ld(w + i);
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh 
     return;
   }
   if (DIFF) {
-    const int n = (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x;
+    const int n = (bid - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x;
     if (n >= m.nbnodes) return;
     double acc = 0.;
     const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
@@ -555,19 +556,24 @@ __global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh 
   }
 }
 
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+                                                      double *__restrict__ rec, double *__restrict__ wn, int ncb) {
+  f2_phase1<ORDER2, DIFF>(m, bc, w, rec, wn, ncb, blockIdx.x);
+}
+
 #ifndef MB_P2_MIN_BLOCKS
 #define MB_P2_MIN_BLOCKS 3
 #endif
 
+// block `bid` of phase 2: fluxes and update of its cells
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
-                                                         const double *__restrict__ w, double *__restrict__ w_out,
-                                                         const double *__restrict__ sign,
-                                                         const double *__restrict__ src,
-                                                         const double *__restrict__ dt_dev,
-                                                         const double *__restrict__ rec,
-                                                         const double *__restrict__ wn) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p,
+                                          const double *__restrict__ w, double *__restrict__ w_out,
+                                          const double *__restrict__ sign, const double *__restrict__ src,
+                                          const double *__restrict__ dt_dev, const double *__restrict__ rec,
+                                          const double *__restrict__ wn, int bid) {
+  const int i = bid * blockDim.x + threadIdx.x;
   if (i >= m.nbcells) return;
   const GhostRule ghost = make_rule(m, bc, w);
   const int4 vt = ld4(m.cell_vtx + 4 * i);
@@ -671,6 +677,17 @@ __global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh 
   w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
 }
 
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+                                                         const double *__restrict__ w, double *__restrict__ w_out,
+                                                         const double *__restrict__ sign,
+                                                         const double *__restrict__ src,
+                                                         const double *__restrict__ dt_dev,
+                                                         const double *__restrict__ rec,
+                                                         const double *__restrict__ wn) {
+  f2_phase2<ORDER2, DIFF>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- fused step, compact 3D layout
 //
 // Tetrahedra.  Local face j of a cell is (v0,v1,v2), (v2,v3,v0), (v0,v1,v3),
@@ -684,7 +701,10 @@ __global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh 
 
 
 #ifndef MB_P1_3D_MIN_BLOCKS
-#define MB_P1_3D_MIN_BLOCKS 3
+#define MB_P1_3D_MIN_BLOCKS 4
+#endif
+#ifndef MB_F3_LSQ_BATCH
+#define MB_F3_LSQ_BATCH 4
 #endif
 
 template <bool ORDER2, bool DIFF>
@@ -702,7 +722,25 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
     const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
     const int L = (se - sb) >> 5;
     const int32_t *ix = m.lsq_sell_idx + sb + lane;
-    for (int k = 0; k < L; ++k) {
+    int k = 0;
+    // batches of MB_F3_LSQ_BATCH neighbours: their gathers in flight together, terms added in order
+    for (; k + MB_F3_LSQ_BATCH <= L; k += MB_F3_LSQ_BATCH) {
+      int cc[MB_F3_LSQ_BATCH];
+      D3 pc[MB_F3_LSQ_BATCH];
+      double wc[MB_F3_LSQ_BATCH];
+#pragma unroll
+      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) { cc[u] = ld(ix + 32 * (k + u)); cc[u] = cc[u] < 0 ? i : cc[u]; }
+#pragma unroll
+      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) { pc[u] = ld3(m.cell_xy + 4 * cc[u]); wc[u] = ld(w + cc[u]); }
+#pragma unroll
+      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) {
+        const double dx = pc[u].x - c.x, dy = pc[u].y - c.y, dz = pc[u].z - c.z, dw = wc[u] - wi;
+        ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+        ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+        jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
+      }
+    }
+    for (; k < L; ++k) {
       int cc = ld(ix + 32 * k);
       cc = cc < 0 ? i : cc;
       const D3 pc = ld3(m.cell_xy + 4 * cc);
@@ -771,8 +809,12 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
   }
 }
 
+#ifndef MB_P2_3D_MIN_BLOCKS
+#define MB_P2_3D_MIN_BLOCKS 2
+#endif
+
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, 2) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+__global__ void __launch_bounds__(kBlock, MB_P2_3D_MIN_BLOCKS) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,

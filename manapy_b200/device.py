@@ -30,6 +30,35 @@ def _upload(a, dev, stream):
         return t.pin_memory().to(dev, non_blocking=True)
 
 
+_TORCH_DT = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64,
+             np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8, np.dtype(np.int8): torch.int8}
+
+
+def staged_nbytes(arrays):
+    return sum((int(a.nbytes) + 255) // 256 * 256 for a in arrays.values())
+
+
+def stage_upload(arrays, device, stream, staging):
+    """Host arrays to ``device`` with one copy: packed at 256-byte aligned offsets into the
+    pinned byte tensor ``staging`` (the caller keeps it unused until the copy on ``stream``
+    has run), copied into one device buffer on ``stream``; returns (views by name, buffer)."""
+    layout, off = [], 0
+    for k, a in arrays.items():
+        a = np.ascontiguousarray(a)
+        layout.append((k, a, off))
+        off += (a.nbytes + 255) // 256 * 256
+    if staging.numel() < off:
+        raise ValueError("staging buffer too small: %d < %d bytes" % (staging.numel(), off))
+    host = staging.numpy()
+    for k, a, o in layout:
+        host[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+    with torch.cuda.stream(stream):
+        buf = torch.empty(max(off, 1), dtype=torch.uint8, device=device)
+        buf.copy_(staging[:max(off, 1)], non_blocking=True)
+    views = {k: buf[o:o + a.nbytes].view(_TORCH_DT[a.dtype]).view(a.shape) for k, a, o in layout}
+    return views, buf
+
+
 def cell_order_codes(faceid_local):
     """uint8 per cell: slot visited k-th in ascending face id, 2 bits per k."""
     order = np.argsort(faceid_local, axis=1, kind="stable").astype(np.uint32)
@@ -261,33 +290,20 @@ class DeviceMesh:
         self.t = {k: v for k, v in self.t.items() if k in names}
         return self
 
-    def upload_staged(self, device, stream, staging):
-        """Upload host-built tables with one copy: packed (256-byte aligned) into the pinned
-        byte tensor ``staging`` (grown as needed; the caller keeps it unused until the copy on
-        ``stream`` has run), copied to one device buffer, tables as views of it.  The
-        permutations stay on the host."""
-        layout, off = [], 0
-        for k, a in self.t.items():
-            off = (off + 255) // 256 * 256
-            layout.append((k, a, off))
-            off += a.nbytes
-        if staging.numel() < off:
-            raise ValueError("staging buffer too small: %d < %d bytes" % (staging.numel(), off))
-        host = staging.numpy()
-        for k, a, o in layout:
-            host[o:o + a.nbytes] = np.ascontiguousarray(a).reshape(-1).view(np.uint8)
-        dev = torch.device(device)
-        with torch.cuda.stream(stream):
-            buf = torch.empty(off, dtype=torch.uint8, device=dev)
-            buf.copy_(staging[:off], non_blocking=True)
-        tdt = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64,
-               np.dtype(np.float32): torch.float32, np.dtype(np.uint8): torch.uint8}
-        self.t = {k: buf[o:o + a.nbytes].view(tdt[a.dtype]).view(a.shape) for k, a, o in layout}
+    def upload_staged(self, device, stream, staging, extra=None):
+        """Upload host-built tables with one copy (``stage_upload``); the permutations stay on
+        the host.  ``extra``: more host arrays to send in the same copy; returns their device
+        views."""
+        arrays = dict(self.t)
+        for k, a in (extra or {}).items():
+            arrays["extra." + k] = a
+        views, buf = stage_upload(arrays, device, stream, staging)
+        self.t = {k: v for k, v in views.items() if not k.startswith("extra.")}
         self._buf = buf
-        self.device = dev
+        self.device = torch.device(device)
         self.A = None
         self.struct = self._make_struct()
-        return off
+        return {k[6:]: v for k, v in views.items() if k.startswith("extra.")}
 
     def strip(self):
         """Drop the host arrays ``A`` (before sending host-built tables to another process)."""

@@ -131,15 +131,27 @@ def _p(t):
 class _Slot:
     """One admitted request: its device tables, fields and batch item."""
 
-    def __init__(self, req, dm, bc, init, dev, stream, staging):
+    def __init__(self, req, dm, bc, init, dev, stream, staging, stats=None):
+        stats = stats if stats is not None else {}
+        t0 = time.perf_counter()
         self.req = req
-        dm.upload_staged(dev, stream, staging)
+        extra = {"init%d" % k: np.ascontiguousarray(a, dtype=np.float64) for k, a in enumerate(init)}
+        if bc is not None:
+            extra.update(bc_kind=bc.kind, bc_value=bc.value, bc_grad=bc.face_grad_on)
+        views = dm.upload_staged(dev, stream, staging, extra)   # tables, rules and state: one copy
         self.dm = dm
-        self.bc = bc.upload(dev, stream) if bc is not None else None
+        t1 = time.perf_counter()
+        if bc is not None:
+            bc.kind, bc.value, bc.face_grad_on = views["bc_kind"], views["bc_value"], views["bc_grad"]
+            bc.struct = bc._make_struct()
+        self.bc = bc
+        t2 = time.perf_counter()
+        stats["admit_tables"] = stats.get("admit_tables", 0.0) + t1 - t0
+        stats["admit_bc"] = stats.get("admit_bc", 0.0) + t2 - t1
         nc, nf = dm.nbcells, dm.nbfaces
         f32 = torch.float32
         with torch.cuda.stream(stream):
-            up = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(dev, non_blocking=True) for a in init]
+            up = [views["init%d" % k] for k in range(len(init))]
             if req.kind == "advdiff":
                 self.w = [up[0].float(), torch.empty(nc, dtype=f32, device=dev)]
                 self.lo = [(up[0] - self.w[0].double()).float(), torch.empty(nc, dtype=f32, device=dev)]
@@ -172,6 +184,7 @@ class _Slot:
                           _p(self.dt), stream.cuda_stream)
             self.ready = torch.cuda.Event()
             self.ready.record(stream)
+        stats["admit_setup"] = stats.get("admit_setup", 0.0) + time.perf_counter() - t2
         self._keep = up  # the uploads stay alive until the copies have run
         self.start = self.end = None
         self.fam = None
@@ -248,8 +261,13 @@ class BatchServer:
         return self._staging
 
     def _admit(self, req, dm, bc, init):
-        need = sum(int(a.nbytes) + 256 for a in dm.t.values())
-        slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream, self._stage(need))
+        from .device import staged_nbytes
+        need = staged_nbytes(dm.t) + sum(int(np.asarray(a).nbytes) + 512 for a in init) + (
+            0 if bc is None else staged_nbytes({"k": bc.kind, "v": bc.value, "g": bc.face_grad_on}))
+        t0 = time.perf_counter()
+        staging = self._stage(need)
+        self.stats["admit_stage_wait"] = self.stats.get("admit_stage_wait", 0.0) + time.perf_counter() - t0
+        slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream, staging, self.stats)
         self._staging_ev = torch.cuda.Event()
         self._staging_ev.record(self.upload_stream)
         self.stream.wait_event(slot.ready)
@@ -386,6 +404,8 @@ class BatchServer:
             self.start_pool()
         pool = self.pool if self.workers > 0 else None
         st = self.stats = {k: 0.0 for k in ("receive", "admit", "retable", "launch", "throttle", "complete", "idle")}
+        for k in ("admit_stage_wait", "admit_tables", "admit_bc", "admit_setup"):
+            st[k] = 0.0
         inflight = []          # events of the chunks on the device, oldest first
         futures = {}
         prepared = []          # (req, dm, bc, init), in arrival order
