@@ -44,7 +44,9 @@ class AdvectionDiffusionSolver:
                    ("cfl", float, .4, 0, "cfl of the explicit scheme"),
                    ("precision", str, "fp64", 0, "fp64 (manapy's arithmetic) or fp32c: FP32 state and "
                                                  "fluxes with compensated per-cell sums, FP64 geometry and dt "
-                                                 "(no counterpart in manapy)")]
+                                                 "(no counterpart in manapy)"),
+                   ("graph_depth", object, "auto", 0, "steps per CUDA-graph replay in advance(graph=True): an "
+                                                      "even number, or 'auto' (measured by manapy_b200.autotune)")]
 
     @classmethod
     def process_conf(cls, conf, kwargs):
@@ -84,6 +86,10 @@ class AdvectionDiffusionSolver:
         self.precision = str(get("precision"))
         if self.precision not in ("fp64", "fp32c"):
             raise ValueError("precision must be 'fp64' or 'fp32c'")
+        depth = get("graph_depth")
+        if depth != "auto" and (int(depth) < 2 or int(depth) % 2):
+            raise ValueError("graph_depth must be 'auto' or an even number >= 2")
+        self.graph_depth = depth if depth == "auto" else int(depth)
         self.diffusion = not (self.Dxx == self.Dyy == self.Dzz == 0)
         self.backend = self.domain.backend
         self.signature = self.domain.signature
@@ -359,7 +365,8 @@ class AdvectionDiffusionSolver:
         var.dev("cell")
         if self._spare is None:
             self._spare = torch.empty_like(var.dev("cell"))
-        if not graph or n < 2:
+        depth = self._depth() if graph else 2
+        if not graph or n < depth:
             for _ in range(n):
                 self._fused_step()
         else:
@@ -373,12 +380,12 @@ class AdvectionDiffusionSolver:
                 a.copy_(cur)
                 var.swap_cell(a)
                 self._spare = b
-            for _ in range(n // 2):
+            for _ in range(n // depth):
                 g.replay()
-            if n // 2:
+            if n // depth:
                 var._s.version["cell"] += 1
                 self._install_lazies(self._spare)
-            if n % 2:
+            for _ in range(n % depth):
                 self._fused_step()
         if self._dt_host is None:
             self._dt_host = float(self._dt_dev.item())
@@ -386,7 +393,8 @@ class AdvectionDiffusionSolver:
         return n * self._dt_host
 
     def _advance_f32c(self, n, graph):
-        if not graph or n < 2:
+        depth = self._depth() if graph else 2
+        if not graph or n < depth:
             for _ in range(n):
                 self._fused_step_f32c()
             return
@@ -403,19 +411,28 @@ class AdvectionDiffusionSolver:
             with torch.cuda.stream(s):
                 with torch.cuda.graph(g, stream=s):
                     st = torch.cuda.current_stream(self._dm.device).cuda_stream
-                    self._call_f32c(0, src, st)
-                    self._call_f32c(1, src, st)
+                    for _ in range(depth // 2):
+                        self._call_f32c(0, src, st)
+                        self._call_f32c(1, src, st)
             torch.cuda.current_stream(self._dm.device).wait_stream(s)
             self._graph, self._graph_src = g, _p(src)
-        for _ in range(n // 2):
+        for _ in range(n // depth):
             self._graph.replay()
-        if n // 2:
+        if n // depth:
             self._f32_publish(1)
-        if n % 2:
+        for _ in range(n % depth):
             self._fused_step_f32c()
 
+    def _depth(self):
+        """Steps per graph replay (measured once per mesh size and scheme when 'auto')."""
+        if self.graph_depth == "auto":
+            from . import autotune
+            self.graph_depth = autotune.graph_depth(self)
+        return int(self.graph_depth)
+
     def _get_graph(self):
-        """Two fused steps (A->B, B->A) captured once; the cell buffer ends where it began."""
+        """``graph_depth`` fused steps (A->B, B->A, ...) captured once; the cell buffer ends
+        where it began."""
         if self._graph is not None:
             return self._graph
         var = self.var
@@ -432,7 +449,7 @@ class AdvectionDiffusionSolver:
             # warm-up outside capture is not needed: the library performs no lazy init
             with torch.cuda.graph(g, stream=s):
                 st = torch.cuda.current_stream(dm.device).cuda_stream
-                for x, y in ((a, b), (b, a)):
+                for x, y in ((a, b), (b, a)) * (int(self.graph_depth) // 2):
                     _lib.call("mb_advdiff_step", dm.struct, args[0], args[1], _p(x), _p(y), _p(self._sign),
                               src, _p(self._dt_dev), _p(cs), _p(ns), st)
         torch.cuda.current_stream(dm.device).wait_stream(s)

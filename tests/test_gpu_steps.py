@@ -81,8 +81,8 @@ def test_graph_and_eager_agree_bitwise(cuda):
     assert np.array_equal(w1.cell, w2.cell)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
-def test_graph_runs_resume_after_odd_step_counts(precision, cuda):
+@pytest.mark.parametrize("precision,depth", [("fp64", 2), ("fp32c", 2), ("fp64", 4), ("fp32c", 4)])
+def test_graph_runs_resume_after_odd_step_counts(precision, depth, cuda):
     """advance() calls of odd lengths, a manapy-style step and a cell edit in between: the
     replayed graphs continue from the current state exactly as eager steps do."""
     wl = W.C2.scaled(n=30)
@@ -97,13 +97,14 @@ def test_graph_runs_resume_after_odd_step_counts(precision, cuda):
         u.interpolate_facetocell(); v.interpolate_facetocell()
         w.cell = wl.init(dom.cells.center)
         S = M.AdvectionDiffusionSolver(w, vel=(u, v), conf=M.Struct(Dxx=5e-4, Dyy=5e-4, order=2, cfl=0.8,
-                                                                     precision=precision))
+                                                                     precision=precision, graph_depth=depth))
         S.advance(3, graph=graph)
         S.advance(4, graph=graph)
         S.stepper(); S.compute_fluxes(); S.compute_new_val()
         S.advance(5, graph=graph)
         w.cell = w.cell * 0.75
         S.advance(6, graph=graph)
+        S.advance(11, graph=graph)
         runs.append(w.cell)
     assert np.array_equal(runs[0], runs[1])
 
@@ -202,3 +203,17 @@ def test_shallow_water_matches_reference(name, cuda):
         S.stepper(); S.compute_fluxes(); S.compute_new_val()
     for k, var in zip(("h", "hu", "hv"), vs[:3]):
         assert rel_max(var.cell, g[k + "_final"]) < TOL, k
+
+
+def test_autotuned_graph_depth_changes_no_result(cuda):
+    """graph_depth='auto' times several depths on the solver's own state and restores it."""
+    from manapy_b200 import autotune
+    autotune.clear()
+    wl = W.C1.scaled(n=30, steps=40)
+    el, vx = wl.mesh()
+    _, w1, S1 = _advdiff_api(el, vx, wl)
+    _, w2, S2 = _advdiff_api(el, vx, wl)
+    S1.advance(wl.steps, graph=True)
+    assert S1.graph_depth in autotune.CANDIDATES
+    S2.advance(wl.steps, graph=False)
+    assert np.array_equal(w1.cell, w2.cell)
