@@ -304,7 +304,8 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
         if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
         // Dxx n0 gx + Dyy n1 gy = sum_k c_k t_k, t = (vi1 + vl, vl + vi2, vi2 + vr, vr + vi1);
         // regrouped per value: a1 vi1 + a2 vi2 + al vl + ar vr
-        const double gxk = p.Dxx * n0 / (2 * air), gyk = p.Dyy * n1 / (2 * air);
+        const double r2a = 1. / (2 * air);
+        const double gxk = p.Dxx * n0 * r2a, gyk = p.Dyy * n1 * r2a;
         const double c1 = gxk * f1y - gyk * f1x, c2 = gxk * f2y - gyk * f2x;
         const double c3 = gxk * f3y - gyk * f3x, c4 = gxk * f4y - gyk * f4x;
         const double a1 = c1 + c4, a2 = c2 + c3, al = c1 + c2, ar = c3 + c4;
