@@ -28,7 +28,7 @@ from . import _lib
 from .base import Struct, make_get_conf, process_conf
 from .variable import Variable
 
-__all__ = ["AdvectionDiffusionSolver", "ShallowWaterSolver"]
+__all__ = ["AdvectionDiffusionSolver", "AdvectionSolver", "DiffusionSolver", "ShallowWaterSolver"]
 
 
 def _p(t):
@@ -456,6 +456,32 @@ class AdvectionDiffusionSolver:
         self._graph = g
         self._graph_bufs = (a, b)
         return g
+
+
+class AdvectionSolver(AdvectionDiffusionSolver):
+    """manapy/solvers/advec/system.py:20-154: the convective flux only (manapy's options:
+    dt, order, cfl).  Same step as ``AdvectionDiffusionSolver`` with no diffusion; manapy's
+    advection time step has no zero-speed guard (a cell with zero speed on every face
+    divides by zero there), here such a cell does not limit dt."""
+    _parameters = [p for p in AdvectionDiffusionSolver._parameters if p[0] not in ("Dxx", "Dyy", "Dzz")]
+
+    def __init__(self, var=None, vel=(None, None, None), conf=None, **kwargs):
+        super().__init__(var, vel, conf, **kwargs)
+        self.Dxx = self.Dyy = self.Dzz = np.float64(0.)
+        self.diffusion = False
+
+
+class DiffusionSolver(AdvectionDiffusionSolver):
+    """manapy/solvers/diffusion/system.py:20-156: the diamond diffusion flux only.  manapy
+    takes the velocity variables but uses none of them (its time step is the diffusion
+    bound alone, ``manapy/solvers/diffusion/fvm_utils.py:30-47``); here the step runs with
+    zero velocity, which adds exact zeros to the same sums."""
+
+    def __init__(self, var=None, vel=(None, None, None), conf=None, **kwargs):
+        super().__init__(var, vel, conf, **kwargs)
+        self.vel_given = (self.u, self.v, self.w)
+        self.u, self.v, self.w = (Variable(domain=self.domain) for _ in range(3))
+        self.order = np.int32(1)  # no convective flux, so no reconstruction either
 
 
 class ShallowWaterSolver:

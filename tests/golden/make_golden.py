@@ -19,6 +19,8 @@ Outputs (``*.npz``, committed):
   (200 steps), final field and dt sequence.
 * ``traj_o2.npz``, ``traj_3d.npz``, ``traj_sw1.npz``, ``traj_sw2.npz``:
   short second-order 2D, 3D and shallow-water runs.
+* ``traj_advec.npz``, ``traj_diff.npz``: the advection-only and diffusion-only solvers
+  (``manapy/solvers/advec``, ``manapy/solvers/diffusion``), short 2D runs.
 """
 from __future__ import annotations
 
@@ -38,7 +40,8 @@ sys.path.insert(0, HERE)
 from manapy_b200 import meshgen  # noqa: E402
 from manapy_b200 import workloads  # noqa: E402
 
-PARTS = ["dom2d", "dom3d", "k2d", "k3d", "traj_c1", "traj_o2", "traj_3d", "traj_sw1", "traj_sw2"]
+PARTS = ["dom2d", "dom3d", "k2d", "k3d", "traj_c1", "traj_o2", "traj_3d", "traj_sw1", "traj_sw2", "traj_advec",
+         "traj_diff"]
 
 
 def _domain_arrays(d, dim):
@@ -228,11 +231,16 @@ def _sw_kernels(d, rng):
     return out
 
 
-def _adv_run(dim, mesh, init, vel, D, order, cfl, steps, bcs, vals, snap=()):
+def _adv_run(dim, mesh, init, vel, D, order, cfl, steps, bcs, vals, snap=(), solver="advecdiff"):
     _ref()
     from manapy.ast import Variable
-    from manapy.solvers.advecdiff import AdvectionDiffusionSolver
     from manapy.base.base import Struct
+    if solver == "advec":
+        from manapy.solvers.advec import AdvectionSolver as AdvectionDiffusionSolver
+    elif solver == "diffusion":
+        from manapy.solvers.diffusion import DiffusionSolver as AdvectionDiffusionSolver
+    else:
+        from manapy.solvers.advecdiff import AdvectionDiffusionSolver
     r = _run(mesh, dim)
     d = r.domain
     w = Variable(domain=d, BC=bcs, values=vals)
@@ -284,6 +292,15 @@ def part_traj(name):
         el, vx = meshgen.cube_tetrahedra(wl.n, seed=wl.seed)
         out = _adv_run(3, (el, vx), wl.init, wl.velocity, wl.diffusion, wl.order, wl.cfl,
                        wl.steps, wl.bc, wl.bc_values, snap=(1, 10))
+    elif name in ("traj_advec", "traj_diff"):
+        wl = workloads.C2.scaled(n=24, steps=60)
+        el, vx = meshgen.square_triangles(wl.n, seed=wl.seed)
+        if name == "traj_advec":
+            out = _adv_run(2, (el, vx), wl.init, wl.velocity, (0.0, 0.0, 0.0), 2, wl.cfl, wl.steps, wl.bc,
+                           wl.bc_values, snap=(1, 10), solver="advec")
+        else:
+            out = _adv_run(2, (el, vx), wl.init, wl.velocity, (1e-3, 1e-3, 0.0), 1, wl.cfl, wl.steps, wl.bc,
+                           wl.bc_values, snap=(1, 10), solver="diffusion")
     else:
         order = 1 if name == "traj_sw1" else 2
         wl = workloads.C3.scaled(n=30, steps=100 if order == 1 else 60, order=order)

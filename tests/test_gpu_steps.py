@@ -217,3 +217,30 @@ def test_autotuned_graph_depth_changes_no_result(cuda):
     assert S1.graph_depth in autotune.CANDIDATES
     S2.advance(wl.steps, graph=False)
     assert np.array_equal(w1.cell, w2.cell)
+
+
+@pytest.mark.parametrize("name", ["traj_advec", "traj_diff"])
+def test_advection_and_diffusion_solvers_match_reference(name, cuda):
+    g = golden(name)
+    wl = W.C2.scaled(n=24)
+    dom = M.Domain(dim=2, mesh=(g["in_elements"], g["in_vertex"]))
+    w = M.Variable(domain=dom, BC=wl.bc, values=wl.bc_values)
+    u, v, wz = (M.Variable(domain=dom) for _ in range(3))
+    uf, vf, wf = wl.velocity(dom.faces.center)
+    u.face, v.face, wz.face = uf, vf, wf
+    for x in (u, v, wz):
+        x.interpolate_facetocell()
+    w.cell = g["w0"]
+    if name == "traj_advec":
+        S = M.AdvectionSolver(w, vel=(u, v, wz), conf=M.Struct(order=2, cfl=wl.cfl))
+    else:
+        S = M.DiffusionSolver(w, vel=(u, v, wz), conf=M.Struct(Dxx=1e-3, Dyy=1e-3, cfl=wl.cfl))
+    dts = []
+    for it in range(int(g["steps"])):
+        dts.append(S.stepper())
+        S.compute_fluxes()
+        S.compute_new_val()
+        if it + 1 in (1, 10):
+            assert rel_max(w.cell, g["w_step%d" % (it + 1)]) < TOL
+    assert rel_max(np.array(dts), g["dts"]) < 1e-14
+    assert rel_max(w.cell, g["w_final"]) < TOL

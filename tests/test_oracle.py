@@ -119,3 +119,25 @@ def test_sw_trajectories_match_reference(name):
     assert rel_max(np.array(mass), g["mass"]) < 1e-14
     for k in ("h", "hu", "hv"):
         assert rel_max(so.state()[k], g[k + "_final"]) < 1e-12, k
+
+
+@pytest.mark.parametrize("name", ["traj_advec", "traj_diff"])
+def test_oracle_matches_reference_advection_and_diffusion_solvers(name):
+    """manapy's advection-only and diffusion-only solvers are the advection-diffusion step
+    with no diffusion / with zero velocity (their own time steps differ only where those
+    terms vanish)."""
+    from manapy_b200 import workloads as W
+    g = golden(name)
+    wl = W.C2.scaled(n=24)
+    A = G.build(g["in_elements"], g["in_vertex"], 2)
+    if name == "traj_advec":
+        D, order, vel = (0., 0., 0.), 2, wl.velocity(A["faces_center"])
+    else:
+        D, order = (1e-3, 1e-3, 0.), 1
+        vel = tuple(np.zeros(A["nbfaces"]) for _ in range(3))
+    o = O.AdvDiffOracle(A, B.resolve(A, wl.bc, wl.bc_values), *D, order=order, cfl=wl.cfl)
+    o.set_velocity(*vel)
+    o.w[:] = g["w0"]
+    dts = [o.step() for _ in range(int(g["steps"]))]
+    assert rel_max(np.array(dts), g["dts"]) < 1e-15
+    assert rel_max(o.w, g["w_final"]) < 1e-14
