@@ -32,6 +32,8 @@ extern "C" {
 #define MB_EINVAL (-1)   /* bad argument (null pointer, bad size, bad dim) */
 #define MB_ECUDA (-2)    /* a CUDA launch or call failed */
 #define MB_ETOOBIG (-3)  /* the mesh needs more scratch than mb_advdiff_step_noalloc holds */
+#define MB_ENONFINITE (-4) /* mb_check_state: a NaN or infinite value */
+#define MB_ENEGATIVE (-5)  /* mb_check_state: a negative value where none is allowed (water depth) */
 
 /* Ghost rule of a boundary face (manapy/boundary/bc_utils.py:45-68). */
 #define MB_G_NONE 0
@@ -355,6 +357,13 @@ int mb_sw_batch_step_f32c(const mb_sw_item *items, const int32_t *face_map, int3
 int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                             const double *w_in, double *w_out, const double *sign_cf,
                             const double *src, const double *dt_dev, void *stream);
+
+/* State check (no counterpart in manapy, where NaNs propagate silently): scans n FP64 values
+ * (f64 != NULL) or FP32 values (f32 != NULL) for NaN / infinity and, with nonneg != 0, for
+ * negative values; ORs bit 0 (non-finite) and bit 1 (negative) into *flags (device int,
+ * zeroed by the caller).  The host reads flags after the stream: MB_ENONFINITE /
+ * MB_ENEGATIVE. */
+int mb_check_state(const double *f64, const float *f32, int64_t n, int32_t nonneg, int32_t *flags, void *stream);
 
 /* Library build information (architecture string), for diagnostics. */
 const char *mb_build_info(void);

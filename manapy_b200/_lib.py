@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # MANAPY_B200_LIB selects another build of the same library (A/B comparisons of build options)
 LIB_PATH = os.environ.get("MANAPY_B200_LIB") or os.path.join(HERE, "lib", "libmanapy_b200.so")
 
-MB_OK, MB_EINVAL, MB_ECUDA, MB_ETOOBIG = 0, -1, -2, -3
+MB_OK, MB_EINVAL, MB_ECUDA, MB_ETOOBIG, MB_ENONFINITE, MB_ENEGATIVE = 0, -1, -2, -3, -4, -5
 NOALLOC_SCRATCH_DOUBLES = 2 * 1024 * 1024
 G_NONE, G_DIRICHLET, G_NEUMANN, G_NONSLIP, G_NEUMANN_NH, G_CELL_AT_FACE = 0, 1, 2, 3, 4, 5
 
@@ -93,6 +93,7 @@ _SIGS = {
     "mb_advdiff_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],
+    "mb_check_state": [_vp, _vp, ctypes.c_int64, _i32, _vp, _vp],
     "mb_build_info": [],
 }
 _RESTYPES = {"mb_build_info": ctypes.c_char_p}
@@ -127,7 +128,8 @@ class MbError(RuntimeError):
 def check(rc: int, name: str = "call"):
     if rc != MB_OK:
         what = {MB_EINVAL: "invalid argument", MB_ECUDA: "CUDA error",
-                MB_ETOOBIG: "mesh too large for the built-in scratch"}.get(rc, "error %d" % rc)
+                MB_ETOOBIG: "mesh too large for the built-in scratch", MB_ENONFINITE: "non-finite value",
+                MB_ENEGATIVE: "negative value"}.get(rc, "error %d" % rc)
         raise MbError("%s failed: %s" % (name, what))
 
 

@@ -35,6 +35,24 @@ def _p(t):
     return t.data_ptr() if t is not None else None
 
 
+def check_state(arrays, nonneg=(), names=None):
+    """Raise ``FloatingPointError`` if a device array holds NaN or infinity, ``ValueError``
+    if an array listed in ``nonneg`` (by position) holds a negative value (the statuses
+    MB_ENONFINITE / MB_ENEGATIVE of ``mb_check_state``)."""
+    for k, t in enumerate(arrays):
+        flags = torch.zeros(1, dtype=torch.int32, device=t.device)
+        f64 = t if t.dtype == torch.float64 else None
+        f32 = t if t.dtype == torch.float32 else None
+        _lib.call("mb_check_state", _p(f64), _p(f32), t.numel(), int(k in nonneg), _p(flags),
+                  torch.cuda.current_stream(t.device).cuda_stream)
+        f = int(flags.item())
+        name = names[k] if names else "array %d" % k
+        if f & 1:
+            raise FloatingPointError("non-finite values in %s" % name)
+        if f & 2:
+            raise ValueError("negative values in %s" % name)
+
+
 class AdvectionDiffusionSolver:
     _parameters = [("Dxx", float, 0., 0., "Diffusion in x direction"),
                    ("Dyy", float, 0., 0., "Diffusion in y direction"),
@@ -338,6 +356,14 @@ class AdvectionDiffusionSolver:
         self._call_f32c(k, src, self._stream())
         self._w32_i = 1 - k
         self._f32_publish(k)
+
+    def check(self):
+        """Raise if the state holds NaN or infinity (manapy lets them propagate)."""
+        self._setup()
+        if self.precision == "fp32c" and self._w32 is not None and self.var.version("cell") == self._w32_key:
+            check_state([self._w32[self._w32_i]], names=["the FP32 state"])
+        else:
+            check_state([self.var.dev("cell")], names=["the cell values"])
 
     def launches_per_step(self):
         """Kernel launches of one fused step."""
@@ -751,6 +777,16 @@ class ShallowWaterSolver:
         self._cur = 1 - self._cur
         self._dt_key = self._state_key()
         self._dt_host = None
+
+    def check(self):
+        """Raise if h, hu, hv or hc holds NaN or infinity, or h is negative (a dry-out the
+        scheme does not handle; manapy lets both propagate)."""
+        self._setup()
+        if self.precision == "fp32c" and self._q32 is not None and self._keys() == self._q32_key:
+            arrays = self._q32[self._q32_i]
+        else:
+            arrays = [self.varbs[k].dev("cell") for k in ("h", "hu", "hv", "hc")]
+        check_state(arrays, nonneg=(0,), names=["h", "hu", "hv", "hc"])
 
     def mass(self):
         """FP64 sum of volume x h over the cells (no counterpart in manapy)."""

@@ -244,3 +244,30 @@ def test_advection_and_diffusion_solvers_match_reference(name, cuda):
             assert rel_max(w.cell, g["w_step%d" % (it + 1)]) < TOL
     assert rel_max(np.array(dts), g["dts"]) < 1e-14
     assert rel_max(w.cell, g["w_final"]) < TOL
+
+
+def test_state_checks_raise(cuda):
+    wl = W.C3.scaled(n=10, steps=1, order=1)
+    el, vx = wl.mesh()
+    dom, vs, S = _sw_api(el, vx, wl)
+    S.advance(2)
+    S.check()                        # a sound state passes
+    h = vs[0].cell
+    h[3] = -0.5
+    vs[0].cell = h
+    with pytest.raises(ValueError, match="negative"):
+        S.check()
+    h[3] = np.nan
+    vs[0].cell = h
+    with pytest.raises(FloatingPointError):
+        S.check()
+    wl2 = W.C1.scaled(n=10, steps=1)
+    el, vx = wl2.mesh()
+    _, w, S2 = _advdiff_api(el, vx, wl2)
+    S2.advance(2)
+    S2.check()
+    x = w.cell
+    x[0] = np.inf
+    w.cell = x
+    with pytest.raises(FloatingPointError):
+        S2.check()
