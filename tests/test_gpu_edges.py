@@ -22,10 +22,10 @@ def _run(el, vx, dim, bc, vals, D, order, vel, steps, src=None, init=None):
         var.interpolate_facetocell()
     cc = dom.cells.center
     w.cell = init(cc) if init else np.exp(-((cc[:, 0] - 0.4) ** 2 + (cc[:, 1] - 0.6) ** 2) / 0.05)
-    if src is not None:
-        w.source = src(cc)
     S = M.AdvectionDiffusionSolver(w, vel=tuple(vs), conf=M.Struct(Dxx=D, Dyy=D, Dzz=D if dim == 3 else 0.,
                                                                     order=order, cfl=0.5))
+    if src is not None:
+        w.source = src(cc)  # after the solver: constructing it resets the source term, as in manapy
     A = G.build(el, vx, dim)
     o = O.AdvDiffOracle(A, B.resolve(A, bc, vals), D, D, D if dim == 3 else 0., order=order, cfl=0.5)
     o.set_velocity(*vel(A["faces_center"]))
@@ -46,7 +46,8 @@ def _vel(fc):
 SIDES2 = ("in", "out", "upper", "bottom")
 
 
-@pytest.mark.parametrize("n", [1, 2, 3])
+@pytest.mark.parametrize("n", [2, 3, 4])  # n = 1: the bottom edge joins tags 1 and 2, which
+                                          # name no side (manapy rejects that mesh too)
 @pytest.mark.parametrize("order", [1, 2])
 def test_smallest_meshes(n, order, cuda):
     el, vx = meshgen.square_triangles(n, seed=n)
@@ -118,7 +119,7 @@ def test_lake_at_rest_initial_state(cuda):
                                  conf=M.Struct(order=1, cfl=0.5, precision=precision))
         S.advance(20)
         assert rel_max(vs[0].cell, so.h) < tol, precision
+        # near rest the momenta are rounding-level: compare them on the scale of h
         for k, var in zip(("hu", "hv"), vs[1:3]):
             ref = so.state()[k]
-            scale = max(np.abs(ref).max(), 1e-300)
-            assert np.max(np.abs(var.cell - ref)) / scale < (TOL if precision == "fp64" else 1e-4), (precision, k)
+            assert np.max(np.abs(var.cell - ref)) / np.abs(so.h).max() < tol, (precision, k)
