@@ -633,3 +633,97 @@ void or_term_source_srnh_sw(double *src_h, double *src_hu, double *src_hv, doubl
     src_Z[i] = 0.;
   }
 }
+
+/* ---- Euler, 2D, first-order Rusanov (manapy/solvers/euler/fvm_utils2d.py) ---- */
+
+static double pymax3(double a, double b, double c) {
+  /* Python's max(a, b, c): the first of the largest */
+  double m = a;
+  if (b > m) m = b;
+  if (c > m) m = c;
+  return m;
+}
+
+/* fvm_utils2d.py:1248-1292 compute_flux_euler_2d_rusanov (qr reads rhovl, as manapy does) */
+static void euler_rusanov(double rhol, double Pl, double rhoul, double rhovl, double rhoEl, double rhor, double Pr,
+                          double rhour, double rhovr, double rhoEr, const double *normal, double mesure,
+                          double gamma, double *F) {
+  double ql = (rhoul * normal[0] + rhovl * normal[1]);
+  double qr = (rhour * normal[0] + rhovl * normal[1]);
+  double cl = sqrt(gamma * Pl / rhol);
+  double cr = sqrt(gamma * Pr / rhor);
+  double fl_rho = (rhoul * normal[0] + rhovl * normal[1]);
+  double fl_rhou = ((rhoul * rhoul / rhol + Pl) * normal[0] + (rhoul * rhovl / rhol) * normal[1]);
+  double fl_rhov = ((rhovl * rhoul / rhol) * normal[0] + (rhovl * rhovl / rhol + Pl) * normal[1]);
+  double fl_rhoE = (rhoul / rhol * (rhoEl + Pl) * normal[0] + rhovl / rhol * (rhoEl + Pl) * normal[1]);
+  double fr_rho = (rhour * normal[0] + rhovr * normal[1]);
+  double fr_rhou = ((rhour * rhour / rhor + Pr) * normal[0] + (rhour * rhovr / rhor) * normal[1]);
+  double fr_rhov = ((rhovr * rhour / rhor) * normal[0] + (rhovr * rhovr / rhor + Pr) * normal[1]);
+  double fr_rhoE = (rhour / rhor * (rhoEr + Pr) * normal[0] + rhovr / rhor * (rhoEr + Pr) * normal[1]);
+  double Ll = pymax3(fabs((ql) / rhol - cl), fabs((ql) / rhol), fabs((ql) / rhol + cl));
+  double Lr = pymax3(fabs((qr) / rhor - cr), fabs((qr) / rhor), fabs((qr) / rhor + cr));
+  double S = Ll > Lr ? Ll : Lr;
+  F[0] = (0.5 * (fl_rho + fr_rho) - 0.5 * S * (rhor - rhol)) * mesure;
+  F[1] = (0.5 * (fl_rhou + fr_rhou) - 0.5 * S * (rhour - rhoul)) * mesure;
+  F[2] = (0.5 * (fl_rhov + fr_rhov) - 0.5 * S * (rhovr - rhovl)) * mesure;
+  F[3] = (0.5 * (fl_rhoE + fr_rhoE) - 0.5 * S * (rhoEr - rhoEl)) * mesure;
+}
+
+/* fvm_utils2d.py:1490-1611 explicitscheme_euler_2d_rusanov, face loop in face-id order
+ * (single rank: every face not named 0 reads the ghost arrays).
+ * q, g: rho, P, rhou, rhov, rhoE (cells / faces); rez: rho, rhou, rhov, rhoE */
+void or_euler_rusanov_2d(double *const rez[4], const double *const q[5], const double *const g[5],
+                         const int32_t *cellidf, const double *normalf, const double *mesuref,
+                         const int32_t *namef, int nf, int nc, double gamma) {
+  for (int c = 0; c < 4; c++)
+    for (int i = 0; i < nc; i++) rez[c][i] = 0.;
+  for (int i = 0; i < nf; i++) {
+    double norm[2] = {normalf[3 * i] / mesuref[i], normalf[3 * i + 1] / mesuref[i]};
+    double mesu = mesuref[i];
+    int l = cellidf[2 * i], r = cellidf[2 * i + 1];
+    double F[4];
+    if (namef[i] == 0) {
+      euler_rusanov(q[0][l], q[1][l], q[2][l], q[3][l], q[4][l], q[0][r], q[1][r], q[2][r], q[3][r], q[4][r], norm,
+                    mesu, gamma, F);
+      for (int c = 0; c < 4; c++) {
+        rez[c][l] -= F[c];
+        rez[c][r] += F[c];
+      }
+    } else {
+      euler_rusanov(q[0][l], q[1][l], q[2][l], q[3][l], q[4][l], g[0][i], g[1][i], g[2][i], g[3][i], g[4][i], norm,
+                    mesu, gamma, F);
+      for (int c = 0; c < 4; c++) rez[c][l] -= F[c];
+    }
+  }
+}
+
+/* fvm_utils2d.py:1083-1102 time_step_euler_2d (faces in the cell's own order) */
+void or_time_step_euler_2d(const double *rho, const double *P, const double *rhou, const double *rhov, double cfl,
+                           const double *normalf, const double *mesuref, const double *volume,
+                           const int32_t *faceid, int wf, int nc, double gamma, double *dt_c) {
+  for (int i = 0; i < nc; i++) {
+    double lam = 0.;
+    double velson = sqrt(gamma * fabs(P[i] / rho[i]));
+    for (int j = 0; j < 3; j++) {
+      int f = ROW(faceid, wf, i)[j];
+      double n0 = normalf[3 * f], n1 = normalf[3 * f + 1];
+      double u_n = fabs((rhou[i] * n0 + rhov[i] * n1) / rho[i]) / sqrt(n0 * n0 + n1 * n1);
+      double lam_convect = u_n + velson;
+      lam += lam_convect * mesuref[f];
+    }
+    dt_c[i] = cfl * volume[i] / lam;
+  }
+}
+
+/* fvm_utils2d.py:1687-1696 update_euler_2d_fvc; q = rho, P, rhou, rhov, rhoE */
+void or_update_euler_2d(double *const q[5], const double *const rez[4], double gamma, double dtime,
+                        const double *vol, int nc) {
+  for (int i = 0; i < nc; i++) {
+    q[0][i] += dtime * ((rez[0][i]) / vol[i]);
+    q[2][i] += dtime * ((rez[1][i]) / vol[i]);
+    q[3][i] += dtime * ((rez[2][i]) / vol[i]);
+    q[4][i] += dtime * ((rez[3][i]) / vol[i]);
+  }
+  for (int i = 0; i < nc; i++)
+    q[1][i] = (gamma - 1) * (q[4][i] - 0.5 * (q[2][i] * q[2][i] + q[3][i] * q[3][i]) / q[0][i]);
+}

@@ -336,3 +336,60 @@ class ShallowWaterOracle:
         self.compute_fluxes()
         self.compute_new_val()
         return self.dt
+
+
+# ---------------------------------------------------------------- Euler, 2D (manapy/solvers/euler/fvm_utils2d.py)
+
+def _arr_ptrs(arrs):
+    return (_dp * len(arrs))(*[a.ctypes.data_as(_dp) for a in arrs])
+
+
+def ghost_neumann_euler_2d(m, q):
+    """fvm_utils2d.py:592-646 ghost_value_Neumann: faces named 1-4 copy their cell's state.
+    Returns (g[rho, P, rhou, rhov, rhoE], ug, vg) face arrays (zero elsewhere)."""
+    g = [np.zeros(m.nf) for _ in range(5)]
+    ug, vg = np.zeros(m.nf), np.zeros(m.nf)
+    sel = np.isin(m.namef, (1, 2, 3, 4))
+    c = m.cellidf[sel, 0]
+    for k in range(5):
+        g[k][sel] = np.asarray(q[k])[c]
+    ug[sel] = g[2][sel] / g[0][sel]
+    vg[sel] = g[3][sel] / g[0][sel]
+    return g, ug, vg
+
+
+def euler_rusanov_2d(m, q, g, gamma):
+    """fvm_utils2d.py:1490-1611: residuals (rho, rhou, rhov, rhoE) of cell state q and face ghosts g."""
+    q = [f64(a) for a in q]
+    g = [f64(a) for a in g]
+    rez = [np.zeros(m.nc) for _ in range(4)]
+    lib().or_euler_rusanov_2d(_arr_ptrs(rez), _arr_ptrs(q), _arr_ptrs(g), I(m.cellidf), D(m.normal), D(m.mesure),
+                              I(m.namef), m.nf, m.nc, ctypes.c_double(gamma))
+    return rez
+
+
+def time_step_euler_2d(m, q, cfl, gamma):
+    """fvm_utils2d.py:1083-1102: per-cell dt of q = (rho, P, rhou, rhov, ...)."""
+    q = [f64(a) for a in q]
+    dt = np.zeros(m.nc)
+    lib().or_time_step_euler_2d(D(q[0]), D(q[1]), D(q[2]), D(q[3]), ctypes.c_double(cfl), D(m.normal),
+                                D(m.mesure), D(m.volume), I(m.faceid), m.faceid.shape[1], m.nc,
+                                ctypes.c_double(gamma), D(dt))
+    return dt
+
+
+def update_euler_2d(m, q, rez, gamma, dt):
+    """fvm_utils2d.py:1687-1696, in place on the float64 arrays q = (rho, P, rhou, rhov, rhoE)."""
+    rez = [f64(a) for a in rez]
+    lib().or_update_euler_2d(_arr_ptrs(q), _arr_ptrs(rez), ctypes.c_double(gamma), ctypes.c_double(dt),
+                             D(m.volume), m.nc)
+
+
+def euler_step_2d(m, q, cfl, gamma):
+    """One first-order Euler step composed of the kernels above: Neumann ghosts, Rusanov
+    residuals, dt = min of the per-cell dt, update (q in place).  Returns dt."""
+    g, _, _ = ghost_neumann_euler_2d(m, q)
+    rez = euler_rusanov_2d(m, q, g, gamma)
+    dt = float(np.min(time_step_euler_2d(m, q, cfl, gamma)))
+    update_euler_2d(m, q, rez, gamma, dt)
+    return dt

@@ -21,6 +21,9 @@ Outputs (``*.npz``, committed):
   short second-order 2D, 3D and shallow-water runs.
 * ``traj_advec.npz``, ``traj_diff.npz``: the advection-only and diffusion-only solvers
   (``manapy/solvers/advec``, ``manapy/solvers/diffusion``), short 2D runs.
+* ``k_euler.npz``: the 2D Euler kernels of ``manapy/solvers/euler/fvm_utils2d.py``
+  (Neumann ghosts, Rusanov residuals, per-cell dt, update) on seeded random
+  states, plus a 20-step first-order run driven by those kernels.
 """
 from __future__ import annotations
 
@@ -37,11 +40,12 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, HERE)
 
+import refharness  # noqa: E402,F401  (first: keeps caches out of the reference tree)
 from manapy_b200 import meshgen  # noqa: E402
 from manapy_b200 import workloads  # noqa: E402
 
 PARTS = ["dom2d", "dom3d", "k2d", "k3d", "traj_c1", "traj_o2", "traj_3d", "traj_sw1", "traj_sw2", "traj_advec",
-         "traj_diff"]
+         "traj_diff", "k_euler"]
 
 
 def _domain_arrays(d, dim):
@@ -344,6 +348,68 @@ def _sw_run(mesh, wl):
             "cells": d.nbcells}
 
 
+def part_euler():
+    """The Euler kernels of ``manapy/solvers/euler/fvm_utils2d.py`` composed into a step:
+    Neumann ghosts (names 1-4), Rusanov residuals, per-cell dt and its min, update."""
+    _ref()
+    from manapy.solvers.euler import fvm_utils2d as E
+    el, vx = meshgen.square_triangles(7, seed=21)
+    d = _run((el, vx), 2).domain
+    nc, nf = d.nbcells, d.nbfaces
+    gamma, cfl = 1.4, 0.5
+    rng = np.random.default_rng(2024)
+    rho = rng.uniform(0.5, 2.0, nc)
+    P = rng.uniform(0.5, 2.0, nc)
+    rhou = rng.uniform(-0.5, 0.5, nc)
+    rhov = rng.uniform(-0.5, 0.5, nc)
+    rhoE = P / (gamma - 1) + 0.5 * (rhou * rhou + rhov * rhov) / rho
+    out = {"in_elements": el, "in_vertex": vx, "gamma": gamma, "cfl": cfl,
+           "rho0": rho.copy(), "P0": P.copy(), "rhou0": rhou.copy(), "rhov0": rhov.copy(), "rhoE0": rhoE.copy()}
+    cellid = np.ascontiguousarray(d.faces.cellid, dtype=np.int32)
+    name = np.ascontiguousarray(d.faces.name, dtype=np.uint32)
+    normal = np.ascontiguousarray(d.faces.normal, dtype=np.float64)
+    mesure = np.ascontiguousarray(d.faces.mesure, dtype=np.float64)
+    centerf = np.ascontiguousarray(d.faces.center, dtype=np.float64)
+    faceid = np.ascontiguousarray(d.cells.faceid, dtype=np.int32)
+    vol = np.ascontiguousarray(d.cells.volume, dtype=np.float64)
+    halofid = np.zeros(1, dtype=np.int32)
+    hal = [np.zeros(1) for _ in range(5)]
+
+    def one_step(rho, P, rhou, rhov, rhoE):
+        g = [np.zeros(nf) for _ in range(5)]
+        ug, vg = np.zeros(nf), np.zeros(nf)
+        E.ghost_value_Neumann(g[0], g[1], g[2], g[3], ug, vg, g[4], rho, P, rhou, rhov, rhoE, cellid, name, normal,
+                              mesure, centerf, 0.0)
+        rez = [np.zeros(nc) for _ in range(4)]
+        E.explicitscheme_euler_2d_rusanov(*rez, rho, P, rhou, rhov, rhoE, *g, *hal, cellid, halofid, normal, mesure,
+                                          name, gamma)
+        dt_c = np.zeros(nc)
+        E.time_step_euler_2d(rho, P, rhou, rhov, cfl, normal, mesure, vol, faceid, gamma, dt_c)
+        return g, ug, vg, rez, dt_c
+
+    g, ug, vg, rez, dt_c = one_step(rho, P, rhou, rhov, rhoE)
+    for k, a in zip(("rho", "P", "rhou", "rhov", "rhoE"), g):
+        out["g_" + k] = a.copy()
+    out["g_u"], out["g_v"] = ug, vg
+    for k, a in zip(("rho", "rhou", "rhov", "rhoE"), rez):
+        out["rez_" + k] = a.copy()
+    out["dt_c"] = dt_c.copy()
+    dt = float(np.min(dt_c))
+    E.update_euler_2d_fvc(rho, P, rhou, rhov, rhoE, *rez, gamma, dt, vol)
+    for k, a in zip(("rho", "P", "rhou", "rhov", "rhoE"), (rho, P, rhou, rhov, rhoE)):
+        out["new_" + k] = a.copy()
+    dts = [dt]
+    for _ in range(19):
+        g, ug, vg, rez, dt_c = one_step(rho, P, rhou, rhov, rhoE)
+        dt = float(np.min(dt_c))
+        E.update_euler_2d_fvc(rho, P, rhou, rhov, rhoE, *rez, gamma, dt, vol)
+        dts.append(dt)
+    for k, a in zip(("rho", "P", "rhou", "rhov", "rhoE"), (rho, P, rhou, rhov, rhoE)):
+        out["final_" + k] = a.copy()
+    out["dts"] = np.array(dts)
+    return out
+
+
 def run_part(part):
     t0 = time.perf_counter()
     if part == "dom2d":
@@ -354,6 +420,8 @@ def run_part(part):
         out = part_kernels(2)
     elif part == "k3d":
         out = part_kernels(3)
+    elif part == "k_euler":
+        out = part_euler()
     else:
         out = part_traj(part)
     np.savez_compressed(os.path.join(HERE, part + ".npz"), **out)

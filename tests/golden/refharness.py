@@ -28,6 +28,11 @@ import numpy as np
 
 REFERENCE_ROOT = os.environ.get("MANAPY_REFERENCE", "/root/reference")
 
+# The reference tree is read-only input: keep Python's bytecode and numba's on-disk
+# kernel cache (``@njit(cache=True)`` writes next to the source) out of it.
+sys.dont_write_bytecode = True
+os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "manapy_reference_numba_cache"))
+
 
 def _install_stubs():
     if "mpi4py" in sys.modules and getattr(sys.modules["mpi4py"], "_is_stub", False):
