@@ -200,6 +200,46 @@ int mb_term_source_srnh_sw(const mb_mesh *m, const double *h, const double *Z, c
 int mb_update_sw(const mb_mesh *m, double *const q[5], const double *const rez[5],
                  const double *src_hu, const double *src_hv, const double *dt_dev, void *stream);
 
+/* ---- Euler equations, 2D, first-order Rusanov (manapy/solvers/euler/fvm_utils2d.py) ----
+ * q: cell arrays rho, P, rhou, rhov, rhoE; g: the same on the faces (ghost values).
+ * Results are bit-identical to manapy's kernels (no multiply-add contraction). */
+
+/* fvm_utils2d.py:1490-1611 explicitscheme_euler_2d_rusanov (flux :1248-1292) -> rez rho, rhou,
+ * rhov, rhoE (each face flux evaluated by both of its cells; cells add faces by ascending id).
+ * Every face not named 0 reads its right state from g, halo faces (name 10) included: on a
+ * shard the caller places the neighbour rank's values there. */
+int mb_euler_rusanov_2d(const mb_mesh *m, const double *const q[5], const double *const g[5],
+                        double *const rez[4], double gamma, void *stream);
+
+/* fvm_utils2d.py:1083-1102 time_step_euler_2d: the CFL dt of every cell into dt_c
+ * (reads q[0..3]; q[4] must be non-null) */
+int mb_time_step_euler_2d(const mb_mesh *m, const double *const q[5], double cfl, double gamma,
+                          double *dt_c, void *stream);
+
+/* fvm_utils2d.py:1687-1696 update_euler_2d_fvc: conserved variables += dt rez / V, then P */
+int mb_update_euler_2d(const mb_mesh *m, double *const q[5], const double *const rez[4], double gamma,
+                       double dt, void *stream);
+
+/* fvm_utils2d.py:592-648 ghost_value_Neumann: faces named 1-4 copy their cell's state
+ * into g (rho, P, rhou, rhov, rhoE) and set ug = rhou / rho, vg = rhov / rho */
+int mb_ghost_euler_neumann_2d(const mb_mesh *m, const double *const q[5], double *const g[5], double *ug,
+                              double *vg, void *stream);
+
+/* Fused Euler step (manapy ships the kernels above without a driver):
+ * ghost_value_Neumann + explicitscheme_euler_2d_rusanov + update_euler_2d_fvc with
+ * dt = min(time_step_euler_2d), bit-identical to that sequence, in two launches (every face
+ * flux once into face_flux, then update + next dt per cell).  Every boundary face must carry
+ * the Neumann rule (names 1-4); no halo faces.
+ * face_flux: device scratch of 4 * nbfaces doubles, 16-byte aligned.
+ * ring: 3 device doubles.  mb_euler_dt_2d resets the ring and puts the dt of q into slot t%3;
+ * mb_euler_step_2d at time index t reads slot t%3, writes q_out (buffers distinct from q_in),
+ * min-reduces the dt of q_out into slot (t+1)%3 and resets slot (t+2)%3, so consecutive calls
+ * with t, t+1, ... need no host synchronisation.  time (nullable, device): += the dt used. */
+int mb_euler_dt_2d(const mb_mesh *m, const double *const q[5], double cfl, double gamma, double *ring, int t,
+                   void *stream);
+int mb_euler_step_2d(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl,
+                     double gamma, double *face_flux, double *ring, int t, double *time, void *stream);
+
 /* ---- fused steps ---------------------------------------------------------------------- */
 
 typedef struct mb_advdiff_params {

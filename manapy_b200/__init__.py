@@ -9,6 +9,7 @@ arithmetic runs in hand-written CUDA kernels behind the C ABI of
 from .base import Struct, make_get_conf  # noqa: F401
 from .domain import Domain  # noqa: F401
 from .variable import Variable  # noqa: F401
-from .solvers import AdvectionDiffusionSolver, AdvectionSolver, DiffusionSolver, ShallowWaterSolver  # noqa: F401
+from .solvers import (AdvectionDiffusionSolver, AdvectionSolver, DiffusionSolver, EulerSolver,  # noqa: F401
+                      ShallowWaterSolver)
 
 __version__ = "0.1.0"

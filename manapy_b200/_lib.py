@@ -82,6 +82,12 @@ _SIGS = {
     "mb_explicitscheme_convective_sw": [_M, _P5, _P5, _P5, _P4, _vp, _d, _i32, _vp, _vp],
     "mb_term_source_srnh_sw": [_M, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp],
     "mb_update_sw": [_M, _P5, _P5, _vp, _vp, _vp, _vp],
+    "mb_euler_rusanov_2d": [_M, _P5, _P5, _P4, _d, _vp],
+    "mb_time_step_euler_2d": [_M, _P5, _d, _d, _vp, _vp],
+    "mb_update_euler_2d": [_M, _P5, _P4, _d, _d, _vp],
+    "mb_ghost_euler_neumann_2d": [_M, _P5, _P5, _vp, _vp, _vp],
+    "mb_euler_dt_2d": [_M, _P5, _d, _d, _vp, _i32, _vp],
+    "mb_euler_step_2d": [_M, _P5, _P5, _d, _d, _vp, _vp, _i32, _vp, _vp],
     "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],

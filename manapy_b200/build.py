@@ -21,8 +21,10 @@ def nvcc():
 
 # Per-file options.  The FP32-compensated kernels are compiled without multiply-add
 # contraction: every FP32 operation rounds as written (explicit fmaf calls excepted), so
-# the single-mesh and batched instantiations of one block body give identical bits.
-FILE_FLAGS = {"fv_advdiff_f32c.cu": ["-fmad=false"], "fv_sw_f32c.cu": ["-fmad=false"]}
+# the single-mesh and batched instantiations of one block body give identical bits.  The
+# Euler kernels likewise round every FP64 operation as manapy's (uncontracted) code does.
+FILE_FLAGS = {"fv_advdiff_f32c.cu": ["-fmad=false"], "fv_sw_f32c.cu": ["-fmad=false"],
+              "fv_euler.cu": ["-fmad=false"]}
 
 
 def build(verbose=False, force=False):

@@ -337,3 +337,65 @@ _register(["update_SW"], _Spec(
     dict([(q + "_c", "cell") for q in _SWQ] + [("rez_" + q, "cell") for q in _SWQ]
          + [("src_hu", "cell"), ("src_hv", "cell")]),
     {q + "_c": "cell" for q in _SWQ}, _update_sw, sizes={"vol": "cell"}))
+
+
+# ---------------------------------------------------------------- manapy/solvers/euler/fvm_utils2d.py (2D Euler)
+_EQ = ["rho", "P", "rhou", "rhov", "rhoE"]
+_EC = [q for q in _EQ if q != "P"]          # conserved: the residual components
+
+
+def _euler_rusanov(c, d, v):
+    _lib.call("mb_euler_rusanov_2d", c.dm.struct, _lib.p5([_p(d[q + "_c"]) for q in _EQ]),
+              _lib.p5([_p(d[q + "_g"]) for q in _EQ]), _lib.p4([_p(d["rez_" + q]) for q in _EC]),
+              float(v["gamma"]), c.stream)
+    torch.cuda.current_stream(c.dm.device).synchronize()
+
+
+# fvm_utils2d.py:1490 (halo arrays accepted, unused on a single rank)
+_register(["explicitscheme_euler_2d_rusanov"], _Spec(
+    ["rez_" + q for q in _EC] + [q + "_c" for q in _EQ] + [q + "_g" for q in _EQ] + [q + "_h" for q in _EQ]
+    + ["cellidf", "halofid", "normal", "mesurf", "name", "gamma"],
+    dict([(q + "_c", "cell") for q in _EQ] + [(q + "_g", "face") for q in _EQ]),
+    {"rez_" + q: "cell" for q in _EC}, _euler_rusanov,
+    sizes={"cellidf": "face", "normal": "face", "mesurf": "face", "name": "face"}))
+
+
+def _time_step_euler(c, d, v):
+    # reads rho, P, rhou, rhov; the fifth pointer is unused
+    _lib.call("mb_time_step_euler_2d", c.dm.struct, _lib.p5([_p(d[q]) for q in _EQ[:4]] + [_p(d["rho"])]),
+              float(v["cfl"]), float(v["gamma"]), _p(d["dt_c"]), c.stream)
+    torch.cuda.current_stream(c.dm.device).synchronize()
+
+
+# fvm_utils2d.py:1083
+_register(["time_step_euler_2d"], _Spec(
+    ["rho", "P", "rhou", "rhov", "cfl", "normal", "mesure", "volume", "faceid", "gamma", "dt_c"],
+    {q: "cell" for q in _EQ[:4]}, {"dt_c": "cell"}, _time_step_euler,
+    sizes={"normal": "face", "mesure": "face", "volume": "cell", "faceid": "cell"}))
+
+
+def _update_euler(c, d, v):
+    _lib.call("mb_update_euler_2d", c.dm.struct, _lib.p5([_p(d[q + "_c"]) for q in _EQ]),
+              _lib.p4([_p(d["rez_" + q]) for q in _EC]), float(v["gamma"]), float(v["dtime"]), c.stream)
+    torch.cuda.current_stream(c.dm.device).synchronize()
+
+
+# fvm_utils2d.py:1687
+_register(["update_euler_2d_fvc"], _Spec(
+    [q + "_c" for q in _EQ] + ["rez_" + q for q in _EC] + ["gamma", "dtime", "vol"],
+    dict([(q + "_c", "cell") for q in _EQ] + [("rez_" + q, "cell") for q in _EC]),
+    {q + "_c": "cell" for q in _EQ}, _update_euler, sizes={"vol": "cell"}))
+
+
+def _ghost_euler(c, d, v):
+    _lib.call("mb_ghost_euler_neumann_2d", c.dm.struct, _lib.p5([_p(d[q + "c"]) for q in _EQ]),
+              _lib.p5([_p(d[q + "g"]) for q in _EQ]), _p(d["ug"]), _p(d["vg"]), c.stream)
+    torch.cuda.current_stream(c.dm.device).synchronize()
+
+
+# fvm_utils2d.py:592 (faces named 1-4 are written; the others keep the caller's values)
+_register(["ghost_value_Neumann"], _Spec(
+    ["rhog", "Pg", "rhoug", "rhovg", "ug", "vg", "rhoEg", "rhoc", "Pc", "rhouc", "rhovc", "rhoEc", "cellid", "name",
+     "normal", "mesure", "center", "t"],
+    {q + "c": "cell" for q in _EQ}, dict([(q + "g", "face") for q in _EQ] + [("ug", "face"), ("vg", "face")]),
+    _ghost_euler, sizes={"cellid": "face", "name": "face", "normal": "face", "mesure": "face", "center": "face"}))

@@ -28,7 +28,7 @@ from . import _lib
 from .base import Struct, make_get_conf, process_conf
 from .variable import Variable
 
-__all__ = ["AdvectionDiffusionSolver", "AdvectionSolver", "DiffusionSolver", "ShallowWaterSolver"]
+__all__ = ["AdvectionDiffusionSolver", "AdvectionSolver", "DiffusionSolver", "ShallowWaterSolver", "EulerSolver"]
 
 
 def _p(t):
@@ -812,3 +812,195 @@ class ShallowWaterSolver:
             raise NotImplementedError("advance() runs the fused step, which needs Neumann boundaries")
         for _ in range(int(nsteps)):
             self._fused_step()
+
+
+class EulerSolver:
+    """Compressible Euler equations in 2D, first-order Rusanov scheme, on the kernels of
+    ``manapy/solvers/euler/fvm_utils2d.py`` (manapy ships them without a driver class).
+
+    One step composes them as: Neumann ghosts (``ghost_value_Neumann``, :592), residuals
+    (``explicitscheme_euler_2d_rusanov``, :1490), ``dt`` = the min over cells of
+    ``time_step_euler_2d`` (:1083), then ``update_euler_2d_fvc`` (:1687).
+    ``compute_new_val()`` / ``advance(n)`` run that step in two launches (every face flux once,
+    then update per cell), bit-identical to the sequence; the next step's ``dt`` is reduced on
+    the device in the update launch.  Every
+    boundary keeps the default Neumann rule.  ``compute_fluxes()`` leaves the residuals in
+    ``var.convective`` (rho, rhou, rhov, rhoE) and the ghosts in ``var.ghost``, as the
+    unfused kernels produce them.
+    """
+    _parameters = [("cfl", float, .5, 0, "cfl of the explicit scheme"),
+                   ("gamma", float, 1.4, 0, "ratio of specific heats"),
+                   ("dt", float, 0., 0., "time step")]
+    _NAMES = ("rho", "P", "rhou", "rhov", "rhoE")
+    GRAPH_DEPTH = 24        # steps per CUDA-graph replay: a multiple of 6 (buffer pair x dt ring)
+
+    @classmethod
+    def process_conf(cls, conf, kwargs):
+        return process_conf(cls._parameters, conf, kwargs)
+
+    def __init__(self, rho=None, P=None, rhou=None, rhov=None, rhoE=None, conf=None, **kwargs):
+        if conf is None:
+            conf = Struct()
+        self.conf = self.process_conf(conf, kwargs)
+        get = make_get_conf(self.conf, kwargs)
+        vs = dict(zip(self._NAMES, (rho, P, rhou, rhov, rhoE)))
+        for k, v in vs.items():
+            if not isinstance(v, Variable):
+                raise ValueError("%s must be a Variable type" % k)
+        self.domain = rho.domain
+        if any(v.domain is not self.domain for v in vs.values()):
+            raise ValueError("the five variables must live on one domain")
+        self.dim = rho.dim
+        if self.dim != 2:
+            raise ValueError("the Euler Rusanov scheme is two-dimensional")
+        self.varbs = vs
+        for k in ("rho", "rhou", "rhov", "rhoE"):
+            vs[k].add_term("convective")
+        self.cfl = float(get("cfl"))
+        self.gamma = float(get("gamma"))
+        self.dt = float(get("dt"))
+        self.backend = self.domain.backend
+        self._dm = None
+        self._graphs = {}
+
+    # ------------------------------------------------------------ state
+    def _setup(self):
+        if self._dm is None:
+            from . import boundary as B
+            for k, v in self.varbs.items():
+                kind = v.resolved_bc.kind
+                if np.any((kind != B.G_NEUMANN) & (kind != B.G_NONE)):
+                    raise NotImplementedError("Euler boundaries other than manapy's Neumann rule (%s)" % k)
+            if np.any(np.asarray(self.domain.host_arrays["faces_name"]) == 10):
+                raise NotImplementedError("halo faces: the Euler step runs on a single-rank mesh")
+            dm = self._dm = self.domain.device_mesh
+            f64 = torch.float64
+            self._bufs = [[torch.empty(dm.nbcells, dtype=f64, device=dm.device) for _ in self._NAMES]
+                          for _ in range(2)]
+            self._ring = torch.full((3,), 1e300, dtype=f64, device=dm.device)
+            self._time = torch.zeros(1, dtype=f64, device=dm.device)
+            self._ff = torch.empty(4 * dm.nbfaces, dtype=f64, device=dm.device)   # face fluxes
+            self._t = 0
+            self._key = None
+            self._dt_host = None
+        return self._dm
+
+    def _stream(self):
+        return torch.cuda.current_stream(self._dm.device).cuda_stream
+
+    def _versions(self):
+        return tuple(self.varbs[k].version("cell") for k in self._NAMES)
+
+    def _sync(self):
+        """Make buffer set t%2 hold (and be) the variables' cell arrays, with the dt of that
+        state in ring slot t%3."""
+        self._setup()
+        if self._key == self._versions():
+            return
+        cur = self._bufs[self._t % 2]
+        for k, b in zip(self._NAMES, cur):
+            t = self.varbs[k].dev("cell")
+            if t.data_ptr() != b.data_ptr():
+                b.copy_(t)
+                self.varbs[k].swap_cell(b)
+        _lib.call("mb_euler_dt_2d", self._dm.struct, _lib.p5([_p(b) for b in cur]), self.cfl, self.gamma,
+                  _p(self._ring), int(self._t), self._stream())
+        self._key = self._versions()
+        self._dt_host = None
+
+    def _slot(self):
+        return self._ring[self._t % 3:self._t % 3 + 1]
+
+    def stepper(self):
+        """dt of the current state: the min over cells of time_step_euler_2d."""
+        self._sync()
+        if self._dt_host is None:
+            self._dt_host = float(self._slot().item())
+        self.dt = self._dt_host
+        return self.dt
+
+    @property
+    def time(self):
+        """Simulated time: the sum of the dt of every step taken (device accumulator)."""
+        self._setup()
+        return float(self._time.item())
+
+    # ------------------------------------------------------------ the unfused kernels
+    def update_ghost_values(self):
+        """ghost_value_Neumann into var.ghost of the five variables."""
+        self._sync()
+        nf = self._dm.nbfaces
+        uv = torch.empty(2 * nf, dtype=torch.float64, device=self._dm.device)
+        _lib.call("mb_ghost_euler_neumann_2d", self._dm.struct,
+                  _lib.p5([_p(self.varbs[k].dev("cell")) for k in self._NAMES]),
+                  _lib.p5([_p(self.varbs[k].dev_out("ghost")) for k in self._NAMES]), _p(uv[:nf]), _p(uv[nf:]),
+                  self._stream())
+
+    def compute_fluxes(self):
+        """Neumann ghosts, then the Rusanov residuals into var.convective."""
+        self.update_ghost_values()
+        _lib.call("mb_euler_rusanov_2d", self._dm.struct,
+                  _lib.p5([_p(self.varbs[k].dev("cell")) for k in self._NAMES]),
+                  _lib.p5([_p(self.varbs[k].dev("ghost")) for k in self._NAMES]),
+                  _lib.p4([_p(self.varbs[k].dev_out("convective")) for k in ("rho", "rhou", "rhov", "rhoE")]),
+                  self.gamma, self._stream())
+
+    # ------------------------------------------------------------ fused step
+    def _launch(self, t):
+        a, b = self._bufs[t % 2], self._bufs[(t + 1) % 2]
+        _lib.call("mb_euler_step_2d", self._dm.struct, _lib.p5([_p(x) for x in a]), _lib.p5([_p(x) for x in b]),
+                  self.cfl, self.gamma, _p(self._ff), _p(self._ring), int(t), _p(self._time), self._stream())
+
+    def _publish(self):
+        for k, b in zip(self._NAMES, self._bufs[self._t % 2]):
+            self.varbs[k].swap_cell(b)
+        self._key = self._versions()
+        self._dt_host = None
+
+    def compute_new_val(self):
+        """One step.  dt is the state's CFL dt, or ``self.dt`` when it was assigned after
+        ``stepper()`` returned (manapy's solvers step with ``self.dt``)."""
+        self._sync()
+        if self._dt_host is not None and float(self.dt) != self._dt_host:
+            self._slot().fill_(float(self.dt))
+        self._launch(self._t)
+        self._t += 1
+        self._publish()
+
+    def advance(self, n, graph=False):
+        """``n`` fused steps on the device without host synchronisation (CUDA-graph replays of
+        GRAPH_DEPTH steps when ``graph``)."""
+        self._sync()
+        n = int(n)
+        D = self.GRAPH_DEPTH
+        while n > 0:
+            if graph and n >= D and self._t % 6 == 0:
+                g = self._graphs.get("main")
+                if g is None:
+                    s = torch.cuda.Stream(self._dm.device)
+                    s.wait_stream(torch.cuda.current_stream(self._dm.device))
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=s):
+                        for k in range(D):
+                            self._launch(k)
+                    torch.cuda.current_stream(self._dm.device).wait_stream(s)
+                    self._graphs["main"] = g
+                g.replay()
+                self._t += D
+                n -= D
+            else:
+                self._launch(self._t)
+                self._t += 1
+                n -= 1
+        self._publish()
+
+    def release_graphs(self):
+        self._graphs.clear()
+
+    def check(self):
+        """Raise if a variable holds NaN or infinity, or rho or P is negative."""
+        self._sync()
+        check_state([self.varbs[k].dev("cell") for k in self._NAMES], nonneg=(0, 1), names=list(self._NAMES))
+
+    def launches_per_step(self):
+        return 2

@@ -57,3 +57,135 @@ def test_oracle_run_matches_reference_run(gold, mesh):
     assert np.allclose(dts, gold["dts"], rtol=1e-13, atol=0)
     for k, a in zip(NAMES, q):
         assert _close(a, gold["final_" + k], 1e-12), k
+
+
+# ---------------------------------------------------------------- GPU: the CUDA kernels
+def _fn(name):
+    def f():
+        pass
+    f.__name__ = name
+    return f
+
+
+def _solver(el, vx, q0, cfl=0.5, gamma=1.4):
+    import manapy_b200 as M
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    vs = [M.Variable(domain=dom) for _ in NAMES]
+    for v, a in zip(vs, q0):
+        v.cell = a
+    return dom, vs, M.EulerSolver(*vs, conf=M.Struct(cfl=cfl, gamma=gamma))
+
+
+@pytest.mark.gpu
+def test_compiled_kernels_take_manapy_arguments(gold, mesh, cuda):
+    """ghost_value_Neumann, explicitscheme_euler_2d_rusanov, time_step_euler_2d and
+    update_euler_2d_fvc with manapy's argument lists, bit for bit against the oracle."""
+    import manapy_b200 as M
+    import oracle as O
+    dom = M.Domain(dim=2, mesh=(gold["in_elements"], gold["in_vertex"]))
+    be, c, f = dom.backend, dom.cells, dom.faces
+    gamma, cfl = float(gold["gamma"]), float(gold["cfl"])
+    q = _q0(gold)
+    nf, nc = mesh.nf, mesh.nc
+    g = [np.zeros(nf) for _ in NAMES]
+    ug, vg = np.zeros(nf), np.zeros(nf)
+    be.compile(_fn("ghost_value_Neumann"))(g[0], g[1], g[2], g[3], ug, vg, g[4], *q, f.cellid, f.name, f.normal,
+                                           f.mesure, f.center, 0.0)
+    og, oug, ovg = O.ghost_neumann_euler_2d(mesh, q)
+    for k, a, b in zip(NAMES, g, og):
+        assert np.array_equal(a, b) and np.array_equal(a, gold["g_" + k]), k
+    assert np.array_equal(ug, oug) and np.array_equal(vg, ovg)
+    rez = [np.zeros(nc) for _ in range(4)]
+    z = np.zeros(1)
+    be.compile(_fn("explicitscheme_euler_2d_rusanov"))(*rez, *q, *g, z, z, z, z, z, f.cellid, np.zeros(1, np.int32),
+                                                       f.normal, f.mesure, f.name, gamma)
+    for k, a in zip(("rho", "rhou", "rhov", "rhoE"), rez):
+        assert np.array_equal(a, gold["rez_" + k]), k
+    dt_c = np.zeros(nc)
+    be.compile(_fn("time_step_euler_2d"))(q[0], q[1], q[2], q[3], cfl, f.normal, f.mesure, c.volume, c.faceid, gamma,
+                                          dt_c)
+    assert np.array_equal(dt_c, O.time_step_euler_2d(mesh, q, cfl, gamma))
+    dt = float(gold["dts"][0])
+    be.compile(_fn("update_euler_2d_fvc"))(*q, *rez, gamma, dt, c.volume)
+    oq = _q0(gold)
+    O.update_euler_2d(mesh, oq, rez, gamma, dt)
+    for k, a, b in zip(NAMES, q, oq):
+        assert np.array_equal(a, b), k
+
+
+@pytest.mark.gpu
+def test_fused_steps_match_reference_run(gold, mesh, cuda):
+    """20 fused steps: the reference run's trajectory, and the oracle's bit for bit."""
+    import oracle as O
+    _, vs, S = _solver(gold["in_elements"], gold["in_vertex"], _q0(gold), float(gold["cfl"]), float(gold["gamma"]))
+    oq = _q0(gold)
+    dts = []
+    for _ in range(len(gold["dts"])):
+        dts.append(S.stepper())
+        S.compute_new_val()
+        assert dts[-1] == O.euler_step_2d(mesh, oq, float(gold["cfl"]), float(gold["gamma"]))
+    assert np.allclose(dts, gold["dts"], rtol=1e-13, atol=0)
+    for k, v, b in zip(NAMES, vs, oq):
+        assert np.array_equal(v.cell, b), k
+        assert _close(v.cell, gold["final_" + k], 1e-12), k
+    assert abs(S.time - sum(dts)) <= 1e-15 * len(dts)
+
+
+def smooth_state(center, gamma=1.4, seed=5):
+    """A pressure pulse in a smooth density field with a shear flow (positive rho and P)."""
+    rng = np.random.default_rng(seed)
+    x, y = center[:, 0], center[:, 1]
+    rho = 1.0 + 0.2 * np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y) + 0.01 * rng.standard_normal(len(x))
+    P = 1.0 + 0.3 * np.exp(-40 * ((x - 0.5) ** 2 + (y - 0.5) ** 2))
+    u = 0.3 * np.cos(np.pi * y)
+    v = 0.2 * np.sin(np.pi * x)
+    return [rho, P, rho * u, rho * v, P / (gamma - 1) + 0.5 * rho * (u * u + v * v)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [60, 200])
+def test_fused_step_bit_identical_to_kernel_sequence(n, cuda):
+    """The fused launch against the oracle's ghost -> residual -> min dt -> update sequence,
+    on a pressure pulse (n = 200: 80,000 triangles); graph and eager runs agree."""
+    import manapy_b200 as M
+    import oracle as O
+    from manapy_b200 import meshgen
+    el, vx = meshgen.square_triangles(n, seed=3)
+    q0 = smooth_state(M.Domain(dim=2, mesh=(el, vx)).cells.center)
+    dom, vs, S = _solver(el, vx, q0)
+    m = O.Mesh(dom.host_arrays)
+    oq = [a.copy() for a in q0]
+    steps = 30
+    for _ in range(steps):
+        O.euler_step_2d(m, oq, S.cfl, S.gamma)
+    S.advance(steps, graph=True)
+    for k, v, b in zip(NAMES, vs, oq):
+        assert np.array_equal(v.cell, b), k
+    # residuals of the unfused kernels on the final state
+    S.compute_fluxes()
+    g, _, _ = O.ghost_neumann_euler_2d(m, oq)
+    rez = O.euler_rusanov_2d(m, oq, g, S.gamma)
+    for k, r in zip(("rho", "rhou", "rhov", "rhoE"), rez):
+        assert np.array_equal(vs[NAMES.index(k)].convective, r), k
+    # the same run eagerly, from the start
+    _, vs2, S2 = _solver(el, vx, q0)
+    S2.advance(steps)
+    for v, w in zip(vs, vs2):
+        assert np.array_equal(v.cell, w.cell)
+    S.check()
+
+
+@pytest.mark.gpu
+def test_solver_rejects_non_neumann_boundaries(cuda):
+    import manapy_b200 as M
+    from manapy_b200 import meshgen
+    el, vx = meshgen.square_triangles(4, seed=1)
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    vs = [M.Variable(domain=dom) for _ in NAMES]
+    vs[0] = M.Variable(domain=dom, BC={"in": "dirichlet", "out": "neumann", "upper": "neumann",
+                                       "bottom": "neumann"}, values={"in": 1.0})
+    S = M.EulerSolver(*vs)
+    with pytest.raises(NotImplementedError):
+        S._setup()
+    with pytest.raises(ValueError):
+        M.EulerSolver(vs[0], vs[1], vs[2], vs[3], None)
