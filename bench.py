@@ -34,7 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # compulsory-traffic bytes per cell-update (FP64), per workload
-CTM_BYTES = {"C1": 146.6, "C2": 198.8, "C3": 152.4, "C4": 265.9}
+CTM_BYTES = {"C1": 146.6, "C2": 198.8, "C3": 152.4, "C4": 265.9, "E1": 171.0}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="C2", choices=["C1", "C2", "C3", "C4"])
+    ap.add_argument("--workload", default="C2", choices=["C1", "C2", "C3", "C4", "E1"])
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-steps", type=int, default=5, help="oracle steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -272,13 +272,110 @@ def run_fp32c_sw(wl, dom, vs64, S64, K, Wm, world):
     return out
 
 
+def build_euler(wl, seed):
+    import manapy_b200 as M
+    el, vx = wl.scaled(seed=seed).mesh()
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    vs = [M.Variable(domain=dom) for _ in range(5)]
+    for var, a in zip(vs, wl.init_euler(dom.cells.center, wl.gamma)):
+        var.cell = a
+    S = M.EulerSolver(*vs, conf=M.Struct(cfl=wl.cfl, gamma=wl.gamma))
+    return dom, vs, S
+
+
+def cpu_baseline_euler(dom, wl, steps):
+    """The oracle's Euler step (serial C restatement of manapy's kernels) on this host."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    A = dom.host_arrays
+    m = O.Mesh(A)
+    q = [np.ascontiguousarray(a, dtype=np.float64) for a in wl.init_euler(A["cells_center"], wl.gamma)]
+    O.euler_step_2d(m, q, wl.cfl, wl.gamma)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.euler_step_2d(m, q, wl.cfl, wl.gamma)
+    el = time.perf_counter() - t0
+    return {"value": wl.cells * steps / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": "%d steps of the full %d-cell mesh, serial C restatement of manapy's euler kernels"
+                      % (steps, wl.cells)}
+
+
+def run_euler(args, wl):
+    """The 2D Euler Rusanov step (EulerSolver): two launches per step, dt reduced on the device."""
+    import torch
+    world, rank, local = dist_setup(args)
+    # warm-up long enough to capture the step graph (GRAPH_DEPTH steps, aligned to 6)
+    K, Wm = args.steps, max(args.warmup, 3)
+    dom, vs, S = build_euler(wl, seed=wl.seed + rank)
+    Wm = max(Wm, S.GRAPH_DEPTH + 6)
+    S.advance(Wm, graph=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local if world > 1 else 0)
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    S.advance(K, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    ck = clocks.stop()
+    ms_max = max_over_ranks(ms, world)
+    value = world * wl.cells * K / (ms_max / 1e3)
+    ms_step = ms_max / K
+    S.check()
+    # end to end, a manapy-style driver loop: dt read back every step
+    E = max(args.e2e_steps, 1)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(E):
+        S.stepper()
+        S.compute_new_val()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    peak, peak_kind = measured_peak()
+    ctm = CTM_BYTES["E1"]
+    achieved = ctm * wl.cells / (ms_step / 1e3) / 1e9
+    traffic = ncu_traffic("E1")
+    line = {
+        "metric": "cell-updates/s (FP64 Euler Rusanov step, %s)" % wl.name,
+        "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: seeded jittered mesh, pressure pulse in a sheared flow",
+        "config": {"workload": wl.name, "cells": wl.cells, "order": 1, "kind": "euler",
+                   "parallelism": "replicas%d" % world if world > 1 else "single",
+                   "l2": "working set %.0f MB > 126 MB L2 (no flush needed)" % (dom.device_mesh.nbytes() / 1e6)},
+        "e2e": {"value": world * wl.cells * E / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8, "steps": E},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": (traffic * wl.cells if traffic else None),
+                     "kernel": "face flux + cell update (2 launches), compulsory traffic %.1f B/cell-update" % ctm},
+        "clocks": ck,
+        "gpu_launches": S.launches_per_step() * K,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_euler(dom, wl, args.cpu_steps)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        S.release_graphs()
+        dist.destroy_process_group()
+
+
 def run_ours(args):
     import torch
     from manapy_b200 import workloads as W
-    world, rank, local = dist_setup(args)
     wl = W.ALL[args.workload]
     if args.n:
         wl = wl.scaled(n=args.n)
+    if wl.kind == "euler":
+        return run_euler(args, wl)
+    world, rank, local = dist_setup(args)
     K, Wm = args.steps, max(args.warmup, 3)
     if wl.kind == "advdiff":
         dom, w, vel, S, (uf, vf) = build_advdiff(wl, seed=wl.seed + rank)
@@ -402,16 +499,23 @@ def _ref_worker(wk, steps, warmup, start, out):
                             mesh=m)
         o.set_velocity(*wl.velocity(A["faces_center"]))
         o.w[:] = wl.init(A["cells_center"])
+        step = o.step
+    elif wl.kind == "euler":
+        q = [np.ascontiguousarray(a, dtype=np.float64) for a in wl.init_euler(A["cells_center"], wl.gamma)]
+
+        def step():
+            O.euler_step_2d(m, q, wl.cfl, wl.gamma)
     else:
         o = O.ShallowWaterOracle(A, order=wl.order, cfl=wl.cfl, grav=wl.grav, mesh=m)
         for k, a in zip(("h", "hu", "hv", "hc", "Z"), wl.init_sw(A["cells_center"])):
             o.state()[k][:] = a
+        step = o.step
     for _ in range(warmup):
-        o.step()
+        step()
     start.wait()  # every process starts its timed steps together
     t0 = time.perf_counter()
     for _ in range(steps):
-        o.step()
+        step()
     out.put(time.perf_counter() - t0)
 
 
@@ -449,7 +553,8 @@ def run_reference(args):
         p.join()
     value = procs_n * wl.cells * steps / wall
     line = {
-        "metric": "cell-updates/s (FP64 explicit FV step, %s)" % wl.name, "impl": "reference",
+        "metric": ("cell-updates/s (FP64 Euler Rusanov step, %s)" if wl.kind == "euler"
+                   else "cell-updates/s (FP64 explicit FV step, %s)") % wl.name, "impl": "reference",
         "value": value, "unit": "cell-updates/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": steps, "steps_requested": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * max(times) / steps,

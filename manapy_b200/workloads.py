@@ -13,6 +13,8 @@ uses (``manapy/examples/2D/advecdiff2d.py:104-147``,
   (8,000,000 triangles), SRNH flux, 500 steps.
 * ``C4``: 3D second-order advection-diffusion, 64^3 hexes x 6 tetrahedra
   (1,572,864 cells), 300 steps.
+* ``E1``: 2D compressible Euler, first-order Rusanov (manapy's euler kernels), a
+  pressure pulse in a sheared flow, 1000x1000 squares (2,000,000 triangles), 1000 steps.
 """
 from __future__ import annotations
 
@@ -21,7 +23,7 @@ from typing import Callable, Optional
 
 import numpy as np
 
-__all__ = ["Workload", "C1", "C2", "C3", "C4", "ALL"]
+__all__ = ["Workload", "C1", "C2", "C3", "C4", "E1", "ALL", "pressure_pulse"]
 
 
 def _gauss2d(cc):
@@ -55,6 +57,18 @@ def _dam_break(cc, left=2.0, right=1.0):
     return h, zero.copy(), zero.copy(), zero.copy(), z
 
 
+def pressure_pulse(cc, gamma=1.4, seed=5):
+    """Euler state (rho, P, rhou, rhov, rhoE): a Gaussian pressure pulse in a smooth density
+    field with a shear flow; rho and P stay positive."""
+    rng = np.random.default_rng(seed)
+    x, y = cc[:, 0], cc[:, 1]
+    rho = 1.0 + 0.2 * np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y) + 0.01 * rng.standard_normal(len(x))
+    P = 1.0 + 0.3 * np.exp(-40 * ((x - 0.5) ** 2 + (y - 0.5) ** 2))
+    u = 0.3 * np.cos(np.pi * y)
+    v = 0.2 * np.sin(np.pi * x)
+    return [rho, P, rho * u, rho * v, P / (gamma - 1) + 0.5 * rho * (u * u + v * v)]
+
+
 _DIRICHLET0_2D = ({"in": "dirichlet", "out": "dirichlet", "upper": "dirichlet", "bottom": "dirichlet"},
                   {"in": 0.0, "out": 0.0, "upper": 0.0, "bottom": 0.0})
 _DIRICHLET0_3D = ({"in": "dirichlet", "out": "dirichlet", "upper": "dirichlet", "bottom": "dirichlet",
@@ -65,7 +79,7 @@ _DIRICHLET0_3D = ({"in": "dirichlet", "out": "dirichlet", "upper": "dirichlet", 
 @dataclasses.dataclass(frozen=True)
 class Workload:
     name: str
-    kind: str  # "advdiff" or "sw"
+    kind: str  # "advdiff", "sw" or "euler"
     dim: int
     n: int
     steps: int
@@ -77,6 +91,8 @@ class Workload:
     init: Optional[Callable] = None
     init_sw: Optional[Callable] = None
     grav: float = 9.81
+    init_euler: Optional[Callable] = None
+    gamma: float = 1.4
     bc: Optional[dict] = None
     bc_values: Optional[dict] = None
 
@@ -106,4 +122,7 @@ C4 = Workload("C4-adv-diff-3d-o2-1.57M", "advdiff", 3, n=64, steps=300, order=2,
               diffusion=(1e-3, 1e-3, 1e-3), velocity=_const_vel(1.0, 0.5, 0.25), init=_gauss3d,
               bc=_DIRICHLET0_3D[0], bc_values=_DIRICHLET0_3D[1])
 
-ALL = {"C1": C1, "C2": C2, "C3": C3, "C4": C4}
+E1 = Workload("E1-euler-rusanov-2d-2M", "euler", 2, n=1000, steps=1000, order=1, cfl=0.5,
+              init_euler=pressure_pulse, gamma=1.4)
+
+ALL = {"C1": C1, "C2": C2, "C3": C3, "C4": C4, "E1": E1}

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from manapy_b200 import geometry as G
+from manapy_b200.workloads import pressure_pulse
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 NAMES = ("rho", "P", "rhou", "rhov", "rhoE")
@@ -131,17 +132,6 @@ def test_fused_steps_match_reference_run(gold, mesh, cuda):
     assert abs(S.time - sum(dts)) <= 1e-15 * len(dts)
 
 
-def smooth_state(center, gamma=1.4, seed=5):
-    """A pressure pulse in a smooth density field with a shear flow (positive rho and P)."""
-    rng = np.random.default_rng(seed)
-    x, y = center[:, 0], center[:, 1]
-    rho = 1.0 + 0.2 * np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y) + 0.01 * rng.standard_normal(len(x))
-    P = 1.0 + 0.3 * np.exp(-40 * ((x - 0.5) ** 2 + (y - 0.5) ** 2))
-    u = 0.3 * np.cos(np.pi * y)
-    v = 0.2 * np.sin(np.pi * x)
-    return [rho, P, rho * u, rho * v, P / (gamma - 1) + 0.5 * rho * (u * u + v * v)]
-
-
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [60, 200])
 def test_fused_step_bit_identical_to_kernel_sequence(n, cuda):
@@ -151,7 +141,7 @@ def test_fused_step_bit_identical_to_kernel_sequence(n, cuda):
     import oracle as O
     from manapy_b200 import meshgen
     el, vx = meshgen.square_triangles(n, seed=3)
-    q0 = smooth_state(M.Domain(dim=2, mesh=(el, vx)).cells.center)
+    q0 = pressure_pulse(M.Domain(dim=2, mesh=(el, vx)).cells.center)
     dom, vs, S = _solver(el, vx, q0)
     m = O.Mesh(dom.host_arrays)
     oq = [a.copy() for a in q0]
