@@ -508,7 +508,14 @@ __device__ __forceinline__ double2 ldd2s(const double *p) { return __ldg(reinter
 __device__ __forceinline__ int compi(const int4 v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : v.z); }
 
 template <bool ORDER2, bool FAST>
-__global__ void __launch_bounds__(kBlock) k_sw2_flux(mb_mesh m, SWState s, double grav, double *ff,
+#ifndef MB_SW_FLUX_MIN_BLOCKS
+#define MB_SW_FLUX_MIN_BLOCKS 3
+#endif
+#ifndef MB_SW_CELL_MIN_BLOCKS
+#define MB_SW_CELL_MIN_BLOCKS 4
+#endif
+
+__global__ void __launch_bounds__(kBlock, MB_SW_FLUX_MIN_BLOCKS) k_sw2_flux(mb_mesh m, SWState s, double grav, double *ff,
                                                      double *dt_next) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f == 0 && dt_next) *dt_next = 1e6;
@@ -544,7 +551,7 @@ __device__ __forceinline__ double sw2_cell_body(const mb_mesh &m, const SWState 
                                                 const double *dt_cur, bool want_dt, double cfl, double grav,
                                                 int i);
 
-__global__ void __launch_bounds__(kBlock) k_sw2_cell(mb_mesh m, SWState s, SWQ out, const double *ff,
+__global__ void __launch_bounds__(kBlock, MB_SW_CELL_MIN_BLOCKS) k_sw2_cell(mb_mesh m, SWState s, SWQ out, const double *ff,
                                                      const double *dt_cur, double *dt_next, double cfl,
                                                      double grav) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

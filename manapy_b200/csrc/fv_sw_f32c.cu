@@ -251,7 +251,14 @@ __device__ __forceinline__ double sw2c_cell_body(const mb_mesh &m, const SWState
   return cfl * vol / lam;
 }
 
-__global__ void __launch_bounds__(kBlock) k_sw2c_cell(mb_mesh m, SWStateF s, SWOutF out, const float *ff,
+#ifndef MB_SW2C_CELL_MIN_BLOCKS
+#define MB_SW2C_CELL_MIN_BLOCKS 4
+#endif
+#ifndef MB_SW2C_BATCH_CELL_MIN_BLOCKS
+#define MB_SW2C_BATCH_CELL_MIN_BLOCKS 1
+#endif
+
+__global__ void __launch_bounds__(kBlock, MB_SW2C_CELL_MIN_BLOCKS) k_sw2c_cell(mb_mesh m, SWStateF s, SWOutF out, const float *ff,
                                                       const double *dt_cur, double *dt_next, double cfl,
                                                       double grav) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -277,7 +284,7 @@ __global__ void __launch_bounds__(kBlock) k_sw2c_batch_flux(const mb_sw_item *__
             ((int)blockIdx.x - it.f_begin) * blockDim.x + threadIdx.x);
 }
 
-__global__ void __launch_bounds__(kBlock) k_sw2c_batch_cell(const mb_sw_item *__restrict__ items,
+__global__ void __launch_bounds__(kBlock, MB_SW2C_BATCH_CELL_MIN_BLOCKS) k_sw2c_batch_cell(const mb_sw_item *__restrict__ items,
                                                             const int32_t *__restrict__ map,
                                                             const int32_t *__restrict__ clock) {
   const mb_sw_item &it = items[map[blockIdx.x]];
