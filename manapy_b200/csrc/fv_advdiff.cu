@@ -449,6 +449,9 @@ __global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_
 #ifndef MB_P1_MIN_BLOCKS
 #define MB_P1_MIN_BLOCKS 6
 #endif
+#ifndef MB_P1_BLOCK
+#define MB_P1_BLOCK kBlock
+#endif
 
 // block `bid` of phase 1: blocks [0, ncb) gradient + limiter records, the rest node values
 template <bool ORDER2, bool DIFF>
@@ -557,13 +560,16 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
 }
 
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+__global__ void __launch_bounds__(MB_P1_BLOCK, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                       double *__restrict__ rec, double *__restrict__ wn, int ncb) {
   f2_phase1<ORDER2, DIFF>(m, bc, w, rec, wn, ncb, blockIdx.x);
 }
 
 #ifndef MB_P2_MIN_BLOCKS
-#define MB_P2_MIN_BLOCKS 3
+#define MB_P2_MIN_BLOCKS 7
+#endif
+#ifndef MB_P2_BLOCK
+#define MB_P2_BLOCK 128
 #endif
 
 // block `bid` of phase 2: fluxes and update of its cells
@@ -678,7 +684,7 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
 }
 
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+__global__ void __launch_bounds__(MB_P2_BLOCK, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,
@@ -812,9 +818,12 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
 #ifndef MB_P2_3D_MIN_BLOCKS
 #define MB_P2_3D_MIN_BLOCKS 2
 #endif
+#ifndef MB_P2_3D_BLOCK
+#define MB_P2_3D_BLOCK kBlock
+#endif
 
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P2_3D_MIN_BLOCKS) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+__global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,
@@ -972,13 +981,15 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
   if (compact_tables(m)) {
     if (DIM == 2) {
-      if (ncb + nnb > 0) k_f2_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
-      k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt,
-                                                                          cs, wn);
+      const int ncb2 = O2 ? ceil_div(m.nbcells, MB_P1_BLOCK) : 0;
+      const int nnb2 = DF ? ceil_div(m.nbnodes, MB_P1_BLOCK) : 0;
+      if (ncb2 + nnb2 > 0) k_f2_phase1<O2, DF><<<ncb2 + nnb2, MB_P1_BLOCK, 0, st>>>(m, bc, w_in, cs, wn, ncb2);
+      k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_BLOCK), MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign,
+                                                                                    src, dt, cs, wn);
     } else {
       if (ncb + nnb > 0) k_f3_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
-      k_f3_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt,
-                                                                          cs, wn);
+      k_f3_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_3D_BLOCK), MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out,
+                                                                                          sign, src, dt, cs, wn);
     }
     return check_launch();
   }

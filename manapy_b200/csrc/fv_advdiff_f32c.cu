@@ -127,8 +127,14 @@ __device__ __forceinline__ void node_value_f32(const mb_mesh &m, const GhostRule
 #ifndef MB_P1C_MIN_BLOCKS
 #define MB_P1C_MIN_BLOCKS 6
 #endif
+#ifndef MB_P2C_BLOCK
+#define MB_P2C_BLOCK 128   // threads per block of the single-mesh phase 2 (batches: kBlock)
+#endif
+#ifndef MB_P2C_BATCH_MIN_BLOCKS
+#define MB_P2C_BATCH_MIN_BLOCKS 3
+#endif
 #ifndef MB_P2C_MIN_BLOCKS
-#define MB_P2C_MIN_BLOCKS 3
+#define MB_P2C_MIN_BLOCKS 7
 #endif
 
 // phase 1 of block `bid` of one mesh: blocks [0, ncb) gradient + limiter records,
@@ -344,7 +350,7 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
 }
 
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P2C_MIN_BLOCKS)
+__global__ void __launch_bounds__(MB_P2C_BLOCK, MB_P2C_MIN_BLOCKS)
     k_f2c_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p, const float *__restrict__ w, float *__restrict__ w_out,
                  const float *__restrict__ sign, const float *__restrict__ src, const double *__restrict__ dt_dev,
                  const float *__restrict__ rec, const float *__restrict__ wn, const float *__restrict__ lo_in,
@@ -376,7 +382,7 @@ __global__ void __launch_bounds__(kBlock, MB_P1C_MIN_BLOCKS)
 }
 
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P2C_MIN_BLOCKS)
+__global__ void __launch_bounds__(kBlock, MB_P2C_BATCH_MIN_BLOCKS)
     k_f2c_batch_phase2(const mb_advdiff_item *__restrict__ items, const int32_t *__restrict__ map,
                        const int32_t *__restrict__ clock) {
   const mb_advdiff_item &it = items[map[blockIdx.x]];
@@ -619,7 +625,7 @@ int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params 
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
   if (m.dim == 2) {
     if (ncb + nnb > 0) k_f2c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
-    k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
+    k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2C_BLOCK), MB_P2C_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
                                                                            lo_in, lo_out);
   } else {
     if (ncb + nnb > 0) k_f3c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
