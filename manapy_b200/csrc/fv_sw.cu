@@ -511,11 +511,14 @@ template <bool ORDER2, bool FAST>
 #ifndef MB_SW_FLUX_MIN_BLOCKS
 #define MB_SW_FLUX_MIN_BLOCKS 3
 #endif
+#ifndef MB_SW_FLUX_BLOCK
+#define MB_SW_FLUX_BLOCK kBlock
+#endif
 #ifndef MB_SW_CELL_MIN_BLOCKS
 #define MB_SW_CELL_MIN_BLOCKS 4
 #endif
 
-__global__ void __launch_bounds__(kBlock, MB_SW_FLUX_MIN_BLOCKS) k_sw2_flux(mb_mesh m, SWState s, double grav, double *ff,
+__global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS) k_sw2_flux(mb_mesh m, SWState s, double grav, double *ff,
                                                      double *dt_next) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f == 0 && dt_next) *dt_next = 1e6;
@@ -800,7 +803,7 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
   }
   if (dt_next == dt_cur) return MB_EINVAL;
   cudaStream_t st = ST(stream);
-  const int fb = ceil_div(m->nbfaces, kBlock);
+  const int fb = ceil_div(m->nbfaces, MB_SW_FLUX_BLOCK);
   if (order == 2) {
     if (!scratch) return MB_EINVAL;
     const long long n = m->nbcells;
@@ -809,9 +812,9 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
     if (rc != MB_OK) return rc;
     s.gr[0] = hx; s.gr[1] = hy; s.gr[2] = cx; s.gr[3] = cy;
     s.psi = psi;
-    k_sw2_flux<true, MB_SW_FAST><<<fb, kBlock, 0, st>>>(*m, s, grav, face_flux, dt_next);
+    k_sw2_flux<true, MB_SW_FAST><<<fb, MB_SW_FLUX_BLOCK, 0, st>>>(*m, s, grav, face_flux, dt_next);
   } else {
-    k_sw2_flux<false, MB_SW_FAST><<<fb, kBlock, 0, st>>>(*m, s, grav, face_flux, dt_next);
+    k_sw2_flux<false, MB_SW_FAST><<<fb, MB_SW_FLUX_BLOCK, 0, st>>>(*m, s, grav, face_flux, dt_next);
   }
   k_sw2_cell<<<ceil_div(m->nbcells, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_cur, dt_next, cfl, grav);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
