@@ -593,8 +593,7 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
   const double s2 = ldd_stream(sign + 4 * i + 2, pst);
   double wi, gxi = 0., gyi = 0., psii = 0.;
   if (ORDER2) {
-    const double2 r0 = ldd2(rec + 4 * i), r1 = ldd2(rec + 4 * i + 2);
-    wi = r0.x; gxi = r0.y; gyi = r1.x; psii = r1.y;
+    ld4d(rec + 4 * i, wi, gxi, gyi, psii);
   } else {
     wi = ld(w + i);
   }
@@ -617,8 +616,7 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
       co = make_double2(ld(m.face_ghostcenter + 3 * f), ld(m.face_ghostcenter + 3 * f + 1));
     } else {
       if (ORDER2) {
-        const double2 r0 = ldd2(rec + 4 * o), r1 = ldd2(rec + 4 * o + 2);
-        vo = r0.x; gxo = r0.y; gyo = r1.x; pso = r1.y;
+        ld4d(rec + 4 * o, vo, gxo, gyo, pso);
       } else {
         vo = ld(w + o);
       }
@@ -980,6 +978,12 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
   const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
   if (compact_tables(m)) {
+#if MB_LD256
+    // 256-bit loads of [n][4] rows: the phase-1 records (2D) and the centre and vertex
+    // tables (3D) must start on 32-byte boundaries
+    auto a32 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 31) == 0; };
+    if ((DIM == 2 && O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord)))) return MB_EINVAL;
+#endif
     if (DIM == 2) {
       const int ncb2 = O2 ? ceil_div(m.nbcells, MB_P1_BLOCK) : 0;
       const int nnb2 = DF ? ceil_div(m.nbnodes, MB_P1_BLOCK) : 0;

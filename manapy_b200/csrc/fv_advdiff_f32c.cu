@@ -652,6 +652,11 @@ extern "C" int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_
   const bool o2 = p->order == 2, df = p->diffusion != 0;
   if (p->order != 1 && !o2) return MB_EINVAL;
   if ((o2 && !cell_scratch) || (df && !node_scratch) || (df && !bc->face_grad_on)) return MB_EINVAL;
+#if MB_LD256
+  // 256-bit loads of the [n][4] centre and vertex rows of a tetrahedral mesh
+  if (m->dim == 3 && (((reinterpret_cast<uintptr_t>(m->cell_xy) | reinterpret_cast<uintptr_t>(m->node_coord)) & 31) != 0))
+    return MB_EINVAL;
+#endif
   cudaStream_t st = (cudaStream_t)stream;
 #define MB_F32C(O, D) \
   return launch_step_f32c<O, D>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, lo_in, \

@@ -21,6 +21,24 @@ __device__ __forceinline__ T pick3(T a, T b, T c, int k) { return k == 0 ? a : (
 #ifndef MB_L2_HINTS
 #define MB_L2_HINTS 1
 #endif
+// streamed loads: optionally without an L1 allocation (the gathers own L1), and as
+// non-volatile asm so the compiler may schedule them freely (they read read-only data)
+#ifndef MB_STREAM_L1NA
+#define MB_STREAM_L1NA 0
+#endif
+#ifndef MB_STREAM_VOLATILE
+#define MB_STREAM_VOLATILE 1
+#endif
+#if MB_STREAM_L1NA
+#define MB_LDNC "ld.global.nc.L1::no_allocate.L2::cache_hint"
+#else
+#define MB_LDNC "ld.global.nc.L2::cache_hint"
+#endif
+#if MB_STREAM_VOLATILE
+#define MB_ASM_LD asm volatile
+#else
+#define MB_ASM_LD asm
+#endif
 __device__ __forceinline__ uint64_t l2_keep() {
   uint64_t p;
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
@@ -48,7 +66,7 @@ __device__ __forceinline__ void st1_keep(double *a, double x, uint64_t pol) {
 __device__ __forceinline__ int ld1_stream(const int32_t *a, uint64_t pol) {
 #if MB_L2_HINTS
   int v;
-  asm volatile("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  MB_ASM_LD(MB_LDNC ".s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
   return v;
 #else
   return __ldg(a);
@@ -57,7 +75,7 @@ __device__ __forceinline__ int ld1_stream(const int32_t *a, uint64_t pol) {
 __device__ __forceinline__ double2 ldd2_stream(const double *a, uint64_t pol) {
 #if MB_L2_HINTS
   double2 v;
-  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+  MB_ASM_LD(MB_LDNC ".v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
   return v;
 #else
   return __ldg(reinterpret_cast<const double2 *>(a));
@@ -66,7 +84,7 @@ __device__ __forceinline__ double2 ldd2_stream(const double *a, uint64_t pol) {
 __device__ __forceinline__ double ldd_stream(const double *a, uint64_t pol) {
 #if MB_L2_HINTS
   double v;
-  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  MB_ASM_LD(MB_LDNC ".f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
   return v;
 #else
   return __ldg(a);
@@ -100,9 +118,23 @@ __device__ __forceinline__ D3 cross(D3 a, D3 b) {
   return d3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 __device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// 32-byte rows ([n][4] doubles, 32-byte aligned) in one 256-bit load (sm_100), or as two
+// 16-byte loads
+#ifndef MB_LD256
+#define MB_LD256 1
+#endif
+__device__ __forceinline__ void ld4d(const double *p, double &a, double &b, double &c, double &d) {
+#if MB_LD256
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+#else
+  const double2 u = __ldg(reinterpret_cast<const double2 *>(p)), v = __ldg(reinterpret_cast<const double2 *>(p + 2));
+  a = u.x; b = u.y; c = v.x; d = v.y;
+#endif
+}
 __device__ __forceinline__ D3 ld3(const double *p) {  // [n][4] rows
-  const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p + 2));
-  return d3(a.x, a.y, b.x);
+  double a, b, c, d;
+  ld4d(p, a, b, c, d);
+  return d3(a, b, c);
 }
 __device__ __forceinline__ D3 pick4(const D3 *P, int k) { return k == 0 ? P[0] : (k == 1 ? P[1] : (k == 2 ? P[2] : P[3])); }
 template <class T>
