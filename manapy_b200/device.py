@@ -232,6 +232,27 @@ class DeviceMesh:
         self.struct = self._make_struct() if dev is not None else None
 
     @classmethod
+    def from_host_tables(cls, A, T, R, device=None):
+        """A mesh from tables built earlier on the host (``meshcache``): ``A`` the host
+        geometry, ``T`` the table dict of ``DeviceMesh(A, device=None)``, ``R`` its
+        renumbering (``cperm``, ``cinv``, ``fperm``, ``finv``, ``nperm``, ``ninv``, ``enabled``)."""
+        self = cls.__new__(cls)
+        dim = int(A["dim"])
+        self.dim, self.nbcells, self.nbfaces, self.nbnodes = dim, int(A["nbcells"]), int(A["nbfaces"]), int(A["nbnodes"])
+        self.nlf = 3 if dim == 2 else 4
+        self.A = A
+        self.R = R
+        self.reordered = bool(R.enabled)
+        dev = torch.device(device) if device is not None else None
+        self.device = dev
+        self.t = {k: _t(v, v.dtype, dev) for k, v in T.items()}
+        i64 = np.int64
+        self.perm = {"cell": _t(R.cperm, i64, dev), "face": _t(R.fperm, i64, dev), "node": _t(R.nperm, i64, dev)}
+        self.inv = {"cell": _t(R.cinv, i64, dev), "face": _t(R.finv, i64, dev), "node": _t(R.ninv, i64, dev)}
+        self.struct = self._make_struct() if dev is not None else None
+        return self
+
+    @classmethod
     def from_native(cls, elements, vertex, device=None, reorder=True):
         """The tables of a 2D triangle mesh from the native host builder (``native.tables2d``),
         bit-identical to ``DeviceMesh(geometry.build(...))``; ``A`` then holds only the

@@ -56,6 +56,9 @@ class Domain:
         ("float_precision", "str", "double", None, "precision of the float arrays"),
         ("int_precision", "str", "signed", None, "precision of the integer arrays"),
         ("device", "str", "cuda", None, "torch device holding the mesh tables"),
+        ("mesh_cache", "str", None, None, "directory of the persistent mesh cache (geometry and device tables "
+                                           "stored once per mesh; also MANAPY_B200_MESH_CACHE); no counterpart "
+                                           "in manapy"),
     ]
 
     @classmethod
@@ -85,7 +88,15 @@ class Domain:
         elements, vertex = mesh
         self._comm = comm if comm is not None else _OneRankComm()
         self._dim = np.int32(dim)
-        self._A = geometry.build(elements, vertex, int(dim))
+        cache_dir = get("mesh_cache") or os.environ.get("MANAPY_B200_MESH_CACHE")
+        self._host_dm = None
+        self.mesh_cache_hit = False
+        if cache_dir:
+            from . import meshcache
+            self._A, self._host_dm, self.mesh_cache_hit = meshcache.load_or_build(elements, vertex, int(dim),
+                                                                                  cache_dir)
+        else:
+            self._A = geometry.build(elements, vertex, int(dim))
         if len(self._A["unmatched_boundary_faces"]):
             raise ValueError("%d boundary faces match no boundary side (their vertices carry "
                              "incompatible tags)" % len(self._A["unmatched_boundary_faces"]))
@@ -147,8 +158,11 @@ class Domain:
     def device_mesh(self):
         """The device tables (``mb_mesh``), built on first use."""
         if self._dmesh is None:
-            from .device import DeviceMesh
-            self._dmesh = DeviceMesh(self._A, self.device)
+            if self._host_dm is not None:          # tables from the mesh cache
+                self._dmesh, self._host_dm = self._host_dm.upload(self.device), None
+            else:
+                from .device import DeviceMesh
+                self._dmesh = DeviceMesh(self._A, self.device)
         return self._dmesh
 
     @property
