@@ -230,15 +230,20 @@ int mb_ghost_euler_neumann_2d(const mb_mesh *m, const double *const q[5], double
  * dt = min(time_step_euler_2d), bit-identical to that sequence, in two launches (every face
  * flux once into face_flux, then update + next dt per cell).  Every boundary face must carry
  * the Neumann rule (names 1-4); no halo faces.
- * face_flux: device scratch of 4 * nbfaces doubles, 16-byte aligned.
+ * mb_euler_tables_2d fills, once per mesh, face_rec (4 * nbfaces doubles, 32-byte aligned:
+ * normal x, y, mesure and the two cells of each face) and cell_left (nbcells bytes: bit j set
+ * when the cell is the left cell of its local face j).
+ * face_flux: device scratch of 4 * nbfaces doubles, 32-byte aligned.
  * ring: 3 device doubles.  mb_euler_dt_2d resets the ring and puts the dt of q into slot t%3;
  * mb_euler_step_2d at time index t reads slot t%3, writes q_out (buffers distinct from q_in),
  * min-reduces the dt of q_out into slot (t+1)%3 and resets slot (t+2)%3, so consecutive calls
  * with t, t+1, ... need no host synchronisation.  time (nullable, device): += the dt used. */
 int mb_euler_dt_2d(const mb_mesh *m, const double *const q[5], double cfl, double gamma, double *ring, int t,
                    void *stream);
+int mb_euler_tables_2d(const mb_mesh *m, double *face_rec, uint8_t *cell_left, void *stream);
 int mb_euler_step_2d(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl,
-                     double gamma, double *face_flux, double *ring, int t, double *time, void *stream);
+                     double gamma, const double *face_rec, const uint8_t *cell_left, double *face_flux,
+                     double *ring, int t, double *time, void *stream);
 
 /* ---- fused steps ---------------------------------------------------------------------- */
 

@@ -87,7 +87,8 @@ _SIGS = {
     "mb_update_euler_2d": [_M, _P5, _P4, _d, _d, _vp],
     "mb_ghost_euler_neumann_2d": [_M, _P5, _P5, _vp, _vp, _vp],
     "mb_euler_dt_2d": [_M, _P5, _d, _d, _vp, _i32, _vp],
-    "mb_euler_step_2d": [_M, _P5, _P5, _d, _d, _vp, _vp, _i32, _vp, _vp],
+    "mb_euler_tables_2d": [_M, _vp, _vp, _vp],
+    "mb_euler_step_2d": [_M, _P5, _P5, _d, _d, _vp, _vp, _vp, _vp, _i32, _vp, _vp],
     "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],

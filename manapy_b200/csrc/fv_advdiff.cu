@@ -449,6 +449,9 @@ __global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_
 #ifndef MB_P1_MIN_BLOCKS
 #define MB_P1_MIN_BLOCKS 6
 #endif
+#ifndef MB_F2_LSQ_BATCH
+#define MB_F2_LSQ_BATCH 4
+#endif
 #ifndef MB_P1_BLOCK
 #define MB_P1_BLOCK kBlock
 #endif
@@ -474,18 +477,21 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
     const int32_t *ix = m.lsq_sell_idx + sb + lane;
     const uint64_t pst = l2_stream();
     int k = 0;
-    // batches of four: four index loads, then eight gathers in flight, then the
-    // four terms accumulated in manapy's order
-    for (; k + 4 <= L; k += 4) {
-      int cc[4];
+    // batches of MB_F2_LSQ_BATCH: the index loads, then twice as many gathers in flight,
+    // then the terms accumulated in manapy's order
+    for (; k + MB_F2_LSQ_BATCH <= L; k += MB_F2_LSQ_BATCH) {
+      int cc[MB_F2_LSQ_BATCH];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) { cc[u] = ld1_stream(ix + 32 * (k + u), pst); cc[u] = cc[u] < 0 ? i : cc[u]; }
-      double2 pc[4];
-      double wc[4];
+      for (int u = 0; u < MB_F2_LSQ_BATCH; ++u) {
+        cc[u] = ld1_stream(ix + 32 * (k + u), pst);
+        cc[u] = cc[u] < 0 ? i : cc[u];
+      }
+      double2 pc[MB_F2_LSQ_BATCH];
+      double wc[MB_F2_LSQ_BATCH];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) { pc[u] = ldd2(m.cell_xy + 2 * cc[u]); wc[u] = ld(w + cc[u]); }
+      for (int u = 0; u < MB_F2_LSQ_BATCH; ++u) { pc[u] = ldd2(m.cell_xy + 2 * cc[u]); wc[u] = ld(w + cc[u]); }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < MB_F2_LSQ_BATCH; ++u) {
         const double dx = pc[u].x - c.x, dy = pc[u].y - c.y, dw = wc[u] - wi;
         ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
         jx += (dx * dw); jy += (dy * dw);

@@ -157,11 +157,17 @@ __global__ void __launch_bounds__(kBlock) k_ghost_euler_neumann(mb_mesh m, Euler
 // ---- fused step: face fluxes, then update + the next step's dt in one pass over the cells ----
 //
 // Two launches per step.  k_euler_face evaluates every face flux once (faces in device
-// order, Neumann ghost = the cell's own state on faces named 1-4) into face_flux (four
-// doubles per face, two 16-byte stores).  k_euler_cell adds its three fluxes in ascending
-// face id with manapy's signs, updates the state and min-reduces the dt of the new state.
-// Evaluating each flux once instead of from both cells halves the FP64 division work that
-// bounds the single-pass form, at the price of 32 bytes per face written and read back.
+// order, Neumann ghost = the cell's own state on boundary faces) into face_flux (four
+// doubles per face).  k_euler_cell adds its three fluxes in ascending face id with manapy's
+// signs, updates the state and min-reduces the dt of the new state.  Evaluating each flux
+// once instead of from both cells halves the FP64 division work that bounds the
+// single-pass form, at the price of 32 bytes per face written and read back.
+//
+// Both kernels read two static tables built once per mesh (mb_euler_tables_2d): a 32-byte
+// record per face {n0, n1, mesure, (c0, c1)} -- one 256-bit load where four arrays would
+// take five loads -- and a byte per cell whose bit j says the cell is the left cell
+// (faces.cellid[f][0]) of its local face j.  Flux records are read and written as one
+// 256-bit access each.
 //
 // dt ring of three device slots: the step of time index t reads slot t%3 (the dt of its
 // input state, complete since the previous step), min-reduces the dt of its output state
@@ -173,28 +179,63 @@ constexpr double kNoDt = 1e300;
 #define MB_EULER_MIN_BLOCKS 4
 #endif
 
-__global__ void __launch_bounds__(kBlock) k_euler_face(mb_mesh m, EulerQ q, double gamma, double *ff) {
+// the two cells of a face in the fourth double of its record (bit pattern only; never used
+// in arithmetic); c1 = -1 on boundary faces
+__device__ __forceinline__ double pack_cells(int c0, int c1) {
+  return __longlong_as_double((long long)(((unsigned long long)(unsigned)c1 << 32) | (unsigned)c0));
+}
+__device__ __forceinline__ void unpack_cells(double v, int &c0, int &c1) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  c0 = (int)(unsigned)(u & 0xffffffffull);
+  c1 = (int)(unsigned)(u >> 32);
+}
+
+__device__ __forceinline__ void st4d(double *p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+
+__global__ void __launch_bounds__(kBlock) k_euler_face_rec(mb_mesh m, double *rec) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= m.nbfaces) return;
   const int c0 = ld(m.face_cellid + 2 * f);
-  const double mes = ld(m.face_mesure + f);
-  const double nx = ld(m.face_normal + 3 * f) / mes, ny = ld(m.face_normal + 3 * f + 1) / mes;
+  const int c1 = ld(m.face_name + f) == 0 ? ld(m.face_cellid + 2 * f + 1) : -1;
+  st4d(rec + 4 * (long long)f, ld(m.face_normal + 3 * f), ld(m.face_normal + 3 * f + 1), ld(m.face_mesure + f),
+       pack_cells(c0, c1));
+}
+
+__global__ void __launch_bounds__(kBlock) k_euler_cell_left(mb_mesh m, uint8_t *left) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  unsigned bits = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) bits |= (ld(m.face_cellid + 2 * ld(m.cell_faces + 4 * i + j)) == i ? 1u : 0u) << j;
+  left[i] = (uint8_t)bits;
+}
+
+__global__ void __launch_bounds__(kBlock) k_euler_face(int nf, EulerQ q, double gamma, const double *rec,
+                                                       double *ff) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  double r0, r1, mes, cb;
+  ld4d(rec + 4 * (long long)f, r0, r1, mes, cb);
+  int c0, c1;
+  unpack_cells(cb, c0, c1);
+  const double nx = r0 / mes, ny = r1 / mes;
   const double rl = ld(q.rho + c0), Pl = ld(q.P + c0), ul = ld(q.rhou + c0), vl = ld(q.rhov + c0),
                El = ld(q.rhoE + c0);
   double F[4];
-  if (ld(m.face_name + f) == 0) {
-    const int c1 = ld(m.face_cellid + 2 * f + 1);
+  if (c1 >= 0) {
     rusanov(rl, Pl, ul, vl, El, ld(q.rho + c1), ld(q.P + c1), ld(q.rhou + c1), ld(q.rhov + c1), ld(q.rhoE + c1), nx,
             ny, mes, gamma, F);
   } else {
     rusanov(rl, Pl, ul, vl, El, rl, Pl, ul, vl, El, nx, ny, mes, gamma, F);
   }
-  double2 *o = reinterpret_cast<double2 *>(ff) + 2 * (long long)f;
-  o[0] = make_double2(F[0], F[1]);
-  o[1] = make_double2(F[2], F[3]);
+  st4d(ff + 4 * (long long)f, F[0], F[1], F[2], F[3]);
 }
 
 __global__ void __launch_bounds__(kBlock, MB_EULER_MIN_BLOCKS) k_euler_cell(mb_mesh m, EulerQ q, EulerW out,
+                                                                            const double *rec,
+                                                                            const uint8_t *cell_left,
                                                                             const double *ff, double cfl,
                                                                             double gamma, double *ring, int a, int b,
                                                                             int c, double *time) {
@@ -202,18 +243,24 @@ __global__ void __launch_bounds__(kBlock, MB_EULER_MIN_BLOCKS) k_euler_cell(mb_m
   const double dt = ld(ring + a);
   double dtc = kNoDt;
   if (i < m.nbcells) {
-    int f[3];
+    const int4 fc = ld4(m.cell_faces + 4 * i);
+    const int f[3] = {fc.x, fc.y, fc.z};
     double n0[3], n1[3], mes[3];
-    cell_face_geom(m, i, f, n0, n1, mes);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double unused;
+      ld4d(rec + 4 * (long long)f[j], n0[j], n1[j], mes[j], unused);
+    }
     const uint8_t code = ld(m.cell_order + i);
-    const double2 *F2 = reinterpret_cast<const double2 *>(ff);
+    const unsigned lb = ld(cell_left + i);
     double rez[4] = {0., 0., 0., 0.};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const int fk = pick3(f[0], f[1], f[2], order_slot(code, k));
-      const bool left = ld(m.face_cellid + 2 * fk) == i;
-      const double2 A = ld(F2 + 2 * (long long)fk), B = ld(F2 + 2 * (long long)fk + 1);
-      const double F[4] = {A.x, A.y, B.x, B.y};
+      const int s = order_slot(code, k);
+      const int fk = pick3(f[0], f[1], f[2], s);
+      const bool left = (lb >> s) & 1u;
+      double F[4];
+      ld4d(ff + 4 * (long long)fk, F[0], F[1], F[2], F[3]);
 #pragma unroll
       for (int e = 0; e < 4; ++e) rez[e] = left ? rez[e] - F[e] : rez[e] + F[e];
     }
@@ -326,18 +373,32 @@ int mb_euler_dt_2d(const mb_mesh *m, const double *const q[5], double cfl, doubl
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }
 
+static bool a32(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 31) == 0; }
+
+int mb_euler_tables_2d(const mb_mesh *m, double *face_rec, uint8_t *cell_left, void *stream) {
+  if (!euler_mesh_ok(m) || !face_rec || !cell_left || m->nbfaces <= 0 || !a32(face_rec)) return MB_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_euler_face_rec<<<(m->nbfaces + kBlock - 1) / kBlock, kBlock, 0, st>>>(*m, face_rec);
+  k_euler_cell_left<<<(m->nbcells + kBlock - 1) / kBlock, kBlock, 0, st>>>(*m, cell_left);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
 int mb_euler_step_2d(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl,
-                     double gamma, double *face_flux, double *ring, int t, double *time, void *stream) {
-  if (!euler_mesh_ok(m) || !q_ok(q_in) || !q_out || !ring || !face_flux || t < 0 || m->nbfaces <= 0) return MB_EINVAL;
-  if (reinterpret_cast<uintptr_t>(face_flux) % 16) return MB_EINVAL;
+                     double gamma, const double *face_rec, const uint8_t *cell_left, double *face_flux, double *ring,
+                     int t, double *time, void *stream) {
+  if (!euler_mesh_ok(m) || !q_ok(q_in) || !q_out || !ring || !face_flux || !face_rec || !cell_left || t < 0 ||
+      m->nbfaces <= 0)
+    return MB_EINVAL;
+  if (!a32(face_flux) || !a32(face_rec)) return MB_EINVAL;
   for (int k = 0; k < 5; ++k)
     if (!q_out[k] || q_out[k] == q_in[k]) return MB_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   EulerQ qq{q_in[0], q_in[1], q_in[2], q_in[3], q_in[4]};
   EulerW oo{q_out[0], q_out[1], q_out[2], q_out[3], q_out[4]};
-  k_euler_face<<<(m->nbfaces + kBlock - 1) / kBlock, kBlock, 0, st>>>(*m, qq, gamma, face_flux);
-  k_euler_cell<<<(m->nbcells + kBlock - 1) / kBlock, kBlock, 0, st>>>(*m, qq, oo, face_flux, cfl, gamma, ring,
-                                                                      t % 3, (t + 1) % 3, (t + 2) % 3, time);
+  k_euler_face<<<(m->nbfaces + kBlock - 1) / kBlock, kBlock, 0, st>>>(m->nbfaces, qq, gamma, face_rec, face_flux);
+  k_euler_cell<<<(m->nbcells + kBlock - 1) / kBlock, kBlock, 0, st>>>(*m, qq, oo, face_rec, cell_left, face_flux,
+                                                                      cfl, gamma, ring, t % 3, (t + 1) % 3,
+                                                                      (t + 2) % 3, time);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }
 

@@ -880,6 +880,11 @@ class EulerSolver:
             self._ring = torch.full((3,), 1e300, dtype=f64, device=dm.device)
             self._time = torch.zeros(1, dtype=f64, device=dm.device)
             self._ff = torch.empty(4 * dm.nbfaces, dtype=f64, device=dm.device)   # face fluxes
+            # static tables of the fused step: face records and left-cell bits
+            self._frec = torch.empty(4 * dm.nbfaces, dtype=f64, device=dm.device)
+            self._cleft = torch.empty(dm.nbcells, dtype=torch.uint8, device=dm.device)
+            _lib.call("mb_euler_tables_2d", dm.struct, _p(self._frec), _p(self._cleft),
+                      torch.cuda.current_stream(dm.device).cuda_stream)
             self._t = 0
             self._key = None
             self._dt_host = None
@@ -949,7 +954,8 @@ class EulerSolver:
     def _launch(self, t):
         a, b = self._bufs[t % 2], self._bufs[(t + 1) % 2]
         _lib.call("mb_euler_step_2d", self._dm.struct, _lib.p5([_p(x) for x in a]), _lib.p5([_p(x) for x in b]),
-                  self.cfl, self.gamma, _p(self._ff), _p(self._ring), int(t), _p(self._time), self._stream())
+                  self.cfl, self.gamma, _p(self._frec), _p(self._cleft), _p(self._ff), _p(self._ring), int(t),
+                  _p(self._time), self._stream())
 
     def _publish(self):
         for k, b in zip(self._NAMES, self._bufs[self._t % 2]):
