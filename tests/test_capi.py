@@ -52,3 +52,27 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert int(got[name]) == ctypes.sizeof(cls), name
         for field, _ in cls._fields_:
             assert int(got[name + "." + field]) == getattr(cls, field).offset, (name, field)
+
+
+def test_entry_points_reject_null_arguments():
+    """Every entry point validates its arguments on the host: null meshes, states and
+    scratch give MB_EINVAL before any CUDA call (runs without a GPU).  mb_srnh_flux with
+    zero states has nothing to do and succeeds."""
+    import ctypes
+    from manapy_b200 import _lib
+    L = _lib.lib()
+    for name, argt in _lib._SIGS.items():
+        if name == "mb_build_info":
+            continue
+        args = []
+        for t in argt:
+            if isinstance(t, type) and issubclass(t, ctypes.Array):
+                args.append(t())
+            elif t in (ctypes.c_double, ctypes.c_float):
+                args.append(0.0)
+            elif t in (ctypes.c_int32, ctypes.c_int64, ctypes.c_int):
+                args.append(0)
+            else:
+                args.append(None)
+        rc = getattr(L, name)(*args)
+        assert rc == (_lib.MB_OK if name == "mb_srnh_flux" else _lib.MB_EINVAL), (name, rc)
