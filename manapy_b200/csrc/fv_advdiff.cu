@@ -543,8 +543,12 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
       ps = pmin(ps, psi_ij);
     }
     const uint64_t keep = l2_keep();
+#if MB_V4_IO
+    st4_keep(rec + 4 * i, wi, x, y, ps, keep);
+#else
     st2_keep(rec + 4 * i, wi, x, keep);
     st2_keep(rec + 4 * i + 2, y, ps, keep);
+#endif
     return;
   }
   if (DIFF) {
@@ -595,8 +599,14 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
                 P2 = ldd2(m.node_coord + 2 * vt.z);
   const double2 ci = ldd2(m.cell_xy + 2 * i);
   const uint64_t pst = l2_stream();
+#if MB_V4_IO
+  double2 s01;
+  double s2, s_pad;
+  ld4d_stream(sign + 4 * i, s01.x, s01.y, s2, s_pad, pst);
+#else
   const double2 s01 = ldd2_stream(sign + 4 * i, pst);
   const double s2 = ldd_stream(sign + 4 * i + 2, pst);
+#endif
   double wi, gxi = 0., gyi = 0., psii = 0.;
   if (ORDER2) {
     ld4d(rec + 4 * i, wi, gxi, gyi, psii);
@@ -989,6 +999,9 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
     // tables (3D) must start on 32-byte boundaries
     auto a32 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 31) == 0; };
     if ((DIM == 2 && O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord)))) return MB_EINVAL;
+#endif
+#if MB_V4_IO
+    if (DIM == 2 && (reinterpret_cast<uintptr_t>(sign) & 31) != 0) return MB_EINVAL;
 #endif
     if (DIM == 2) {
       const int ncb2 = O2 ? ceil_div(m.nbcells, MB_P1_BLOCK) : 0;

@@ -131,6 +131,22 @@ __device__ __forceinline__ void ld4d(const double *p, double &a, double &b, doub
   a = u.x; b = u.y; c = v.x; d = v.y;
 #endif
 }
+// one 256-bit access per 32-byte record where a kernel writes or streams whole rows
+#ifndef MB_V4_IO
+#define MB_V4_IO 1
+#endif
+__device__ __forceinline__ void st4_keep(double *a, double x, double y, double z, double w, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f64 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "d"(x), "d"(y), "d"(z), "d"(w),
+               "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st4d_plain(double *a, double x, double y, double z, double w) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(a), "d"(x), "d"(y), "d"(z), "d"(w) : "memory");
+}
+__device__ __forceinline__ void ld4d_stream(const double *p, double &a, double &b, double &c, double &d,
+                                            uint64_t pol) {
+  MB_ASM_LD(MB_LDNC ".v4.f64 {%0, %1, %2, %3}, [%4], %5;" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p), "l"(pol));
+}
 __device__ __forceinline__ D3 ld3(const double *p) {  // [n][4] rows
   double a, b, c, d;
   ld4d(p, a, b, c, d);

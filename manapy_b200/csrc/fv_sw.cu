@@ -12,6 +12,7 @@
 // five residuals are gathered per cell in manapy's order (inner faces by
 // ascending id, then boundary faces by ascending id).
 #include "fv_common.cuh"
+#include "fv_compact.cuh"
 
 namespace mb {
 
@@ -544,8 +545,12 @@ __global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS) k_sw2
   double fl[4];
   srnh0<FAST>(ld(s.q[1] + l), ld(s.q[1] + rr), ld(s.q[2] + l), ld(s.q[2] + rr), h_l, h_r, hc_l, hc_r,
               ld(s.q[4] + l), ld(s.q[4] + rr), n0, n1, mes, grav, fl);
+#if MB_V4_IO
+  st4d_plain(ff + 4 * (long long)f, fl[0], fl[1], fl[2], fl[3]);
+#else
   reinterpret_cast<double2 *>(ff)[2 * f] = make_double2(fl[0], fl[1]);
   reinterpret_cast<double2 *>(ff)[2 * f + 1] = make_double2(fl[2], fl[3]);
+#endif
 }
 
 // flags of the compact 2D layout (cell_flags): bit j own, 3+j node order, 6+j normal
@@ -588,8 +593,12 @@ __device__ __forceinline__ double sw2_cell_body(const mb_mesh &m, const SWState 
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int f = compi(cf, j);
+#if MB_V4_IO
+    ld4d(ff + 4 * (long long)f, F[j][0], F[j][1], F[j][2], F[j][3]);
+#else
     const double2 a = ldd2s(ff + 4 * f), b = ldd2s(ff + 4 * f + 2);
     F[j][0] = a.x; F[j][1] = a.y; F[j][2] = b.x; F[j][3] = b.y;
+#endif
     const bool rev = (fl >> (3 + j)) & 1u;
     const double2 Pj = j == 0 ? P0 : (j == 1 ? P1 : P2), Pk = j == 0 ? P1 : (j == 1 ? P2 : P0);
     const double2 Xa = rev ? Pk : Pj, Xb = rev ? Pj : Pk;
@@ -802,6 +811,9 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
     out.q[k] = q_out[k];
   }
   if (dt_next == dt_cur) return MB_EINVAL;
+#if MB_V4_IO
+  if ((reinterpret_cast<uintptr_t>(face_flux) & 31) != 0) return MB_EINVAL;   // 256-bit flux records
+#endif
   cudaStream_t st = ST(stream);
   const int fb = ceil_div(m->nbfaces, MB_SW_FLUX_BLOCK);
   if (order == 2) {
