@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="C2", choices=["C1", "C2", "C3", "C4", "E1"])
     ap.add_argument("--e2e-steps", type=int, default=30)
-    ap.add_argument("--cpu-steps", type=int, default=5, help="oracle steps of the CPU baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=15,
+                    help="oracle steps of the CPU baseline sample (about 10-30 s of serial work at 2M cells)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32c", action="store_true", help="skip the FP32-compensated measurement")
     ap.add_argument("--serve", action="store_true", help="continuous-batching serving run instead of one workload")
