@@ -253,13 +253,14 @@ class DeviceMesh:
         return self
 
     @classmethod
-    def from_native(cls, elements, vertex, device=None, reorder=True):
+    def from_native(cls, elements, vertex, device=None, reorder=True, full=False):
         """The tables of a 2D triangle mesh from the native host builder (``native.tables2d``),
         bit-identical to ``DeviceMesh(geometry.build(...))``; ``A`` then holds only the
-        manapy-numbered arrays the boundary set-up reads."""
+        manapy-numbered arrays the boundary set-up reads, or with ``full`` every array of
+        ``geometry.build`` (bit-identical too)."""
         from types import SimpleNamespace
         from . import native
-        T = native.tables2d(elements, vertex, reorder=reorder)
+        T = native.tables2d(elements, vertex, reorder=reorder, full=full)
         self = cls.__new__(cls)
         nc, nf, nn = len(T["cell_volume"]), len(T["face_name"]), len(T["node_coord"])
         self.dim, self.nbcells, self.nbfaces, self.nbnodes, self.nlf = 2, nc, nf, nn, 3

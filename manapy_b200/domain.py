@@ -47,6 +47,23 @@ class _OneRankComm:
         return x
 
 
+def build_host_mesh(elements, vertex, dim):
+    """(A, host-built DeviceMesh or None): 2D meshes through the native host builder (every
+    ``geometry.build`` array and device table in one C++ pass, bit-identical to the Python
+    builder), anything else -- or a mesh the native builder rejects, so that the Python
+    builder reports it -- through ``geometry.build``."""
+    if dim == 2:
+        from . import native
+        from .device import DeviceMesh
+        try:
+            if native.available():
+                dm = DeviceMesh.from_native(elements, vertex, device=None, full=True)
+                return dm.A, dm
+        except ValueError:
+            pass
+    return geometry.build(elements, vertex, dim), None
+
+
 class Domain:
     _parameters = [
         ("backend", "str", "cuda", False, "kernel backend: cuda (sm_100a)"),
@@ -96,7 +113,7 @@ class Domain:
             self._A, self._host_dm, self.mesh_cache_hit = meshcache.load_or_build(elements, vertex, int(dim),
                                                                                   cache_dir)
         else:
-            self._A = geometry.build(elements, vertex, int(dim))
+            self._A, self._host_dm = build_host_mesh(elements, vertex, int(dim))
         if len(self._A["unmatched_boundary_faces"]):
             raise ValueError("%d boundary faces match no boundary side (their vertices carry "
                              "incompatible tags)" % len(self._A["unmatched_boundary_faces"]))

@@ -150,7 +150,7 @@ std::vector<i64> stable_argsort(const std::vector<K> &key) {
   return o;
 }
 
-Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder) {
+Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, bool full) {
   auto *res = new Result();
   for (i64 c = 0; c < nc; ++c)
     if (el[4 * c + 3] != 3) {
@@ -592,6 +592,82 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder) {
     static const char *LN[5] = {"A.innerfaces", "A.infaces", "A.outfaces", "A.upperfaces", "A.bottomfaces"};
     for (int t = 0; t < 5; ++t) res->add(LN[t], 'i', {(i64)lists[t].size()}, to32(lists[t]));
   }
+  if (full) {
+    // every array of geometry.build (manapy's Domain arrays, manapy numbering)
+    std::vector<i32> nodeid(4 * nc), faceid(4 * nc), cfid(4 * nc);
+    for (i64 c = 0; c < nc; ++c) {
+      int k = 0;
+      for (int j = 0; j < 4; ++j) nodeid[4 * c + j] = el[4 * c + j];
+      for (int j = 0; j < 3; ++j) {
+        faceid[4 * c + j] = (i32)inv[3 * c + j];
+        cfid[4 * c + j] = (i32)cellfid[3 * c + j];
+        if (cellfid[3 * c + j] != -1) ++k;
+      }
+      faceid[4 * c + 3] = 3;
+      cfid[4 * c + 3] = k;
+    }
+    res->add("A.cells_nodeid", 'i', {nc, 4}, nodeid);
+    res->add("A.cells_faceid", 'i', {nc, 4}, faceid);
+    res->add("A.cells_cellfid", 'i', {nc, 4}, cfid);
+    res->add("A.cells_volume", 'd', {nc}, vol);
+    res->add("A.cells_nf", 'd', {nc, 3, 3}, cnf);
+    res->add("A.n2c_ptr", 'l', {nn + 1}, n2c_ptr);
+    res->add("A.n2c_idx", 'i', {(i64)n2c_idx.size()}, to32(n2c_idx));
+    res->add("A.n2g_ptr", 'l', {nn + 1}, n2g_ptr);
+    res->add("A.n2g_idx", 'i', {(i64)n2g_idx.size()}, to32(n2g_idx));
+    res->add("A.cellnid_ptr", 'l', {nc + 1}, cnid_ptr);
+    res->add("A.cellnid_idx", 'i', {(i64)cnid_idx.size()}, to32(cnid_idx));
+    res->add("A.ghostnid_ptr", 'l', {nc + 1}, gnid_ptr);
+    res->add("A.ghostnid_idx", 'i', {(i64)gnid_idx.size()}, to32(gnid_idx));
+    std::vector<i32> fnid(3 * nf), fcid(2 * nf);
+    std::vector<double> nrm(3 * nf), fdn[4], par[4];
+    for (int k = 0; k < 4; ++k) {
+      fdn[k].resize(2 * nf);
+      par[k].resize(nf);
+    }
+    for (i64 f = 0; f < nf; ++f) {
+      fnid[3 * f] = (i32)fa[f]; fnid[3 * f + 1] = (i32)fb[f]; fnid[3 * f + 2] = 2;
+      fcid[2 * f] = (i32)f0[f]; fcid[2 * f + 1] = (i32)f1[f];
+      nrm[3 * f] = nx[f]; nrm[3 * f + 1] = ny[f]; nrm[3 * f + 2] = nz[f];
+      const double *F = &ff[8 * f];
+      for (int k = 0; k < 4; ++k) { fdn[k][2 * f] = F[2 * k]; fdn[k][2 * f + 1] = F[2 * k + 1]; }
+      // diamond coefficients (ddm_utils2d.py:602-605): pairs (f1, f2), (f2, f3), (f3, f4), (f4, f1)
+      const double inv2a = 1.0 / (2.0 * air[f]);
+      for (int k = 0; k < 4; ++k) {
+        const int a = k, b = (k + 1) % 4;
+        par[k][f] = inv2a * ((F[2 * a + 1] + F[2 * b + 1]) * nx[f] - (F[2 * a] + F[2 * b]) * ny[f]);
+      }
+    }
+    res->add("A.faces_nodeid", 'i', {nf, 3}, fnid);
+    res->add("A.faces_cellid", 'i', {nf, 2}, fcid);
+    res->add("A.faces_name", 'i', {nf}, name);
+    res->add("A.faces_normal", 'd', {nf, 3}, nrm);
+    res->add("A.faces_mesure", 'd', {nf}, mes);
+    res->add("A.faces_ghostcenter", 'd', {nf, 3}, gc);
+    res->add("A.faces_airDiamond", 'd', {nf}, air);
+    static const char *FN[4] = {"A.faces_f_1", "A.faces_f_2", "A.faces_f_3", "A.faces_f_4"};
+    static const char *PN[4] = {"A.faces_param1", "A.faces_param2", "A.faces_param3", "A.faces_param4"};
+    for (int k = 0; k < 4; ++k) {
+      res->add(FN[k], 'd', {nf, 2}, fdn[k]);
+      res->add(PN[k], 'd', {nf}, par[k]);
+    }
+    res->add("A.faces_dist_ortho", 'd', {nf}, dist);
+    std::vector<double> vtx(vx, vx + 4 * nn), zero(nn, 0.0);
+    res->add("A.nodes_vertex", 'd', {nn, 4}, vtx);
+    res->add("A.nodes_name", 'i', {nn}, namen);
+    res->add("A.nodes_R_x", 'd', {nn}, Rx);
+    res->add("A.nodes_R_y", 'd', {nn}, Ry);
+    res->add("A.nodes_R_z", 'd', {nn}, zero);
+    res->add("A.nodes_lambda_x", 'd', {nn}, lx);
+    res->add("A.nodes_lambda_y", 'd', {nn}, ly);
+    res->add("A.nodes_lambda_z", 'd', {nn}, zero);
+    res->add("A.nodes_number", 'i', {nn}, to32(number));
+    res->add("A.boundaryfaces", 'i', {(i64)bfaces.size()}, to32(bfaces));
+    const std::vector<i32> none;
+    res->add("A.halofaces", 'i', {0}, none);
+    res->add("A.periodicboundaryfaces", 'i', {0}, none);
+    res->add("A.unmatched_boundary_faces", 'i', {0}, none);
+  }
   return res;
 }
 
@@ -599,9 +675,11 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder) {
 
 extern "C" {
 
-void *mbh_build2d(const int32_t *elements, int64_t nbcells, const double *vertex, int64_t nbnodes, int32_t reorder) {
+// full != 0 also returns every array of geometry.build as "A.<name>" (manapy numbering)
+void *mbh_build2d(const int32_t *elements, int64_t nbcells, const double *vertex, int64_t nbnodes, int32_t reorder,
+                  int32_t full) {
   if (!elements || !vertex || nbcells <= 0 || nbnodes <= 0) return nullptr;
-  return build2d(elements, nbcells, vertex, nbnodes, reorder != 0);
+  return build2d(elements, nbcells, vertex, nbnodes, reorder != 0, full != 0);
 }
 
 const char *mbh_error(void *h) { return h ? static_cast<Result *>(h)->error.c_str() : "null handle"; }

@@ -26,7 +26,7 @@ import numpy as np
 __all__ = ["mesh_key", "load_or_build", "entry_path"]
 
 FORMAT = 1
-_SOURCES = ("geometry.py", "reorder.py", "device.py", "meshcache.py")
+_SOURCES = ("geometry.py", "reorder.py", "device.py", "meshcache.py", "host/mesh2d.cpp")
 _digest = None
 
 
@@ -106,9 +106,15 @@ def load_or_build(elements, vertex, dim, cache_dir, reorder=True):
     if os.path.exists(path):
         A, dm = _load(path)
         return A, dm, True
-    A = geometry.build(elements, vertex, int(dim))
+    dm = None
+    if int(dim) == 2 and reorder:
+        from .domain import build_host_mesh
+        A, dm = build_host_mesh(elements, vertex, 2)
+    else:
+        A = geometry.build(elements, vertex, int(dim))
     if len(A["unmatched_boundary_faces"]):
         return A, None, False          # the caller raises manapy's error; nothing is cached
-    dm = DeviceMesh(A, device=None, reorder=reorder)
+    if dm is None:
+        dm = DeviceMesh(A, device=None, reorder=reorder)
     _save(path, A, dm)
     return A, dm, False

@@ -27,7 +27,8 @@ def lib():
             build_host()
         L = ctypes.CDLL(HOST_OUT)
         L.mbh_build2d.restype = ctypes.c_void_p
-        L.mbh_build2d.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32]
+        L.mbh_build2d.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                  ctypes.c_int32]
         L.mbh_error.restype = ctypes.c_char_p
         L.mbh_error.argtypes = [ctypes.c_void_p]
         L.mbh_count.restype = ctypes.c_int32
@@ -42,14 +43,24 @@ def lib():
     return _lib
 
 
-def tables2d(elements, vertex, reorder=True):
-    """dict name -> numpy array (see ``host/mesh2d.cpp``); raises ValueError on a bad mesh."""
+def available():
+    """True when the native host library loads (it is built with the CUDA library)."""
+    try:
+        lib()
+        return True
+    except OSError:
+        return False
+
+
+def tables2d(elements, vertex, reorder=True, full=False):
+    """dict name -> numpy array (see ``host/mesh2d.cpp``); raises ValueError on a bad mesh.
+    ``full``: also every array of ``geometry.build`` as ``"A.<name>"``."""
     el = np.ascontiguousarray(elements, dtype=np.int32)
     vx = np.ascontiguousarray(vertex, dtype=np.float64)
     if el.ndim != 2 or el.shape[1] != 4 or vx.ndim != 2 or vx.shape[1] != 4:
         raise ValueError("expected elements [nc, 4] and vertex [nn, 4]")
     L = lib()
-    h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)))
+    h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)), int(bool(full)))
     if not h:
         raise ValueError("empty mesh")
     try:

@@ -34,3 +34,35 @@ def test_rejects_unmatched_boundary_faces():
     vx[:, 3] = 0  # no boundary tags at all
     with pytest.raises(ValueError, match="match no boundary side"):
         D.DeviceMesh.from_native(el, vx)
+
+
+@pytest.mark.parametrize("n,seed", [(7, 1), (33, 5)])
+def test_native_full_geometry_is_bit_identical(n, seed):
+    """With full=True the native builder also returns every geometry.build array (what a
+    Domain exposes): same keys, dtypes, shapes and bits (signs of zeros included)."""
+    import numpy as np
+    from manapy_b200 import geometry as G, meshgen
+    from manapy_b200.device import DeviceMesh
+    el, vx = meshgen.square_triangles(n, seed=seed)
+    A = G.build(el, vx, 2)
+    B = DeviceMesh.from_native(el, vx, full=True).A
+    assert set(A) == set(B)
+    for k, a in A.items():
+        b = B[k]
+        if isinstance(a, (int, np.integer)):
+            assert int(a) == int(b), k
+            continue
+        assert a.dtype == b.dtype and a.shape == b.shape, k
+        assert np.array_equal(a, b), k
+        if a.dtype.kind == "f":
+            assert np.array_equal(np.signbit(a), np.signbit(b)), k
+
+
+def test_domain_uses_the_native_builder_for_triangles():
+    import manapy_b200 as M
+    from manapy_b200 import geometry as G, meshgen
+    el, vx = meshgen.square_triangles(9, seed=2)
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    assert dom._host_dm is not None                     # tables built natively, uploaded on first use
+    A = G.build(el, vx, 2)
+    assert all(np.array_equal(np.asarray(dom.host_arrays[k]), np.asarray(A[k])) for k in A)
