@@ -63,23 +63,37 @@ def tables2d(elements, vertex, reorder=True, full=False):
     h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)), int(bool(full)))
     if not h:
         raise ValueError("empty mesh")
-    try:
-        err = L.mbh_error(h)
-        if err:
-            raise ValueError(err.decode())
-        out = {}
-        name = ctypes.c_char_p()
-        dt = ctypes.create_string_buffer(1)
-        shape = (ctypes.c_int64 * 3)()
-        for k in range(L.mbh_count(h)):
-            nd = L.mbh_info(h, k, ctypes.byref(name), dt, shape)
-            shp = tuple(shape[d] for d in range(nd))
-            dtype = np.dtype(_DT[dt.raw])
-            n = int(np.prod(shp)) if shp else 0
-            ptr = L.mbh_data(h, k)
-            buf = (ctypes.c_char * (n * dtype.itemsize)).from_address(ptr) if n else b""
-            out[name.value.decode()] = np.frombuffer(buf, dtype=dtype).reshape(shp).copy() if n else \
-                np.zeros(shp, dtype=dtype)
-        return out
-    finally:
-        L.mbh_free(h)
+    owner = _Handle(L, h)
+    err = L.mbh_error(h)
+    if err:
+        raise ValueError(err.decode())
+    # the arrays view the builder's own buffers (no copy); the handle is released when the
+    # last of them is gone
+    out = {}
+    name = ctypes.c_char_p()
+    dt = ctypes.create_string_buffer(1)
+    shape = (ctypes.c_int64 * 3)()
+    for k in range(L.mbh_count(h)):
+        nd = L.mbh_info(h, k, ctypes.byref(name), dt, shape)
+        shp = tuple(shape[d] for d in range(nd))
+        dtype = np.dtype(_DT[dt.raw])
+        n = int(np.prod(shp)) if shp else 0
+        if n:
+            buf = (ctypes.c_char * (n * dtype.itemsize)).from_address(L.mbh_data(h, k))
+            buf.owner = owner
+            out[name.value.decode()] = np.frombuffer(buf, dtype=dtype).reshape(shp)
+        else:
+            out[name.value.decode()] = np.zeros(shp, dtype=dtype)
+    return out
+
+
+class _Handle:
+    """Owns one builder result; frees it when the last array viewing it is collected."""
+
+    def __init__(self, L, h):
+        self.L, self.h = L, h
+
+    def __del__(self):
+        if self.h:
+            self.L.mbh_free(self.h)
+            self.h = None
