@@ -63,9 +63,10 @@ HOST_OUT = os.path.join(HERE, "lib", "libmanapy_b200_host.so")
 def build_host(force=False):
     """The native host mesh builder (``host/*.cpp``, C++17, no GPU code)."""
     srcs = sorted(glob.glob(os.path.join(HERE, "host", "*.cpp")))
+    hdrs = sorted(glob.glob(os.path.join(HERE, "host", "*.hpp")))
     if not force and os.path.exists(HOST_OUT):
         t = os.path.getmtime(HOST_OUT)
-        if all(os.path.getmtime(s) <= t for s in srcs + [os.path.abspath(__file__)]):
+        if all(os.path.getmtime(s) <= t for s in srcs + hdrs + [os.path.abspath(__file__)]):
             return HOST_OUT
     os.makedirs(os.path.dirname(HOST_OUT), exist_ok=True)
     cxx = shutil.which("g++") or "g++"

@@ -48,19 +48,22 @@ class _OneRankComm:
 
 
 def build_host_mesh(elements, vertex, dim):
-    """(A, host-built DeviceMesh or None): 2D meshes through the native host builder (every
-    ``geometry.build`` array and device table in one C++ pass, bit-identical to the Python
-    builder), anything else -- or a mesh the native builder rejects, so that the Python
-    builder reports it -- through ``geometry.build``."""
-    if dim == 2:
-        from . import native
-        from .device import DeviceMesh
-        try:
-            if native.available():
+    """(A, host-built DeviceMesh or None) through the native host builder, bit-identical to
+    the Python builder: for triangles every ``geometry.build`` array and device table in one
+    C++ pass; for tetrahedra the ``geometry.build`` arrays (the device tables then come from
+    ``DeviceMesh``).  A mesh the native builder rejects goes through ``geometry.build``, which
+    reports it."""
+    from . import native
+    try:
+        if native.available():
+            if dim == 2:
+                from .device import DeviceMesh
                 dm = DeviceMesh.from_native(elements, vertex, device=None, full=True)
                 return dm.A, dm
-        except ValueError:
-            pass
+            if dim == 3:
+                return native.geometry3d(elements, vertex), None
+    except ValueError:
+        pass
     return geometry.build(elements, vertex, dim), None
 
 

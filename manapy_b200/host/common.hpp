@@ -1,0 +1,172 @@
+// Shared pieces of the native host mesh builders (mesh2d.cpp, geom3d.cpp): the table
+// container returned through the C ABI and the CSR / SELL-32 / ordering helpers.  Each
+// helper reproduces the numpy operation it replaces (stable orders, sorted unique unions).
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace mbh {
+
+using i32 = int32_t;
+using i64 = int64_t;
+
+struct Table {
+  std::string name;
+  char dtype;  // 'i' int32, 'l' int64, 'd' float64, 'f' float32, 'b' uint8
+  std::vector<i64> shape;
+  std::vector<unsigned char> bytes;
+};
+
+struct Result {
+  std::vector<Table> tables;
+  std::string error;
+  template <class T>
+  void add(const std::string &name, char dt, std::vector<i64> shape, const std::vector<T> &v) {
+    Table t;
+    t.name = name;
+    t.dtype = dt;
+    t.shape = std::move(shape);
+    t.bytes.resize(v.size() * sizeof(T));
+    if (!v.empty()) std::memcpy(t.bytes.data(), v.data(), t.bytes.size());
+    tables.push_back(std::move(t));
+  }
+};
+
+// CSR from (key, value) pairs grouped by key in [0, n), values kept in input order (a
+// stable counting sort, as numpy's stable argsort of the keys)
+inline void group_csr(const std::vector<i64> &key, const std::vector<i64> &val, i64 n, std::vector<i64> &ptr,
+               std::vector<i64> &idx) {
+  ptr.assign(n + 1, 0);
+  for (i64 k : key) ptr[k + 1]++;
+  for (i64 i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+  idx.resize(key.size());
+  std::vector<i64> pos(ptr.begin(), ptr.end() - 1);
+  for (size_t e = 0; e < key.size(); ++e) idx[pos[key[e]]++] = val[e];
+}
+
+// for each row r: sorted unique union of the lists of its items (CSR), optionally without r.
+// Item lists that are ascending (node -> cell and node -> face lists are) are merged; any
+// other row is gathered and sorted.
+inline void ragged_union(i64 nrows, const std::vector<i64> &row_items_ptr, const std::vector<i64> &row_items,
+                         const std::vector<i64> &item_ptr, const std::vector<i64> &item_vals, bool exclude_self,
+                         std::vector<i64> &ptr, std::vector<i64> &idx) {
+  ptr.assign(nrows + 1, 0);
+  idx.clear();
+  const i64 nitems = (i64)item_ptr.size() - 1;
+  std::vector<char> ascending(nitems, 1);
+  for (i64 it = 0; it < nitems; ++it)
+    for (i64 b = item_ptr[it] + 1; b < item_ptr[it + 1]; ++b)
+      if (item_vals[b] < item_vals[b - 1]) {
+        ascending[it] = 0;
+        break;
+      }
+  std::vector<i64> buf, pos, end;
+  for (i64 r = 0; r < nrows; ++r) {
+    bool merge = true;
+    for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) merge = merge && ascending[row_items[a]];
+    bool have = false;
+    i64 last = 0;
+    auto emit = [&](i64 v) {
+      if (have && v == last) return;
+      have = true;
+      last = v;
+      if (exclude_self && v == r) return;
+      idx.push_back(v);
+    };
+    if (merge) {
+      pos.clear();
+      end.clear();
+      for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
+        const i64 it = row_items[a];
+        if (item_ptr[it] < item_ptr[it + 1]) {
+          pos.push_back(item_ptr[it]);
+          end.push_back(item_ptr[it + 1]);
+        }
+      }
+      const size_t k = pos.size();
+      for (;;) {
+        int best = -1;
+        i64 v = 0;
+        for (size_t h = 0; h < k; ++h)
+          if (pos[h] < end[h] && (best < 0 || item_vals[pos[h]] < v)) {
+            best = (int)h;
+            v = item_vals[pos[h]];
+          }
+        if (best < 0) break;
+        ++pos[best];
+        emit(v);
+      }
+    } else {
+      buf.clear();
+      for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
+        const i64 it = row_items[a];
+        for (i64 b = item_ptr[it]; b < item_ptr[it + 1]; ++b) buf.push_back(item_vals[b]);
+      }
+      std::sort(buf.begin(), buf.end());
+      for (i64 v : buf) emit(v);
+    }
+    ptr[r + 1] = (i64)idx.size();
+  }
+}
+
+// SELL-32 of a CSR table (rows in warps of 32, entry k of the 32 rows contiguous);
+// padding: -1, or (fill_first) the row's first entry with value 0
+inline void sell32(const std::vector<i64> &ptr, const std::vector<i64> &idx, const std::vector<double> *vals,
+            bool fill_first, std::vector<i32> &gptr, std::vector<i32> &out, std::vector<double> &outv) {
+  const i64 n = (i64)ptr.size() - 1;
+  const i64 ng = (n + 31) / 32;
+  gptr.assign(ng + 1, 0);
+  std::vector<i64> g64(ng + 1, 0);
+  for (i64 g = 0; g < ng; ++g) {
+    i64 len = 0;
+    for (i64 r = 32 * g; r < std::min(n, 32 * g + 32); ++r) len = std::max(len, ptr[r + 1] - ptr[r]);
+    g64[g + 1] = g64[g] + 32 * len;
+  }
+  out.assign(g64[ng], -1);
+  outv.assign(vals ? g64[ng] : 0, 0.0);
+  for (i64 g = 0; g < ng; ++g) {
+    const i64 len = (g64[g + 1] - g64[g]) / 32;
+    for (i64 l = 0; l < 32; ++l) {
+      const i64 r = 32 * g + l;
+      const i64 cnt = r < n ? ptr[r + 1] - ptr[r] : 0;
+      const i64 first = (r < n && cnt > 0) ? idx[ptr[r]] : 0;
+      for (i64 k = 0; k < len; ++k) {
+        const i64 d = g64[g] + 32 * k + l;
+        if (k < cnt) {
+          out[d] = (i32)idx[ptr[r] + k];
+          if (vals) outv[d] = (*vals)[ptr[r] + k];
+        } else if (fill_first) {
+          out[d] = (i32)first;
+        }
+      }
+    }
+  }
+  for (i64 g = 0; g <= ng; ++g) gptr[g] = (i32)g64[g];
+}
+
+inline uint64_t part1by1(uint64_t v) {
+  v &= 0xFFFFFFFFull;
+  v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+  v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+  v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  v = (v | (v << 2)) & 0x3333333333333333ull;
+  v = (v | (v << 1)) & 0x5555555555555555ull;
+  return v;
+}
+
+template <class K>
+inline std::vector<i64> stable_argsort(const std::vector<K> &key) {
+  std::vector<i64> o(key.size());
+  std::iota(o.begin(), o.end(), 0);
+  std::stable_sort(o.begin(), o.end(), [&](i64 a, i64 b) { return key[a] < key[b]; });
+  return o;
+}
+
+
+}  // namespace mbh

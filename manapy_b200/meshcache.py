@@ -26,7 +26,8 @@ import numpy as np
 __all__ = ["mesh_key", "load_or_build", "entry_path"]
 
 FORMAT = 1
-_SOURCES = ("geometry.py", "reorder.py", "device.py", "meshcache.py", "host/mesh2d.cpp")
+_SOURCES = ("geometry.py", "reorder.py", "device.py", "meshcache.py", "host/common.hpp", "host/mesh2d.cpp",
+            "host/geom3d.cpp")
 _digest = None
 
 
@@ -107,9 +108,9 @@ def load_or_build(elements, vertex, dim, cache_dir, reorder=True):
         A, dm = _load(path)
         return A, dm, True
     dm = None
-    if int(dim) == 2 and reorder:
+    if reorder:
         from .domain import build_host_mesh
-        A, dm = build_host_mesh(elements, vertex, 2)
+        A, dm = build_host_mesh(elements, vertex, int(dim))
     else:
         A = geometry.build(elements, vertex, int(dim))
     if len(A["unmatched_boundary_faces"]):

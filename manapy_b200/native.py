@@ -39,6 +39,8 @@ def lib():
         L.mbh_data.restype = ctypes.c_void_p
         L.mbh_data.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.mbh_free.argtypes = [ctypes.c_void_p]
+        L.mbh_geometry3d.restype = ctypes.c_void_p
+        L.mbh_geometry3d.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
         _lib = L
     return _lib
 
@@ -63,6 +65,28 @@ def tables2d(elements, vertex, reorder=True, full=False):
     h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)), int(bool(full)))
     if not h:
         raise ValueError("empty mesh")
+    return _read(L, h)
+
+
+def geometry3d(elements, vertex):
+    """Every array of ``geometry.build(elements, vertex, 3)`` from the native host builder
+    (``host/geom3d.cpp``), bit-identical; raises ValueError on a bad mesh."""
+    el = np.ascontiguousarray(elements, dtype=np.int32)
+    vx = np.ascontiguousarray(vertex, dtype=np.float64)
+    if el.ndim != 2 or el.shape[1] != 5 or vx.ndim != 2 or vx.shape[1] != 4:
+        raise ValueError("expected elements [nc, 5] and vertex [nn, 4]")
+    L = lib()
+    h = L.mbh_geometry3d(el.ctypes.data, len(el), vx.ctypes.data, len(vx))
+    if not h:
+        raise ValueError("empty mesh")
+    T = _read(L, h)
+    A = {k[2:]: v for k, v in T.items()}
+    A.update(dim=3, nbcells=len(el), nbnodes=len(vx), nbfaces=len(A["faces_name"]))
+    return A
+
+
+def _read(L, h):
+    """The named tables of a builder result as numpy arrays viewing its buffers."""
     owner = _Handle(L, h)
     err = L.mbh_error(h)
     if err:

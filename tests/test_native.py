@@ -66,3 +66,35 @@ def test_domain_uses_the_native_builder_for_triangles():
     assert dom._host_dm is not None                     # tables built natively, uploaded on first use
     A = G.build(el, vx, 2)
     assert all(np.array_equal(np.asarray(dom.host_arrays[k]), np.asarray(A[k])) for k in A)
+
+
+@pytest.mark.parametrize("n,seed", [(2, 1), (6, 7)])
+def test_native_3d_geometry_is_bit_identical(n, seed):
+    """host/geom3d.cpp: every geometry.build array of a tetrahedral mesh, bit for bit."""
+    from manapy_b200 import native
+    el, vx = meshgen.cube_tetrahedra(n, seed=seed)
+    A = G.build(el, vx, 3)
+    B = native.geometry3d(el, vx)
+    assert set(A) == set(B)
+    for k, a in A.items():
+        b = B[k]
+        if isinstance(a, (int, np.integer)):
+            assert int(a) == int(b), k
+            continue
+        assert a.dtype == b.dtype and a.shape == b.shape, k
+        assert np.array_equal(a, b), k
+        if a.dtype.kind == "f":
+            assert np.array_equal(np.signbit(a), np.signbit(b)), k
+
+
+@pytest.mark.filterwarnings("ignore::RuntimeWarning")
+def test_native_3d_rejects_untagged_boundaries_like_the_python_builder():
+    import manapy_b200 as M
+    from manapy_b200 import native
+    el, vx = meshgen.cube_tetrahedra(2, seed=1)
+    vx = vx.copy()
+    vx[:, 3] = 0                                    # no boundary tags at all
+    with pytest.raises(ValueError):
+        native.geometry3d(el, vx)
+    with pytest.raises(ValueError, match="match no boundary side"):
+        M.Domain(dim=3, mesh=(el, vx))
