@@ -119,5 +119,8 @@ class _Handle:
 
     def __del__(self):
         if self.h:
-            self.L.mbh_free(self.h)
+            try:
+                self.L.mbh_free(self.h)
+            except Exception:          # interpreter shutdown: the library may be gone already
+                pass
             self.h = None
