@@ -70,7 +70,8 @@ def build_host(force=False):
             return HOST_OUT
     os.makedirs(os.path.dirname(HOST_OUT), exist_ok=True)
     cxx = shutil.which("g++") or "g++"
-    subprocess.run([cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-o", HOST_OUT + ".tmp", *srcs],
+    subprocess.run([cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-ffp-contract=off", "-o",
+                    HOST_OUT + ".tmp", *srcs],
                    check=True)
     os.replace(HOST_OUT + ".tmp", HOST_OUT)
     return HOST_OUT

@@ -9,6 +9,7 @@
 #include <map>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace mbh {
@@ -52,12 +53,11 @@ inline void group_csr(const std::vector<i64> &key, const std::vector<i64> &val, 
 
 // for each row r: sorted unique union of the lists of its items (CSR), optionally without r.
 // Item lists that are ascending (node -> cell and node -> face lists are) are merged; any
-// other row is gathered and sorted.
+// other row is gathered and sorted.  Large tables are split into row ranges handled by
+// separate threads; each range's output is concatenated in row order (same result).
 inline void ragged_union(i64 nrows, const std::vector<i64> &row_items_ptr, const std::vector<i64> &row_items,
                          const std::vector<i64> &item_ptr, const std::vector<i64> &item_vals, bool exclude_self,
                          std::vector<i64> &ptr, std::vector<i64> &idx) {
-  ptr.assign(nrows + 1, 0);
-  idx.clear();
   const i64 nitems = (i64)item_ptr.size() - 1;
   std::vector<char> ascending(nitems, 1);
   for (i64 it = 0; it < nitems; ++it)
@@ -66,53 +66,74 @@ inline void ragged_union(i64 nrows, const std::vector<i64> &row_items_ptr, const
         ascending[it] = 0;
         break;
       }
-  std::vector<i64> buf, pos, end;
-  for (i64 r = 0; r < nrows; ++r) {
-    bool merge = true;
-    for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) merge = merge && ascending[row_items[a]];
-    bool have = false;
-    i64 last = 0;
-    auto emit = [&](i64 v) {
-      if (have && v == last) return;
-      have = true;
-      last = v;
-      if (exclude_self && v == r) return;
-      idx.push_back(v);
-    };
-    if (merge) {
-      pos.clear();
-      end.clear();
-      for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
-        const i64 it = row_items[a];
-        if (item_ptr[it] < item_ptr[it + 1]) {
-          pos.push_back(item_ptr[it]);
-          end.push_back(item_ptr[it + 1]);
-        }
-      }
-      const size_t k = pos.size();
-      for (;;) {
-        int best = -1;
-        i64 v = 0;
-        for (size_t h = 0; h < k; ++h)
-          if (pos[h] < end[h] && (best < 0 || item_vals[pos[h]] < v)) {
-            best = (int)h;
-            v = item_vals[pos[h]];
+  // rows [r0, r1): per-row counts into cnt[r], values appended to out
+  auto rows = [&](i64 r0, i64 r1, i64 *cnt, std::vector<i64> &out) {
+    std::vector<i64> buf, pos, end;
+    for (i64 r = r0; r < r1; ++r) {
+      const size_t before = out.size();
+      bool merge = true;
+      for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) merge = merge && ascending[row_items[a]];
+      bool have = false;
+      i64 last = 0;
+      auto emit = [&](i64 v) {
+        if (have && v == last) return;
+        have = true;
+        last = v;
+        if (exclude_self && v == r) return;
+        out.push_back(v);
+      };
+      if (merge) {
+        pos.clear();
+        end.clear();
+        for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
+          const i64 it = row_items[a];
+          if (item_ptr[it] < item_ptr[it + 1]) {
+            pos.push_back(item_ptr[it]);
+            end.push_back(item_ptr[it + 1]);
           }
-        if (best < 0) break;
-        ++pos[best];
-        emit(v);
+        }
+        const size_t k = pos.size();
+        for (;;) {
+          int best = -1;
+          i64 v = 0;
+          for (size_t h = 0; h < k; ++h)
+            if (pos[h] < end[h] && (best < 0 || item_vals[pos[h]] < v)) {
+              best = (int)h;
+              v = item_vals[pos[h]];
+            }
+          if (best < 0) break;
+          ++pos[best];
+          emit(v);
+        }
+      } else {
+        buf.clear();
+        for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
+          const i64 it = row_items[a];
+          for (i64 b = item_ptr[it]; b < item_ptr[it + 1]; ++b) buf.push_back(item_vals[b]);
+        }
+        std::sort(buf.begin(), buf.end());
+        for (i64 v : buf) emit(v);
       }
-    } else {
-      buf.clear();
-      for (i64 a = row_items_ptr[r]; a < row_items_ptr[r + 1]; ++a) {
-        const i64 it = row_items[a];
-        for (i64 b = item_ptr[it]; b < item_ptr[it + 1]; ++b) buf.push_back(item_vals[b]);
-      }
-      std::sort(buf.begin(), buf.end());
-      for (i64 v : buf) emit(v);
+      cnt[r] = (i64)(out.size() - before);
     }
-    ptr[r + 1] = (i64)idx.size();
+  };
+  std::vector<i64> cnt(nrows);
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const i64 nthreads = nrows >= (i64)1 << 16 ? (i64)hw : 1;
+  std::vector<std::vector<i64>> parts(nthreads);
+  if (nthreads == 1) {
+    rows(0, nrows, cnt.data(), parts[0]);
+  } else {
+    std::vector<std::thread> pool;
+    for (i64 t = 0; t < nthreads; ++t)
+      pool.emplace_back([&, t] { rows(nrows * t / nthreads, nrows * (t + 1) / nthreads, cnt.data(), parts[t]); });
+    for (auto &th : pool) th.join();
   }
+  ptr.assign(nrows + 1, 0);
+  for (i64 r = 0; r < nrows; ++r) ptr[r + 1] = ptr[r] + cnt[r];
+  idx.clear();
+  idx.reserve(ptr[nrows]);
+  for (auto &p : parts) idx.insert(idx.end(), p.begin(), p.end());
 }
 
 // SELL-32 of a CSR table (rows in warps of 32, entry k of the 32 rows contiguous);

@@ -36,7 +36,7 @@ def test_rejects_unmatched_boundary_faces():
         D.DeviceMesh.from_native(el, vx)
 
 
-@pytest.mark.parametrize("n,seed", [(7, 1), (33, 5)])
+@pytest.mark.parametrize("n,seed", [(7, 1), (33, 5), (200, 4)])   # 200: 80,000 cells, threaded union
 def test_native_full_geometry_is_bit_identical(n, seed):
     """With full=True the native builder also returns every geometry.build array (what a
     Domain exposes): same keys, dtypes, shapes and bits (signs of zeros included)."""
@@ -68,7 +68,7 @@ def test_domain_uses_the_native_builder_for_triangles():
     assert all(np.array_equal(np.asarray(dom.host_arrays[k]), np.asarray(A[k])) for k in A)
 
 
-@pytest.mark.parametrize("n,seed", [(2, 1), (6, 7)])
+@pytest.mark.parametrize("n,seed", [(2, 1), (6, 7), (24, 2)])   # 24: 82,944 cells, threaded union
 def test_native_3d_geometry_is_bit_identical(n, seed):
     """host/geom3d.cpp: every geometry.build array of a tetrahedral mesh, bit for bit."""
     from manapy_b200 import native
