@@ -8,11 +8,22 @@ rotating velocity, D = 5e-4), FP64, 1000 steps.
 
 One step = manapy's ``stepper()`` + ``compute_fluxes()`` + ``compute_new_val()``
 on the whole mesh.  ``value`` is timed on the device (CUDA events, inputs
-resident, K steps replayed from CUDA graphs); ``e2e`` runs the manapy driver
-loop through the public API (per step: the face velocities copied from pinned
-host memory, ``interpolate_facetocell``, ``stepper()`` returning dt to the
-host, ``compute_fluxes()``, ``compute_new_val()``).  Under torchrun every rank
-solves its own copy of the workload (weak scaling, no collective in the step).
+resident, K steps replayed from CUDA graphs), as the median of R repeats of
+exactly K steps each (R = ceil(500 / K) by default, so that at least 500 steps
+are timed; every repeat is bracketed by a barrier and a synchronisation).
+``e2e`` runs the manapy driver loop through the public API (per step: the face
+velocities copied from pinned host memory, ``interpolate_facetocell``,
+``stepper()`` returning dt to the host, ``compute_fluxes()``,
+``compute_new_val()``, and the new state copied back into pinned host memory).
+Under torchrun every rank solves its own copy of the workload (weak scaling, no
+collective in the step); ``--sharded`` instead splits one mesh over the ranks
+(halo exchange and dt min-reduction over NCCL).
+
+The single-GPU default run adds the other stated targets to the same line
+(``extras``): the 3D workload C4 at full size, a resident batch of uneven meshes
+(batched FP32-compensated vs batched FP64 vs the same meshes solved serially in
+FP64) and a continuous-batching serving run (p50/p99 latency at a stated arrival
+rate).
 
 ``--impl reference`` times the CPU restatement of manapy's kernels (the
 oracle, one process per host core, each on its own copy of the mesh).
@@ -59,6 +70,12 @@ def parse():
     ap.add_argument("--serial-sample", type=int, default=60, help="serving: requests timed serially in FP64")
     ap.add_argument("--workers", type=int, default=None, help="serving: mesh-preparation processes")
     ap.add_argument("--n", type=int, default=None, help="mesh resolution override (small profiling cases)")
+    ap.add_argument("--min-timed-steps", type=int, default=500,
+                    help="repeat the K timed steps until at least this many steps are timed (median reported)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="single workload only (no C4 / batched / serving sections)")
+    ap.add_argument("--extras-requests", type=int, default=1000, help="serving section: requests")
+    ap.add_argument("--extras-rate", type=float, default=18.0, help="serving section: arrival rate (requests/s)")
     return ap.parse_args()
 
 
@@ -153,6 +170,29 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def timed_repeats(run, K, R, world):
+    """R repeats of exactly K steps, each bracketed by a barrier and a synchronisation and
+    timed with CUDA events on the launching stream; per repeat the max over ranks (ms)."""
+    import torch
+    out = []
+    for _ in range(R):
+        barrier(world)
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        run(K)
+        e1.record(st)
+        torch.cuda.synchronize()
+        barrier(world)
+        out.append(max_over_ranks(e0.elapsed_time(e1), world))
+    return out
+
+
+def repeats_for(K, args):
+    return max(1, -(-int(args.min_timed_steps) // max(int(K), 1)))
+
+
 def build_advdiff(wl, seed):
     import manapy_b200 as M
     el, vx = wl.scaled(seed=seed).mesh()
@@ -209,9 +249,10 @@ def cpu_baseline(dom, wl, steps):
                       % (steps, wl.cells)}
 
 
-def run_fp32c(wl, dom, w64, vel, K, Wm, world):
+def run_fp32c(wl, dom, w64, vel, K, Wm, world, R=1):
     """The FP32-compensated step on the same mesh and initial state: device-timed
-    throughput, and its L2 / Linf error against the FP64 state after the same steps."""
+    throughput (median of R repeats of K steps), and its L2 / Linf error against the FP64
+    state after the same number of steps (Wm + R K)."""
     import torch
     import manapy_b200 as M
     ref = w64.cell.copy()          # FP64 state after Wm + K steps
@@ -222,24 +263,17 @@ def run_fp32c(wl, dom, w64, vel, K, Wm, world):
         precision="fp32c"))
     S.advance(Wm, graph=True)
     torch.cuda.synchronize()
-    barrier(world)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    S.advance(K, graph=True)
-    e1.record()
-    torch.cuda.synchronize()
-    barrier(world)
-    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    ms = statistics.median(timed_repeats(lambda n: S.advance(n, graph=True), K, R, world))
     got = w.cell
     l2 = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     linf = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
     S.release_graphs()
     return {"value": world * wl.cells * K / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / K,
             "dtype": "f32 state + compensated sums, f64 geometry and dt",
-            "l2_rel_err_vs_fp64": l2, "linf_rel_err_vs_fp64": linf, "steps_compared": Wm + K}
+            "l2_rel_err_vs_fp64": l2, "linf_rel_err_vs_fp64": linf, "steps_compared": Wm + K * R}
 
 
-def run_fp32c_sw(wl, dom, vs64, S64, K, Wm, world):
+def run_fp32c_sw(wl, dom, vs64, S64, K, Wm, world, R=1):
     """FP32-compensated shallow water on the same mesh and initial state: throughput, L2 /
     Linf error of h, hu, hv against the FP64 state after the same steps, FP64 mass drift."""
     import torch
@@ -254,17 +288,10 @@ def run_fp32c_sw(wl, dom, vs64, S64, K, Wm, world):
     m0 = S.mass()
     S.advance(Wm)
     torch.cuda.synchronize()
-    barrier(world)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    S.advance(K)
-    e1.record()
-    torch.cuda.synchronize()
-    barrier(world)
-    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    ms = statistics.median(timed_repeats(S.advance, K, R, world))
     out = {"value": world * wl.cells * K / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / K,
            "dtype": "f32 state and fluxes + compensated sums, f64 geometry, source and dt",
-           "steps_compared": Wm + K}
+           "steps_compared": Wm + K * R}
     for name, r, v in zip(("h", "hu", "hv"), ref, vs[:3]):
         got = v.cell
         out["l2_rel_err_vs_fp64_" + name] = float(np.linalg.norm(got - r) / np.linalg.norm(r))
@@ -368,8 +395,169 @@ def run_euler(args, wl):
         dist.destroy_process_group()
 
 
-def run_ours(args):
+def measure_workload(wl, args, world, rank, local, K, fp32c=True, seed_offset=0):
+    """Device-timed FP64 step of one workload (median of repeats), its FP32-compensated
+    twin, and the objects the end-to-end leg needs."""
     import torch
+    Wm = max(args.warmup, 3)
+    if wl.kind == "advdiff":
+        dom, w, vel, S, (uf, vf) = build_advdiff(wl, seed=wl.seed + seed_offset)
+    else:
+        dom, vs, S = build_sw(wl, seed=wl.seed + seed_offset)
+    # warm-up: also tunes the steps per graph replay and captures the step graph, so that
+    # neither happens inside the timed region (the deepest candidate bounds the steps needed)
+    if wl.kind == "advdiff":
+        from manapy_b200 import autotune
+        Wm = Wm + max(autotune.CANDIDATES)
+        run = lambda n: S.advance(n, graph=True)  # noqa: E731
+    else:
+        run = S.advance
+    run(Wm)
+    torch.cuda.synchronize()
+    R = repeats_for(K, args)
+    clocks = ClockSampler(local if world > 1 else 0)
+    time.sleep(0.3)
+    reps = timed_repeats(run, K, R, world)
+    ck = clocks.stop()
+    ms_med = statistics.median(reps)
+    out = {"dom": dom, "S": S, "K": K, "R": R, "Wm": Wm, "reps": reps, "ms_step": ms_med / K, "clocks": ck,
+           "value": world * wl.cells * K / (ms_med / 1e3), "launches": S.launches_per_step()}
+    if wl.kind == "advdiff":
+        out.update(w=w, vel=vel, uf=uf, vf=vf)
+    else:
+        out.update(vs=vs)
+    if fp32c and not args.no_fp32c:
+        # the FP32c run takes as many steps as the FP64 run (warm-up + R K) for the comparison
+        if wl.kind == "advdiff":
+            out["fp32c"] = run_fp32c(wl, dom, w, vel, K, Wm, world, R)
+        elif wl.order == 1:
+            out["fp32c"] = run_fp32c_sw(wl, dom, vs, S, K, Wm, world, R)
+        if "fp32c" in out:
+            out["fp32c"]["vs_fp64"] = out["fp32c"]["value"] / out["value"]
+    return out
+
+
+def roofline(wl_key, cells, ms_step, launches):
+    peak, peak_kind = measured_peak()
+    ctm = CTM_BYTES[wl_key]
+    achieved = ctm * cells / (ms_step / 1e3) / 1e9
+    traffic = ncu_traffic(wl_key)
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "traffic": (traffic * cells if traffic else None),
+            "kernel": "fused step (%d launches), compulsory traffic %.1f B/cell-update" % (launches, ctm)}
+
+
+def e2e_advdiff(m, E, world):
+    """manapy's driver loop through the public API: per step the face velocities uploaded
+    from pinned memory, facetocell, stepper() (dt to the host), compute_fluxes(),
+    compute_new_val(), and the new state copied back into pinned memory."""
+    import torch
+    S, w = m["S"], m["w"]
+    u, v, _ = m["vel"]
+    pu = torch.from_numpy(m["uf"]).pin_memory()
+    pv = torch.from_numpy(m["vf"]).pin_memory()
+    out = torch.empty(int(m["dom"].nbcells), dtype=torch.float64, pin_memory=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(E):
+        u.face = pu
+        v.face = pv
+        u.interpolate_facetocell()
+        v.interpolate_facetocell()
+        S.stepper()
+        S.compute_fluxes()
+        S.compute_new_val()
+        w.fetch("cell", out=out)
+    torch.cuda.synchronize()
+    sec = max_over_ranks(time.perf_counter() - t0, world)
+    return sec, pu.numel() * 8 + pv.numel() * 8, out.numel() * 8 + 8
+
+
+def e2e_sw(m, E, world):
+    import torch
+    S, vs = m["S"], m["vs"]
+    outs = [torch.empty(int(m["dom"].nbcells), dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(E):
+        S.stepper()
+        S.compute_fluxes()
+        S.compute_new_val()
+        for var, o in zip(vs[:3], outs):
+            var.fetch("cell", out=o)
+    torch.cuda.synchronize()
+    sec = max_over_ranks(time.perf_counter() - t0, world)
+    return sec, 0, sum(o.numel() * 8 for o in outs) + 8
+
+
+def extra_c4(args):
+    """The 3D workload C4 at full size (1,572,864 tetrahedra): FP64 and FP32-compensated."""
+    from manapy_b200 import workloads as W
+    wl = W.C4
+    m = measure_workload(wl, args, 1, 0, 0, K=50)
+    out = {"workload": wl.name, "cells": wl.cells, "value": m["value"], "unit": "cell-updates/s",
+           "ms_per_step": m["ms_step"], "steps": m["K"], "repeats": m["R"],
+           "roofline": roofline("C4", wl.cells, m["ms_step"], m["launches"]), "clocks": m["clocks"]}
+    if "fp32c" in m:
+        out["fp32c"] = m["fp32c"]
+    m["S"].release_graphs()
+    return out
+
+
+def extra_batched(args):
+    """A resident batch of uneven meshes (the serving mix): batched FP32c, batched FP64 and
+    the same meshes solved one after another in FP64, all device-timed over the same steps."""
+    import torch
+    from manapy_b200 import serving as SV
+    reqs = SV.make_requests(args.meshes, 0.0, seed=77)
+    K = 200
+    srv = SV.BatchServer(workers=args.workers)
+    srv.start_pool()
+    rate32, _ = srv.run_resident(reqs, K)
+    srv.stop_pool()
+    srv64 = SV.BatchServer(workers=args.workers, precision="fp64")
+    srv64.start_pool()
+    rate64, _ = srv64.run_resident(reqs, K)
+    srv64.stop_pool()
+    del srv, srv64
+    torch.cuda.empty_cache()
+    ser = _serial_fp64(reqs, K)
+    cu = sum(r.cells for r in reqs) * K
+    serial = cu / ser
+    return {"meshes": len(reqs), "cells": sum(r.cells for r in reqs), "steps": K,
+            "mix": "70% adv-diff o2 + diffusion, 30% SW o1", "sizes": "log-uniform 2e3-5e5 cells",
+            "batched_fp32c": rate32, "batched_fp64": rate64, "serial_fp64": serial, "unit": "cell-updates/s",
+            "fp32c_vs_batched_fp64": rate32 / rate64, "batched_fp64_vs_serial_fp64": rate64 / serial,
+            "fp32c_vs_serial_fp64": rate32 / serial}
+
+
+def extra_serving(args):
+    """Continuous batching of a seeded request stream (FP32-compensated): sustained rate and
+    p50/p99 latency from arrival to the result on the host."""
+    import torch
+    from manapy_b200 import serving as SV
+    reqs = SV.make_requests(args.extras_requests, args.extras_rate, seed=2024)
+    total_cu = sum(r.cells * r.steps for r in reqs)
+    srv = SV.BatchServer(workers=args.workers)
+    srv.start_pool()
+    srv.serve(SV.make_requests(8, 0.0, seed=1, cells=(2e3, 2e4), steps=(20, 40)))
+    t0 = time.perf_counter()
+    recs = srv.serve(reqs)
+    wall = time.perf_counter() - t0
+    srv.stop_pool()
+    lat = np.array([r["latency"] for r in recs])
+    torch.cuda.empty_cache()
+    return {"requests": len(reqs), "rate_per_s": args.extras_rate, "workers": srv.workers,
+            "cells": "log-uniform 2e3-5e5", "steps": "uniform 100-2000", "mix": "70% adv-diff o2, 30% SW o1",
+            "precision": "fp32c", "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "makespan_s": wall, "sustained_requests_per_s": len(reqs) / wall,
+            "cell_updates_per_s": total_cu / wall,
+            "latency": "arrival to result on the host, mesh preparation included"}
+
+
+def run_ours(args):
     from manapy_b200 import workloads as W
     wl = W.ALL[args.workload]
     if args.n:
@@ -377,110 +565,56 @@ def run_ours(args):
     if wl.kind == "euler":
         return run_euler(args, wl)
     world, rank, local = dist_setup(args)
-    K, Wm = args.steps, max(args.warmup, 3)
-    if wl.kind == "advdiff":
-        dom, w, vel, S, (uf, vf) = build_advdiff(wl, seed=wl.seed + rank)
-    else:
-        dom, vs, S = build_sw(wl, seed=wl.seed + rank)
-    dev = torch.device("cuda", local if world > 1 else 0)
-    # warm-up: also tunes the steps per graph replay and captures the step graph, so that
-    # neither happens inside the timed region (the deepest candidate bounds the steps needed)
-    if wl.kind == "advdiff":
-        from manapy_b200 import autotune
-        Wm = Wm + max(autotune.CANDIDATES)
-        S.advance(Wm, graph=True)
-    else:
-        S.advance(Wm)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local if world > 1 else 0)
-    time.sleep(0.3)
-    barrier(world)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    if wl.kind == "advdiff":
-        S.advance(K, graph=True)
-    else:
-        S.advance(K)
-    e1.record()
-    torch.cuda.synchronize()
-    barrier(world)
-    ms = e0.elapsed_time(e1)
-    ck = clocks.stop()
-    ms_max = max_over_ranks(ms, world)
-    value = world * wl.cells * K / (ms_max / 1e3)
-    ms_step = ms_max / K
-    launches_per_step = S.launches_per_step()
-    fp32c = None
-    if not args.no_fp32c:
-        if wl.kind == "advdiff":
-            fp32c = run_fp32c(wl, dom, w, vel, K, Wm, world)
-        elif wl.order == 1:
-            fp32c = run_fp32c_sw(wl, dom, vs, S, K, Wm, world)
+    K = args.steps
+    m = measure_workload(wl, args, world, rank, local, K, seed_offset=rank)
+    dom, S = m["dom"], m["S"]
+    ms_step, value = m["ms_step"], m["value"]
 
     # end to end through the public API, manapy's driver loop
     E = max(args.e2e_steps, 1)
-    h2d = d2h = 0
     if wl.kind == "advdiff":
-        u, v, _ = vel
-        pu = torch.from_numpy(uf).pin_memory()
-        pv = torch.from_numpy(vf).pin_memory()
-        barrier(world)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(E):
-            u.face = pu
-            v.face = pv
-            u.interpolate_facetocell()
-            v.interpolate_facetocell()
-            S.stepper()
-            S.compute_fluxes()
-            S.compute_new_val()
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        h2d = pu.numel() * 8 + pv.numel() * 8
-        d2h = 8
+        e2e_s, h2d, d2h = e2e_advdiff(m, E, world)
     else:
-        barrier(world)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(E):
-            S.stepper()
-            S.compute_fluxes()
-            S.compute_new_val()
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        d2h = 8
-    e2e_s = max_over_ranks(e2e_s, world)
+        e2e_s, h2d, d2h = e2e_sw(m, E, world)
     e2e_value = world * wl.cells * E / e2e_s
 
-    peak, peak_kind = measured_peak()
-    ctm = CTM_BYTES[args.workload]
-    achieved = ctm * wl.cells / (ms_step / 1e3) / 1e9
-    traffic = ncu_traffic(args.workload)
     line = {
         "metric": "cell-updates/s (FP64 explicit FV step, %s)" % wl.name,
-        "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K, "warmup": m["Wm"],
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic: seeded jittered mesh of the workload, manapy's initial state",
         "config": {"workload": wl.name, "cells": wl.cells, "order": wl.order, "kind": wl.kind,
                    "parallelism": "replicas%d" % world if world > 1 else "single",
                    "l2": "working set %.0f MB > 126 MB L2 (no flush needed)" % (dom.device_mesh.nbytes() / 1e6)},
+        "timing": {"repeats": m["R"], "steps_per_repeat": K, "timed_steps": K * m["R"],
+                   "ms_per_step_min": min(m["reps"]) / K, "ms_per_step_median": ms_step,
+                   "ms_per_step_max": max(m["reps"]) / K},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "steps": E},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": (traffic * wl.cells if traffic else None),
-                     "kernel": "fused step (%d launches), compulsory traffic %.1f B/cell-update"
-                               % (launches_per_step, ctm)},
-        "clocks": ck,
-        "gpu_launches": launches_per_step * K,
+                "d2h_bytes_per_step": d2h, "steps": E,
+                "copies": ("face velocities u, v uploaded from pinned memory; state w and dt read back"
+                           if wl.kind == "advdiff" else "state h, hu, hv and dt read back into pinned memory")},
+        "roofline": roofline(args.workload, wl.cells, ms_step, m["launches"]),
+        "clocks": m["clocks"],
+        "gpu_launches": m["launches"] * K * m["R"],
     }
-    if fp32c is not None:
-        fp32c["vs_fp64"] = fp32c["value"] / value
-        line["fp32c"] = fp32c
+    if "fp32c" in m:
+        line["fp32c"] = m["fp32c"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(dom, wl, args.cpu_steps)
+    if world == 1 and not args.no_extras and args.workload == "C2" and not args.n:
+        S.release_graphs()
+        del m, S
+        import gc
+        gc.collect()
+        extras = {}
+        for name, fn in (("c4", extra_c4), ("batched", extra_batched), ("serving", extra_serving)):
+            t0 = time.perf_counter()
+            try:
+                extras[name] = fn(args)
+            except Exception as e:          # a failing section is reported, not hidden
+                extras[name] = {"error": "%s: %s" % (type(e).__name__, e)}
+            extras[name]["section_seconds"] = round(time.perf_counter() - t0, 1)
+        line["extras"] = extras
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -690,23 +824,19 @@ def _serial_fp64(reqs, steps, warmup=3):
 
 
 def run_batched(args):
-    """A resident batch of uneven meshes (the serving mix's sizes and kinds) advanced by
-    the batched FP32-compensated kernels, against the same meshes solved one after another
-    in plain FP64 through the public API; both device-timed over the same steps."""
+    """A resident batch of uneven meshes (the serving mix's sizes and kinds): batched
+    FP32-compensated and batched FP64 kernels against the same meshes solved one after
+    another in plain FP64 through the public API; all device-timed over the same steps."""
     import torch
-    from manapy_b200 import serving as SV
     torch.cuda.set_device(0)
-    reqs = SV.make_requests(args.meshes, 0.0, seed=77)
-    K = max(args.steps, 1)
-    rate, sec = SV.BatchServer(workers=args.workers).run_resident(reqs, K)
-    ser = _serial_fp64(reqs, K)
-    cu = sum(r.cells for r in reqs) * K
-    line = {"metric": "cell-updates/s, batched FP32-compensated vs serial plain FP64 (resident meshes)",
-            "value": rate, "unit": "cell-updates/s", "n_gpus": 1, "steps": K, "higher_is_better": True,
-            "dtype": "f32 state + compensated sums, f64 geometry and dt", "data": "synthetic seeded meshes",
-            "config": {"workload": "C5-batched-resident", "meshes": len(reqs), "cells": sum(r.cells for r in reqs),
-                       "mix": "70% adv-diff o2, 30% SW o1", "sizes": "log-uniform 2e3-5e5 cells"},
-            "serial_fp64": {"value": cu / ser, "unit": "cell-updates/s"}, "vs_serial_fp64": rate / (cu / ser)}
+    b = extra_batched(args)
+    line = {"metric": "cell-updates/s, batched FP32-compensated vs batched and serial plain FP64 (resident meshes)",
+            "value": b["batched_fp32c"], "unit": "cell-updates/s", "n_gpus": 1, "steps": b["steps"],
+            "higher_is_better": True, "dtype": "f32 state + compensated sums, f64 geometry and dt",
+            "data": "synthetic seeded meshes",
+            "config": {"workload": "C5-batched-resident", "meshes": b["meshes"], "cells": b["cells"],
+                       "mix": b["mix"], "sizes": b["sizes"]},
+            "batched": b}
     print(json.dumps(line), flush=True)
 
 

@@ -314,6 +314,20 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
                double cfl, double grav, int32_t order, double *scratch, double *face_flux,
                const double *dt_cur, double *dt_next, void *stream);
 
+/* Boundary treatment of the shallow-water steps' boundary faces. */
+#define MB_WALLS_NEUMANN 0  /* ghost = the interior cell's state (manapy's default, and what its
+                               `slip` condition degrades to, manapy/boundary/bc.py:59-76) */
+#define MB_WALLS_REFLECT 1  /* reflective wall: ghost h, hc, Z copied, momentum mirrored,
+                               q - 2 (q.n) n / |n|^2; no counterpart in manapy (its `slip` ghost
+                               function is commented out, manapy/boundary/bc.py:68-72): the mass
+                               flux through a wall vanishes up to rounding */
+
+/* mb_sw_step with a choice of wall treatment (walls: MB_WALLS_*); mb_sw_step is this with
+ * MB_WALLS_NEUMANN. */
+int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q_out[5],
+                  double cfl, double grav, int32_t order, int32_t walls, double *scratch,
+                  double *face_flux, const double *dt_cur, double *dt_next, void *stream);
+
 /* FP32-compensated twin of mb_sw_step (no counterpart in manapy), first order, Neumann
  * ghosts: FP32 state (q_in, q_out: h, hu, hv, hc, Z), FP32 SRNH flux arithmetic and face
  * fluxes (face_flux [nbfaces][4] floats), residuals summed per cell with compensated
@@ -324,6 +338,12 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
 int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
                     const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
                     int32_t order, float *face_flux, const double *dt_cur, double *dt_next, void *stream);
+
+/* mb_sw_step_f32c with a choice of wall treatment (walls: MB_WALLS_*). */
+int mb_sw_step_f32c_ex(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
+                       const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
+                       int32_t order, int32_t walls, float *face_flux, const double *dt_cur,
+                       double *dt_next, void *stream);
 
 /* ---- batches of independent triangle meshes (serving) ----------------------------------
  *
@@ -382,6 +402,48 @@ typedef struct mb_sw_item {
 int mb_sw_batch_step_f32c(const mb_sw_item *items, const int32_t *face_map, int32_t face_blocks,
                           const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream);
 
+/* FP64 batches: the same block -> item maps, clock and [start_step, end_step) windows as
+ * the FP32-compensated batches above, running the plain FP64 steps (mb_advdiff_step and
+ * mb_sw_step per mesh, bit-identical to them).  No counterpart in manapy.  Block maps use
+ * 256-cell (and 256-face) blocks. */
+typedef struct mb_advdiff_item_f64 {
+  mb_mesh m;                /* compact 2D tables required */
+  mb_bc bc;
+  mb_advdiff_params p;
+  double *w[2];             /* ping-pong FP64 state; step t reads w[(t - start_step) & 1] */
+  const double *sign_cf;    /* [4*nbcells] from mb_cell_face_sign, 32-byte aligned */
+  const double *src;        /* NULL: no source */
+  const double *dt_dev;     /* the item's dt */
+  double *cell_scratch;     /* [4*nbcells] records (order 2), 32-byte aligned */
+  double *node_scratch;     /* [nbnodes] (diffusion) */
+  int32_t start_step, end_step;
+  int32_t p1_begin;         /* first block of the item in the phase-1 launch */
+  int32_t p1_cell_blocks;   /* its phase-1 blocks [p1_begin, p1_begin + this) do cells, the rest nodes */
+  int32_t p2_begin;         /* first block of the item in the phase-2 launch */
+  int32_t pad_;
+} mb_advdiff_item_f64;
+
+int mb_advdiff_batch_step(const mb_advdiff_item_f64 *items, const int32_t *p1_map, int32_t p1_blocks,
+                          const int32_t *p2_map, int32_t p2_blocks, int32_t order, int32_t diffusion,
+                          int32_t *clock, void *stream);
+
+typedef struct mb_sw_item_f64 {
+  mb_mesh m;                /* compact 2D tables required */
+  double *q[2][5];          /* ping-pong h, hu, hv, hc, Z (the Z slots may be one array) */
+  double *face_flux;        /* [nbfaces][4] scratch, 32-byte aligned */
+  double *dt;               /* [2]: step t uses dt[(t - start_step) & 1], writes the next one into
+                               the other slot; dt[0] must hold the first step's dt */
+  double cfl, grav;
+  int32_t start_step, end_step;
+  int32_t f_begin;          /* first block of the item in the face launch */
+  int32_t c_begin;          /* first block of the item in the cell launch */
+} mb_sw_item_f64;
+
+/* One first-order FP64 shallow-water step (Neumann walls) of every active item; then
+ * *clock += 1. */
+int mb_sw_batch_step(const mb_sw_item_f64 *items, const int32_t *face_map, int32_t face_blocks,
+                     const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream);
+
 /* Same step as mb_advdiff_step, for callers that cannot allocate device memory.
  *
  * No counterpart in the reference: manapy allocates its work arrays with numpy.
@@ -394,7 +456,10 @@ int mb_sw_batch_step_f32c(const mb_sw_item *items, const int32_t *face_map, int3
  * MB_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), which every GPU that loads the
  * library keeps reserved until the process exits; larger meshes get MB_ETOOBIG.
  * The first call on each device looks up that array's device address, so make
- * it before any stream capture.  All calls share the one array: calls that may
+ * it before any stream capture.  The address is kept for the life of the
+ * process: after cudaDeviceReset on a device the library's module is loaded
+ * again and the kept address is stale, so a process that resets a device must
+ * not call this entry point on that device afterwards.  All calls share the one array: calls that may
  * overlap on the GPU (different streams, or host threads) race with each other
  * and must be serialised by the caller.  Nothing in the array needs clearing
  * between calls.  Arguments as for mb_advdiff_step, without the scratch. */

@@ -60,6 +60,20 @@ class MbSwItem(ctypes.Structure):
                 ("c_begin", _i32)]
 
 
+class MbAdvDiffItemF64(ctypes.Structure):
+    _fields_ = [("m", MbMesh), ("bc", MbBC), ("p", MbAdvDiffParams), ("w", _vp * 2), ("sign_cf", _vp),
+                ("src", _vp), ("dt_dev", _vp), ("cell_scratch", _vp), ("node_scratch", _vp),
+                ("start_step", _i32), ("end_step", _i32), ("p1_begin", _i32), ("p1_cell_blocks", _i32),
+                ("p2_begin", _i32), ("pad_", _i32)]
+
+
+class MbSwItemF64(ctypes.Structure):
+    _fields_ = [("m", MbMesh), ("q", (_vp * 5) * 2), ("face_flux", _vp), ("dt", _vp), ("cfl", _d), ("grav", _d),
+                ("start_step", _i32), ("end_step", _i32), ("f_begin", _i32), ("c_begin", _i32)]
+
+
+WALLS = {"neumann": 0, "reflective": 1}
+
 _M = ctypes.POINTER(MbMesh)
 _B = ctypes.POINTER(MbBC)
 _P5 = _vp * 5
@@ -100,6 +114,10 @@ _SIGS = {
     "mb_advdiff_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],
+    "mb_sw_step_ex": [_M, _P5, _P5, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
+    "mb_sw_step_f32c_ex": [_M, _P5, _P5, _P4, _P4, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp],
+    "mb_advdiff_batch_step": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
+    "mb_sw_batch_step": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_check_state": [_vp, _vp, ctypes.c_int64, _i32, _vp, _vp],
     "mb_build_info": [],
 }

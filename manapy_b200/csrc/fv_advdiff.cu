@@ -708,6 +708,42 @@ __global__ void __launch_bounds__(MB_P2_BLOCK, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_
   f2_phase2<ORDER2, DIFF>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x);
 }
 
+// ---------------------------------------------------------------- batches of triangle meshes, FP64
+//
+// Block b of a launch belongs to item map[b] (blocks never straddle two meshes) and runs
+// the single-mesh block body above on that item's tables, so each item computes exactly
+// what mb_advdiff_step computes for it alone.  The batch clock selects each item's
+// ping-pong state and skips items outside their [start_step, end_step) window.
+
+#ifndef MB_P2_BATCH_MIN_BLOCKS
+#define MB_P2_BATCH_MIN_BLOCKS 3
+#endif
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS)
+    k_f2_batch_phase1(const mb_advdiff_item_f64 *__restrict__ items, const int32_t *__restrict__ map,
+                      const int32_t *__restrict__ clock) {
+  const mb_advdiff_item_f64 &it = items[map[blockIdx.x]];
+  const int t = *clock;
+  if (t < it.start_step || t >= it.end_step) return;
+  f2_phase1<ORDER2, DIFF>(it.m, it.bc, it.w[(t - it.start_step) & 1], it.cell_scratch, it.node_scratch,
+                          it.p1_cell_blocks, (int)blockIdx.x - it.p1_begin);
+}
+
+template <bool ORDER2, bool DIFF>
+__global__ void __launch_bounds__(kBlock, MB_P2_BATCH_MIN_BLOCKS)
+    k_f2_batch_phase2(const mb_advdiff_item_f64 *__restrict__ items, const int32_t *__restrict__ map,
+                      const int32_t *__restrict__ clock) {
+  const mb_advdiff_item_f64 &it = items[map[blockIdx.x]];
+  const int t = *clock;
+  if (t < it.start_step || t >= it.end_step) return;
+  const int par = (t - it.start_step) & 1;
+  f2_phase2<ORDER2, DIFF>(it.m, it.bc, it.p, it.w[par], it.w[par ^ 1], it.sign_cf, it.src, it.dt_dev,
+                          it.cell_scratch, it.node_scratch, (int)blockIdx.x - it.p2_begin);
+}
+
+__global__ void k_batch_tick(int32_t *clock) { *clock += 1; }
+
 // ---------------------------------------------------------------- fused step, compact 3D layout
 //
 // Tetrahedra.  Local face j of a cell is (v0,v1,v2), (v2,v3,v0), (v0,v1,v3),
@@ -1176,6 +1212,27 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
     else { if (df) MB_STEP(3, false, true); else MB_STEP(3, false, false); }
   }
 #undef MB_STEP
+}
+
+int mb_advdiff_batch_step(const mb_advdiff_item_f64 *items, const int32_t *p1_map, int32_t p1_blocks,
+                          const int32_t *p2_map, int32_t p2_blocks, int32_t order, int32_t diffusion,
+                          int32_t *clock, void *stream) {
+  if (!items || !p2_map || !clock || p2_blocks <= 0 || p1_blocks < 0 || (order != 1 && order != 2)) return MB_EINVAL;
+  const bool o2 = order == 2, df = diffusion != 0;
+  if ((o2 || df) && (!p1_map || p1_blocks <= 0)) return MB_EINVAL;
+  cudaStream_t st = ST(stream);
+#define MB_BATCH(O, F)                                                                              \
+  do {                                                                                              \
+    if (O || F) k_f2_batch_phase1<O, F><<<p1_blocks, kBlock, 0, st>>>(items, p1_map, clock);        \
+    k_f2_batch_phase2<O, F><<<p2_blocks, kBlock, 0, st>>>(items, p2_map, clock);                    \
+  } while (0)
+  if (o2 && df) MB_BATCH(true, true);
+  else if (o2) MB_BATCH(true, false);
+  else if (df) MB_BATCH(false, true);
+  else MB_BATCH(false, false);
+#undef MB_BATCH
+  k_batch_tick<<<1, 1, 0, st>>>(clock);
+  return check_launch();
 }
 
 }  // extern "C"

@@ -271,7 +271,16 @@ struct SWState {
   const double *g[5];  // ghosts (faces); null -> neumann copy of the interior cell
   const double *gr[4]; // h_x, h_y, hc_x, hc_y (order 2)
   const double *psi;   // hc's limiter (order 2)
+  int walls;           // boundary faces of the fused step: MB_WALLS_NEUMANN or MB_WALLS_REFLECT
 };
+
+// Momentum of a reflective-wall ghost: the interior momentum with its normal
+// component reversed, q - 2 (q.n) n / |n|^2 (no counterpart in manapy).
+__device__ __forceinline__ void wall_mirror(double hu, double hv, double n0, double n1, double &gu, double &gv) {
+  const double k = 2 * (hu * n0 + hv * n1) / (n0 * n0 + n1 * n1);
+  gu = hu - k * n0;
+  gv = hv - k * n1;
+}
 
 __device__ __forceinline__ double sw_ghost(const SWState &s, int k, int f, int c0) {
   return s.g[k] ? ld(s.g[k] + f) : ld(s.q[k] + c0);
@@ -508,7 +517,6 @@ __device__ __forceinline__ int4 ldi4(const int32_t *p) { return __ldg(reinterpre
 __device__ __forceinline__ double2 ldd2s(const double *p) { return __ldg(reinterpret_cast<const double2 *>(p)); }
 __device__ __forceinline__ int compi(const int4 v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : v.z); }
 
-template <bool ORDER2, bool FAST>
 #ifndef MB_SW_FLUX_MIN_BLOCKS
 #define MB_SW_FLUX_MIN_BLOCKS 3
 #endif
@@ -519,11 +527,9 @@ template <bool ORDER2, bool FAST>
 #define MB_SW_CELL_MIN_BLOCKS 4
 #endif
 
-__global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS) k_sw2_flux(mb_mesh m, SWState s, double grav, double *ff,
-                                                     double *dt_next) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f == 0 && dt_next) *dt_next = 1e6;
-  if (f >= m.nbfaces) return;
+// SRNH flux of face f of the compact-layout step, written as one 32-byte record.
+template <bool ORDER2, bool FAST>
+__device__ __forceinline__ void sw2_flux_face(const mb_mesh &m, const SWState &s, double grav, double *ff, int f) {
   const int l = ld(m.face_cellid + 2 * f), r = ld(m.face_cellid + 2 * f + 1);
   const double n0 = ld(m.face_normal + 3 * f), n1 = ld(m.face_normal + 3 * f + 1), mes = ld(m.face_mesure + f);
   double h_l = ld(s.q[0] + l), hc_l = ld(s.q[3] + l);
@@ -542,15 +548,31 @@ __global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS) k_sw2
       hc_r = hc_r + pr * (ld(s.gr[2] + r) * rr0 + ld(s.gr[3] + r) * rr1);
     }
   }
+  const double hu_l = ld(s.q[1] + l), hv_l = ld(s.q[2] + l);
+  double hu_r, hv_r;
+  if (r < 0 && s.walls == MB_WALLS_REFLECT) {
+    wall_mirror(hu_l, hv_l, n0, n1, hu_r, hv_r);
+  } else {
+    hu_r = ld(s.q[1] + rr);
+    hv_r = ld(s.q[2] + rr);
+  }
   double fl[4];
-  srnh0<FAST>(ld(s.q[1] + l), ld(s.q[1] + rr), ld(s.q[2] + l), ld(s.q[2] + rr), h_l, h_r, hc_l, hc_r,
-              ld(s.q[4] + l), ld(s.q[4] + rr), n0, n1, mes, grav, fl);
+  srnh0<FAST>(hu_l, hu_r, hv_l, hv_r, h_l, h_r, hc_l, hc_r, ld(s.q[4] + l), ld(s.q[4] + rr), n0, n1, mes, grav, fl);
 #if MB_V4_IO
   st4d_plain(ff + 4 * (long long)f, fl[0], fl[1], fl[2], fl[3]);
 #else
   reinterpret_cast<double2 *>(ff)[2 * f] = make_double2(fl[0], fl[1]);
   reinterpret_cast<double2 *>(ff)[2 * f + 1] = make_double2(fl[2], fl[3]);
 #endif
+}
+
+template <bool ORDER2, bool FAST>
+__global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS) k_sw2_flux(mb_mesh m, SWState s, double grav, double *ff,
+                                                     double *dt_next) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f == 0 && dt_next) *dt_next = 1e6;
+  if (f >= m.nbfaces) return;
+  sw2_flux_face<ORDER2, FAST>(m, s, grav, ff, f);
 }
 
 // flags of the compact 2D layout (cell_flags): bit j own, 3+j node order, 6+j normal
@@ -728,6 +750,53 @@ int sw_gradients(const mb_mesh &m, const double *h, const double *hc, double *hx
                  double *cy, double *psi, cudaStream_t st);
 }
 
+namespace mb {
+
+// ---------------------------------------------------------------- batches of meshes, FP64
+//
+// The FP64 twin of mb_sw_batch_step_f32c: block b of a launch belongs to item
+// map[b] and runs the single-mesh block body (first order, Neumann walls) on
+// that item's tables; the batch clock picks each item's ping-pong state and dt.
+
+__global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS)
+    k_sw2_batch_flux(const mb_sw_item_f64 *__restrict__ items, const int32_t *__restrict__ map,
+                     const int32_t *__restrict__ clock) {
+  const mb_sw_item_f64 &it = items[map[blockIdx.x]];
+  const int t = *clock;
+  if (t < it.start_step || t >= it.end_step) return;
+  const int par = (t - it.start_step) & 1;
+  const int f = ((int)blockIdx.x - it.f_begin) * blockDim.x + threadIdx.x;
+  if (f == 0) it.dt[par ^ 1] = 1e6;
+  if (f >= it.m.nbfaces) return;
+  SWState s{};
+  for (int k = 0; k < 5; ++k) s.q[k] = it.q[par][k];
+  sw2_flux_face<false, MB_SW_FAST>(it.m, s, it.grav, it.face_flux, f);
+}
+
+__global__ void __launch_bounds__(kBlock, MB_SW_CELL_MIN_BLOCKS)
+    k_sw2_batch_cell(const mb_sw_item_f64 *__restrict__ items, const int32_t *__restrict__ map,
+                     const int32_t *__restrict__ clock) {
+  const mb_sw_item_f64 &it = items[map[blockIdx.x]];
+  const int t = *clock;
+  if (t < it.start_step || t >= it.end_step) return;  // uniform over the block
+  const int par = (t - it.start_step) & 1;
+  SWState s{};
+  SWQ out;
+  for (int k = 0; k < 5; ++k) {
+    s.q[k] = it.q[par][k];
+    out.q[k] = it.q[par ^ 1][k];
+  }
+  const int i = ((int)blockIdx.x - it.c_begin) * blockDim.x + threadIdx.x;
+  double best = 1e300;
+  if (i < it.m.nbcells) best = sw2_cell_body(it.m, s, out, it.face_flux, it.dt + par, true, it.cfl, it.grav, i);
+  best = block_min(best);
+  if (threadIdx.x == 0 && best < 1e300) atomic_min_pos(it.dt + (par ^ 1), best);
+}
+
+__global__ void k_sw_batch_tick(int32_t *clock) { *clock += 1; }
+
+}  // namespace mb
+
 extern "C" {
 
 int mb_srnh_flux(int32_t n, const double *states, const double *normals, const double *mesure, double grav,
@@ -799,7 +868,15 @@ int mb_update_sw(const mb_mesh *m, double *const q[5], const double *const rez[5
 int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
                int32_t order, double *scratch, double *face_flux, const double *dt_cur, double *dt_next,
                void *stream) {
+  return mb_sw_step_ex(m, q_in, q_out, cfl, grav, order, MB_WALLS_NEUMANN, scratch, face_flux, dt_cur, dt_next,
+                       stream);
+}
+
+int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
+                  int32_t order, int32_t walls, double *scratch, double *face_flux, const double *dt_cur,
+                  double *dt_next, void *stream) {
   if (!sw_mesh_ok(m) || !q_in || !q_out || !face_flux || !dt_cur || (order != 1 && order != 2)) return MB_EINVAL;
+  if (walls != MB_WALLS_NEUMANN && walls != MB_WALLS_REFLECT) return MB_EINVAL;
   if (!m->cell_cellfid || !m->cell_vtx || !m->cell_nbr || !m->cell_flags || !m->node_coord || !m->cell_xy)
     return MB_EINVAL;
   SWState s{};
@@ -810,6 +887,7 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
     s.g[k] = nullptr;  // neumann ghosts
     out.q[k] = q_out[k];
   }
+  s.walls = walls;
   if (dt_next == dt_cur) return MB_EINVAL;
 #if MB_V4_IO
   if ((reinterpret_cast<uintptr_t>(face_flux) & 31) != 0) return MB_EINVAL;   // 256-bit flux records
@@ -829,6 +907,16 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
     k_sw2_flux<false, MB_SW_FAST><<<fb, MB_SW_FLUX_BLOCK, 0, st>>>(*m, s, grav, face_flux, dt_next);
   }
   k_sw2_cell<<<ceil_div(m->nbcells, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_cur, dt_next, cfl, grav);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_sw_batch_step(const mb_sw_item_f64 *items, const int32_t *face_map, int32_t face_blocks,
+                     const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream) {
+  if (!items || !face_map || !cell_map || !clock || face_blocks <= 0 || cell_blocks <= 0) return MB_EINVAL;
+  cudaStream_t st = ST(stream);
+  k_sw2_batch_flux<<<face_blocks, MB_SW_FLUX_BLOCK, 0, st>>>(items, face_map, clock);
+  k_sw2_batch_cell<<<cell_blocks, kBlock, 0, st>>>(items, cell_map, clock);
+  k_sw_batch_tick<<<1, 1, 0, st>>>(clock);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }
 

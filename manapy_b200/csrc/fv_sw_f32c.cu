@@ -103,6 +103,7 @@ __device__ __forceinline__ void srnh_f32(float hu_l, float hu_r, float hv_l, flo
 struct SWStateF {
   const float *q[5];   // h, hu, hv, hc, Z
   const float *lo[4];  // rounding errors of h, hu, hv, hc (all NULL: plain FP32 state)
+  int walls;           // MB_WALLS_NEUMANN or MB_WALLS_REFLECT
 };
 struct SWOutF {
   float *q[5];
@@ -130,9 +131,20 @@ __device__ __forceinline__ void sw2c_face(const mb_mesh &m, const SWStateF &s, f
   const int l = ld(m.face_cellid + 2 * f), r = ld(m.face_cellid + 2 * f + 1);
   const int rr = r >= 0 ? r : l;  // Neumann ghost: the interior cell's state
   const float4 nm = __ldg(reinterpret_cast<const float4 *>(m.face_nm_f32) + f);  // n0, n1, 1/mesure
+  const float hu_l = ld(s.q[1] + l), hv_l = ld(s.q[2] + l);
+  float hu_r, hv_r;
+  if (r < 0 && s.walls == MB_WALLS_REFLECT) {
+    // reflective wall: normal momentum reversed, q - 2 (q.n) n / |n|^2 with 1/|n| = nm.z
+    const float k = 2.f * (hu_l * nm.x + hv_l * nm.y) * (nm.z * nm.z);
+    hu_r = hu_l - k * nm.x;
+    hv_r = hv_l - k * nm.y;
+  } else {
+    hu_r = ld(s.q[1] + rr);
+    hv_r = ld(s.q[2] + rr);
+  }
   float fl[4];
-  srnh_f32(ld(s.q[1] + l), ld(s.q[1] + rr), ld(s.q[2] + l), ld(s.q[2] + rr), ld(s.q[0] + l), ld(s.q[0] + rr),
-           ld(s.q[3] + l), ld(s.q[3] + rr), ld(s.q[4] + l), ld(s.q[4] + rr), nm.x, nm.y, nm.z, grav, fl);
+  srnh_f32(hu_l, hu_r, hv_l, hv_r, ld(s.q[0] + l), ld(s.q[0] + rr), ld(s.q[3] + l), ld(s.q[3] + rr),
+           ld(s.q[4] + l), ld(s.q[4] + rr), nm.x, nm.y, nm.z, grav, fl);
   reinterpret_cast<float4 *>(ff)[f] = make_float4(fl[0], fl[1], fl[2], fl[3]);
 }
 
@@ -311,7 +323,16 @@ using namespace mb;
 extern "C" int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
                                const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
                                int32_t order, float *face_flux, const double *dt_cur, double *dt_next, void *stream) {
+  return mb_sw_step_f32c_ex(m, q_in, q_out, lo_in, lo_out, cfl, grav, order, MB_WALLS_NEUMANN, face_flux, dt_cur,
+                            dt_next, stream);
+}
+
+extern "C" int mb_sw_step_f32c_ex(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
+                                  const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
+                                  int32_t order, int32_t walls, float *face_flux, const double *dt_cur,
+                                  double *dt_next, void *stream) {
   if (!m || m->dim != 2 || m->nlf != 3 || m->nbcells <= 0 || m->nbfaces <= 0) return MB_EINVAL;
+  if (walls != MB_WALLS_NEUMANN && walls != MB_WALLS_REFLECT) return MB_EINVAL;
   if (!q_in || !q_out || !face_flux || !dt_cur || dt_next == dt_cur || order != 1) return MB_EINVAL;
   if (!m->cell_cellfid || !m->cell_vtx || !m->cell_nbr || !m->cell_flags || !m->node_coord || !m->cell_xy ||
       !m->cell_faces || !m->face_nm_f32)
@@ -323,6 +344,7 @@ extern "C" int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], flo
     s.q[k] = q_in[k];
     out.q[k] = q_out[k];
   }
+  s.walls = walls;
   if ((lo_in == nullptr) != (lo_out == nullptr)) return MB_EINVAL;
   if (lo_in) {
     for (int k = 0; k < 4; ++k) {

@@ -131,8 +131,9 @@ def _p(t):
 class _Slot:
     """One admitted request: its device tables, fields and batch item."""
 
-    def __init__(self, req, dm, bc, init, dev, stream, staging, stats=None):
+    def __init__(self, req, dm, bc, init, dev, stream, staging, stats=None, precision="fp32c"):
         stats = stats if stats is not None else {}
+        self.precision = precision
         t0 = time.perf_counter()
         self.req = req
         extra = {"init%d" % k: np.ascontiguousarray(a, dtype=np.float64) for k, a in enumerate(init)}
@@ -150,9 +151,12 @@ class _Slot:
         stats["admit_bc"] = stats.get("admit_bc", 0.0) + t2 - t1
         nc, nf = dm.nbcells, dm.nbfaces
         f32 = torch.float32
+        f64 = torch.float64
         with torch.cuda.stream(stream):
             up = [views["init%d" % k] for k in range(len(init))]
-            if req.kind == "advdiff":
+            if precision == "fp64":
+                self._setup_fp64(req, up, dev, stream, nc, nf, f64)
+            elif req.kind == "advdiff":
                 self.w = [up[0].float(), torch.empty(nc, dtype=f32, device=dev)]
                 self.lo = [(up[0] - self.w[0].double()).float(), torch.empty(nc, dtype=f32, device=dev)]
                 uf = torch.full((nf,), req.ux, dtype=torch.float64, device=dev)
@@ -190,6 +194,35 @@ class _Slot:
         self.fam = None
         self.nbytes = self.dm.nbytes() + sum(t.numel() * t.element_size() for t in self._tensors())
 
+    def _setup_fp64(self, req, up, dev, stream, nc, nf, f64):
+        """Plain FP64 buffers of the request (the batched FP64 steps)."""
+        st = stream.cuda_stream
+        if req.kind == "advdiff":
+            self.w = [up[0].clone(), torch.empty(nc, dtype=f64, device=dev)]
+            self.lo = []
+            uf = torch.full((nf,), req.ux, dtype=f64, device=dev)
+            vf = torch.full((nf,), req.uy, dtype=f64, device=dev)
+            zf = torch.zeros(nf, dtype=f64, device=dev)
+            self.sign = torch.empty(4 * nc, dtype=f64, device=dev)
+            _lib.call("mb_cell_face_sign", self.dm.struct, _p(uf), _p(vf), _p(zf), _p(self.sign), st)
+            uc = torch.full((nc,), req.ux, dtype=f64, device=dev)
+            vc = torch.full((nc,), req.uy, dtype=f64, device=dev)
+            zc = torch.zeros(nc, dtype=f64, device=dev)
+            self.dt = torch.empty(1, dtype=f64, device=dev)
+            _lib.call("mb_time_step", self.dm.struct, _p(uc), _p(vc), _p(zc), 0.8, req.D, req.D, 0.0, _p(self.dt), st)
+            self.cs = torch.empty(4 * nc, dtype=f64, device=dev)
+            self.ns = torch.empty(self.dm.nbnodes, dtype=f64, device=dev)
+            self.params = _lib.MbAdvDiffParams(2, 1, req.D, req.D, 0.0)
+        else:
+            q = [up[k].clone() for k in range(4)]
+            self.q = [q, [torch.empty(nc, dtype=f64, device=dev) for _ in range(4)]]
+            self.lo = [[], []]
+            self.Z = up[4].clone()
+            self.ff = torch.empty(4 * nf, dtype=f64, device=dev)
+            self.dt = torch.empty(2, dtype=f64, device=dev)
+            _lib.call("mb_time_step_sw", self.dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), 0.5, 9.81, 0.0, 0.0,
+                      _p(self.dt), st)
+
     def _tensors(self):
         if self.req.kind == "advdiff":
             return self.w + self.lo + [self.sign, self.dt, self.cs, self.ns]
@@ -205,6 +238,10 @@ class _Slot:
     def result(self):
         """Final state (device tensors, device numbering): [w] or [h, hu, hv]."""
         par = (self.end - self.start) & 1
+        if self.precision == "fp64":
+            if self.req.kind == "advdiff":
+                return [self.w[par].clone()]
+            return [self.q[par][c].clone() for c in range(3)]
         if self.req.kind == "advdiff":
             return [self.w[par].double() + self.lo[par].double()]
         return [self.q[par][c].double() + self.lo[par][c].double() for c in range(3)]
@@ -215,11 +252,16 @@ class BatchServer:
 
     ``hbm_budget``: bytes of device memory the admitted requests may hold;
     ``max_active``: slots; ``chunk``: steps per graph replay between admission points;
-    ``workers``: host processes preparing meshes (0: prepare in this process).
+    ``workers``: host processes preparing meshes (0: prepare in this process);
+    ``precision``: "fp32c" (FP32 state with compensated sums, the serving default) or "fp64"
+    (manapy's plain arithmetic, each result bit-identical to the single-mesh FP64 solver).
     """
 
     def __init__(self, device="cuda:0", hbm_budget=40e9, max_active=256, chunk=16, workers=None,
-                 graphs=True):
+                 graphs=True, precision="fp32c"):
+        if precision not in ("fp32c", "fp64"):
+            raise ValueError("precision must be 'fp32c' or 'fp64'")
+        self.precision = precision
         self.dev = torch.device(device)
         self.budget = float(hbm_budget)
         self.max_active = int(max_active)
@@ -267,7 +309,7 @@ class BatchServer:
         t0 = time.perf_counter()
         staging = self._stage(need)
         self.stats["admit_stage_wait"] = self.stats.get("admit_stage_wait", 0.0) + time.perf_counter() - t0
-        slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream, staging, self.stats)
+        slot = _Slot(req, dm, bc, init, self.dev, self.upload_stream, staging, self.stats, self.precision)
         self._staging_ev = torch.cuda.Event()
         self._staging_ev.record(self.upload_stream)
         self.stream.wait_event(slot.ready)
@@ -279,9 +321,10 @@ class BatchServer:
         ad = [s for s in self.active.values() if s.req.kind == "advdiff"]
         sw = [s for s in self.active.values() if s.req.kind == "sw"]
         tabs = {}
+        fp64 = self.precision == "fp64"
         with torch.cuda.stream(self.stream):
             if ad:
-                items = (_lib.MbAdvDiffItem * len(ad))()
+                items = ((_lib.MbAdvDiffItemF64 if fp64 else _lib.MbAdvDiffItem) * len(ad))()
                 p1, p2 = [], []
                 b1 = b2 = 0
                 for k, s in enumerate(ad):
@@ -289,7 +332,8 @@ class BatchServer:
                     it = items[k]
                     it.m, it.bc, it.p = s.dm.struct, s.bc.struct, s.params
                     it.w[0], it.w[1] = _p(s.w[0]), _p(s.w[1])
-                    it.lo[0], it.lo[1] = _p(s.lo[0]), _p(s.lo[1])
+                    if not fp64:
+                        it.lo[0], it.lo[1] = _p(s.lo[0]), _p(s.lo[1])
                     it.sign_cf, it.src, it.dt_dev = _p(s.sign), None, _p(s.dt)
                     it.cell_scratch, it.node_scratch = _p(s.cs), _p(s.ns)
                     it.start_step, it.end_step = s.start, s.end
@@ -301,7 +345,7 @@ class BatchServer:
                 tabs["ad"] = (self._dev_bytes(items), self._dev_i32(np.concatenate(p1)), b1,
                               self._dev_i32(np.concatenate(p2)), b2)
             if sw:
-                items = (_lib.MbSwItem * len(sw))()
+                items = ((_lib.MbSwItemF64 if fp64 else _lib.MbSwItem) * len(sw))()
                 fm, cm = [], []
                 bf = bc = 0
                 for k, s in enumerate(sw):
@@ -311,8 +355,13 @@ class BatchServer:
                     for par in range(2):
                         for c in range(4):
                             it.q[par][c] = _p(s.q[par][c])
-                            it.lo[par][c] = _p(s.lo[par][c])
-                    it.Z, it.face_flux, it.dt = _p(s.Z), _p(s.ff), _p(s.dt)
+                            if not fp64:
+                                it.lo[par][c] = _p(s.lo[par][c])
+                        if fp64:
+                            it.q[par][4] = _p(s.Z)   # the bed does not change: one array for both
+                    if not fp64:
+                        it.Z = _p(s.Z)
+                    it.face_flux, it.dt = _p(s.ff), _p(s.dt)
                     it.cfl, it.grav = 0.5, 9.81
                     it.start_step, it.end_step = s.start, s.end
                     it.f_begin, it.c_begin = bf, bc
@@ -332,13 +381,15 @@ class BatchServer:
         return torch.from_numpy(a).pin_memory().to(self.dev, non_blocking=True)
 
     def _launch_step(self, tabs, st):
+        fp64 = self.precision == "fp64"
         if "ad" in tabs:
             items, m1, b1, m2, b2 = tabs["ad"]
-            _lib.call("mb_advdiff_batch_step_f32c", _p(items), _p(m1), b1, _p(m2), b2, 2, 1, _p(self.clock[0:1]),
-                      st)
+            _lib.call("mb_advdiff_batch_step" if fp64 else "mb_advdiff_batch_step_f32c", _p(items), _p(m1), b1,
+                      _p(m2), b2, 2, 1, _p(self.clock[0:1]), st)
         if "sw" in tabs:
             items, m1, b1, m2, b2 = tabs["sw"]
-            _lib.call("mb_sw_batch_step_f32c", _p(items), _p(m1), b1, _p(m2), b2, _p(self.clock[1:2]), st)
+            _lib.call("mb_sw_batch_step" if fp64 else "mb_sw_batch_step_f32c", _p(items), _p(m1), b1, _p(m2), b2,
+                      _p(self.clock[1:2]), st)
 
     def _run_chunk(self, nsteps):
         """``nsteps`` batch steps on the compute stream (each family ticks its own clock)."""

@@ -522,7 +522,10 @@ class ShallowWaterSolver:
                    ("wind", bool, False, True, "wind"),
                    ("precision", str, "fp64", 0, "fp64 (manapy's arithmetic) or fp32c: FP32 state and fluxes "
                                                  "with compensated per-cell sums, FP64 geometry, source and dt "
-                                                 "(first order; no counterpart in manapy)")]
+                                                 "(first order; no counterpart in manapy)"),
+                   ("walls", str, "neumann", 0, "boundary faces of the fused step: neumann (manapy's default "
+                                                "ghosts, the interior state) or reflective (mirrored momentum, "
+                                                "no mass flux; no counterpart in manapy)")]
 
     @classmethod
     def process_conf(cls, conf, kwargs):
@@ -579,6 +582,9 @@ class ShallowWaterSolver:
             raise ValueError("precision must be 'fp64' or 'fp32c'")
         if self.precision == "fp32c" and self.order != 1:
             raise NotImplementedError("the fp32c shallow-water step is first order")
+        self.walls = str(get("walls"))
+        if self.walls not in _lib.WALLS:
+            raise ValueError("walls must be 'neumann' or 'reflective'")
         self._q32 = None
         self._q32_key = None
         self._q32_i = 0
@@ -675,6 +681,9 @@ class ShallowWaterSolver:
         every variable has manapy's default (Neumann) boundaries."""
         self._setup()
         self._fused = self._all_neumann()
+        if not self._fused and self.walls != "neumann":
+            raise NotImplementedError("reflective walls run in the fused step, which needs the variables' "
+                                      "default (Neumann) boundaries")
         if not self._fused:
             self.stepper()
             self.update_ghost_values()
@@ -719,10 +728,10 @@ class ShallowWaterSolver:
         qout = self._spare
         cur = self._use_dt()
         nxt = self._dt_buf[1 - self._cur:2 - self._cur]
-        _lib.call("mb_sw_step", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
+        _lib.call("mb_sw_step_ex", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
                   _lib.p5([_p(t) for t in qout] + [_p(z)]), float(self.cfl), float(self.grav), int(self.order),
-                  _p(self._scratch) if self._scratch is not None else None, _p(self._ff), _p(cur), _p(nxt),
-                  self._stream())
+                  _lib.WALLS[self.walls], _p(self._scratch) if self._scratch is not None else None, _p(self._ff),
+                  _p(cur), _p(nxt), self._stream())
         self._spare = [self.varbs[k].swap_cell(t) for k, t in zip(names, qout)]
         self._cur = 1 - self._cur
         self._dt_key = self._state_key()
@@ -759,10 +768,10 @@ class ShallowWaterSolver:
         cur = self._use_dt()
         nxt = self._dt_buf[1 - self._cur:2 - self._cur]
         k0 = self._q32_i
-        _lib.call("mb_sw_step_f32c", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
+        _lib.call("mb_sw_step_f32c_ex", self._dm.struct, _lib.p5([_p(t) for t in qin] + [_p(z)]),
                   _lib.p5([_p(t) for t in qout] + [_p(z)]), _lib.p4([_p(t) for t in self._lo32[k0]]),
                   _lib.p4([_p(t) for t in self._lo32[1 - k0]]), float(self.cfl), float(self.grav), int(self.order),
-                  _p(self._ff32), _p(cur), _p(nxt), self._stream())
+                  _lib.WALLS[self.walls], _p(self._ff32), _p(cur), _p(nxt), self._stream())
         self._q32_i = 1 - k0
         for k, buf, lo in zip(self._NAMES[:4], qout, self._lo32[1 - k0]):
             var = self.varbs[k]
@@ -796,6 +805,21 @@ class ShallowWaterSolver:
         else:
             h = self.h.dev("cell")
         return float(torch.dot(h, dm.t["cell_volume"]).item())
+
+    def boundary_mass_flux(self):
+        """FP64 sum over the boundary faces of the h flux (outward, times the face length) of
+        the last fused step, as that step applied it: the step changed the FP64 mass
+        ``mass()`` by ``-dt * boundary_mass_flux()`` up to rounding, and by nothing up to
+        rounding with reflective walls (no counterpart in manapy)."""
+        dm = self._setup()
+        if getattr(self, "_bfaces", None) is None:
+            cid = dm.t["face_cellid"].view(-1, 2)
+            self._bfaces = torch.nonzero(cid[:, 1] < 0).flatten()
+        if self.precision == "fp32c" and self._q32 is not None:
+            ff = self._ff32.view(-1, 4)[:, 0]
+        else:
+            ff = self._ff.view(-1)[:4 * dm.nbfaces].view(-1, 4)[:, 0]
+        return float(ff.index_select(0, self._bfaces).double().sum().item())
 
     def launches_per_step(self):
         """Kernel launches of one fused step: face fluxes, cells (+ next dt), [gradients]."""

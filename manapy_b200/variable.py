@@ -168,6 +168,24 @@ class Variable:
     def dev_out(self, name):
         return self._s.w(name)
 
+    def fetch(self, name="cell", out=None):
+        """Copy array ``name`` (manapy's numbering) into the host tensor ``out`` without a
+        host synchronisation and without handing authority to the host: the copy is queued
+        on the current stream (asynchronous when ``out`` is pinned memory), the device
+        array stays the one kernels use.  Returns ``out`` (allocated pinned if None); its
+        contents are valid once the stream has reached the copy (``torch.cuda.synchronize``
+        or an event).  No counterpart in manapy, whose arrays are host arrays."""
+        s = self._s
+        t = s.d(name)
+        if out is None:
+            out = torch.empty(t.numel(), dtype=torch.float64, pin_memory=True)
+        if out.numel() != t.numel() or out.dtype != torch.float64:
+            raise ValueError("%s needs a float64 tensor of %d values" % (name, t.numel()))
+        if s.kind[name] is not None:
+            t = s.mesh_fn().to_host_order(s.kind[name], t)
+        out.copy_(t, non_blocking=True)
+        return out
+
     def set_lazy(self, name, fn):
         self._s.lazy[name] = fn
 

@@ -1,9 +1,10 @@
 """Generate the golden vectors in this directory by running the reference manapy.
 
-Usage (needs the reference source tree; not run by the test suite)::
+Usage (needs the reference source tree, named by ``MANAPY_REFERENCE``; not run by
+the test suite)::
 
-    python tests/golden/make_golden.py            # all parts, one process each
-    python tests/golden/make_golden.py --part dom2d
+    MANAPY_REFERENCE=<reference tree> python tests/golden/make_golden.py    # all parts
+    MANAPY_REFERENCE=<reference tree> python tests/golden/make_golden.py --part dom2d
 
 Each part runs in its own process because the reference compiles its
 ``Variable`` kernels once per process for the first dimension it sees

@@ -26,7 +26,9 @@ import types
 
 import numpy as np
 
-REFERENCE_ROOT = os.environ.get("MANAPY_REFERENCE", "/root/reference")
+# The reference source tree: the directory holding the ``manapy`` package, given by the
+# environment (``MANAPY_REFERENCE=<path> python tests/golden/make_golden.py``).
+REFERENCE_ROOT = os.environ.get("MANAPY_REFERENCE")
 
 # The reference tree is read-only input: keep Python's bytecode and numba's on-disk
 # kernel cache (``@njit(cache=True)`` writes next to the source) out of it.
@@ -119,6 +121,8 @@ def _install_stubs():
 
 def import_reference():
     """Import the reference package with the stubs installed."""
+    if not REFERENCE_ROOT or not os.path.isdir(os.path.join(REFERENCE_ROOT, "manapy")):
+        raise RuntimeError("set MANAPY_REFERENCE to the reference source tree (the directory holding manapy/)")
     _install_stubs()
     if REFERENCE_ROOT not in sys.path:
         sys.path.insert(0, REFERENCE_ROOT)

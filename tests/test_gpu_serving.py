@@ -100,3 +100,51 @@ def test_batched_shallow_water_matches_the_single_mesh_step(cuda):
     S.advance(r.steps)
     for a, var in zip(got, vs[:3]):
         assert np.array_equal(a, var.cell)
+
+
+def _single_fp64(r):
+    """The request solved alone through the public FP64 solvers (manapy's arithmetic)."""
+    el, vx = meshgen.square_triangles(r.n, seed=r.seed)
+    dom = M.Domain(dim=2, mesh=(el, vx))
+    if r.kind == "advdiff":
+        w = M.Variable(domain=dom, BC={s: "dirichlet" for s in SIDES}, values={s: 0.0 for s in SIDES})
+        u, v = M.Variable(domain=dom), M.Variable(domain=dom)
+        u.face = np.full(dom.nbfaces, r.ux)
+        v.face = np.full(dom.nbfaces, r.uy)
+        u.cell = np.full(dom.nbcells, r.ux)
+        v.cell = np.full(dom.nbcells, r.uy)
+        w.cell = initial_state(r, dom.cells.center)[0]
+        S = M.AdvectionDiffusionSolver(w, vel=(u, v), conf=M.Struct(Dxx=r.D, Dyy=r.D, order=2, cfl=0.8))
+        S.advance(r.steps)
+        return [w.cell]
+    vs = [M.Variable(domain=dom) for _ in range(5)]
+    for var, a in zip(vs, initial_state(r, dom.cells.center)):
+        var.cell = a
+    S = M.ShallowWaterSolver(vs[0], hvel=(vs[1], vs[2]), hc=vs[3], Z=vs[4],
+                             conf=M.Struct(order=1, cfl=0.5, grav=9.81))
+    S.advance(r.steps)
+    return [var.cell for var in vs[:3]]
+
+
+def test_batched_fp64_is_bit_identical_to_the_single_mesh_fp64_solver(cuda):
+    """The FP64 batches run the single-mesh FP64 block bodies: every request of a mix equals
+    its own plain FP64 solve bit for bit (so it inherits that solve's parity with manapy)."""
+    reqs = _mix()
+    mixed = _by_rid(BatchServer(workers=0, chunk=8, precision="fp64").serve(reqs, keep_results=True))
+    for r in reqs:
+        for a, b in zip(mixed[r.rid]["result"], _single_fp64(r)):
+            assert np.array_equal(a, b), r
+
+
+def test_batched_fp64_staggered_admission(cuda):
+    reqs = _mix()
+    for k, r in enumerate(reqs):
+        r.arrival = 0.03 * k
+    staggered = _by_rid(BatchServer(workers=0, chunk=4, max_active=3, precision="fp64").serve(reqs,
+                                                                                             keep_results=True))
+    for r in reqs:
+        r.arrival = 0.0
+    at_once = _by_rid(BatchServer(workers=0, chunk=16, precision="fp64").serve(reqs, keep_results=True))
+    for r in reqs:
+        for a, b in zip(staggered[r.rid]["result"], at_once[r.rid]["result"]):
+            assert np.array_equal(a, b), r

@@ -43,7 +43,10 @@ def test_tag_precedence():
 
 
 def test_reads_a_gmsh_41_file_of_the_reference_if_present():
-    path = "/root/reference/mesh/carre.msh"
+    root = os.environ.get("MANAPY_REFERENCE")
+    if not root:
+        pytest.skip("MANAPY_REFERENCE (the reference source tree) is not set")
+    path = os.path.join(root, "mesh", "carre.msh")
     if not os.path.exists(path):
         pytest.skip("reference mesh not available")
     el, vx = gmsh.read_msh(path, 2)

@@ -68,10 +68,24 @@ def test_noalloc_step_matches_regular_step_twice(wl, cuda):
     assert not np.array_equal(U.H(w1), U.H(w2))  # the two calls really advanced the state
 
 
-def test_noalloc_rejects_meshes_beyond_its_scratch(cuda):
-    U, A, dm, db, prm, sign, dt, w0, st = _setup(W.C2.scaled(n=20))
-    big = _lib.MbMesh.from_buffer_copy(dm.struct)
-    big.nbcells = _lib.NOALLOC_SCRATCH_DOUBLES // 4 + 1   # needs more than the array holds
-    rc = _lib.lib().mb_advdiff_step_noalloc(ctypes.byref(big), db.struct, prm, U.P(w0), U.P(w0), U.P(sign),
-                                            None, U.P(dt), st)
+@pytest.mark.parametrize("wl", [W.C2.scaled(n=20), W.C4.scaled(n=4)])
+def test_noalloc_size_gate_at_its_limit(wl, cuda):
+    """A mesh one double beyond the scratch array is refused with MB_ETOOBIG (2D needs
+    4*cells + nodes doubles, 3D 6*cells + nodes); a mesh exactly at the limit passes the
+    size gate and is then refused for w_in == w_out (MB_EINVAL), before any launch."""
+    U, A, dm, db, prm, sign, dt, w0, st = _setup(wl)
+    per_cell = 4 if wl.dim == 2 else 6
+    limit = _lib.NOALLOC_SCRATCH_DOUBLES
+    lib = _lib.lib()
+    at = _lib.MbMesh.from_buffer_copy(dm.struct)
+    at.nbcells = limit // per_cell - 1000
+    at.nbnodes = limit - per_cell * at.nbcells            # need == limit exactly
+    assert per_cell * at.nbcells + at.nbnodes == limit
+    rc = lib.mb_advdiff_step_noalloc(ctypes.byref(at), db.struct, prm, U.P(w0), U.P(w0), U.P(sign), None,
+                                     U.P(dt), st)
+    assert rc == _lib.MB_EINVAL
+    over = _lib.MbMesh.from_buffer_copy(at)
+    over.nbnodes = at.nbnodes + 1                          # need == limit + 1
+    rc = lib.mb_advdiff_step_noalloc(ctypes.byref(over), db.struct, prm, U.P(w0), U.P(w0), U.P(sign), None,
+                                     U.P(dt), st)
     assert rc == _lib.MB_ETOOBIG
