@@ -76,6 +76,9 @@ def parse():
                     help="single workload only (no C4 / batched / serving sections)")
     ap.add_argument("--extras-requests", type=int, default=1000, help="serving section: requests")
     ap.add_argument("--extras-rate", type=float, default=18.0, help="serving section: arrival rate (requests/s)")
+    ap.add_argument("--section", default=None, choices=["c4", "batched", "serving"],
+                    help="run one extras section alone and print its JSON (the default run starts each "
+                         "section in a process of its own)")
     return ap.parse_args()
 
 
@@ -557,6 +560,35 @@ def extra_serving(args):
             "latency": "arrival to result on the host, mesh preparation included"}
 
 
+SECTIONS = {"c4": extra_c4, "batched": extra_batched, "serving": extra_serving}
+
+
+def run_section(name, args):
+    """One extras section in a process of its own (its GPU memory is returned when it exits,
+    and a failure there is reported in the line instead of ending this run)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--section", name, "--warmup", str(args.warmup),
+           "--min-timed-steps", str(args.min_timed_steps), "--meshes", str(args.meshes),
+           "--extras-requests", str(args.extras_requests), "--extras-rate", str(args.extras_rate)]
+    if args.workers is not None:
+        cmd += ["--workers", str(args.workers)]
+    if args.no_fp32c:
+        cmd.append("--no-fp32c")
+    t0 = time.perf_counter()
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        out = None
+        for ln in reversed(p.stdout.strip().splitlines()):
+            if ln.startswith("{"):
+                out = json.loads(ln)
+                break
+        if p.returncode != 0 or out is None:
+            out = {"error": "exit %d: %s" % (p.returncode, (p.stderr or p.stdout).strip()[-400:])}
+    except subprocess.TimeoutExpired:
+        out = {"error": "timed out after 600 s"}
+    out["section_seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def run_ours(args):
     from manapy_b200 import workloads as W
     wl = W.ALL[args.workload]
@@ -602,19 +634,14 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(dom, wl, args.cpu_steps)
     if world == 1 and not args.no_extras and args.workload == "C2" and not args.n:
-        S.release_graphs()
-        del m, S
         import gc
+        import torch
+        S.release_graphs()
+        del m, S, dom
         gc.collect()
-        extras = {}
-        for name, fn in (("c4", extra_c4), ("batched", extra_batched), ("serving", extra_serving)):
-            t0 = time.perf_counter()
-            try:
-                extras[name] = fn(args)
-            except Exception as e:          # a failing section is reported, not hidden
-                extras[name] = {"error": "%s: %s" % (type(e).__name__, e)}
-            extras[name]["section_seconds"] = round(time.perf_counter() - t0, 1)
-        line["extras"] = extras
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        line["extras"] = {name: run_section(name, args) for name in ("c4", "batched", "serving")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -842,6 +869,11 @@ def run_batched(args):
 
 def main():
     args = parse()
+    if args.section:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(SECTIONS[args.section](args)), flush=True)
+        return
     if args.batched:
         run_batched(args)
         return

@@ -256,10 +256,11 @@ typedef struct mb_advdiff_params {
 /* One advection-diffusion step, the work of AdvectionDiffusionSolver.compute_fluxes +
  * compute_new_val (manapy/solvers/advecdiff/system.py:156-172) in two launches:
  *   1. cell gradients + Barth limiter (order 2) and centre->vertex values (diffusion);
- *   2. per cell: upwind fluxes, diamond diffusion, forward-Euler update.
+ *   2. per cell: upwind fluxes, diamond diffusion, forward-Euler update;
+ * tetrahedra at order 2 add a pack pass before 1 (rows {centre, value} of every cell).
  * w_in is read, w_out written (distinct buffers).  sign_cf[4*i+j] = u.n of the j-th
  * local face of cell i in manapy's face orientation (mb_cell_face_sign); src may be
- * NULL (zero source).  Scratch: cell_scratch [4*nbcells] in 2D, [6*nbcells] in 3D
+ * NULL (zero source).  Scratch: cell_scratch [4*nbcells] in 2D, [8*nbcells] in 3D
  * (order 2), node_scratch [nbnodes] (diffusion); NULL where not needed. */
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
@@ -451,7 +452,7 @@ int mb_sw_batch_step(const mb_sw_item_f64 *items, const int32_t *face_map, int32
  * host application owns every device allocation through its own pool, a service
  * that reserves its device-memory budget up front, or a loop where a cudaMalloc
  * (which can synchronise the device) is not acceptable.  Its scratch
- * (4*nbcells + nbnodes doubles in 2D, 6*nbcells + nbnodes in 3D) lives in a fixed
+ * (4*nbcells + nbnodes doubles in 2D, 8*nbcells + nbnodes in 3D) lives in a fixed
  * array inside the library,
  * MB_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), which every GPU that loads the
  * library keeps reserved until the process exits; larger meshes get MB_ETOOBIG.

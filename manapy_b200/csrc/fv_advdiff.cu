@@ -665,8 +665,10 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
         const int ib = rev ? comp(vt, j) : comp(vt, (j + 1) % 3);
         const double vi1 = ld(wn + ia), vi2 = ld(wn + ib);
         const double t1 = vi1 + vl, t2 = vl + vi2, t3 = vi2 + vr, t4 = vr + vi1;
-        const double fgx = 1 / (2 * air) * (t1 * f1y + t2 * f2y + t3 * f3y + t4 * f4y);
-        const double fgy = -1 / (2 * air) * (t1 * f1x + t2 * f2x + t3 * f3x + t4 * f4x);
+        // -1 / (2 air) is exactly -(1 / (2 air)): one division serves both components
+        const double rda = 1 / (2 * air);
+        const double fgx = rda * (t1 * f1y + t2 * f2y + t3 * f3y + t4 * f4y);
+        const double fgy = -rda * (t1 * f1x + t2 * f2x + t3 * f3x + t4 * f4x);
         double n0 = Xa.y - Xb.y, n1 = Xb.x - Xa.x;
         if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
         v = p.Dxx * fgx * n0 + p.Dyy * fgy * n1;
@@ -753,7 +755,10 @@ __global__ void k_batch_tick(int32_t *clock) { *clock += 1; }
 // the face centre and the stored normal); bit 4 manapy's orientation swap of the
 // last two nodes (the order of the diamond vectors); bit 5 the stored normal is
 // minus 0.5 (v_d1 - v_d0) x (v_d2 - v_d0).  Node coordinates and cell centres
-// are stored [n][4]; the phase-1 record is {w, gx, gy, gz, psi, -} per cell.
+// are stored [n][4].  Cell scratch [8][nbcells]: the phase-1 records {w, psi gx,
+// psi gy, psi gz} ([n][4], the limiter folded into the gradient), then the pack
+// pass's rows {x, y, z, w} ([n][4]) from which the least-squares stencil reads
+// each neighbour's centre and value with one 256-bit load.
 
 
 #ifndef MB_P1_3D_MIN_BLOCKS
@@ -763,21 +768,39 @@ __global__ void k_batch_tick(int32_t *clock) { *clock += 1; }
 #define MB_F3_LSQ_BATCH 4
 #endif
 
+// Pack pass of the 3D step: rows {x, y, z, w} of every cell (centre and value in
+// one 32-byte row), so that the least-squares stencil gathers one row per neighbour.
+__global__ void __launch_bounds__(kBlock) k_f3_pack(mb_mesh m, const double *__restrict__ w, double *__restrict__ rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  double x, y, z, pad;
+  ld4d_stream(m.cell_xy + 4 * (long long)i, x, y, z, pad, l2_stream());
+  st4_keep(rows + 4 * (long long)i, x, y, z, ld(w + i), l2_keep());
+}
+
+// one row {x, y, z, w} (written by the previous launch, read-only in phase 1)
+__device__ __forceinline__ void ld_row(const double *p, double &x, double &y, double &z, double &w) {
+  ld4d(p, x, y, z, w);
+}
+
 template <bool ORDER2, bool DIFF>
 __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                                         double *__restrict__ rec,
+                                                                        const double *__restrict__ rows,
                                                                         double *__restrict__ wn, int ncb) {
   const GhostRule ghost = make_rule(m, bc, w);
   const int lane = threadIdx.x & 31;
   if (ORDER2 && (int)blockIdx.x < ncb) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nbcells) return;
-    const D3 c = ld3(m.cell_xy + 4 * i);
-    const double wi = ld(w + i);
+    D3 c;
+    double wi;
+    ld_row(rows + 4 * (long long)i, c.x, c.y, c.z, wi);
     double ixx = 0., iyy = 0., izz = 0., ixy = 0., ixz = 0., iyz = 0., jx = 0., jy = 0., jz = 0.;
     const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
     const int L = (se - sb) >> 5;
     const int32_t *ix = m.lsq_sell_idx + sb + lane;
+    const uint64_t pst = l2_stream();
     int k = 0;
     // batches of MB_F3_LSQ_BATCH neighbours: their gathers in flight together, terms added in order
     for (; k + MB_F3_LSQ_BATCH <= L; k += MB_F3_LSQ_BATCH) {
@@ -785,9 +808,12 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
       D3 pc[MB_F3_LSQ_BATCH];
       double wc[MB_F3_LSQ_BATCH];
 #pragma unroll
-      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) { cc[u] = ld(ix + 32 * (k + u)); cc[u] = cc[u] < 0 ? i : cc[u]; }
+      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) {
+        cc[u] = ld1_stream(ix + 32 * (k + u), pst);
+        cc[u] = cc[u] < 0 ? i : cc[u];
+      }
 #pragma unroll
-      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) { pc[u] = ld3(m.cell_xy + 4 * cc[u]); wc[u] = ld(w + cc[u]); }
+      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) ld_row(rows + 4 * (long long)cc[u], pc[u].x, pc[u].y, pc[u].z, wc[u]);
 #pragma unroll
       for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) {
         const double dx = pc[u].x - c.x, dy = pc[u].y - c.y, dz = pc[u].z - c.z, dw = wc[u] - wi;
@@ -797,10 +823,12 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
       }
     }
     for (; k < L; ++k) {
-      int cc = ld(ix + 32 * k);
+      int cc = ld1_stream(ix + 32 * k, pst);
       cc = cc < 0 ? i : cc;
-      const D3 pc = ld3(m.cell_xy + 4 * cc);
-      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z, dw = ld(w + cc) - wi;
+      D3 pc;
+      double wcc;
+      ld_row(rows + 4 * (long long)cc, pc.x, pc.y, pc.z, wcc);
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z, dw = wcc - wi;
       ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
       ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
       jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
@@ -847,10 +875,7 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
       }
       ps = pmin(ps, psi_ij);
     }
-    double2 *r2 = reinterpret_cast<double2 *>(rec + 6 * (long long)i);
-    r2[0] = make_double2(wi, gx);
-    r2[1] = make_double2(gy, gz);
-    r2[2] = make_double2(ps, 0.);
+    st4_keep(rec + 4 * (long long)i, wi, ps * gx, ps * gy, ps * gz, l2_keep());
     return;
   }
   if (DIFF) {
@@ -890,11 +915,10 @@ __global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phas
                    ld3(m.node_coord + 4 * vt.w)};
   const D3 ci = ld3(m.cell_xy + 4 * i);
   const double2 sa = ldd2(sign + 4 * i), sb = ldd2(sign + 4 * i + 2);
-  double wi, gxi = 0., gyi = 0., gzi = 0., psii = 0.;
+  // order 2: the record {w, psi gx, psi gy, psi gz} of phase 1
+  double wi, gxi = 0., gyi = 0., gzi = 0.;
   if (ORDER2) {
-    const double2 *r = reinterpret_cast<const double2 *>(rec + 6 * (long long)i);
-    const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
-    wi = a.x; gxi = a.y; gyi = b.x; gzi = b.y; psii = c.x;
+    ld4d(rec + 4 * (long long)i, wi, gxi, gyi, gzi);
   } else {
     wi = ld(w + i);
   }
@@ -909,16 +933,14 @@ __global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phas
     face_desc(fl, j, d0, d1, d2);
     const D3 V0 = pick4(P, d0), V1 = pick4(P, d1), V2 = pick4(P, d2);
     const D3 fc = (1. / 3) * ((V0 + V1) + V2);
-    double vo, gxo = 0., gyo = 0., gzo = 0., pso = 0.;
+    double vo, gxo = 0., gyo = 0., gzo = 0.;
     D3 co;
     if (b) {
       vo = ghost(f);
       co = d3(ld(m.face_ghostcenter + 3 * f), ld(m.face_ghostcenter + 3 * f + 1), ld(m.face_ghostcenter + 3 * f + 2));
     } else {
       if (ORDER2) {
-        const double2 *r = reinterpret_cast<const double2 *>(rec + 6 * (long long)o);
-        const double2 a = __ldg(r), bb = __ldg(r + 1), c = __ldg(r + 2);
-        vo = a.x; gxo = a.y; gyo = bb.x; gzo = bb.y; pso = c.x;
+        ld4d(rec + 4 * (long long)o, vo, gxo, gyo, gzo);
       } else {
         vo = ld(w + o);
       }
@@ -928,11 +950,11 @@ __global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phas
     const bool take_me = (s >= 0) == own;
     double sol;
     if (take_me) {
-      sol = ORDER2 ? wi + psii * (gxi * (fc.x - ci.x) + gyi * (fc.y - ci.y) + gzi * (fc.z - ci.z)) : wi;
+      sol = ORDER2 ? wi + (gxi * (fc.x - ci.x) + gyi * (fc.y - ci.y) + gzi * (fc.z - ci.z)) : wi;
     } else if (b) {
       sol = vo;
     } else {
-      sol = ORDER2 ? vo + pso * (gxo * (fc.x - co.x) + gyo * (fc.y - co.y) + gzo * (fc.z - co.z)) : vo;
+      sol = ORDER2 ? vo + (gxo * (fc.x - co.x) + gyo * (fc.y - co.y) + gzo * (fc.z - co.z)) : vo;
     }
     const double F = s * sol;
     cv[j] = own ? -F : F;
@@ -949,14 +971,15 @@ __global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phas
         const D3 f1 = 0.5 * cross(s1, s2) + 0.5 * cross(s2, s3);
         const D3 s4 = v2 - Q3, s5 = Q1 - Q3, s6 = v1 - Q3;
         const D3 f2 = 0.5 * cross(s4, s5) + 0.5 * cross(s5, s6);
-        const double air = dot(N, v2 - v1);
+        // one reciprocal of the diamond volume instead of three divisions (rounding only)
+        const double rair = 1 / dot(N, v2 - v1);
         const int gi1 = comp(vt, i1), gi2 = comp(vt, i2), gi3 = comp(vt, i3);
         const double VA = ld(wn + gi1), VB = ld(wn + gi2), VC = ld(wn + gi3), VD = VC;
         const double VL = own ? wi : vo, VR = own ? vo : wi;
         const double dAC = VA - VC, dBD = VB - VD, dRL = VR - VL;
-        const double fgx = (f1.x * dAC + f2.x * dBD + N.x * dRL) / air;
-        const double fgy = (f1.y * dAC + f2.y * dBD + N.y * dRL) / air;
-        const double fgz = (f1.z * dAC + f2.z * dBD + N.z * dRL) / air;
+        const double fgx = (f1.x * dAC + f2.x * dBD + N.x * dRL) * rair;
+        const double fgy = (f1.y * dAC + f2.y * dBD + N.y * dRL) * rair;
+        const double fgz = (f1.z * dAC + f2.z * dBD + N.z * dRL) * rair;
         v = p.Dxx * fgx * N.x + p.Dyy * fgy * N.y + p.Dzz * fgz * N.z;
       }
       q[j] = own ? v : -v;
@@ -1021,8 +1044,9 @@ inline bool compact_tables(const mb_mesh &m) {
          m.lsq_sell_idx && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
 }
 
-// cell scratch: [4][nbcells] planes gx, gy, gz, psi (face-table path) or [nbcells][4]
-// records {w, gx, gy, psi} (compact 2D path); node scratch: [nbnodes]
+// cell scratch: [4][nbcells] planes gx, gy, gz, psi (face-table path), [nbcells][4]
+// records {w, gx, gy, psi} (compact 2D path) or [nbcells][4] records {w, psi gx, psi gy,
+// psi gz} then [nbcells][4] rows {x, y, z, w} (compact 3D path); node scratch: [nbnodes]
 template <int DIM, bool O2, bool DF>
 int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                 double *w_out, const double *sign, const double *src, const double *dt, double *cs,
@@ -1034,7 +1058,7 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
     // 256-bit loads of [n][4] rows: the phase-1 records (2D) and the centre and vertex
     // tables (3D) must start on 32-byte boundaries
     auto a32 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 31) == 0; };
-    if ((DIM == 2 && O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord)))) return MB_EINVAL;
+    if ((O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord)))) return MB_EINVAL;
 #endif
 #if MB_V4_IO
     if (DIM == 2 && (reinterpret_cast<uintptr_t>(sign) & 31) != 0) return MB_EINVAL;
@@ -1046,7 +1070,10 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
       k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_BLOCK), MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign,
                                                                                     src, dt, cs, wn);
     } else {
-      if (ncb + nnb > 0) k_f3_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+      // cell scratch: records [0, 4 nbcells), rows [4 nbcells, 8 nbcells)
+      double *rows = cs ? cs + 4 * (long long)m.nbcells : nullptr;
+      if (O2) k_f3_pack<<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, w_in, rows);
+      if (ncb + nnb > 0) k_f3_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, rows, wn, ncb);
       k_f3_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_3D_BLOCK), MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out,
                                                                                           sign, src, dt, cs, wn);
     }
@@ -1239,7 +1266,7 @@ int mb_advdiff_batch_step(const mb_advdiff_item_f64 *items, const int32_t *p1_ma
 
 // ---------------------------------------------------------------- no-allocation variant
 //
-// mb_advdiff_step needs 4*nbcells + nbnodes doubles of scratch that the caller
+// mb_advdiff_step needs 4*nbcells (3D: 8*nbcells) + nbnodes doubles of scratch that the caller
 // allocates.  Some callers cannot allocate device memory at all: a plugin that
 // lives inside a host application owning every device allocation through its
 // own pool, a service that reserves its whole device-memory budget up front,
@@ -1263,7 +1290,7 @@ extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const 
                                        const double *w_in, double *w_out, const double *sign_cf,
                                        const double *src, const double *dt_dev, void *stream) {
   if (!mesh_ok(m) || !bc || !p) return MB_EINVAL;
-  const long long per_cell = m->dim == 2 ? 4 : 6;
+  const long long per_cell = m->dim == 2 ? 4 : 8;
   const long long need = per_cell * m->nbcells + m->nbnodes;
   if (need > (long long)MB_NOALLOC_SCRATCH_DOUBLES) return MB_ETOOBIG;
   int dev = 0;

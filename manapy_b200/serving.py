@@ -96,7 +96,37 @@ def initial_state(req, centers):
     return [h, zero, zero.copy(), zero.copy(), Z]
 
 
-def prepare(req):
+# tables the FP64 batched steps read beyond the FP32-compensated ones (the FP64
+# centre -> vertex weights)
+FP64_EXTRA_TABLES = ("n2c_sell_alpha",)
+
+# mesh tables each batched step dereferences, checked on the host before an item table
+# goes to the device (the kernels cannot check pointers that live in device memory)
+_NEEDS = {
+    ("advdiff", "fp32c"): ("cell_volume", "cell_order", "cell_vtx", "cell_nbr", "cell_flags", "node_coord", "cell_xy",
+                           "lsq_sell_ptr", "lsq_sell_idx", "n2c_sell_ptr", "n2c_sell_idx", "n2c_sell_alpha_f32",
+                           "ghostnid_ptr", "ghostnid_idx", "face_ghostcenter", "n2g_ptr", "n2g_idx", "n2g_alpha",
+                           "face_cellid", "face_dist"),
+    ("advdiff", "fp64"): ("cell_volume", "cell_order", "cell_vtx", "cell_nbr", "cell_flags", "node_coord", "cell_xy",
+                          "lsq_sell_ptr", "lsq_sell_idx", "n2c_sell_ptr", "n2c_sell_idx", "n2c_sell_alpha",
+                          "ghostnid_ptr", "ghostnid_idx", "face_ghostcenter", "n2g_ptr", "n2g_idx", "n2g_alpha",
+                          "face_cellid", "face_dist"),
+    ("sw", "fp32c"): ("cell_volume", "cell_order", "cell_faces", "cell_vtx", "cell_nbr", "cell_flags", "node_coord",
+                      "cell_xy", "cell_cellfid", "face_cellid", "face_nm_f32"),
+    ("sw", "fp64"): ("cell_volume", "cell_order", "cell_faces", "cell_vtx", "cell_nbr", "cell_flags", "node_coord",
+                     "cell_xy", "cell_cellfid", "face_cellid", "face_normal", "face_mesure"),
+}
+
+
+def check_item_tables(kind, precision, mesh_struct):
+    """Raise ValueError if a table the batched step of (kind, precision) reads is missing
+    from the mesh struct (a NULL pointer)."""
+    missing = [n for n in _NEEDS[(kind, precision)] if not getattr(mesh_struct, n)]
+    if missing:
+        raise ValueError("mesh tables missing for the %s %s batched step: %s" % (precision, kind, ", ".join(missing)))
+
+
+def prepare(req, precision="fp32c"):
     """Host work of one request (runs in a worker process): mesh, geometry, device tables
     (as host arrays), boundary rules and the initial state in the device numbering."""
     from . import boundary as B, meshgen
@@ -104,7 +134,7 @@ def prepare(req):
     el, vx = meshgen.square_triangles(req.n, seed=req.seed)
     dm = DeviceMesh.from_native(el, vx)       # the native host builder (C++)
     A = dm.A
-    dm.keep_only(DeviceMesh.SERVE_TABLES)
+    dm.keep_only(DeviceMesh.SERVE_TABLES + (FP64_EXTRA_TABLES if precision == "fp64" else ()))
     bc = None
     if req.kind == "advdiff":
         res = B.resolve(A, {s: "dirichlet" for s in SIDES}, {s: 0.0 for s in SIDES})
@@ -330,6 +360,7 @@ class BatchServer:
                 for k, s in enumerate(ad):
                     n1, ncb, n2 = s.blocks()
                     it = items[k]
+                    check_item_tables("advdiff", self.precision, s.dm.struct)
                     it.m, it.bc, it.p = s.dm.struct, s.bc.struct, s.params
                     it.w[0], it.w[1] = _p(s.w[0]), _p(s.w[1])
                     if not fp64:
@@ -351,6 +382,7 @@ class BatchServer:
                 for k, s in enumerate(sw):
                     nfb, ncb = s.blocks()
                     it = items[k]
+                    check_item_tables("sw", self.precision, s.dm.struct)
                     it.m = s.dm.struct
                     for par in range(2):
                         for c in range(4):
@@ -419,11 +451,11 @@ class BatchServer:
         if self.workers > 0:
             own = self.pool is None
             self.start_pool()
-            prepared = list(self.pool.map(prepare, requests))
+            prepared = list(self.pool.map(prepare, requests, [self.precision] * len(requests)))
             if own:
                 self.stop_pool()
         else:
-            prepared = [prepare(r) for r in requests]
+            prepared = [prepare(r, self.precision) for r in requests]
         for req, dm, bc, init in prepared:
             slot = self._admit(req, dm, bc, init)
             slot.fam = 0 if req.kind == "advdiff" else 1
@@ -472,9 +504,9 @@ class BatchServer:
                 while nxt < len(reqs) and reqs[nxt].arrival <= now:
                     r = reqs[nxt]
                     if pool is not None:
-                        futures[r.rid] = pool.submit(prepare, r)
+                        futures[r.rid] = pool.submit(prepare, r, self.precision)
                     else:
-                        prepared.append(prepare(r))
+                        prepared.append(prepare(r, self.precision))
                     nxt += 1
                 ta = time.perf_counter()
                 for rid in [k for k, f in futures.items() if f.done()]:

@@ -47,7 +47,7 @@ class ShardedAdvectionDiffusion:
         f64 = torch.float64
         self.w = [torch.zeros(nc, dtype=f64, device=self.dev) for _ in range(2)]
         self.cur = 0
-        self.cs = torch.empty((4 if dim == 2 else 6) * nc, dtype=f64, device=self.dev)
+        self.cs = torch.empty((4 if dim == 2 else 8) * nc, dtype=f64, device=self.dev)
         self.ns = torch.empty(nn, dtype=f64, device=self.dev)
         self.sign = torch.empty(4 * nc, dtype=f64, device=self.dev)
         self.dt = torch.zeros(1, dtype=f64, device=self.dev)

@@ -268,7 +268,7 @@ class AdvectionDiffusionSolver:
     def _scratch(self):
         dm = self._dm
         if getattr(self, "_cs", None) is None:
-            self._cs = torch.empty((4 if dm.dim == 2 else 6) * dm.nbcells, dtype=torch.float64, device=dm.device)
+            self._cs = torch.empty((4 if dm.dim == 2 else 8) * dm.nbcells, dtype=torch.float64, device=dm.device)
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
 
@@ -366,8 +366,11 @@ class AdvectionDiffusionSolver:
             check_state([self.var.dev("cell")], names=["the cell values"])
 
     def launches_per_step(self):
-        """Kernel launches of one fused step."""
-        return 1 + int(self.order == 2 or bool(self.diffusion))
+        """Kernel launches of one fused step (tetrahedra at order 2: a pack pass first)."""
+        n = 1 + int(self.order == 2 or bool(self.diffusion))
+        if self.dim == 3 and self.order == 2 and self.precision == "fp64":
+            n += 1
+        return n
 
     def release_graphs(self):
         self._graph = None

@@ -41,3 +41,29 @@ def test_prepare_gives_host_tables_in_device_order():
         ref = SV.initial_state(req, A["cells_center"])
         for a, r in zip(init, ref):
             assert np.array_equal(a, r[dm.R.cperm])
+
+
+def _struct_of(dm):
+    """An MbMesh whose pointer fields are non-NULL exactly for the tables ``dm`` holds."""
+    from manapy_b200 import _lib
+    s = _lib.MbMesh()
+    for name, _ in _lib.MbMesh._fields_:
+        if name in dm.t:
+            setattr(s, name, 1)
+    return s
+
+
+def test_batched_items_are_checked_for_the_tables_their_step_reads():
+    """The batched kernels read mesh tables through pointers held in device memory, which no
+    kernel can check: the server checks each item on the host.  A mesh prepared for the FP32c
+    batches lacks the FP64 centre->vertex weights of the FP64 batches."""
+    import pytest
+    for kind in ("advdiff", "sw"):
+        req = SV.Request(rid=0, kind=kind, n=10, seed=5, steps=10, ux=0.3, uy=0.1, D=1e-3)
+        for prec in ("fp32c", "fp64"):
+            _, dm, _, _ = SV.prepare(req, prec)
+            SV.check_item_tables(kind, prec, _struct_of(dm))
+        _, dm32, _, _ = SV.prepare(req, "fp32c")
+        if kind == "advdiff":
+            with pytest.raises(ValueError, match="n2c_sell_alpha"):
+                SV.check_item_tables(kind, "fp64", _struct_of(dm32))

@@ -44,7 +44,7 @@ def _setup(wl):
 def _regular(U, A, dm, db, prm, sign, dt, w_in, st):
     nc, nn = A["nbcells"], A["nbnodes"]
     out = U.Z(nc)
-    cell_scratch, node_scratch = U.Z((4 if A["dim"] == 2 else 6) * nc), U.Z(nn)
+    cell_scratch, node_scratch = U.Z((4 if A["dim"] == 2 else 8) * nc), U.Z(nn)
     U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w_in), U.P(out), U.P(sign), None, U.P(dt),
            U.P(cell_scratch), U.P(node_scratch), st)
     return out
@@ -74,7 +74,7 @@ def test_noalloc_size_gate_at_its_limit(wl, cuda):
     4*cells + nodes doubles, 3D 6*cells + nodes); a mesh exactly at the limit passes the
     size gate and is then refused for w_in == w_out (MB_EINVAL), before any launch."""
     U, A, dm, db, prm, sign, dt, w0, st = _setup(wl)
-    per_cell = 4 if wl.dim == 2 else 6
+    per_cell = 4 if wl.dim == 2 else 8
     limit = _lib.NOALLOC_SCRATCH_DOUBLES
     lib = _lib.lib()
     at = _lib.MbMesh.from_buffer_copy(dm.struct)
