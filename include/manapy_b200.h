@@ -445,6 +445,21 @@ typedef struct mb_sw_item_f64 {
 int mb_sw_batch_step(const mb_sw_item_f64 *items, const int32_t *face_map, int32_t face_blocks,
                      const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream);
 
+/* ---- halo exchange of a mesh sharded over ranks ---------------------------------------
+ *
+ * manapy exchanges halo values with MPI neighbourhood all-to-alls of per-rank send lists
+ * (manapy/comms/communication.py:93-145).  With every peer's list concatenated into one
+ * index list idx[n] (device, int64 cell indices, each at most once), mb_halo_pack writes
+ * buf[k*nfields + j] = fields[j][idx[k]] for the nfields fields (a host array of device
+ * pointers), and mb_halo_unpack writes fields[j][idx[k]] = buf[k*nfields + j]: one launch
+ * for all peers and fields on each side of the point-to-point transfers, each peer's
+ * entries one contiguous message. */
+#define MB_HALO_MAX_FIELDS 8
+int mb_halo_pack(double *const *fields, int32_t nfields, const int64_t *idx, int64_t n, double *buf,
+                 void *stream);
+int mb_halo_unpack(double *const *fields, int32_t nfields, const int64_t *idx, int64_t n, const double *buf,
+                   void *stream);
+
 /* Same step as mb_advdiff_step, for callers that cannot allocate device memory.
  *
  * No counterpart in the reference: manapy allocates its work arrays with numpy.

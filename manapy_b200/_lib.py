@@ -119,6 +119,8 @@ _SIGS = {
     "mb_advdiff_batch_step": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_check_state": [_vp, _vp, ctypes.c_int64, _i32, _vp, _vp],
+    "mb_halo_pack": [_vp, _i32, _vp, ctypes.c_int64, _vp, _vp],
+    "mb_halo_unpack": [_vp, _i32, _vp, ctypes.c_int64, _vp, _vp],
     "mb_build_info": [],
 }
 _RESTYPES = {"mb_build_info": ctypes.c_char_p}
@@ -160,6 +162,11 @@ def check(rc: int, name: str = "call"):
 
 def call(name, *args):
     check(getattr(lib(), name)(*args), name)
+
+
+def ptrs(addresses):
+    """A host array of device pointers (for the multi-field entry points)."""
+    return (_vp * len(addresses))(*addresses)
 
 
 def p5(ptrs):

@@ -218,38 +218,106 @@ class Domain:
         return np.array([[v[:, k].min(), v[:, k].max()] for k in range(int(self._dim))])
 
     # ------------------------------------------------------------------ output
-    def _save(self, on, dt, time, niter, miter, variables, values, file_format, path):
+    def _device_to_pinned(self, on, values):
+        """Start the copies of device-resident values (``Variable`` objects or CUDA tensors
+        in manapy's numbering) into pinned host buffers; returns (host arrays or pinned
+        tensors, event after which they are valid, or None).  Each Variable's array is
+        gathered into manapy's numbering on the current stream (ordered before any later
+        step that overwrites it); the device-to-host copies run on a side stream."""
+        import torch
+        from .variable import Variable
+        if not any(isinstance(v, Variable) or (isinstance(v, torch.Tensor) and v.is_cuda) for v in values):
+            return [v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v) for v in values], None
+        if getattr(self, "_io_stream", None) is None:
+            self._io_stream = torch.cuda.Stream(device=torch.device(self.device))
+        cur = torch.cuda.current_stream(torch.device(self.device))
+        staged = []
+        for v in values:
+            if isinstance(v, Variable):
+                t = v.dev(on)
+                kind = v._s.kind[on]
+                t = self.device_mesh.to_host_order(kind, t) if kind is not None else t
+                staged.append(t.clone() if t is v.dev(on) else t)
+            elif isinstance(v, torch.Tensor) and v.is_cuda:
+                staged.append(v.detach().to(torch.float64).clone())
+            else:
+                staged.append(np.asarray(v))
+        io = self._io_stream
+        io.wait_stream(cur)
+        out = []
+        with torch.cuda.stream(io):
+            for t in staged:
+                if isinstance(t, np.ndarray):
+                    out.append(t)
+                    continue
+                h = torch.empty(t.numel(), dtype=torch.float64, pin_memory=True)
+                h.copy_(t, non_blocking=True)
+                t.record_stream(io)         # the caching allocator keeps it until the copy ran
+                out.append(h)
+            ev = torch.cuda.Event()
+            ev.record(io)
+        return out, ev
+
+    def _save(self, on, dt, time, niter, miter, variables, values, file_format, path, asynchronous=False):
         from . import vtu
         if values is None:
             raise ValueError("value must be given")
         if file_format != "vtu":
             raise ValueError("only the vtu format is written")
         n = int(self.nbcells if on == "cell" else self.nbnodes)
-        vals = [v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v) for v in values]
-        assert len(vals[0]) == n, "value size != number of %ss" % on
+        vals, ev = self._device_to_pinned(on, values)
         k = 3 if self._dim == 2 else 4
         cells = self._A["cells_nodeid"][:, :k]
         points = self._A["nodes_vertex"][:, :3]
-        data = {variables[j]: vals[j] for j in range(len(vals))}
-        print(" **************************** Computing ****************************")
-        print("$$$$$$$$$$$$$$$$$$$$$$$$$$$$ Saving Results $$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$")
-        print("Iteration = ", niter, "time = ", time, "time step = ", dt)
-        print("max" + variables[0] + " =", float(np.max(vals[0])))
-        piece = "visu%d-%d.vtu" % (self._comm.Get_rank(), miter)
-        vtu.write_vtu(os.path.join(path, piece), points, cells,
-                      cell_data=data if on == "cell" else None, point_data=data if on == "node" else None)
-        vtu.write_pvtu(os.path.join(path, "visu%d.pvtu" % miter), [piece], list(variables), on=on)
+        rank = self._comm.Get_rank()
+
+        def write():
+            if ev is not None:
+                ev.synchronize()
+            arrs = [np.asarray(v.numpy() if hasattr(v, "numpy") else v, dtype=np.float64) for v in vals]
+            assert len(arrs[0]) == n, "value size != number of %ss" % on
+            data = {variables[j]: arrs[j] for j in range(len(arrs))}
+            print(" **************************** Computing ****************************")
+            print("$$$$$$$$$$$$$$$$$$$$$$$$$$$$ Saving Results $$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$$")
+            print("Iteration = ", niter, "time = ", time, "time step = ", dt)
+            print("max" + variables[0] + " =", float(np.max(arrs[0])))
+            piece = "visu%d-%d.vtu" % (rank, miter)
+            vtu.write_vtu(os.path.join(path, piece), points, cells,
+                          cell_data=data if on == "cell" else None, point_data=data if on == "node" else None)
+            vtu.write_pvtu(os.path.join(path, "visu%d.pvtu" % miter), [piece], list(variables), on=on)
+
+        if not asynchronous:
+            write()
+            return None
+        if getattr(self, "_writer", None) is None:
+            import concurrent.futures as cf
+            self._writer = cf.ThreadPoolExecutor(max_workers=1)
+            self._pending = []
+        fut = self._writer.submit(write)
+        self._pending.append(fut)
+        return fut
+
+    def wait_saves(self):
+        """Block until every asynchronous save has been written (re-raises a writer error)."""
+        for f in getattr(self, "_pending", []):
+            f.result()
+        self._pending = []
 
     def save_on_cell_multi(self, dt=0, time=0, niter=0, miter=0, variables=None, values=None, file_format="vtu",
-                           path="results"):
+                           path="results", asynchronous=False):
         """Cell fields to ``results/visu<rank>-<miter>.vtu`` + ``visu<miter>.pvtu``
-        (``manapy/ddm/domain.py:784-849``); values may be device tensors."""
-        self._save("cell", dt, time, niter, miter, variables, values, file_format, path)
+        (``manapy/ddm/domain.py:784-849``).  ``values``: host arrays as in manapy, or
+        device-resident ``Variable`` objects / CUDA tensors (manapy numbering), which are
+        copied to pinned host memory off the compute stream.  ``asynchronous=True`` (no
+        counterpart in manapy) returns at once with a future; the file is written by a
+        background thread once the copies have run, while later steps proceed
+        (``wait_saves()`` joins)."""
+        return self._save("cell", dt, time, niter, miter, variables, values, file_format, path, asynchronous)
 
     def save_on_node_multi(self, dt=0, time=0, niter=0, miter=0, variables=None, values=None, file_format="vtu",
-                           path="results"):
+                           path="results", asynchronous=False):
         """Node fields, as ``save_on_cell_multi`` (``manapy/ddm/domain.py:735-782``)."""
-        self._save("node", dt, time, niter, miter, variables, values, file_format, path)
+        return self._save("node", dt, time, niter, miter, variables, values, file_format, path, asynchronous)
 
     def __str__(self):
         return ("\n> dim   :: %d\n> total cells  :: %d\n> total nodes  :: %d\n> total faces  :: %d\n"

@@ -103,11 +103,16 @@ def build_shards(elements, vertex, dim, nparts, A=None, layers=2):
 
 
 class HaloExchange:
-    """Refresh the halo entries of a per-rank cell array from their owners.
+    """Refresh the halo entries of per-rank cell arrays from their owners.
 
-    Point-to-point sends and receives (``torch.distributed.batch_isend_irecv``) of the
-    packed values, peers in ascending rank order on every rank; with the NCCL backend
-    the buffers stay on the device, with gloo they are staged through host memory.
+    Every peer's send list (and receive list) is concatenated, peers in ascending rank
+    order; an exchange packs all fields for all peers with one launch
+    (``mb_halo_pack``: buffer [entry][field], each peer's entries one contiguous
+    message), sends and receives one message per peer
+    (``torch.distributed.batch_isend_irecv``), and scatters the received buffer with one
+    launch (``mb_halo_unpack``).  With the NCCL backend the buffers stay on the device;
+    with gloo they are staged through host memory.  CPU fields (the oracle-driven tests)
+    are packed with index operations on the host.
     """
 
     def __init__(self, shard, group=None, device=None):
@@ -118,31 +123,58 @@ class HaloExchange:
         self.rank = shard.rank
         self.device = device
         self.peers = sorted(set(shard.send) | set(shard.recv))
+        empty = np.zeros(0, np.int64)
+        send = [np.asarray(shard.send.get(q, empty), np.int64) for q in self.peers]
+        recv = [np.asarray(shard.recv.get(q, empty), np.int64) for q in self.peers]
+        self.send_n = [len(a) for a in send]
+        self.recv_n = [len(a) for a in recv]
         to = (lambda a: torch.from_numpy(a).to(device)) if device is not None else torch.from_numpy
-        self.send_idx = {q: to(shard.send.get(q, np.zeros(0, np.int64))) for q in self.peers}
-        self.recv_idx = {q: to(shard.recv.get(q, np.zeros(0, np.int64))) for q in self.peers}
+        self.send_idx = to(np.concatenate(send) if send else empty)
+        self.recv_idx = to(np.concatenate(recv) if recv else empty)
         backend = dist.get_backend(group)
         self.stage = backend == "gloo"
 
-    def exchange(self, field):
-        """In place: field[halo] = owners' values (field: 1-D tensor over the submesh cells)."""
+    def exchange(self, fields):
+        """In place: fields[halo] = owners' values.  ``fields``: one 1-D float64 tensor over
+        the submesh cells, or a list of them (exchanged together)."""
         import torch
+        from . import _lib
         dist = self.dist
-        ops, recv = [], {}
-        for q in self.peers:
-            s = field.index_select(0, self.send_idx[q])
-            r = torch.empty(len(self.recv_idx[q]), dtype=field.dtype, device=field.device)
-            if self.stage:
-                s, r = s.cpu(), r.cpu()
-            recv[q] = r
-            if len(s):
-                ops.append(dist.P2POp(dist.isend, s, q, group=self.group))
-            if len(r):
-                ops.append(dist.P2POp(dist.irecv, r, q, group=self.group))
+        single = isinstance(fields, torch.Tensor)
+        fl = [fields] if single else list(fields)
+        nf = len(fl)
+        ns, nr = int(sum(self.send_n)), int(sum(self.recv_n))
+        dev = fl[0].device
+        cuda = dev.type == "cuda"
+        st = torch.cuda.current_stream(dev).cuda_stream if cuda else None
+        ptrs = _lib.ptrs([t.data_ptr() for t in fl]) if cuda else None
+        if cuda:
+            sbuf = torch.empty(ns * nf, dtype=torch.float64, device=dev)
+            _lib.call("mb_halo_pack", ptrs, nf, self.send_idx.data_ptr(), ns, sbuf.data_ptr(), st)
+        else:
+            sbuf = torch.stack([f.index_select(0, self.send_idx) for f in fl], dim=1).reshape(-1)
+        rbuf = torch.empty(nr * nf, dtype=torch.float64, device=dev)
+        if self.stage and cuda:
+            sbuf, rdev, rbuf = sbuf.cpu(), rbuf, rbuf.cpu()
+        ops = []
+        so = ro = 0
+        for q, n_s, n_r in zip(self.peers, self.send_n, self.recv_n):
+            if n_s:
+                ops.append(dist.P2POp(dist.isend, sbuf[so * nf:(so + n_s) * nf], q, group=self.group))
+            if n_r:
+                ops.append(dist.P2POp(dist.irecv, rbuf[ro * nf:(ro + n_r) * nf], q, group=self.group))
+            so += n_s
+            ro += n_r
         if ops:
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
-        for q in self.peers:
-            if len(recv[q]):
-                field.index_copy_(0, self.recv_idx[q], recv[q].to(field.device))
-        return field
+        if cuda:
+            if self.stage:
+                rdev.copy_(rbuf)
+                rbuf = rdev
+            _lib.call("mb_halo_unpack", ptrs, nf, self.recv_idx.data_ptr(), nr, rbuf.data_ptr(), st)
+        else:
+            r = rbuf.view(nr, nf)
+            for j, f in enumerate(fl):
+                f.index_copy_(0, self.recv_idx, r[:, j].contiguous())
+        return fields

@@ -98,3 +98,35 @@ def test_compile_rejects_unknown_kernels_and_foreign_tables(cuda):
         f(np.zeros(dom.nbfaces), np.zeros(dom.nbcells), np.zeros((3, 4), np.int32), 2)
     with pytest.raises(TypeError):
         f(np.zeros(dom.nbfaces))
+
+
+def test_maintainer_path_with_a_reference_built_domain(cuda):
+    """CUDABackend.for_manapy_domain on the Domain arrays manapy itself built (dom2d.npz):
+    the kernels take manapy's argument lists with the mesh tables of that Domain and give
+    the oracle's results (the oracle runs on this package's host tables, which
+    tests/test_backend_maintainer.py shows equal manapy's)."""
+    import types
+    from manapy_b200.backend import CUDABackend
+    g = golden("dom2d")
+    md = types.SimpleNamespace(dim=2, cells=types.SimpleNamespace(nodeid=g["cells_nodeid"]),
+                               nodes=types.SimpleNamespace(vertex=g["nodes_vertex"]))
+    be = CUDABackend.for_manapy_domain(md)
+    A = be.domain.host_arrays
+    m = O.Mesh(A)
+    rng = np.random.default_rng(3)
+    w = rng.standard_normal(m.nc)
+    ghost = rng.standard_normal(m.nf)
+    z = np.zeros(0)
+    zi = np.zeros((0, 2), np.int32)
+    gx, gy, gz = (np.zeros(m.nc) for _ in range(3))
+    # arguments as manapy's Variable.compute_cell_gradient passes them, from manapy's Domain
+    be.compile(_fn("cell_gradient_2d"))(w, ghost, z, z, g["cells_center"], g["cells_cellnid"], g["cells_ghostnid"],
+                                         zi, zi, g["cells_nodeid"], zi, zi, g["faces_ghostcenter"], z,
+                                         g["nodes_vertex"], z, z, gx, gy, gz)
+    ox, oy, oz = (np.zeros(m.nc) for _ in range(3))
+    O.cell_gradient(m, w, ghost, ox, oy, oz)
+    assert rel_max(gx, ox) < 1e-13 and rel_max(gy, oy) < 1e-13
+    uc = np.zeros(m.nc)
+    uf = rng.standard_normal(m.nf)
+    be.compile(_fn("facetocell"))(uf, uc, g["cells_faceid"], 2)
+    assert rel_max(uc, O.facetocell(m, uf)) <= 1e-15
