@@ -50,7 +50,7 @@ typedef struct mb_mesh {
   int32_t nbfaces;
   int32_t nbnodes;
   int32_t nlf;       /* faces per cell: 3 or 4 */
-  int32_t pad_;
+  int32_t tile_max_halo; /* largest tile halo of the tile tables below (0: none) */
   /* cells */
   const double *cell_center;    /* [nbcells][3] */
   const double *cell_volume;    /* [nbcells] */
@@ -115,6 +115,19 @@ typedef struct mb_mesh {
   const float *n2c_sell_alpha_f32;
   /* [nbfaces][4] = {n_x, n_y, 1/mesure, 0} rounded to FP32 (FP32-compensated shallow water, 2D) */
   const float *face_nm_f32;
+  /* tile tables of the shared-memory-staged first phase (all NULL: unstaged).  Tile t is
+   * cells [256 t, 256 t + 256); local index of own cell c: c - 256 t, of halo entry p:
+   * 256 + p.  tile_halo_ptr [ntiles+1] / tile_halo_idx: each tile's halo cells (the
+   * cells its stencils read outside it); lsq_loc: the lsq SELL-32 stencils as local
+   * indices (padding 0xFFFF: the cell itself); tile_node_ptr [ntiles+1] /
+   * tile_node_idx: the nodes whose smallest incident cell is in the tile; n2c_loc: the
+   * local index, in the node's tile, of each n2c incidence (n2c_idx order). */
+  const int32_t *tile_halo_ptr;
+  const int32_t *tile_halo_idx;
+  const uint16_t *lsq_loc;
+  const int32_t *tile_node_ptr;
+  const int32_t *tile_node_idx;
+  const uint16_t *n2c_loc;
 } mb_mesh;
 
 typedef struct mb_bc {
