@@ -336,6 +336,12 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
                                function is commented out, manapy/boundary/bc.py:68-72): the mass
                                flux through a wall vanishes up to rounding */
 
+/* The CFL dt of a shallow-water state with the fused step's formula (the next-step dt
+ * that mb_sw_step writes into dt_next, manapy/solvers/shallowater/fvm_utils.py:16-42
+ * without diffusion): *dt_dev = min over cells.  Needs the compact 2D tables. */
+int mb_sw_dt(const mb_mesh *m, const double *h, const double *hu, const double *hv, double cfl, double grav,
+             double *dt_dev, void *stream);
+
 /* mb_sw_step with a choice of wall treatment (walls: MB_WALLS_*); mb_sw_step is this with
  * MB_WALLS_NEUMANN. */
 int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q_out[5],

@@ -116,6 +116,7 @@ _SIGS = {
     "mb_advdiff_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step_f32c": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],
+    "mb_sw_dt": [_M, _vp, _vp, _vp, _d, _d, _vp, _vp],
     "mb_sw_step_ex": [_M, _P5, _P5, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
     "mb_sw_step_f32c_ex": [_M, _P5, _P5, _P4, _P4, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp],
     "mb_advdiff_batch_step": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],

@@ -575,6 +575,55 @@ __global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS) k_sw2
   sw2_flux_face<ORDER2, FAST>(m, s, grav, ff, f);
 }
 
+// CFL dt candidate of a cell (manapy/solvers/shallowater/fvm_utils.py:16-42, without
+// diffusion) from its state and its three face normals, written with explicit
+// round-to-nearest operations: no multiply-add is contracted, so every kernel that calls
+// it (the fused step's next dt, mb_sw_dt) gives the same bits.
+__device__ __forceinline__ double sw_dt_candidate(double h, double hu, double hv, const double n0[3],
+                                                  const double n1[3], double vol, double cfl, double grav) {
+  const double velson = __dsqrt_rn(__dmul_rn(grav, h));
+  const double u = __ddiv_rn(hu, h), v = __ddiv_rn(hv, h);
+  double lam = 0.;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double mes = __dsqrt_rn(__dadd_rn(__dmul_rn(n0[j], n0[j]), __dmul_rn(n1[j], n1[j])));  // faces.mesure
+    const double u_n = fabs(__dadd_rn(__dmul_rn(u, n0[j]), __dmul_rn(v, n1[j])));
+    lam = __dadd_rn(lam, __dmul_rn(__dadd_rn(__ddiv_rn(u_n, mes), velson), mes));
+  }
+  return __ddiv_rn(__dmul_rn(cfl, vol), lam);
+}
+
+// the three stored face normals of cell i (exact), from the compact 2D tables
+__device__ __forceinline__ void sw_cell_normals(const mb_mesh &m, int i, double n0[3], double n1[3]) {
+  const int4 vt = __ldg(reinterpret_cast<const int4 *>(m.cell_vtx + 4 * i));
+  const uint32_t fl = ld(m.cell_flags + i);
+  const double2 P0 = __ldg(reinterpret_cast<const double2 *>(m.node_coord + 2 * vt.x));
+  const double2 P1 = __ldg(reinterpret_cast<const double2 *>(m.node_coord + 2 * vt.y));
+  const double2 P2 = __ldg(reinterpret_cast<const double2 *>(m.node_coord + 2 * vt.z));
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const bool rev = (fl >> (3 + j)) & 1u;
+    const double2 Pj = j == 0 ? P0 : (j == 1 ? P1 : P2), Pk = j == 0 ? P1 : (j == 1 ? P2 : P0);
+    const double2 Xa = rev ? Pk : Pj, Xb = rev ? Pj : Pk;
+    double x = Xa.y - Xb.y, y = Xb.x - Xa.x;
+    if ((fl >> (6 + j)) & 1u) { x = -1 * x; y = -1 * y; }
+    n0[j] = x;
+    n1[j] = y;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_sw_dt(mb_mesh m, const double *h, const double *hu, const double *hv,
+                                                  double cfl, double grav, double *dt) {
+  double best = 1e300;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nbcells; i += gridDim.x * blockDim.x) {
+    double n0[3], n1[3];
+    sw_cell_normals(m, i, n0, n1);
+    best = pmin(best, sw_dt_candidate(ld(h + i), ld(hu + i), ld(hv + i), n0, n1, ld(m.cell_volume + i), cfl, grav));
+  }
+  best = block_min(best);
+  if (threadIdx.x == 0 && best < 1e300) atomic_min_pos(dt, best);
+}
+
 // flags of the compact 2D layout (cell_flags): bit j own, 3+j node order, 6+j normal
 // flipped, 9+j the cell's outward normal table (cells.nf) holds minus the face normal
 __device__ __forceinline__ double sw2_cell_body(const mb_mesh &m, const SWState &s, const SWQ &out, const double *ff,
@@ -705,15 +754,7 @@ __device__ __forceinline__ double sw2_cell_body(const mb_mesh &m, const SWState 
   if (out.q[4] != s.q[4]) out.q[4][i] = Z_i;  // the bed does not move
   // next step's dt from the updated state (manapy/solvers/shallowater/fvm_utils.py:16-42)
   if (!want_dt) return 1e300;
-  const double velson = sqrt(grav * h_n);
-  double lam = 0.;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const double mes = sqrt(__dadd_rn(__dmul_rn(n0[j], n0[j]), __dmul_rn(n1[j], n1[j])));  // faces.mesure
-    const double u_n = fabs(hu_n / h_n * n0[j] + hv_n / h_n * n1[j]);
-    lam += (u_n / mes + velson) * mes;
-  }
-  return cfl * vol / lam;
+  return sw_dt_candidate(h_n, hu_n, hv_n, n0, n1, vol, cfl, grav);
 }
 
 __global__ void __launch_bounds__(kBlock) k_srnh_batch(int n, const double *st, const double *nrm,
@@ -907,6 +948,15 @@ int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q
     k_sw2_flux<false, MB_SW_FAST><<<fb, MB_SW_FLUX_BLOCK, 0, st>>>(*m, s, grav, face_flux, dt_next);
   }
   k_sw2_cell<<<ceil_div(m->nbcells, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_cur, dt_next, cfl, grav);
+  return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_sw_dt(const mb_mesh *m, const double *h, const double *hu, const double *hv, double cfl, double grav,
+             double *dt_dev, void *stream) {
+  if (!sw_mesh_ok(m) || !h || !hu || !hv || !dt_dev || !m->cell_vtx || !m->cell_flags || !m->node_coord)
+    return MB_EINVAL;
+  k_fill_sw<<<1, 1, 0, ST(stream)>>>(dt_dev, 1e6);
+  k_sw_dt<<<grid_for_sw(m->nbcells), kBlock, 0, ST(stream)>>>(*m, h, hu, hv, cfl, grav, dt_dev);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }
 

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import reorder
 
-__all__ = ["partition_cells", "Shard", "build_shards", "HaloExchange"]
+__all__ = ["partition_cells", "Shard", "build_shards", "HaloExchange", "RankFailure", "FailureMonitor"]
 
 
 def partition_cells(center, dim, nparts):
@@ -68,9 +68,14 @@ class Shard:
         return int(self.owned.sum())
 
 
-def build_shards(elements, vertex, dim, nparts, A=None, layers=2):
+def build_shards(elements, vertex, dim, nparts, A=None, layers=2, extra_cells=None):
     """The ``nparts`` shards of a mesh.  ``A``: its ``geometry.build`` arrays (built if
-    not given; only the cell centres and vertex-neighbour lists are read)."""
+    not given; only the cell centres and vertex-neighbour lists are read).  ``extra_cells``:
+    global cells every shard also holds (as halo unless it owns them) -- the shallow-water
+    source term reads the last cell of the mesh for the padding of ``cells.cellfid``
+    (``manapy/solvers/shallowater/fvm_utils.py:95-96``, a negative-index wrap), so those
+    shards hold global cell ``nc - 1``, which stays their last cell because shards keep
+    global order."""
     from . import geometry
     if A is None:
         A = geometry.build(elements, vertex, dim)
@@ -83,6 +88,8 @@ def build_shards(elements, vertex, dim, nparts, A=None, layers=2):
         cur = own.copy()
         for _ in range(layers):
             cur |= _neighbours(A["cellnid_ptr"], A["cellnid_idx"], cur)
+        if extra_cells is not None:
+            cur[np.asarray(extra_cells, dtype=np.int64)] = True
         cells = np.nonzero(cur)[0]
         nodes = np.unique(elements[cells, :k])
         local = np.searchsorted(nodes, elements[cells, :k]).astype(np.int32)
@@ -178,3 +185,77 @@ class HaloExchange:
             for j, f in enumerate(fl):
                 f.index_copy_(0, self.recv_idx, r[:, j].contiguous())
         return fields
+
+
+class RankFailure(RuntimeError):
+    """Another rank of the sharded run failed (reported through the store)."""
+
+
+class FailureMonitor:
+    """Host-side failure detection of a sharded run (no counterpart in manapy, whose MPI
+    ranks abort together).  A rank that fails inside ``guard()`` posts an abort record in
+    the process group's key-value store before it leaves; every rank calls ``check()``
+    before it launches a step, so the others raise ``RankFailure`` instead of waiting in
+    their next exchange.  A rank that dies without posting (killed) is caught by the
+    process group's timeout in the next exchange, which raises on the survivors.
+    No GPU fault is involved: ranks leave only between steps."""
+
+    KEY = "manapy_b200/abort"
+    STEP = "manapy_b200/step/%d"
+
+    def __init__(self, rank, store=None, world=None, timeout=10.0):
+        import torch.distributed as dist
+        self.rank = rank
+        if store is None:
+            store = dist.distributed_c10d._get_default_store()
+        self.store = store
+        self.world = dist.get_world_size() if world is None else int(world)
+        self.timeout = float(timeout)
+
+    def check(self):
+        """Raise RankFailure if a rank has posted a failure (one store lookup, no wait)."""
+        if self.store.check([self.KEY]):
+            raise RankFailure(self.store.get(self.KEY).decode())
+
+    def sync(self, step):
+        """Heartbeat between steps: post this rank's arrival at ``step`` and wait until every
+        rank has arrived; raise RankFailure as soon as a failure is posted, or when a rank has
+        not arrived within ``timeout`` seconds (it died without posting)."""
+        import time
+        key = self.STEP % step
+        self.store.add(key, 1)
+        deadline = time.monotonic() + self.timeout
+        wait = 1e-4
+        while True:
+            self.check()
+            if self.store.add(key, 0) >= self.world:
+                break
+            if time.monotonic() > deadline:
+                raise RankFailure("rank(s) did not reach step %d within %.1f s" % (step, self.timeout))
+            time.sleep(wait)
+            wait = min(2 * wait, 0.01)
+        if step >= 2 and self.rank == 0:
+            try:
+                self.store.delete_key(self.STEP % (step - 2))   # every rank is past it
+            except Exception:
+                pass
+
+    def signal(self, reason):
+        try:
+            self.store.set(self.KEY, "rank %d left: %s" % (self.rank, reason))
+        except Exception:      # the store itself may be gone; the timeout still ends the run
+            pass
+
+    def guard(self):
+        import contextlib
+
+        @contextlib.contextmanager
+        def _guard():
+            try:
+                yield self
+            except RankFailure:
+                raise
+            except BaseException as e:
+                self.signal("%s: %s" % (type(e).__name__, e))
+                raise
+        return _guard()

@@ -1,11 +1,16 @@
-"""One advection-diffusion mesh sharded over ranks (one process per GPU).
+"""One mesh sharded over ranks (one process per GPU): advection-diffusion and shallow water.
 
 Each rank builds its shard (``partition.build_shards``: owned cells plus a two-layer
 halo), runs the fused CUDA step on it, and refreshes its halo from the owners after
-every step (``partition.HaloExchange``: NCCL point-to-point on device buffers, or gloo
-through host memory).  dt is the min over ranks of each rank's CFL dt
-(``manapy/solvers/advecdiff/system.py:152``: manapy's ``allreduce(MIN)``).  The owned
+every step (``partition.HaloExchange``: all fields of all peers packed by one launch,
+NCCL point-to-point on device buffers, or gloo through host memory).  dt is the min over
+ranks of each rank's CFL dt (``manapy/solvers/advecdiff/system.py:152`` and
+``manapy/solvers/shallowater/system.py:188``: manapy's ``allreduce(MIN)``).  The owned
 cells' results are bit-identical to the single-GPU run of the whole mesh.
+
+Before each step every rank checks the run's failure record (``partition.FailureMonitor``):
+a rank that failed between steps has posted it, and the others raise ``RankFailure``
+instead of entering an exchange that would wait for it.
 """
 from __future__ import annotations
 
@@ -15,46 +20,39 @@ import torch
 from . import _lib, boundary as B, geometry as G, partition as P
 from .device import DeviceBC, DeviceMesh
 
-__all__ = ["ShardedAdvectionDiffusion"]
+__all__ = ["ShardedAdvectionDiffusion", "ShardedShallowWater"]
 
 
 def _p(t):
     return t.data_ptr() if t is not None else None
 
 
-class ShardedAdvectionDiffusion:
-    """``elements``/``vertex``: the whole mesh (every rank reads it, as every manapy rank
-    reads the partition it owns); ``velocity``: f(face_centres) -> (u, v, w) face arrays;
-    options as ``AdvectionDiffusionSolver`` (Dxx, Dyy, Dzz, order, cfl)."""
+class _Sharded:
+    """Shard, device mesh, halo exchange and failure monitor of one rank."""
 
-    def __init__(self, elements, vertex, dim, BC, values, velocity, Dxx=0., Dyy=0., Dzz=0., order=1, cfl=0.4,
-                 group=None, device=None):
+    def __init__(self, elements, vertex, dim, group, device, store, extra_cells=None, sync_every=0):
         import torch.distributed as dist
         self.dist, self.group = dist, group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.dim = dim
-        self.shard = P.build_shards(elements, vertex, dim, self.world)[self.rank]
+        self.shard = P.build_shards(elements, vertex, dim, self.world, extra_cells=extra_cells)[self.rank]
         A = G.build(self.shard.elements, self.shard.vertex, dim, halo_rim=True)
         self.A = A
         self.dm = DeviceMesh(A, self.dev)
-        self.bc = DeviceBC(A, B.resolve(A, BC, values), self.dev, mesh=self.dm)
-        self.params = _lib.MbAdvDiffParams(int(order), int(not (Dxx == Dyy == Dzz == 0)), float(Dxx), float(Dyy),
-                                           float(Dzz))
-        self.order = int(order)
-        nc, nn = self.dm.nbcells, self.dm.nbnodes
-        f64 = torch.float64
-        self.w = [torch.zeros(nc, dtype=f64, device=self.dev) for _ in range(2)]
-        self.cur = 0
-        self.cs = torch.empty((4 if dim == 2 else 8) * nc, dtype=f64, device=self.dev)
-        self.ns = torch.empty(nn, dtype=f64, device=self.dev)
-        self.sign = torch.empty(4 * nc, dtype=f64, device=self.dev)
-        self.dt = torch.zeros(1, dtype=f64, device=self.dev)
-        # halo indices in the device numbering of the shard
         inv = self.dm.inv["cell"].cpu().numpy()
         self.exchanger = P.HaloExchange(self._to_device_numbering(inv), group, device=self.dev)
-        self._set_velocity(velocity, Dxx, Dyy, Dzz, cfl)
+        self.monitor = P.FailureMonitor(self.rank, store, world=self.world)
+        self.sync_every = int(sync_every)    # heartbeat every this many steps (0: failure check only)
+        self.steps_done = 0
+
+    def _before_step(self):
+        if self.sync_every and self.steps_done % self.sync_every == 0:
+            self.monitor.sync(self.steps_done)
+        else:
+            self.monitor.check()
+        self.steps_done += 1
 
     def _staged(self):
         return self.dist.get_backend(self.group) == "gloo"
@@ -67,6 +65,60 @@ class ShardedAdvectionDiffusion:
 
     def _stream(self):
         return torch.cuda.current_stream(self.dev).cuda_stream
+
+    def _all_min(self, t):
+        d = t.cpu() if self._staged() else t
+        self.dist.all_reduce(d, op=self.dist.ReduceOp.MIN, group=self.group)
+        if self._staged():
+            t.copy_(d)
+
+    def _local(self, a_global):
+        loc = torch.from_numpy(np.ascontiguousarray(np.asarray(a_global)[self.shard.cells], dtype=np.float64))
+        out = torch.empty(len(loc), dtype=torch.float64, device=self.dev)
+        self.dm.to_device_order("cell", loc.to(self.dev), out)
+        return out
+
+    def _owned(self, t):
+        host = self.dm.to_host_order("cell", t).cpu().numpy()
+        return self.shard.cells[self.shard.owned], host[self.shard.owned]
+
+    def _gather(self, t):
+        ids, vals = self._owned(t)
+        parts = [None] * self.world
+        self.dist.all_gather_object(parts, (ids, vals), group=self.group)
+        n = sum(len(p[0]) for p in parts)
+        out = np.empty(n)
+        for ids_, vals_ in parts:
+            out[ids_] = vals_
+        return out
+
+    def advance(self, n):
+        for _ in range(int(n)):
+            self.step()
+
+
+class ShardedAdvectionDiffusion(_Sharded):
+    """``elements``/``vertex``: the whole mesh (every rank reads it, as every manapy rank
+    reads the partition it owns); ``velocity``: f(face_centres) -> (u, v, w) face arrays;
+    options as ``AdvectionDiffusionSolver`` (Dxx, Dyy, Dzz, order, cfl)."""
+
+    def __init__(self, elements, vertex, dim, BC, values, velocity, Dxx=0., Dyy=0., Dzz=0., order=1, cfl=0.4,
+                 group=None, device=None, store=None, sync_every=0):
+        super().__init__(elements, vertex, dim, group, device, store, sync_every=sync_every)
+        A = self.A
+        self.bc = DeviceBC(A, B.resolve(A, BC, values), self.dev, mesh=self.dm)
+        self.params = _lib.MbAdvDiffParams(int(order), int(not (Dxx == Dyy == Dzz == 0)), float(Dxx), float(Dyy),
+                                           float(Dzz))
+        self.order = int(order)
+        nc, nn = self.dm.nbcells, self.dm.nbnodes
+        f64 = torch.float64
+        self.w = [torch.zeros(nc, dtype=f64, device=self.dev) for _ in range(2)]
+        self.cur = 0
+        self.cs = torch.empty((4 if dim == 2 else 8) * nc, dtype=f64, device=self.dev)
+        self.ns = torch.empty(nn, dtype=f64, device=self.dev)
+        self.sign = torch.empty(4 * nc, dtype=f64, device=self.dev)
+        self.dt = torch.zeros(1, dtype=f64, device=self.dev)
+        self._set_velocity(velocity, Dxx, Dyy, Dzz, cfl)
 
     def _dev_faces(self, a):
         t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.dev)
@@ -83,40 +135,74 @@ class ShardedAdvectionDiffusion:
             _lib.call("mb_facetocell", self.dm.struct, _p(f), _p(c), st)
         _lib.call("mb_time_step", self.dm.struct, *[_p(c) for c in cells], float(cfl), float(Dxx), float(Dyy),
                   float(Dzz), _p(self.dt), st)
-        # global dt: the min over ranks
-        d = self.dt.cpu() if self._staged() else self.dt
-        self.dist.all_reduce(d, op=self.dist.ReduceOp.MIN, group=self.group)
-        if self._staged():
-            self.dt.copy_(d)
+        self._all_min(self.dt)      # steady velocity: the global dt once
 
     def set_cells(self, w_global):
         """The state from a whole-mesh cell array (manapy numbering)."""
-        loc = torch.from_numpy(np.ascontiguousarray(np.asarray(w_global)[self.shard.cells], dtype=np.float64))
-        self.dm.to_device_order("cell", loc.to(self.dev), self.w[self.cur])
+        self.w[self.cur].copy_(self._local(w_global))
 
     def step(self):
-        x, y = self.w[self.cur], self.w[1 - self.cur]
-        _lib.call("mb_advdiff_step", self.dm.struct, self.bc.struct, self.params, _p(x), _p(y), _p(self.sign), None,
-                  _p(self.dt), _p(self.cs), _p(self.ns), self._stream())
-        self.cur = 1 - self.cur
-        self.exchanger.exchange(self.w[self.cur])
-
-    def advance(self, n):
-        for _ in range(int(n)):
-            self.step()
+        self._before_step()
+        with self.monitor.guard():
+            x, y = self.w[self.cur], self.w[1 - self.cur]
+            _lib.call("mb_advdiff_step", self.dm.struct, self.bc.struct, self.params, _p(x), _p(y), _p(self.sign),
+                      None, _p(self.dt), _p(self.cs), _p(self.ns), self._stream())
+            self.cur = 1 - self.cur
+            self.exchanger.exchange(self.w[self.cur])
 
     def owned_values(self):
         """(global cell ids, values) of the cells this rank owns."""
-        host = self.dm.to_host_order("cell", self.w[self.cur]).cpu().numpy()
-        return self.shard.cells[self.shard.owned], host[self.shard.owned]
+        return self._owned(self.w[self.cur])
 
     def gather(self):
         """The whole-mesh cell array on every rank (manapy numbering)."""
-        ids, vals = self.owned_values()
-        parts = [None] * self.world
-        self.dist.all_gather_object(parts, (ids, vals), group=self.group)
-        n = sum(len(p[0]) for p in parts)
-        out = np.empty(n)
-        for ids_, vals_ in parts:
-            out[ids_] = vals_
-        return out
+        return self._gather(self.w[self.cur])
+
+
+class ShardedShallowWater(_Sharded):
+    """First-order shallow water (SRNH flux, bathymetry source) on one sharded triangle
+    mesh, as ``ShallowWaterSolver`` with its default Neumann walls (or ``walls=
+    "reflective"``).  Per step: dt of the current state over the rank's cells (owned and
+    halo, whose values are the owners' after the last exchange) with the fused step's
+    formula, min over ranks; the fused step; the exchange of h, hu, hv, hc."""
+
+    def __init__(self, elements, vertex, cfl=0.8, grav=9.81, walls="neumann", group=None, device=None, store=None,
+                 sync_every=0):
+        # every shard holds the mesh's last cell: the source term reads it for cellfid padding
+        super().__init__(elements, vertex, 2, group, device, store, extra_cells=[len(elements) - 1],
+                         sync_every=sync_every)
+        if walls not in _lib.WALLS:
+            raise ValueError("walls must be 'neumann' or 'reflective'")
+        self.walls = _lib.WALLS[walls]
+        self.cfl, self.grav = float(cfl), float(grav)
+        nc, nf = self.dm.nbcells, self.dm.nbfaces
+        f64 = torch.float64
+        self.q = [[torch.zeros(nc, dtype=f64, device=self.dev) for _ in range(4)] for _ in range(2)]
+        self.Z = torch.zeros(nc, dtype=f64, device=self.dev)
+        self.cur = 0
+        self.ff = torch.empty(4 * nf, dtype=f64, device=self.dev)
+        self.dt = torch.zeros(1, dtype=f64, device=self.dev)
+
+    def set_state(self, h, hu, hv, hc, Z):
+        """The state from whole-mesh cell arrays (manapy numbering)."""
+        for t, a in zip(self.q[self.cur], (h, hu, hv, hc)):
+            t.copy_(self._local(a))
+        self.Z.copy_(self._local(Z))
+
+    def step(self):
+        self._before_step()
+        with self.monitor.guard():
+            qi, qo = self.q[self.cur], self.q[1 - self.cur]
+            st = self._stream()
+            _lib.call("mb_sw_dt", self.dm.struct, _p(qi[0]), _p(qi[1]), _p(qi[2]), self.cfl, self.grav, _p(self.dt),
+                      st)
+            self._all_min(self.dt)
+            _lib.call("mb_sw_step_ex", self.dm.struct, _lib.p5([_p(t) for t in qi] + [_p(self.Z)]),
+                      _lib.p5([_p(t) for t in qo] + [_p(self.Z)]), self.cfl, self.grav, 1, self.walls, None,
+                      _p(self.ff), _p(self.dt), None, st)
+            self.cur = 1 - self.cur
+            self.exchanger.exchange(self.q[self.cur])
+
+    def gather(self):
+        """[h, hu, hv] whole-mesh cell arrays on every rank (manapy numbering)."""
+        return [self._gather(t) for t in self.q[self.cur][:3]]

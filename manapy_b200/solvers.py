@@ -636,8 +636,13 @@ class ShallowWaterSolver:
         slot = self._dt_buf[self._cur:self._cur + 1]
         if self._dt_key != self._state_key():
             q = self._q()
-            _lib.call("mb_time_step_sw", self._dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), float(self.cfl),
-                      float(self.grav), float(self.Dxx), float(self.Dyy), _p(slot), self._stream())
+            if "cell_vtx" in self._dm.t:
+                # the fused step's own dt formula (the one it applies to later steps)
+                _lib.call("mb_sw_dt", self._dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), float(self.cfl),
+                          float(self.grav), _p(slot), self._stream())
+            else:
+                _lib.call("mb_time_step_sw", self._dm.struct, _p(q[0]), _p(q[1]), _p(q[2]), float(self.cfl),
+                          float(self.grav), float(self.Dxx), float(self.Dyy), _p(slot), self._stream())
             self._dt_key = self._state_key()
             self._dt_host = None
         return slot
