@@ -19,6 +19,7 @@ __global__ void __launch_bounds__(kBlock) k_check(const T *__restrict__ v, long 
 
 extern "C" int mb_check_state(const double *f64, const float *f32, int64_t n, int32_t nonneg, int32_t *flags,
                               void *stream) {
+  MB_NVTX();
   if (!flags || n < 0 || (f64 == nullptr) == (f32 == nullptr)) return MB_EINVAL;
   if (n == 0) return MB_OK;
   long long blocks = (n + mb::kBlock - 1) / mb::kBlock;

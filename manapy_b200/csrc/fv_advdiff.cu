@@ -1304,12 +1304,14 @@ static bool mesh_ok(const mb_mesh *m) {
 extern "C" {
 
 int mb_facetocell(const mb_mesh *m, const double *u_face, double *u_cell, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !u_face || !u_cell) return MB_EINVAL;
   k_facetocell<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, u_face, u_cell);
   return check_launch();
 }
 
 int mb_ghost_value(const mb_mesh *m, const mb_bc *bc, const double *w_c, double *w_ghost, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !bc || !w_c || !w_ghost) return MB_EINVAL;
   k_ghost<<<grid_for(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, *bc, w_c, w_ghost);
   return check_launch();
@@ -1317,6 +1319,7 @@ int mb_ghost_value(const mb_mesh *m, const mb_bc *bc, const double *w_c, double 
 
 int mb_cell_gradient(const mb_mesh *m, const double *w_c, const double *w_ghost, double *w_x, double *w_y,
                      double *w_z, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !w_c || !w_ghost || !w_x || !w_y || !w_z) return MB_EINVAL;
   if (m->dim == 2)
     k_cell_gradient<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_x, w_y, w_z);
@@ -1327,6 +1330,7 @@ int mb_cell_gradient(const mb_mesh *m, const double *w_c, const double *w_ghost,
 
 int mb_barthlimiter(const mb_mesh *m, const double *w_c, const double *w_ghost, const double *w_x,
                     const double *w_y, const double *w_z, double *psi, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !w_c || !w_ghost || !w_x || !w_y || !w_z || !psi) return MB_EINVAL;
   if (m->dim == 2)
     k_barth<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_x, w_y, w_z, psi);
@@ -1337,6 +1341,7 @@ int mb_barthlimiter(const mb_mesh *m, const double *w_c, const double *w_ghost, 
 
 int mb_centertovertex(const mb_mesh *m, const double *w_c, const double *w_ghost, double *w_node,
                       void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !w_c || !w_ghost || !w_node) return MB_EINVAL;
   k_centertovertex<<<grid_for(m->nbnodes), kBlock, 0, ST(stream)>>>(*m, w_c, w_ghost, w_node);
   return check_launch();
@@ -1344,6 +1349,7 @@ int mb_centertovertex(const mb_mesh *m, const double *w_c, const double *w_ghost
 
 int mb_face_gradient(const mb_mesh *m, const mb_bc *bc, const double *w_c, const double *w_ghost,
                      const double *w_node, double *wx_face, double *wy_face, double *wz_face, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !bc || !bc->face_grad_on || !w_c || !w_ghost || !w_node || !wx_face || !wy_face ||
       (m->dim == 3 && !wz_face))
     return MB_EINVAL;
@@ -1360,6 +1366,7 @@ int mb_explicitscheme_convective(const mb_mesh *m, double *rez_w, const double *
                                  const double *u_face, const double *v_face, const double *w_face,
                                  const double *w_x, const double *w_y, const double *w_z, const double *psi,
                                  int32_t order, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !rez_w || !w_c || !w_ghost || !u_face || !v_face || !w_face || (order != 1 && order != 2))
     return MB_EINVAL;
   if (order == 2 && (!w_x || !w_y || !w_z || !psi)) return MB_EINVAL;
@@ -1375,6 +1382,7 @@ int mb_explicitscheme_convective(const mb_mesh *m, double *rez_w, const double *
 int mb_explicitscheme_dissipative(const mb_mesh *m, const double *wx_face, const double *wy_face,
                                   const double *wz_face, double *dissip_w, double Dxx, double Dyy, double Dzz,
                                   void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !wx_face || !wy_face || !wz_face || !dissip_w) return MB_EINVAL;
   if (m->dim == 2)
     k_dissipative<2><<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, wx_face, wy_face, wz_face, dissip_w,
@@ -1387,6 +1395,7 @@ int mb_explicitscheme_dissipative(const mb_mesh *m, const double *wx_face, const
 
 int mb_time_step(const mb_mesh *m, const double *u, const double *v, const double *w, double cfl, double Dxx,
                  double Dyy, double Dzz, double *dt_dev, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !u || !v || !w || !dt_dev) return MB_EINVAL;
   k_fill<<<1, 1, 0, ST(stream)>>>(dt_dev, 1e6);
   k_time_step<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, u, v, w, cfl, Dxx, Dyy, Dzz, dt_dev);
@@ -1395,6 +1404,7 @@ int mb_time_step(const mb_mesh *m, const double *u, const double *v, const doubl
 
 int mb_update_new_value(const mb_mesh *m, double *ne_c, const double *rez, const double *dissip,
                         const double *src, const double *dt_dev, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !ne_c || !rez || !dissip || !src || !dt_dev) return MB_EINVAL;
   k_update<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(m->nbcells, ne_c, rez, dissip, src, dt_dev,
                                                             m->cell_volume);
@@ -1403,6 +1413,7 @@ int mb_update_new_value(const mb_mesh *m, double *ne_c, const double *rez, const
 
 int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face, const double *w_face,
                  double *sign_face, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !u_face || !v_face || !w_face || !sign_face) return MB_EINVAL;
   k_face_sign<<<grid_for(m->nbfaces), kBlock, 0, ST(stream)>>>(*m, u_face, v_face, w_face, sign_face);
   return check_launch();
@@ -1410,6 +1421,7 @@ int mb_face_sign(const mb_mesh *m, const double *u_face, const double *v_face, c
 
 int mb_cell_face_sign(const mb_mesh *m, const double *u_face, const double *v_face, const double *w_face,
                       double *sign_cf, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !u_face || !v_face || !w_face || !sign_cf) return MB_EINVAL;
   k_cell_face_sign<<<grid_for(m->nbcells), kBlock, 0, ST(stream)>>>(*m, u_face, v_face, w_face, sign_cf);
   return check_launch();
@@ -1418,6 +1430,7 @@ int mb_cell_face_sign(const mb_mesh *m, const double *u_face, const double *v_fa
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p, const double *w_in,
                     double *w_out, const double *sign_cf, const double *src, const double *dt_dev,
                     double *cell_scratch, double *node_scratch, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !bc || !p || !w_in || !w_out || w_in == w_out || !sign_cf || !dt_dev) return MB_EINVAL;
   if (p->order != 1 && p->order != 2) return MB_EINVAL;
   const bool o2 = p->order == 2, df = p->diffusion != 0;
@@ -1440,6 +1453,7 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
 int mb_advdiff_batch_step(const mb_advdiff_item_f64 *items, const int32_t *p1_map, int32_t p1_blocks,
                           const int32_t *p2_map, int32_t p2_blocks, int32_t order, int32_t diffusion,
                           int32_t *clock, void *stream) {
+  MB_NVTX();
   if (!items || !p2_map || !clock || p2_blocks <= 0 || p1_blocks < 0 || (order != 1 && order != 2)) return MB_EINVAL;
   const bool o2 = order == 2, df = diffusion != 0;
   if ((o2 || df) && (!p1_map || p1_blocks <= 0)) return MB_EINVAL;
@@ -1485,6 +1499,7 @@ double *g_noalloc_base[kMaxDevices] = {};
 extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                                        const double *w_in, double *w_out, const double *sign_cf,
                                        const double *src, const double *dt_dev, void *stream) {
+  MB_NVTX();
   if (!mesh_ok(m) || !bc || !p) return MB_EINVAL;
   const long long per_cell = m->dim == 2 ? 4 : 8;
   const long long need = per_cell * m->nbcells + m->nbnodes;

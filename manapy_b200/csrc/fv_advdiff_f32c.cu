@@ -643,6 +643,7 @@ extern "C" int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_
                                     const float *w_in, float *w_out, const float *lo_in, float *lo_out,
                                     const float *sign_cf, const float *src, const double *dt_dev, float *cell_scratch,
                                     float *node_scratch, void *stream) {
+  MB_NVTX();
   if (!m || !bc || !p || !w_in || !w_out || !sign_cf || !dt_dev || w_in == w_out) return MB_EINVAL;
   if (m->dim != 2 && m->dim != 3) return MB_EINVAL;
   if ((lo_in == nullptr) != (lo_out == nullptr) || (lo_in && lo_in == lo_out)) return MB_EINVAL;
@@ -671,6 +672,7 @@ extern "C" int mb_advdiff_step_f32c(const mb_mesh *m, const mb_bc *bc, const mb_
 extern "C" int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const int32_t *p1_map, int32_t p1_blocks,
                                           const int32_t *p2_map, int32_t p2_blocks, int32_t order,
                                           int32_t diffusion, int32_t *clock, void *stream) {
+  MB_NVTX();
   if (!items || !p2_map || !clock || p2_blocks <= 0 || p1_blocks < 0 || (order != 1 && order != 2)) return MB_EINVAL;
   const bool o2 = order == 2, df = diffusion != 0;
   if ((o2 || df) && (!p1_map || p1_blocks <= 0)) return MB_EINVAL;
@@ -692,6 +694,7 @@ extern "C" int mb_advdiff_batch_step_f32c(const mb_advdiff_item *items, const in
 }
 
 extern "C" int mb_cell_face_sign_f32c(const mb_mesh *m, const double *sign_cf, float *sign_f32, void *stream) {
+  MB_NVTX();
   if (!m || !sign_cf || !sign_f32 || !m->cell_flags || (m->dim != 2 && m->dim != 3)) return MB_EINVAL;
   k_sign_f32c<<<ceil_div(m->nbcells, kBlock), kBlock, 0, (cudaStream_t)stream>>>(*m, sign_cf, sign_f32);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;

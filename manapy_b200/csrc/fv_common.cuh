@@ -8,11 +8,23 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "manapy_b200.h"
 
 namespace mb {
+
+// A named NVTX range over a C-ABI entry point: profilers show each call around the
+// kernels it launches (header-only NVTX v3; without a tool attached a push/pop is a
+// few nanoseconds of host time).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define MB_NVTX() ::mb::NvtxRange mb_nvtx_range_(__func__)
 
 constexpr int kBlock = 256;
 

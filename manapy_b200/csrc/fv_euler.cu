@@ -324,6 +324,7 @@ extern "C" {
 
 int mb_euler_rusanov_2d(const mb_mesh *m, const double *const q[5], const double *const g[5], double *const rez[4],
                         double gamma, void *stream) {
+  MB_NVTX();
   if (!euler_mesh_ok(m) || !q_ok(q) || !q_ok(g) || !rez) return MB_EINVAL;
   for (int k = 0; k < 4; ++k)
     if (!rez[k]) return MB_EINVAL;
@@ -335,6 +336,7 @@ int mb_euler_rusanov_2d(const mb_mesh *m, const double *const q[5], const double
 
 int mb_time_step_euler_2d(const mb_mesh *m, const double *const q[5], double cfl, double gamma, double *dt_c,
                           void *stream) {
+  MB_NVTX();
   if (!euler_mesh_ok(m) || !q_ok(q) || !dt_c) return MB_EINVAL;
   EulerQ qq{q[0], q[1], q[2], q[3], q[4]};
   k_time_step_euler<<<grid_e(m->nbcells), kBlock, 0, (cudaStream_t)stream>>>(*m, qq, cfl, gamma, dt_c);
@@ -343,6 +345,7 @@ int mb_time_step_euler_2d(const mb_mesh *m, const double *const q[5], double cfl
 
 int mb_update_euler_2d(const mb_mesh *m, double *const q[5], const double *const rez[4], double gamma, double dt,
                        void *stream) {
+  MB_NVTX();
   if (!m || !m->cell_volume || m->nbcells <= 0 || !q || !rez) return MB_EINVAL;
   for (int k = 0; k < 5; ++k)
     if (!q[k] || (k < 4 && !rez[k])) return MB_EINVAL;
@@ -354,6 +357,7 @@ int mb_update_euler_2d(const mb_mesh *m, double *const q[5], const double *const
 
 int mb_ghost_euler_neumann_2d(const mb_mesh *m, const double *const q[5], double *const g[5], double *ug, double *vg,
                               void *stream) {
+  MB_NVTX();
   if (!euler_mesh_ok(m) || !q_ok(q) || !g || !ug || !vg || m->nbfaces <= 0) return MB_EINVAL;
   for (int k = 0; k < 5; ++k)
     if (!g[k]) return MB_EINVAL;
@@ -365,6 +369,7 @@ int mb_ghost_euler_neumann_2d(const mb_mesh *m, const double *const q[5], double
 
 int mb_euler_dt_2d(const mb_mesh *m, const double *const q[5], double cfl, double gamma, double *ring, int t,
                    void *stream) {
+  MB_NVTX();
   if (!euler_mesh_ok(m) || !q_ok(q) || !ring || t < 0) return MB_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   EulerQ qq{q[0], q[1], q[2], q[3], q[4]};
@@ -376,6 +381,7 @@ int mb_euler_dt_2d(const mb_mesh *m, const double *const q[5], double cfl, doubl
 static bool a32(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 31) == 0; }
 
 int mb_euler_tables_2d(const mb_mesh *m, double *face_rec, uint8_t *cell_left, void *stream) {
+  MB_NVTX();
   if (!euler_mesh_ok(m) || !face_rec || !cell_left || m->nbfaces <= 0 || !a32(face_rec)) return MB_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   k_euler_face_rec<<<(m->nbfaces + kBlock - 1) / kBlock, kBlock, 0, st>>>(*m, face_rec);
@@ -386,6 +392,7 @@ int mb_euler_tables_2d(const mb_mesh *m, double *face_rec, uint8_t *cell_left, v
 int mb_euler_step_2d(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl,
                      double gamma, const double *face_rec, const uint8_t *cell_left, double *face_flux, double *ring,
                      int t, double *time, void *stream) {
+  MB_NVTX();
   if (!euler_mesh_ok(m) || !q_ok(q_in) || !q_out || !ring || !face_flux || !face_rec || !cell_left || t < 0 ||
       m->nbfaces <= 0)
     return MB_EINVAL;

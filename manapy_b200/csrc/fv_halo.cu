@@ -57,6 +57,7 @@ using namespace mb;
 
 extern "C" int mb_halo_pack(double *const *fields, int32_t nfields, const int64_t *idx, int64_t n, double *buf,
                             void *stream) {
+  MB_NVTX();
   HaloFields fs{};
   const int rc = halo_fields(fields, nfields, fs);
   if (rc != MB_OK || n < 0 || (n > 0 && (!idx || !buf))) return rc != MB_OK ? rc : MB_EINVAL;
@@ -67,6 +68,7 @@ extern "C" int mb_halo_pack(double *const *fields, int32_t nfields, const int64_
 
 extern "C" int mb_halo_unpack(double *const *fields, int32_t nfields, const int64_t *idx, int64_t n,
                               const double *buf, void *stream) {
+  MB_NVTX();
   HaloFields fs{};
   const int rc = halo_fields(fields, nfields, fs);
   if (rc != MB_OK || n < 0 || (n > 0 && (!idx || !buf))) return rc != MB_OK ? rc : MB_EINVAL;

@@ -842,6 +842,7 @@ extern "C" {
 
 int mb_srnh_flux(int32_t n, const double *states, const double *normals, const double *mesure, double grav,
                  double *flux, void *stream) {
+  MB_NVTX();
   if (n < 0 || (n > 0 && (!states || !normals || !mesure || !flux))) return MB_EINVAL;
   if (n == 0) return MB_OK;
   k_srnh_batch<<<grid_for_sw(n), kBlock, 0, ST(stream)>>>(n, states, normals, mesure, grav, flux);
@@ -850,6 +851,7 @@ int mb_srnh_flux(int32_t n, const double *states, const double *normals, const d
 
 int mb_time_step_sw(const mb_mesh *m, const double *h, const double *hu, const double *hv, double cfl,
                     double grav, double Dxx, double Dyy, double *dt_dev, void *stream) {
+  MB_NVTX();
   if (!sw_mesh_ok(m) || !h || !hu || !hv || !dt_dev) return MB_EINVAL;
   k_fill_sw<<<1, 1, 0, ST(stream)>>>(dt_dev, 1e6);
   k_time_step_sw<<<grid_for_sw(m->nbcells), kBlock, 0, ST(stream)>>>(*m, h, hu, hv, cfl, grav, Dxx, Dyy, dt_dev);
@@ -859,6 +861,7 @@ int mb_time_step_sw(const mb_mesh *m, const double *h, const double *hu, const d
 int mb_explicitscheme_convective_sw(const mb_mesh *m, double *const rez[5], const double *const q[5],
                                     const double *const g[5], const double *const grads[4], const double *psi,
                                     double grav, int32_t order, double *face_flux, void *stream) {
+  MB_NVTX();
   if (!sw_mesh_ok(m) || !rez || !q || !g || !face_flux || (order != 1 && order != 2)) return MB_EINVAL;
   SWState s{};
   for (int k = 0; k < 5; ++k) {
@@ -884,6 +887,7 @@ int mb_explicitscheme_convective_sw(const mb_mesh *m, double *const rez[5], cons
 
 int mb_term_source_srnh_sw(const mb_mesh *m, const double *h, const double *Z, const double *h_ghost,
                            const double *Z_ghost, double grav, double *src_hu, double *src_hv, void *stream) {
+  MB_NVTX();
   if (!sw_mesh_ok(m) || !h || !Z || !h_ghost || !Z_ghost || !src_hu || !src_hv || !m->cell_cellfid ||
       !m->cell_nf || !m->cell_vertex1)
     return MB_EINVAL;
@@ -893,6 +897,7 @@ int mb_term_source_srnh_sw(const mb_mesh *m, const double *h, const double *Z, c
 
 int mb_update_sw(const mb_mesh *m, double *const q[5], const double *const rez[5], const double *src_hu,
                  const double *src_hv, const double *dt_dev, void *stream) {
+  MB_NVTX();
   if (!sw_mesh_ok(m) || !q || !rez || !src_hu || !src_hv || !dt_dev) return MB_EINVAL;
   SWQ qq;
   SWR rr;
@@ -909,6 +914,7 @@ int mb_update_sw(const mb_mesh *m, double *const q[5], const double *const rez[5
 int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
                int32_t order, double *scratch, double *face_flux, const double *dt_cur, double *dt_next,
                void *stream) {
+  MB_NVTX();
   return mb_sw_step_ex(m, q_in, q_out, cfl, grav, order, MB_WALLS_NEUMANN, scratch, face_flux, dt_cur, dt_next,
                        stream);
 }
@@ -916,6 +922,7 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
 int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
                   int32_t order, int32_t walls, double *scratch, double *face_flux, const double *dt_cur,
                   double *dt_next, void *stream) {
+  MB_NVTX();
   if (!sw_mesh_ok(m) || !q_in || !q_out || !face_flux || !dt_cur || (order != 1 && order != 2)) return MB_EINVAL;
   if (walls != MB_WALLS_NEUMANN && walls != MB_WALLS_REFLECT) return MB_EINVAL;
   if (!m->cell_cellfid || !m->cell_vtx || !m->cell_nbr || !m->cell_flags || !m->node_coord || !m->cell_xy)
@@ -953,6 +960,7 @@ int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q
 
 int mb_sw_dt(const mb_mesh *m, const double *h, const double *hu, const double *hv, double cfl, double grav,
              double *dt_dev, void *stream) {
+  MB_NVTX();
   if (!sw_mesh_ok(m) || !h || !hu || !hv || !dt_dev || !m->cell_vtx || !m->cell_flags || !m->node_coord)
     return MB_EINVAL;
   k_fill_sw<<<1, 1, 0, ST(stream)>>>(dt_dev, 1e6);
@@ -962,6 +970,7 @@ int mb_sw_dt(const mb_mesh *m, const double *h, const double *hu, const double *
 
 int mb_sw_batch_step(const mb_sw_item_f64 *items, const int32_t *face_map, int32_t face_blocks,
                      const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream) {
+  MB_NVTX();
   if (!items || !face_map || !cell_map || !clock || face_blocks <= 0 || cell_blocks <= 0) return MB_EINVAL;
   cudaStream_t st = ST(stream);
   k_sw2_batch_flux<<<face_blocks, MB_SW_FLUX_BLOCK, 0, st>>>(items, face_map, clock);

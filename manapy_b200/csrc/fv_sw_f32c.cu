@@ -323,6 +323,7 @@ using namespace mb;
 extern "C" int mb_sw_step_f32c(const mb_mesh *m, const float *const q_in[5], float *const q_out[5],
                                const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
                                int32_t order, float *face_flux, const double *dt_cur, double *dt_next, void *stream) {
+  MB_NVTX();
   return mb_sw_step_f32c_ex(m, q_in, q_out, lo_in, lo_out, cfl, grav, order, MB_WALLS_NEUMANN, face_flux, dt_cur,
                             dt_next, stream);
 }
@@ -331,6 +332,7 @@ extern "C" int mb_sw_step_f32c_ex(const mb_mesh *m, const float *const q_in[5], 
                                   const float *const lo_in[4], float *const lo_out[4], double cfl, double grav,
                                   int32_t order, int32_t walls, float *face_flux, const double *dt_cur,
                                   double *dt_next, void *stream) {
+  MB_NVTX();
   if (!m || m->dim != 2 || m->nlf != 3 || m->nbcells <= 0 || m->nbfaces <= 0) return MB_EINVAL;
   if (walls != MB_WALLS_NEUMANN && walls != MB_WALLS_REFLECT) return MB_EINVAL;
   if (!q_in || !q_out || !face_flux || !dt_cur || dt_next == dt_cur || order != 1) return MB_EINVAL;
@@ -361,6 +363,7 @@ extern "C" int mb_sw_step_f32c_ex(const mb_mesh *m, const float *const q_in[5], 
 
 extern "C" int mb_sw_batch_step_f32c(const mb_sw_item *items, const int32_t *face_map, int32_t face_blocks,
                                      const int32_t *cell_map, int32_t cell_blocks, int32_t *clock, void *stream) {
+  MB_NVTX();
   if (!items || !face_map || !cell_map || !clock || face_blocks <= 0 || cell_blocks <= 0) return MB_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   k_sw2c_batch_flux<<<face_blocks, kBlock, 0, st>>>(items, face_map, clock);

@@ -30,27 +30,32 @@ def _p(t):
 class _Sharded:
     """Shard, device mesh, halo exchange and failure monitor of one rank."""
 
-    def __init__(self, elements, vertex, dim, group, device, store, extra_cells=None, sync_every=0):
+    def __init__(self, elements, vertex, dim, group, device, store, extra_cells=None, sync_every=0, check_every=1,
+                 A=None):
         import torch.distributed as dist
         self.dist, self.group = dist, group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.dim = dim
-        self.shard = P.build_shards(elements, vertex, dim, self.world, extra_cells=extra_cells)[self.rank]
+        self.shard = P.build_shards(elements, vertex, dim, self.world, A=A, extra_cells=extra_cells)[self.rank]
         A = G.build(self.shard.elements, self.shard.vertex, dim, halo_rim=True)
         self.A = A
         self.dm = DeviceMesh(A, self.dev)
         inv = self.dm.inv["cell"].cpu().numpy()
         self.exchanger = P.HaloExchange(self._to_device_numbering(inv), group, device=self.dev)
         self.monitor = P.FailureMonitor(self.rank, store, world=self.world)
-        self.sync_every = int(sync_every)    # heartbeat every this many steps (0: failure check only)
+        # heartbeat every sync_every steps; otherwise a failure-record lookup every check_every
+        # steps (0: none; the process group's timeout still ends a run whose peer died)
+        self.sync_every = int(sync_every)
+        self.check_every = int(check_every)
         self.steps_done = 0
 
     def _before_step(self):
-        if self.sync_every and self.steps_done % self.sync_every == 0:
-            self.monitor.sync(self.steps_done)
-        else:
+        k = self.steps_done
+        if self.sync_every and k % self.sync_every == 0:
+            self.monitor.sync(k)
+        elif self.check_every and k % self.check_every == 0:
             self.monitor.check()
         self.steps_done += 1
 
@@ -103,8 +108,9 @@ class ShardedAdvectionDiffusion(_Sharded):
     options as ``AdvectionDiffusionSolver`` (Dxx, Dyy, Dzz, order, cfl)."""
 
     def __init__(self, elements, vertex, dim, BC, values, velocity, Dxx=0., Dyy=0., Dzz=0., order=1, cfl=0.4,
-                 group=None, device=None, store=None, sync_every=0):
-        super().__init__(elements, vertex, dim, group, device, store, sync_every=sync_every)
+                 group=None, device=None, store=None, sync_every=0, check_every=1, A=None):
+        super().__init__(elements, vertex, dim, group, device, store, sync_every=sync_every, check_every=check_every,
+                         A=A)
         A = self.A
         self.bc = DeviceBC(A, B.resolve(A, BC, values), self.dev, mesh=self.dm)
         self.params = _lib.MbAdvDiffParams(int(order), int(not (Dxx == Dyy == Dzz == 0)), float(Dxx), float(Dyy),
@@ -167,10 +173,10 @@ class ShardedShallowWater(_Sharded):
     formula, min over ranks; the fused step; the exchange of h, hu, hv, hc."""
 
     def __init__(self, elements, vertex, cfl=0.8, grav=9.81, walls="neumann", group=None, device=None, store=None,
-                 sync_every=0):
+                 sync_every=0, check_every=1, A=None):
         # every shard holds the mesh's last cell: the source term reads it for cellfid padding
         super().__init__(elements, vertex, 2, group, device, store, extra_cells=[len(elements) - 1],
-                         sync_every=sync_every)
+                         sync_every=sync_every, check_every=check_every, A=A)
         if walls not in _lib.WALLS:
             raise ValueError("walls must be 'neumann' or 'reflective'")
         self.walls = _lib.WALLS[walls]

@@ -366,9 +366,11 @@ class AdvectionDiffusionSolver:
             check_state([self.var.dev("cell")], names=["the cell values"])
 
     def launches_per_step(self):
-        """Kernel launches of one fused step (tetrahedra at order 2: a pack pass first)."""
+        """Kernel launches of one fused step (tetrahedra at order 2 without tile tables: a
+        pack pass first)."""
         n = 1 + int(self.order == 2 or bool(self.diffusion))
-        if self.dim == 3 and self.order == 2 and self.precision == "fp64":
+        staged = self._dm is not None and "lsq_loc" in self._dm.t
+        if self.dim == 3 and self.order == 2 and self.precision == "fp64" and not staged:
             n += 1
         return n
 
