@@ -131,6 +131,15 @@ class Domain:
         from .gmsh import read_msh
         return cls(dim=dim, conf=conf, mesh=read_msh(path, dim), **kwargs)
 
+    @classmethod
+    def from_hdf5(cls, mesh_dir, dim, conf=None, **kwargs):
+        """Build from a manapy mesh directory ``meshes<P>PROC`` (``mesh<r>.hdf5``, written by
+        manapy's partitioner, ``manapy/partitions/meshpartitioning.py:238-275``; read as
+        ``manapy/ddm/pure_ddm.py:13-102`` does, without h5py): one rank's file, or the
+        rank files reassembled into the whole mesh."""
+        from .hdf5 import read_mesh_dir
+        return cls(dim=dim, conf=conf, mesh=read_mesh_dir(mesh_dir), **kwargs)
+
     # ------------------------------------------------------------------ views
     def _build_views(self):
         A = self._A
