@@ -69,7 +69,9 @@ def parse():
     ap.add_argument("--rate", type=float, default=15.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--serial-sample", type=int, default=60, help="serving: requests timed serially in FP64")
     ap.add_argument("--workers", type=int, default=None, help="serving: mesh-preparation processes")
-    ap.add_argument("--n", type=int, default=None, help="mesh resolution override (small profiling cases)")
+    ap.add_argument("--n", "--mesh-n", dest="n", type=int, default=None,
+                    help="mesh resolution override (small profiling cases; --mesh-n under torchrun, whose own "
+                         "options start with --n)")
     ap.add_argument("--min-timed-steps", type=int, default=500,
                     help="repeat the K timed steps until at least this many steps are timed (median reported)")
     ap.add_argument("--no-extras", action="store_true",

@@ -50,7 +50,7 @@ typedef struct mb_mesh {
   int32_t nbfaces;
   int32_t nbnodes;
   int32_t nlf;       /* faces per cell: 3 or 4 */
-  int32_t tile_max_halo; /* largest tile halo of the tile tables below (0: none) */
+  int32_t pad_;
   /* cells */
   const double *cell_center;    /* [nbcells][3] */
   const double *cell_volume;    /* [nbcells] */
@@ -115,19 +115,6 @@ typedef struct mb_mesh {
   const float *n2c_sell_alpha_f32;
   /* [nbfaces][4] = {n_x, n_y, 1/mesure, 0} rounded to FP32 (FP32-compensated shallow water, 2D) */
   const float *face_nm_f32;
-  /* tile tables of the shared-memory-staged first phase (all NULL: unstaged).  Tile t is
-   * cells [256 t, 256 t + 256); local index of own cell c: c - 256 t, of halo entry p:
-   * 256 + p.  tile_halo_ptr [ntiles+1] / tile_halo_idx: each tile's halo cells (the
-   * cells its stencils read outside it); lsq_loc: the lsq SELL-32 stencils as local
-   * indices (padding 0xFFFF: the cell itself); tile_node_ptr [ntiles+1] /
-   * tile_node_idx: the nodes whose smallest incident cell is in the tile; n2c_loc: the
-   * local index, in the node's tile, of each n2c incidence (n2c_idx order). */
-  const int32_t *tile_halo_ptr;
-  const int32_t *tile_halo_idx;
-  const uint16_t *lsq_loc;
-  const int32_t *tile_node_ptr;
-  const int32_t *tile_node_idx;
-  const uint16_t *n2c_loc;
 } mb_mesh;
 
 typedef struct mb_bc {
@@ -278,6 +265,21 @@ typedef struct mb_advdiff_params {
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
                     const double *dt_dev, double *cell_scratch, double *node_scratch, void *stream);
+
+/* Rows {centre, value} of a state, [nbcells][4] doubles, 32-byte aligned: {x, y, w, 0} for
+ * triangles, {x, y, z, w} for tetrahedra (no counterpart in manapy). */
+int mb_pack_rows(const mb_mesh *m, const double *w, double *rows, void *stream);
+
+/* mb_advdiff_step for a run of consecutive steps (no counterpart in manapy): rows_in holds
+ * the rows of w_in (mb_pack_rows, or the previous step's rows_out), from which the first
+ * launch reads each least-squares neighbour's centre and value with one 256-bit load; the
+ * second launch also writes the rows of w_out into rows_out.  Same results as
+ * mb_advdiff_step, same scratch (3D: the first 4*nbcells doubles of cell_scratch are used);
+ * compact tables required; rows_in != rows_out. */
+int mb_advdiff_step_rows(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
+                         const double *w_in, double *w_out, const double *rows_in, double *rows_out,
+                         const double *sign_cf, const double *src, const double *dt_dev,
+                         double *cell_scratch, double *node_scratch, void *stream);
 
 /* The u.n table of the FP32-compensated step from mb_cell_face_sign's FP64 table: per
  * cell the FP32 u.n of each local face and the cell's signed sum of them (sum over its

@@ -24,7 +24,7 @@ _d = ctypes.c_double
 
 class MbMesh(ctypes.Structure):
     _fields_ = [("dim", _i32), ("nbcells", _i32), ("nbfaces", _i32), ("nbnodes", _i32),
-                ("nlf", _i32), ("tile_max_halo", _i32),
+                ("nlf", _i32), ("pad_", _i32),
                 ("cell_center", _vp), ("cell_volume", _vp), ("cell_faces", _vp),
                 ("cell_order", _vp), ("cellnid_ptr", _vp), ("cellnid_idx", _vp),
                 ("ghostnid_ptr", _vp), ("ghostnid_idx", _vp),
@@ -36,9 +36,7 @@ class MbMesh(ctypes.Structure):
                 ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp),
                 ("cell_vtx", _vp), ("cell_nbr", _vp), ("cell_flags", _vp), ("node_coord", _vp), ("cell_xy", _vp),
                 ("lsq_sell_ptr", _vp), ("lsq_sell_idx", _vp), ("n2c_sell_ptr", _vp), ("n2c_sell_idx", _vp),
-                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp),
-                ("tile_halo_ptr", _vp), ("tile_halo_idx", _vp), ("lsq_loc", _vp), ("tile_node_ptr", _vp),
-                ("tile_node_idx", _vp), ("n2c_loc", _vp)]
+                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp)]
 
 
 class MbBC(ctypes.Structure):
@@ -107,6 +105,9 @@ _SIGS = {
     "mb_euler_step_2d": [_M, _P5, _P5, _d, _d, _vp, _vp, _vp, _vp, _i32, _vp, _vp],
     "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
+    "mb_pack_rows": [_M, _vp, _vp, _vp],
+    "mb_advdiff_step_rows": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                             _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_advdiff_step_noalloc": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_cell_face_sign_f32c": [_M, _vp, _vp, _vp],

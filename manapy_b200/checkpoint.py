@@ -69,6 +69,10 @@ def save(path, solver, step=0, time=0.0):
     else:
         for name in ("h", "hu", "hv", "hc", "Z"):
             out[name] = _read(solver.varbs[name], "cell")
+        if solver._dt_key is not None and solver._dt_key == solver._state_key():
+            # the dt the next step applies (in the FP32-compensated step it comes from the FP32
+            # state, so it is carried rather than recomputed)
+            out["dt"] = float(solver._dt_buf[solver._cur].item())
         if solver.precision == "fp32c" and solver._q32 is not None and solver._keys() == solver._q32_key:
             k = solver._q32_i
             for c, name in enumerate(("h", "hu", "hv", "hc")):
@@ -108,4 +112,8 @@ def load(path, solver):
                 solver._q32[k][c].copy_(_dev_cells(solver, g[name + "32"], torch.float32))
                 solver._lo32[k][c].copy_(_dev_cells(solver, g[name + "_lo32"], torch.float32))
             solver._q32[2].copy_(_dev_cells(solver, g["Z32"], torch.float32))
+        if "dt" in g.files:
+            solver._dt_buf[solver._cur].fill_(float(g["dt"]))
+            solver._dt_key = solver._state_key()
+            solver._dt_host = None
     return int(g["step"]), float(g["time"])

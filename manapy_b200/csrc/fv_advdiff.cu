@@ -457,16 +457,26 @@ __global__ void __launch_bounds__(kBlock) k_step_phase2(mb_mesh m, mb_bc bc, mb_
 #endif
 
 // block `bid` of phase 1: blocks [0, ncb) gradient + limiter records, the rest node values
-template <bool ORDER2, bool DIFF>
+// ROWS: the least-squares neighbours are read from rows {x, y, w, 0} of the step's input
+// (one 256-bit load each) instead of the centre table and the state (two loads)
+template <bool ORDER2, bool DIFF, bool ROWS = false>
 __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, const double *__restrict__ w,
-                                          double *__restrict__ rec, double *__restrict__ wn, int ncb, int bid) {
+                                          double *__restrict__ rec, double *__restrict__ wn, int ncb, int bid,
+                                          const double *__restrict__ rows = nullptr) {
   const GhostRule ghost = make_rule(m, bc, w);
   const int lane = threadIdx.x & 31;
   if (ORDER2 && bid < ncb) {
     const int i = bid * blockDim.x + threadIdx.x;
     if (i >= m.nbcells) return;
-    const double2 c = ldd2(m.cell_xy + 2 * i);
-    const double wi = ld(w + i);
+    double2 c;
+    double wi;
+    if (ROWS) {
+      double pad;
+      ld4d(rows + 4 * (long long)i, c.x, c.y, wi, pad);
+    } else {
+      c = ldd2(m.cell_xy + 2 * i);
+      wi = ld(w + i);
+    }
     // least-squares gradient: vertex neighbours (SELL-32), then stencil ghosts
     // every row of the warp runs to the group length (a uniform trip count keeps
     // several gathers in flight); a padding entry points at the cell itself,
@@ -489,7 +499,15 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
       double2 pc[MB_F2_LSQ_BATCH];
       double wc[MB_F2_LSQ_BATCH];
 #pragma unroll
-      for (int u = 0; u < MB_F2_LSQ_BATCH; ++u) { pc[u] = ldd2(m.cell_xy + 2 * cc[u]); wc[u] = ld(w + cc[u]); }
+      for (int u = 0; u < MB_F2_LSQ_BATCH; ++u) {
+        if (ROWS) {
+          double pad;
+          ld4d(rows + 4 * (long long)cc[u], pc[u].x, pc[u].y, wc[u], pad);
+        } else {
+          pc[u] = ldd2(m.cell_xy + 2 * cc[u]);
+          wc[u] = ld(w + cc[u]);
+        }
+      }
 #pragma unroll
       for (int u = 0; u < MB_F2_LSQ_BATCH; ++u) {
         const double dx = pc[u].x - c.x, dy = pc[u].y - c.y, dw = wc[u] - wi;
@@ -500,8 +518,16 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
     for (; k < L; ++k) {
       int cc = ld1_stream(ix + 32 * k, pst);
       cc = cc < 0 ? i : cc;
-      const double2 pc = ldd2(m.cell_xy + 2 * cc);
-      const double dx = pc.x - c.x, dy = pc.y - c.y, dw = ld(w + cc) - wi;
+      double2 pc;
+      double wcc;
+      if (ROWS) {
+        double pad;
+        ld4d(rows + 4 * (long long)cc, pc.x, pc.y, wcc, pad);
+      } else {
+        pc = ldd2(m.cell_xy + 2 * cc);
+        wcc = ld(w + cc);
+      }
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dw = wcc - wi;
       ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
       jx += (dx * dw); jy += (dy * dw);
     }
@@ -569,10 +595,11 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
   }
 }
 
-template <bool ORDER2, bool DIFF>
+template <bool ORDER2, bool DIFF, bool ROWS>
 __global__ void __launch_bounds__(MB_P1_BLOCK, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
-                                                      double *__restrict__ rec, double *__restrict__ wn, int ncb) {
-  f2_phase1<ORDER2, DIFF>(m, bc, w, rec, wn, ncb, blockIdx.x);
+                                                      double *__restrict__ rec, double *__restrict__ wn, int ncb,
+                                                      const double *__restrict__ rows) {
+  f2_phase1<ORDER2, DIFF, ROWS>(m, bc, w, rec, wn, ncb, blockIdx.x, rows);
 }
 
 #ifndef MB_P2_MIN_BLOCKS
@@ -583,12 +610,14 @@ __global__ void __launch_bounds__(MB_P1_BLOCK, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_
 #endif
 
 // block `bid` of phase 2: fluxes and update of its cells
-template <bool ORDER2, bool DIFF>
+// WROWS: also write the rows {x, y, w_out, 0} of the result (the next step's ROWS input)
+template <bool ORDER2, bool DIFF, bool WROWS = false>
 __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p,
                                           const double *__restrict__ w, double *__restrict__ w_out,
                                           const double *__restrict__ sign, const double *__restrict__ src,
                                           const double *__restrict__ dt_dev, const double *__restrict__ rec,
-                                          const double *__restrict__ wn, int bid) {
+                                          const double *__restrict__ wn, int bid,
+                                          double *__restrict__ rows_out = nullptr) {
   const int i = bid * blockDim.x + threadIdx.x;
   if (i >= m.nbcells) return;
   const GhostRule ghost = make_rule(m, bc, w);
@@ -696,18 +725,21 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
   }
   const double dt = *dt_dev;
   const double sc = src ? ld(src + i) : 0.0;
-  w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
+  const double wnew = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
+  w_out[i] = wnew;
+  if (WROWS) st4d_plain(rows_out + 4 * (long long)i, ci.x, ci.y, wnew, 0.0);
 }
 
-template <bool ORDER2, bool DIFF>
+template <bool ORDER2, bool DIFF, bool WROWS>
 __global__ void __launch_bounds__(MB_P2_BLOCK, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,
                                                          const double *__restrict__ dt_dev,
                                                          const double *__restrict__ rec,
-                                                         const double *__restrict__ wn) {
-  f2_phase2<ORDER2, DIFF>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x);
+                                                         const double *__restrict__ wn,
+                                                         double *__restrict__ rows_out) {
+  f2_phase2<ORDER2, DIFF, WROWS>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x, rows_out);
 }
 
 // ---------------------------------------------------------------- batches of triangle meshes, FP64
@@ -768,14 +800,21 @@ __global__ void k_batch_tick(int32_t *clock) { *clock += 1; }
 #define MB_F3_LSQ_BATCH 4
 #endif
 
-// Pack pass of the 3D step: rows {x, y, z, w} of every cell (centre and value in
-// one 32-byte row), so that the least-squares stencil gathers one row per neighbour.
-__global__ void __launch_bounds__(kBlock) k_f3_pack(mb_mesh m, const double *__restrict__ w, double *__restrict__ rows) {
+// Pack pass: rows of every cell with its centre and value in one 32-byte row ({x, y, w, 0}
+// for triangles, {x, y, z, w} for tetrahedra), so that the least-squares stencil gathers
+// one row per neighbour.
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_pack_rows(mb_mesh m, const double *__restrict__ w, double *__restrict__ rows) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.nbcells) return;
-  double x, y, z, pad;
-  ld4d_stream(m.cell_xy + 4 * (long long)i, x, y, z, pad, l2_stream());
-  st4_keep(rows + 4 * (long long)i, x, y, z, ld(w + i), l2_keep());
+  if (DIM == 2) {
+    const double2 c = ldd2(m.cell_xy + 2 * i);
+    st4_keep(rows + 4 * (long long)i, c.x, c.y, ld(w + i), 0.0, l2_keep());
+  } else {
+    double x, y, z, pad;
+    ld4d_stream(m.cell_xy + 4 * (long long)i, x, y, z, pad, l2_stream());
+    st4_keep(rows + 4 * (long long)i, x, y, z, ld(w + i), l2_keep());
+  }
 }
 
 // one row {x, y, z, w} (written by the previous launch, read-only in phase 1)
@@ -897,14 +936,15 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
 #define MB_P2_3D_BLOCK kBlock
 #endif
 
-template <bool ORDER2, bool DIFF>
+template <bool ORDER2, bool DIFF, bool WROWS>
 __global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,
                                                          const double *__restrict__ dt_dev,
                                                          const double *__restrict__ rec,
-                                                         const double *__restrict__ wn) {
+                                                         const double *__restrict__ wn,
+                                                         double *__restrict__ rows_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.nbcells) return;
   const GhostRule ghost = make_rule(m, bc, w);
@@ -1004,176 +1044,9 @@ __global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phas
   }
   const double dt = *dt_dev;
   const double sc = src ? ld(src + i) : 0.0;
-  w_out[i] = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
-}
-
-// ---------------------------------------------------------------- staged first phase (both dimensions)
-//
-// One block per tile of kTile consecutive cells (the tile tables of mb_mesh).  The
-// block first copies the centre and value of every cell its stencils read -- its own
-// cells, then its halo -- into shared memory (structure of arrays, kTile + halo
-// entries), then each thread computes its cell's least-squares gradient from there
-// (same stencil, same order as the unstaged kernel), the Barth limiter and the
-// record; the block's nodes (those whose smallest incident cell is in the tile) take
-// their centre -> vertex values from the same rows.  A neighbour row is fetched once
-// per tile instead of once per cell that reads it.
-
-constexpr int kTile = 256;
-
-#ifndef MB_PS2_MIN_BLOCKS
-#define MB_PS2_MIN_BLOCKS 5
-#endif
-#ifndef MB_PS3_MIN_BLOCKS
-#define MB_PS3_MIN_BLOCKS 4
-#endif
-
-__device__ __forceinline__ int ld_u16(const uint16_t *p) { return (int)__ldg(p); }
-
-template <int DIM, bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kTile, DIM == 2 ? MB_PS2_MIN_BLOCKS : MB_PS3_MIN_BLOCKS)
-    k_fs_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w, double *__restrict__ rec,
-                double *__restrict__ wn) {
-  extern __shared__ double smem[];
-  const int cap = kTile + m.tile_max_halo;
-  double *sx = smem, *sy = smem + cap, *sz = smem + 2 * cap, *sw = smem + DIM * cap;
-  const GhostRule ghost = make_rule(m, bc, w);
-  const int t = blockIdx.x;
-  const int c0 = t * kTile;
-  const int nown = min(kTile, m.nbcells - c0);
-  const int hb = ld(m.tile_halo_ptr + t), nh = ld(m.tile_halo_ptr + t + 1) - hb;
-  const uint64_t pst = l2_stream();
-  // stage: own cells at [0, nown), halo entries at [kTile, kTile + nh)
-  for (int k = threadIdx.x; k < kTile + nh; k += blockDim.x) {
-    if (k >= nown && k < kTile) continue;
-    const int c = k < kTile ? c0 + k : ld1_stream(m.tile_halo_idx + hb + (k - kTile), pst);
-    if (DIM == 2) {
-      const double2 p = ldd2(m.cell_xy + 2 * c);
-      sx[k] = p.x;
-      sy[k] = p.y;
-    } else {
-      const D3 p = ld3(m.cell_xy + 4 * (long long)c);
-      sx[k] = p.x;
-      sy[k] = p.y;
-      sz[k] = p.z;
-    }
-    sw[k] = ld(w + c);
-  }
-  __syncthreads();
-  const uint64_t keep = l2_keep();
-  if (ORDER2 && (int)threadIdx.x < nown) {
-    const int li = threadIdx.x, i = c0 + li, lane = li & 31;
-    const double cx = sx[li], cy = sy[li], cz = DIM == 3 ? sz[li] : 0.0, wi = sw[li];
-    double ixx = 0., iyy = 0., izz = 0., ixy = 0., ixz = 0., iyz = 0., jx = 0., jy = 0., jz = 0.;
-    const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
-    const int L = (se - sb) >> 5;
-    const uint16_t *ix = m.lsq_loc + sb + lane;
-#pragma unroll 4
-    for (int k = 0; k < L; ++k) {
-      int l = ld_u16(ix + 32 * k);
-      l = l == 0xFFFF ? li : l;   // padding: the cell itself, an exact zero term
-      const double dx = sx[l] - cx, dy = sy[l] - cy, dw = sw[l] - wi;
-      ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
-      jx += (dx * dw); jy += (dy * dw);
-      if (DIM == 3) {
-        const double dz = sz[l] - cz;
-        izz += dz * dz; ixz += (dx * dz); iyz += (dy * dz);
-        jz += (dz * dw);
-      }
-    }
-    const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
-    for (int k = gb; k < ge; ++k) {
-      const int f = ld(m.ghostnid_idx + k);
-      const double *gc = m.face_ghostcenter + 3 * f;
-      const double dx = ld(gc) - cx, dy = ld(gc + 1) - cy;
-      const double dw = ghost(f) - wi;
-      ixx += dx * dx; iyy += dy * dy; ixy += (dx * dy);
-      jx += (dx * dw); jy += (dy * dw);
-      if (DIM == 3) {
-        const double dz = ld(gc + 2) - cz;
-        izz += dz * dz; ixz += (dx * dz); iyz += (dy * dz);
-        jz += (dz * dw);
-      }
-    }
-    const int4 vt = ld4(m.cell_vtx + 4 * i);
-    const int4 nb = ld4(m.cell_nbr + 4 * i);
-    if (DIM == 2) {
-      const double dia = ixx * iyy - ixy * ixy;
-      const double x = (iyy * jx - ixy * jy) / dia;
-      const double y = (ixx * jy - ixy * jx) / dia;
-      const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
-                    P2 = ldd2(m.node_coord + 2 * vt.z);
-      double wmax = wi, wmin = wi;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const int o = comp(nb, j);
-        const double b = o < 0 ? ghost(-1 - o) : ld(w + o);
-        wmax = pmax(wmax, b);
-        wmin = pmin(wmin, b);
-      }
-      double ps = 1.;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const double2 a = j == 0 ? P0 : (j == 1 ? P1 : P2), b = j == 0 ? P1 : (j == 1 ? P2 : P0);
-        const double r1 = 0.5 * (a.x + b.x) - cx, r2 = 0.5 * (a.y + b.y) - cy;
-        const double delta = x * r1 + y * r2;
-        double psi_ij = 1.;
-        if (!(fabs(delta) < 1e-8)) {
-          if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
-          if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
-        }
-        ps = pmin(ps, psi_ij);
-      }
-      st4_keep(rec + 4 * (long long)i, wi, x, y, ps, keep);
-    } else {
-      const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) -
-                         izz * (ixy * ixy);
-      const double gx = ((iyy * izz - iyz * iyz) * jx + (ixz * iyz - ixy * izz) * jy + (ixy * iyz - ixz * iyy) * jz) / dia;
-      const double gy = ((ixz * iyz - ixy * izz) * jx + (ixx * izz - ixz * ixz) * jy + (ixy * ixz - iyz * ixx) * jz) / dia;
-      const double gz = ((ixy * iyz - ixz * iyy) * jx + (ixy * ixz - iyz * ixx) * jy + (ixx * iyy - ixy * ixy) * jz) / dia;
-      const uint32_t fl = ld(m.cell_flags + i);
-      const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
-                       ld3(m.node_coord + 4 * vt.w)};
-      double wmax = wi, wmin = wi;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int o = comp(nb, j);
-        const double b = o < 0 ? ghost(-1 - o) : ld(w + o);
-        wmax = pmax(wmax, b);
-        wmin = pmin(wmin, b);
-      }
-      double ps = 1.;
-      const D3 c = d3(cx, cy, cz);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        int d0, d1, d2;
-        face_desc(fl, j, d0, d1, d2);
-        const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
-        const double delta = gx * (fc.x - c.x) + gy * (fc.y - c.y) + gz * (fc.z - c.z);
-        double psi_ij = 1.;
-        if (!(fabs(delta) < 1e-10)) {
-          if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
-          if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
-        }
-        ps = pmin(ps, psi_ij);
-      }
-      st4_keep(rec + 4 * (long long)i, wi, ps * gx, ps * gy, ps * gz, keep);
-    }
-  }
-  if (DIFF) {
-    const int nbeg = ld(m.tile_node_ptr + t), nn = ld(m.tile_node_ptr + t + 1) - nbeg;
-    for (int q = threadIdx.x; q < max(nn, kTile); q += blockDim.x) {
-      // the first kTile positions spread over all warps (position 32 (q % 8) + q / 8)
-      const int p = q < kTile ? ((q & 7) << 5) + (q >> 3) : q;
-      if (p >= nn) continue;
-      const int n = ld(m.tile_node_idx + nbeg + p);
-      double acc = 0.;
-      const int e0 = ld(m.n2c_ptr + n), e1 = ld(m.n2c_ptr + n + 1);
-      for (int e = e0; e < e1; ++e) acc += ldd_stream(m.n2c_alpha + e, pst) * sw[ld_u16(m.n2c_loc + e)];
-      const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
-      for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
-      st1_keep(wn + n, acc, keep);
-    }
-  }
+  const double wnew = wi + dt * ((rez + dis) / ld(m.cell_volume + i) + sc);
+  w_out[i] = wnew;
+  if (WROWS) st4d_plain(rows_out + 4 * (long long)i, ci.x, ci.y, ci.z, wnew);
 }
 
 // ---------------------------------------------------------------- shallow-water order-2 pre-pass
@@ -1208,22 +1081,6 @@ inline int grid_for(long long n) {
 
 inline int check_launch() { return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA; }
 
-inline bool staged_tables(const mb_mesh &m) {
-  return m.tile_halo_ptr && m.tile_halo_idx && m.lsq_loc && m.tile_node_ptr && m.tile_node_idx && m.n2c_loc &&
-         m.n2c_ptr && m.n2c_alpha && m.tile_max_halo >= 0 && kTile + m.tile_max_halo <= 2048;
-}
-
-// dynamic shared memory above the 48 KiB default needs the kernel's opt-in (set once per
-// kernel and size; a host-side attribute, not a stream operation)
-template <class K>
-inline cudaError_t staged_smem_attr(K kernel, size_t bytes) {
-  static size_t done = 0;
-  if (bytes <= 48 * 1024 || bytes <= done) return cudaSuccess;
-  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) done = bytes;
-  return e;
-}
-
 inline bool compact_tables(const mb_mesh &m) {
   return m.cell_vtx && m.cell_nbr && m.cell_flags && m.node_coord && m.cell_xy && m.lsq_sell_ptr &&
          m.lsq_sell_idx && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
@@ -1235,7 +1092,7 @@ inline bool compact_tables(const mb_mesh &m) {
 template <int DIM, bool O2, bool DF>
 int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                 double *w_out, const double *sign, const double *src, const double *dt, double *cs,
-                double *wn, cudaStream_t st) {
+                double *wn, cudaStream_t st, const double *rows_in = nullptr, double *rows_out = nullptr) {
   const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
   if (compact_tables(m)) {
@@ -1244,34 +1101,40 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
     // tables (3D) must start on 32-byte boundaries
     auto a32 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 31) == 0; };
     if ((O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord)))) return MB_EINVAL;
+    if ((rows_in && !a32(rows_in)) || (rows_out && !a32(rows_out))) return MB_EINVAL;
 #endif
 #if MB_V4_IO
     if (DIM == 2 && (reinterpret_cast<uintptr_t>(sign) & 31) != 0) return MB_EINVAL;
 #endif
-    if (staged_tables(m) && (O2 || DF)) {
-      // staged first phase: one block per tile, the tile's stencil rows in shared memory
-      const size_t smem = (size_t)(kTile + m.tile_max_halo) * (DIM + 1) * sizeof(double);
-      if (staged_smem_attr(k_fs_phase1<DIM, O2, DF>, smem) != cudaSuccess) return MB_ECUDA;
-      k_fs_phase1<DIM, O2, DF><<<ceil_div(m.nbcells, kTile), kTile, smem, st>>>(m, bc, w_in, cs, wn);
-      if (DIM == 2)
-        k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_BLOCK), MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign,
-                                                                                      src, dt, cs, wn);
-      else
-        k_f3_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_3D_BLOCK), MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out,
-                                                                                            sign, src, dt, cs, wn);
-    } else if (DIM == 2) {
+    const int gp2 = ceil_div(m.nbcells, DIM == 2 ? MB_P2_BLOCK : MB_P2_3D_BLOCK);
+    if (DIM == 2) {
       const int ncb2 = O2 ? ceil_div(m.nbcells, MB_P1_BLOCK) : 0;
       const int nnb2 = DF ? ceil_div(m.nbnodes, MB_P1_BLOCK) : 0;
-      if (ncb2 + nnb2 > 0) k_f2_phase1<O2, DF><<<ncb2 + nnb2, MB_P1_BLOCK, 0, st>>>(m, bc, w_in, cs, wn, ncb2);
-      k_f2_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_BLOCK), MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign,
-                                                                                    src, dt, cs, wn);
+      if (ncb2 + nnb2 > 0) {
+        if (rows_in)
+          k_f2_phase1<O2, DF, true><<<ncb2 + nnb2, MB_P1_BLOCK, 0, st>>>(m, bc, w_in, cs, wn, ncb2, rows_in);
+        else
+          k_f2_phase1<O2, DF, false><<<ncb2 + nnb2, MB_P1_BLOCK, 0, st>>>(m, bc, w_in, cs, wn, ncb2, nullptr);
+      }
+      if (rows_out)
+        k_f2_phase2<O2, DF, true><<<gp2, MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out);
+      else
+        k_f2_phase2<O2, DF, false><<<gp2, MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr);
     } else {
-      // cell scratch: records [0, 4 nbcells), rows [4 nbcells, 8 nbcells)
-      double *rows = cs ? cs + 4 * (long long)m.nbcells : nullptr;
-      if (O2) k_f3_pack<<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, w_in, rows);
+      // cell scratch: records [0, 4 nbcells), then (without rows_in) the pack pass's rows
+      const double *rows = rows_in;
+      if (O2 && !rows) {
+        double *pk = cs + 4 * (long long)m.nbcells;
+        k_pack_rows<3><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, w_in, pk);
+        rows = pk;
+      }
       if (ncb + nnb > 0) k_f3_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, rows, wn, ncb);
-      k_f3_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2_3D_BLOCK), MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out,
-                                                                                          sign, src, dt, cs, wn);
+      if (rows_out)
+        k_f3_phase2<O2, DF, true><<<gp2, MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
+                                                                 rows_out);
+      else
+        k_f3_phase2<O2, DF, false><<<gp2, MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
+                                                                  nullptr);
     }
     return check_launch();
   }
@@ -1440,6 +1303,42 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
   cudaStream_t st = ST(stream);
 #define MB_STEP(D, O, F) \
   return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, st)
+  if (m->dim == 2) {
+    if (o2) { if (df) MB_STEP(2, true, true); else MB_STEP(2, true, false); }
+    else { if (df) MB_STEP(2, false, true); else MB_STEP(2, false, false); }
+  } else {
+    if (o2) { if (df) MB_STEP(3, true, true); else MB_STEP(3, true, false); }
+    else { if (df) MB_STEP(3, false, true); else MB_STEP(3, false, false); }
+  }
+#undef MB_STEP
+}
+
+int mb_pack_rows(const mb_mesh *m, const double *w, double *rows, void *stream) {
+  MB_NVTX();
+  if (!mesh_ok(m) || !w || !rows || !m->cell_xy || (reinterpret_cast<uintptr_t>(rows) & 31) != 0) return MB_EINVAL;
+  if (m->dim == 2)
+    k_pack_rows<2><<<ceil_div(m->nbcells, kBlock), kBlock, 0, ST(stream)>>>(*m, w, rows);
+  else
+    k_pack_rows<3><<<ceil_div(m->nbcells, kBlock), kBlock, 0, ST(stream)>>>(*m, w, rows);
+  return check_launch();
+}
+
+int mb_advdiff_step_rows(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p, const double *w_in,
+                         double *w_out, const double *rows_in, double *rows_out, const double *sign_cf,
+                         const double *src, const double *dt_dev, double *cell_scratch, double *node_scratch,
+                         void *stream) {
+  MB_NVTX();
+  if (!mesh_ok(m) || !bc || !p || !w_in || !w_out || w_in == w_out || !sign_cf || !dt_dev) return MB_EINVAL;
+  if (!rows_in || !rows_out || rows_in == rows_out || !compact_tables(*m)) return MB_EINVAL;
+  if (p->order != 1 && p->order != 2) return MB_EINVAL;
+  const bool o2 = p->order == 2, df = p->diffusion != 0;
+  if (o2 && !cell_scratch) return MB_EINVAL;
+  if (df && (!node_scratch || !bc->face_grad_on)) return MB_EINVAL;
+  if (!bc->kind || !bc->value) return MB_EINVAL;
+  cudaStream_t st = ST(stream);
+#define MB_STEP(D, O, F)                                                                                     \
+  return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, st, \
+                              rows_in, rows_out)
   if (m->dim == 2) {
     if (o2) { if (df) MB_STEP(2, true, true); else MB_STEP(2, true, false); }
     else { if (df) MB_STEP(2, false, true); else MB_STEP(2, false, false); }

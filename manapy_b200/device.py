@@ -8,8 +8,6 @@ kernels are called through the C ABI with their raw pointers.
 """
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 import torch
 
@@ -225,7 +223,6 @@ class DeviceMesh:
             self._compact_2d(A, T, dev)
         else:
             self._compact_3d(A, T, dev)
-        self._add_tiles(T, dev)
         self.t = T
         # field permutations: device[k] = host[perm[k]], host[j] = device[inv[j]]
         i64 = np.int64
@@ -277,7 +274,6 @@ class DeviceMesh:
         self.reordered = bool(reorder)
         dev = torch.device(device) if device is not None else None
         self.device = dev
-        self._add_tiles(T, None)
         self.t = {k: _t(v, v.dtype, dev) for k, v in T.items()}
         self.perm = {k: _t(v, np.int64, dev) for k, v in perm.items()}
         self.inv = {k: _t(v, np.int64, dev) for k, v in inv.items()}
@@ -286,13 +282,10 @@ class DeviceMesh:
 
     def _make_struct(self):
         s = _lib.MbMesh()
-        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf = (self.dim, self.nbcells, self.nbfaces, self.nbnodes,
-                                                         self.nlf)
-        # "tile_halo_max": a one-element table (it travels with the tables through caches and
-        # uploads); the struct takes its value
-        s.tile_max_halo = int(self.t["tile_halo_max"][0]) if "tile_halo_max" in self.t else 0
-        for name, typ in _lib.MbMesh._fields_:
-            if name in self.t and typ is ctypes.c_void_p:
+        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = (self.dim, self.nbcells, self.nbfaces,
+                                                                  self.nbnodes, self.nlf, 0)
+        for name, _ in _lib.MbMesh._fields_:
+            if name in self.t:
                 setattr(s, name, self.t[name].data_ptr())
         return s
 
@@ -338,21 +331,6 @@ class DeviceMesh:
         """Drop the host arrays ``A`` (before sending host-built tables to another process)."""
         self.A = None
         return self
-
-    def _add_tiles(self, T, dev):
-        """The tile tables of the staged first phase (``tiles.py``), when the mesh has
-        least-squares stencils and every tile's stencil union fits the shared memory."""
-        from . import tiles
-        if "cellnid_ptr" not in T or "lsq_sell_ptr" not in T:
-            return
-        host = {k: (T[k].cpu().numpy() if isinstance(T[k], torch.Tensor) else T[k])
-                for k in ("cellnid_ptr", "cellnid_idx", "n2c_ptr", "n2c_idx", "lsq_sell_ptr")}
-        tt = tiles.tile_tables(host, self.nbcells)
-        if tt is None:
-            return
-        T["tile_halo_max"] = _t(np.array([tt.pop("tile_max_halo")], np.int32), np.int32, dev)
-        for k, v in tt.items():
-            T[k] = _t(v, v.dtype, dev)
 
     def _compact_2d(self, A, T, dev):
         """Cell-centred tables of the fused 2D step (see ``mb_mesh`` in the C header)."""

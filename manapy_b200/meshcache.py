@@ -26,8 +26,8 @@ import numpy as np
 __all__ = ["mesh_key", "load_or_build", "entry_path"]
 
 FORMAT = 1
-_SOURCES = ("geometry.py", "reorder.py", "device.py", "tiles.py", "meshcache.py", "host/common.hpp",
-            "host/mesh2d.cpp", "host/geom3d.cpp")
+_SOURCES = ("geometry.py", "reorder.py", "device.py", "meshcache.py", "host/common.hpp", "host/mesh2d.cpp",
+            "host/geom3d.cpp")
 _digest = None
 
 

@@ -272,6 +272,28 @@ class AdvectionDiffusionSolver:
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
 
+    # rows {centre, value} carried from step to step (second order): each cell buffer has a
+    # rows buffer; _rows_version is the cell version whose rows are current
+    def _use_rows(self):
+        return self.order == 2 and "cell_vtx" in self._dm.t
+
+    def _rows_of(self, buf):
+        if getattr(self, "_rowbufs", None) is None:
+            self._rowbufs = {}
+        r = self._rowbufs.get(buf.data_ptr())
+        if r is None:
+            r = torch.empty(4 * self._dm.nbcells, dtype=torch.float64, device=self._dm.device)
+            self._rowbufs[buf.data_ptr()] = r
+        return r
+
+    def _ensure_rows(self, buf):
+        """Rows of ``buf`` (the current cell array), packed if the state changed since a step
+        wrote them."""
+        if getattr(self, "_rows_version", None) != self.var.version("cell"):
+            _lib.call("mb_pack_rows", self._dm.struct, _p(buf), _p(self._rows_of(buf)), self._stream())
+            self._rows_version = self.var.version("cell")
+        return self._rows_of(buf)
+
     def _fused_step(self):
         if self.precision == "fp32c":
             return self._fused_step_f32c()
@@ -283,10 +305,17 @@ class AdvectionDiffusionSolver:
             self._spare = torch.empty_like(w_in)
         w_out = self._spare
         cs, ns = self._scratch()
-        _lib.call("mb_advdiff_step", dm.struct, var.device_bc.struct, self._params, _p(w_in), _p(w_out),
-                  _p(self._sign), self._source_ptr(), _p(self._dt_dev), _p(cs), _p(ns), self._stream())
+        if self._use_rows():
+            rin = self._ensure_rows(w_in)
+            _lib.call("mb_advdiff_step_rows", dm.struct, var.device_bc.struct, self._params, _p(w_in), _p(w_out),
+                      _p(rin), _p(self._rows_of(w_out)), _p(self._sign), self._source_ptr(), _p(self._dt_dev), _p(cs),
+                      _p(ns), self._stream())
+        else:
+            _lib.call("mb_advdiff_step", dm.struct, var.device_bc.struct, self._params, _p(w_in), _p(w_out),
+                      _p(self._sign), self._source_ptr(), _p(self._dt_dev), _p(cs), _p(ns), self._stream())
         self._spare = var.swap_cell(w_out)
         self._install_lazies(self._spare)
+        self._rows_version = var.version("cell")
 
     # ------------------------------------------------------------ fp32c mode
     def _f32_state(self):
@@ -366,13 +395,10 @@ class AdvectionDiffusionSolver:
             check_state([self.var.dev("cell")], names=["the cell values"])
 
     def launches_per_step(self):
-        """Kernel launches of one fused step (tetrahedra at order 2 without tile tables: a
-        pack pass first)."""
-        n = 1 + int(self.order == 2 or bool(self.diffusion))
-        staged = self._dm is not None and "lsq_loc" in self._dm.t
-        if self.dim == 3 and self.order == 2 and self.precision == "fp64" and not staged:
-            n += 1
-        return n
+        """Kernel launches of one fused step."""
+        # (tetrahedra at order 2 through mb_advdiff_step pack rows first; the solver's steps
+        # carry them from one step to the next instead)
+        return 1 + int(self.order == 2 or bool(self.diffusion))
 
     def release_graphs(self):
         self._graph = None
@@ -411,11 +437,14 @@ class AdvectionDiffusionSolver:
                 a.copy_(cur)
                 var.swap_cell(a)
                 self._spare = b
+            if self._use_rows() and n // depth:
+                self._ensure_rows(a)         # the captured steps start from a's rows
             for _ in range(n // depth):
                 g.replay()
             if n // depth:
                 var._s.version["cell"] += 1
                 self._install_lazies(self._spare)
+                self._rows_version = var.version("cell")
             for _ in range(n % depth):
                 self._fused_step()
         if self._dt_host is None:
@@ -478,11 +507,19 @@ class AdvectionDiffusionSolver:
         g = torch.cuda.CUDAGraph()
         with torch.cuda.stream(s):
             # warm-up outside capture is not needed: the library performs no lazy init
+            rows = self._use_rows()
+            if rows:
+                self._rows_of(a), self._rows_of(b)   # allocated before the capture
             with torch.cuda.graph(g, stream=s):
                 st = torch.cuda.current_stream(dm.device).cuda_stream
                 for x, y in ((a, b), (b, a)) * (int(self.graph_depth) // 2):
-                    _lib.call("mb_advdiff_step", dm.struct, args[0], args[1], _p(x), _p(y), _p(self._sign),
-                              src, _p(self._dt_dev), _p(cs), _p(ns), st)
+                    if rows:
+                        _lib.call("mb_advdiff_step_rows", dm.struct, args[0], args[1], _p(x), _p(y),
+                                  _p(self._rows_of(x)), _p(self._rows_of(y)), _p(self._sign), src, _p(self._dt_dev),
+                                  _p(cs), _p(ns), st)
+                    else:
+                        _lib.call("mb_advdiff_step", dm.struct, args[0], args[1], _p(x), _p(y), _p(self._sign),
+                                  src, _p(self._dt_dev), _p(cs), _p(ns), st)
         torch.cuda.current_stream(dm.device).wait_stream(s)
         self._graph = g
         self._graph_bufs = (a, b)

@@ -115,7 +115,7 @@ def test_bench_sharded_mode_runs_two_ranks(tmp_path, cuda):
     env = dict(os.environ, MANAPY_B200_BENCH_BACKEND="gloo")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), os.path.join(root, "bench.py"), "--gpus", "2",
-           "--steps", "3", "--warmup", "3", "--n", "60", "--min-timed-steps", "3", "--e2e-steps", "2"]
+           "--steps", "3", "--warmup", "3", "--mesh-n", "60", "--min-timed-steps", "3", "--e2e-steps", "2"]
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env, cwd=root)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]

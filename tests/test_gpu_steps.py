@@ -271,3 +271,41 @@ def test_state_checks_raise(cuda):
     w.cell = x
     with pytest.raises(FloatingPointError):
         S2.check()
+
+
+@pytest.mark.parametrize("wl", [W.C2.scaled(n=50), W.C4.scaled(n=7)])
+def test_row_carrying_step_matches_the_plain_step(wl, cuda):
+    """mb_advdiff_step_rows (rows {centre, value} in, rows of the result out) gives the
+    results of mb_advdiff_step, and its rows_out are the rows mb_pack_rows makes of w_out."""
+    import gpuutil as U
+    from manapy_b200 import _lib
+    el, vx = wl.mesh()
+    A = G.build(el, vx, wl.dim)
+    dm = U.mesh(A, reorder=True)
+    db = U.bc(A, B.resolve(A, wl.bc, wl.bc_values), dm)
+    R = dm.R
+    uf, vf, wf = wl.velocity(A["faces_center"])
+    st = U.stream()
+    nc, nn = A["nbcells"], A["nbnodes"]
+    sign = U.Z(4 * nc)
+    u_, v_, w_ = U.T(uf[R.fperm]), U.T(vf[R.fperm]), U.T(wf[R.fperm])
+    U.call("mb_cell_face_sign", dm.struct, U.P(u_), U.P(v_), U.P(w_), U.P(sign), st)
+    cells = [U.Z(nc) for _ in range(3)]
+    for f, c in zip((u_, v_, w_), cells):
+        U.call("mb_facetocell", dm.struct, U.P(f), U.P(c), st)
+    dt = U.Z(1)
+    U.call("mb_time_step", dm.struct, *[U.P(c) for c in cells], wl.cfl, *wl.diffusion, U.P(dt), st)
+    prm = _lib.MbAdvDiffParams(wl.order, 1, *wl.diffusion)
+    w0 = U.T(wl.init(A["cells_center"])[R.cperm])
+    cs, ns = U.Z(8 * nc), U.Z(nn)
+    ref = U.Z(nc)
+    U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w0), U.P(ref), U.P(sign), None, U.P(dt), U.P(cs),
+           U.P(ns), st)
+    rin, rout, packed = U.Z(4 * nc), U.Z(4 * nc), U.Z(4 * nc)
+    U.call("mb_pack_rows", dm.struct, U.P(w0), U.P(rin), st)
+    got = U.Z(nc)
+    U.call("mb_advdiff_step_rows", dm.struct, db.struct, prm, U.P(w0), U.P(got), U.P(rin), U.P(rout), U.P(sign),
+           None, U.P(dt), U.P(cs), U.P(ns), st)
+    U.call("mb_pack_rows", dm.struct, U.P(got), U.P(packed), st)
+    assert rel_max(U.H(got), U.H(ref)) <= 1e-14
+    assert np.array_equal(U.H(rout), U.H(packed))
