@@ -50,7 +50,8 @@ typedef struct mb_mesh {
   int32_t nbfaces;
   int32_t nbnodes;
   int32_t nlf;       /* faces per cell: 3 or 4 */
-  int32_t pad_;
+  int32_t variant;   /* launch shapes of the fused advection-diffusion phases (second order with
+                        diffusion): bits 0-1 first phase, bits 2-3 second; 0 = the defaults */
   /* cells */
   const double *cell_center;    /* [nbcells][3] */
   const double *cell_volume;    /* [nbcells] */

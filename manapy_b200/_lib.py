@@ -24,7 +24,7 @@ _d = ctypes.c_double
 
 class MbMesh(ctypes.Structure):
     _fields_ = [("dim", _i32), ("nbcells", _i32), ("nbfaces", _i32), ("nbnodes", _i32),
-                ("nlf", _i32), ("pad_", _i32),
+                ("nlf", _i32), ("variant", _i32),
                 ("cell_center", _vp), ("cell_volume", _vp), ("cell_faces", _vp),
                 ("cell_order", _vp), ("cellnid_ptr", _vp), ("cellnid_idx", _vp),
                 ("ghostnid_ptr", _vp), ("ghostnid_idx", _vp),

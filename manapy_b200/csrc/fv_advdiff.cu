@@ -595,8 +595,15 @@ __device__ __forceinline__ void f2_phase1(const mb_mesh &m, const mb_bc &bc, con
   }
 }
 
-template <bool ORDER2, bool DIFF, bool ROWS>
-__global__ void __launch_bounds__(MB_P1_BLOCK, MB_P1_MIN_BLOCKS) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+// Launch shapes of the fused phases: variant v of a kernel runs blocks of kP*B[v] threads
+// with launch bounds for kP*M[v] resident blocks per SM.  Variant 0 is the measured default;
+// the others are selected per mesh (mb_mesh.variant, picked by the autotuner) for second
+// order with diffusion.
+constexpr int kP1B[4] = {MB_P1_BLOCK, 128, 256, 512};
+constexpr int kP1M[4] = {MB_P1_MIN_BLOCKS, 12, 4, 3};
+
+template <bool ORDER2, bool DIFF, bool ROWS, int VAR>
+__global__ void __launch_bounds__(kP1B[VAR], kP1M[VAR]) k_f2_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                       double *__restrict__ rec, double *__restrict__ wn, int ncb,
                                                       const double *__restrict__ rows) {
   f2_phase1<ORDER2, DIFF, ROWS>(m, bc, w, rec, wn, ncb, blockIdx.x, rows);
@@ -730,8 +737,11 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
   if (WROWS) st4d_plain(rows_out + 4 * (long long)i, ci.x, ci.y, wnew, 0.0);
 }
 
-template <bool ORDER2, bool DIFF, bool WROWS>
-__global__ void __launch_bounds__(MB_P2_BLOCK, MB_P2_MIN_BLOCKS) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+constexpr int kP2B[4] = {MB_P2_BLOCK, 256, 64, 128};
+constexpr int kP2M[4] = {MB_P2_MIN_BLOCKS, 3, 14, 8};
+
+template <bool ORDER2, bool DIFF, bool WROWS, int VAR>
+__global__ void __launch_bounds__(kP2B[VAR], kP2M[VAR]) k_f2_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,
@@ -822,8 +832,11 @@ __device__ __forceinline__ void ld_row(const double *p, double &x, double &y, do
   ld4d(p, x, y, z, w);
 }
 
-template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+constexpr int kQ1B[4] = {kBlock, 128, 256, 128};
+constexpr int kQ1M[4] = {MB_P1_3D_MIN_BLOCKS, 8, 3, 6};
+
+template <bool ORDER2, bool DIFF, int VAR>
+__global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                                         double *__restrict__ rec,
                                                                         const double *__restrict__ rows,
                                                                         double *__restrict__ wn, int ncb) {
@@ -936,8 +949,11 @@ __global__ void __launch_bounds__(kBlock, MB_P1_3D_MIN_BLOCKS) k_f3_phase1(mb_me
 #define MB_P2_3D_BLOCK kBlock
 #endif
 
-template <bool ORDER2, bool DIFF, bool WROWS>
-__global__ void __launch_bounds__(MB_P2_3D_BLOCK, MB_P2_3D_MIN_BLOCKS) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
+constexpr int kQ2B[4] = {MB_P2_3D_BLOCK, 128, 128, 64};
+constexpr int kQ2M[4] = {MB_P2_3D_MIN_BLOCKS, 4, 5, 8};
+
+template <bool ORDER2, bool DIFF, bool WROWS, int VAR>
+__global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
                                                          const double *__restrict__ w, double *__restrict__ w_out,
                                                          const double *__restrict__ sign,
                                                          const double *__restrict__ src,
@@ -1086,6 +1102,77 @@ inline bool compact_tables(const mb_mesh &m) {
          m.lsq_sell_idx && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
 }
 
+// launches of the fused phases in launch-shape variant v (variants beyond 0 exist for
+// second order with diffusion only)
+template <bool O2, bool DF, bool ROWS, int V>
+inline void f2_p1_run(const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, double *wn,
+                      const double *rows, cudaStream_t st) {
+  const int ncb = O2 ? ceil_div(m.nbcells, kP1B[V]) : 0, nnb = DF ? ceil_div(m.nbnodes, kP1B[V]) : 0;
+  k_f2_phase1<O2, DF, ROWS, V><<<ncb + nnb, kP1B[V], 0, st>>>(m, bc, w, cs, wn, ncb, rows);
+}
+template <bool O2, bool DF, bool ROWS>
+inline void f2_p1_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, double *wn,
+                       const double *rows, cudaStream_t st) {
+  if constexpr (O2 && DF) {
+    if (v == 1) return f2_p1_run<O2, DF, ROWS, 1>(m, bc, w, cs, wn, rows, st);
+    if (v == 2) return f2_p1_run<O2, DF, ROWS, 2>(m, bc, w, cs, wn, rows, st);
+    if (v == 3) return f2_p1_run<O2, DF, ROWS, 3>(m, bc, w, cs, wn, rows, st);
+  }
+  f2_p1_run<O2, DF, ROWS, 0>(m, bc, w, cs, wn, rows, st);
+}
+template <bool O2, bool DF, bool WROWS, int V>
+inline void f2_p2_run(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
+                      double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
+                      const double *wn, double *rows_out, cudaStream_t st) {
+  k_f2_phase2<O2, DF, WROWS, V><<<ceil_div(m.nbcells, kP2B[V]), kP2B[V], 0, st>>>(m, bc, p, w_in, w_out, sign, src,
+                                                                                   dt, cs, wn, rows_out);
+}
+template <bool O2, bool DF, bool WROWS>
+inline void f2_p2_pick(int v, const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
+                       double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
+                       const double *wn, double *rows_out, cudaStream_t st) {
+  if constexpr (O2 && DF) {
+    if (v == 1) return f2_p2_run<O2, DF, WROWS, 1>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+    if (v == 2) return f2_p2_run<O2, DF, WROWS, 2>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+    if (v == 3) return f2_p2_run<O2, DF, WROWS, 3>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+  }
+  f2_p2_run<O2, DF, WROWS, 0>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+}
+template <bool O2, bool DF, int V>
+inline void f3_p1_run(const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows, double *wn,
+                      cudaStream_t st) {
+  const int ncb = O2 ? ceil_div(m.nbcells, kQ1B[V]) : 0, nnb = DF ? ceil_div(m.nbnodes, kQ1B[V]) : 0;
+  k_f3_phase1<O2, DF, V><<<ncb + nnb, kQ1B[V], 0, st>>>(m, bc, w, cs, rows, wn, ncb);
+}
+template <bool O2, bool DF>
+inline void f3_p1_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows,
+                       double *wn, cudaStream_t st) {
+  if constexpr (O2 && DF) {
+    if (v == 1) return f3_p1_run<O2, DF, 1>(m, bc, w, cs, rows, wn, st);
+    if (v == 2) return f3_p1_run<O2, DF, 2>(m, bc, w, cs, rows, wn, st);
+    if (v == 3) return f3_p1_run<O2, DF, 3>(m, bc, w, cs, rows, wn, st);
+  }
+  f3_p1_run<O2, DF, 0>(m, bc, w, cs, rows, wn, st);
+}
+template <bool O2, bool DF, bool WROWS, int V>
+inline void f3_p2_run(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
+                      double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
+                      const double *wn, double *rows_out, cudaStream_t st) {
+  k_f3_phase2<O2, DF, WROWS, V><<<ceil_div(m.nbcells, kQ2B[V]), kQ2B[V], 0, st>>>(m, bc, p, w_in, w_out, sign, src,
+                                                                                   dt, cs, wn, rows_out);
+}
+template <bool O2, bool DF, bool WROWS>
+inline void f3_p2_pick(int v, const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
+                       double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
+                       const double *wn, double *rows_out, cudaStream_t st) {
+  if constexpr (O2 && DF) {
+    if (v == 1) return f3_p2_run<O2, DF, WROWS, 1>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+    if (v == 2) return f3_p2_run<O2, DF, WROWS, 2>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+    if (v == 3) return f3_p2_run<O2, DF, WROWS, 3>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+  }
+  f3_p2_run<O2, DF, WROWS, 0>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+}
+
 // cell scratch: [4][nbcells] planes gx, gy, gz, psi (face-table path), [nbcells][4]
 // records {w, gx, gy, psi} (compact 2D path) or [nbcells][4] records {w, psi gx, psi gy,
 // psi gz} then [nbcells][4] rows {x, y, z, w} (compact 3D path); node scratch: [nbnodes]
@@ -1106,20 +1193,15 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
 #if MB_V4_IO
     if (DIM == 2 && (reinterpret_cast<uintptr_t>(sign) & 31) != 0) return MB_EINVAL;
 #endif
-    const int gp2 = ceil_div(m.nbcells, DIM == 2 ? MB_P2_BLOCK : MB_P2_3D_BLOCK);
+    // launch-shape variants (second order with diffusion only): bits 0-1 phase 1, bits 2-3 phase 2
+    const int v1 = (O2 && DF) ? (m.variant & 3) : 0, v2 = (O2 && DF) ? ((m.variant >> 2) & 3) : 0;
     if (DIM == 2) {
-      const int ncb2 = O2 ? ceil_div(m.nbcells, MB_P1_BLOCK) : 0;
-      const int nnb2 = DF ? ceil_div(m.nbnodes, MB_P1_BLOCK) : 0;
-      if (ncb2 + nnb2 > 0) {
-        if (rows_in)
-          k_f2_phase1<O2, DF, true><<<ncb2 + nnb2, MB_P1_BLOCK, 0, st>>>(m, bc, w_in, cs, wn, ncb2, rows_in);
-        else
-          k_f2_phase1<O2, DF, false><<<ncb2 + nnb2, MB_P1_BLOCK, 0, st>>>(m, bc, w_in, cs, wn, ncb2, nullptr);
+      if (O2 || DF) {
+        if (rows_in) f2_p1_pick<O2, DF, true>(v1, m, bc, w_in, cs, wn, rows_in, st);
+        else f2_p1_pick<O2, DF, false>(v1, m, bc, w_in, cs, wn, nullptr, st);
       }
-      if (rows_out)
-        k_f2_phase2<O2, DF, true><<<gp2, MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out);
-      else
-        k_f2_phase2<O2, DF, false><<<gp2, MB_P2_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr);
+      if (rows_out) f2_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+      else f2_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, st);
     } else {
       // cell scratch: records [0, 4 nbcells), then (without rows_in) the pack pass's rows
       const double *rows = rows_in;
@@ -1128,13 +1210,9 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
         k_pack_rows<3><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, w_in, pk);
         rows = pk;
       }
-      if (ncb + nnb > 0) k_f3_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, rows, wn, ncb);
-      if (rows_out)
-        k_f3_phase2<O2, DF, true><<<gp2, MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
-                                                                 rows_out);
-      else
-        k_f3_phase2<O2, DF, false><<<gp2, MB_P2_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
-                                                                  nullptr);
+      if (O2 || DF) f3_p1_pick<O2, DF>(v1, m, bc, w_in, cs, rows, wn, st);
+      if (rows_out) f3_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+      else f3_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, st);
     }
     return check_launch();
   }

@@ -282,8 +282,9 @@ class DeviceMesh:
 
     def _make_struct(self):
         s = _lib.MbMesh()
-        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf, s.pad_ = (self.dim, self.nbcells, self.nbfaces,
-                                                                  self.nbnodes, self.nlf, 0)
+        s.dim, s.nbcells, s.nbfaces, s.nbnodes, s.nlf = (self.dim, self.nbcells, self.nbfaces, self.nbnodes,
+                                                         self.nlf)
+        s.variant = int(getattr(self, "variant", 0))
         for name, _ in _lib.MbMesh._fields_:
             if name in self.t:
                 setattr(s, name, self.t[name].data_ptr())

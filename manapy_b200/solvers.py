@@ -64,7 +64,10 @@ class AdvectionDiffusionSolver:
                                                  "fluxes with compensated per-cell sums, FP64 geometry and dt "
                                                  "(no counterpart in manapy)"),
                    ("graph_depth", object, "auto", 0, "steps per CUDA-graph replay in advance(graph=True): an "
-                                                      "even number, or 'auto' (measured by manapy_b200.autotune)")]
+                                                      "even number, or 'auto' (measured by manapy_b200.autotune)"),
+                   ("launch", object, "auto", 0, "launch shapes of the fused phases: 'auto' (measured by "
+                                                 "manapy_b200.autotune at the first graph advance), or a variant "
+                                                 "number (bits 0-1 first phase, 2-3 second; 0 = defaults)")]
 
     @classmethod
     def process_conf(cls, conf, kwargs):
@@ -108,6 +111,11 @@ class AdvectionDiffusionSolver:
         if depth != "auto" and (int(depth) < 2 or int(depth) % 2):
             raise ValueError("graph_depth must be 'auto' or an even number >= 2")
         self.graph_depth = depth if depth == "auto" else int(depth)
+        launch = get("launch")
+        if launch != "auto" and int(launch) not in range(16):
+            raise ValueError("launch must be 'auto' or a variant number 0-15")
+        self.launch = launch if launch == "auto" else int(launch)
+        self.launch_variant = 0 if launch == "auto" else int(launch)
         self.diffusion = not (self.Dxx == self.Dyy == self.Dzz == 0)
         self.backend = self.domain.backend
         self.signature = self.domain.signature
@@ -135,6 +143,8 @@ class AdvectionDiffusionSolver:
     def _setup(self):
         if self._dm is None:
             self._dm = self.domain.device_mesh
+            if self.launch != "auto":
+                self._dm.struct.variant = int(self.launch)
             dev = self._dm.device
             self._dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
             self._sign = torch.zeros(4 * self._dm.nbcells, dtype=torch.float64, device=dev)
@@ -275,7 +285,9 @@ class AdvectionDiffusionSolver:
     # rows {centre, value} carried from step to step (second order): each cell buffer has a
     # rows buffer; _rows_version is the cell version whose rows are current
     def _use_rows(self):
-        return self.order == 2 and "cell_vtx" in self._dm.t
+        # tetrahedra only: a triangle's 16-byte centre row shares its 32-byte sector with its
+        # Morton neighbour's, so 32-byte rows would double the gathered sectors (measured slower)
+        return self.order == 2 and self.dim == 3 and "cell_vtx" in self._dm.t
 
     def _rows_of(self, buf):
         if getattr(self, "_rowbufs", None) is None:
@@ -484,10 +496,14 @@ class AdvectionDiffusionSolver:
             self._fused_step_f32c()
 
     def _depth(self):
-        """Steps per graph replay (measured once per mesh size and scheme when 'auto')."""
+        """Steps per graph replay (measured once per mesh size and scheme when 'auto'); with
+        ``launch="auto"`` also the launch shapes of the fused phases (once per solver)."""
+        from . import autotune
         if self.graph_depth == "auto":
-            from . import autotune
             self.graph_depth = autotune.graph_depth(self)
+        if self.launch == "auto":
+            self.launch = "tuned"
+            self.launch_variant = autotune.launch_variant(self)
         return int(self.graph_depth)
 
     def _get_graph(self):
@@ -643,6 +659,8 @@ class ShallowWaterSolver:
     def _setup(self):
         if self._dm is None:
             self._dm = self.domain.device_mesh
+            if self.launch != "auto":
+                self._dm.struct.variant = int(self.launch)
             dev = self._dm.device
             # dt double buffer: slot _cur holds the dt of the current state when _dt_key matches
             self._dt_buf = torch.zeros(2, dtype=torch.float64, device=dev)

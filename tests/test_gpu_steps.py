@@ -309,3 +309,29 @@ def test_row_carrying_step_matches_the_plain_step(wl, cuda):
     U.call("mb_pack_rows", dm.struct, U.P(got), U.P(packed), st)
     assert rel_max(U.H(got), U.H(ref)) <= 1e-14
     assert np.array_equal(U.H(rout), U.H(packed))
+
+
+@pytest.mark.parametrize("wl", [W.C2.scaled(n=60, steps=6), W.C4.scaled(n=8, steps=6)])
+def test_every_launch_variant_gives_the_default_result(wl, cuda):
+    """The pre-built launch shapes of the fused phases (mb_mesh.variant) compute the same
+    operations: results agree with the default shapes to rounding (1e-13), and tuning
+    leaves the state as it found it."""
+    from manapy_b200 import autotune
+    el, vx = wl.mesh()
+    outs = {}
+    for v in (0, 1, 2, 3, 4, 8, 12, 15):
+        _, w, S = _advdiff_api(el, vx, wl)
+        S.launch = v
+        S._setup()
+        S._dm.struct.variant = v
+        S.advance(wl.steps, graph=True)
+        outs[v] = w.cell
+    for v, a in outs.items():
+        assert rel_max(a, outs[0]) <= 1e-13, v
+    autotune.clear()
+    big = wl.scaled(n=200) if wl.dim == 2 else wl.scaled(n=24)     # above the tuner's lower size bound
+    el, vx = big.mesh()
+    _, w, S = _advdiff_api(el, vx, big)
+    w0 = w.cell.copy()
+    assert autotune.launch_variant(S, steps=4) in range(16)
+    assert np.array_equal(w.cell, w0)
