@@ -278,7 +278,9 @@ class AdvectionDiffusionSolver:
     def _scratch(self):
         dm = self._dm
         if getattr(self, "_cs", None) is None:
-            self._cs = torch.empty((4 if dm.dim == 2 else 8) * dm.nbcells, dtype=torch.float64, device=dm.device)
+            # 4 nbcells + 4 nbnodes (2D: records, node sums) or 8 nbcells (3D: records, rows)
+            n = 4 * dm.nbcells + 4 * dm.nbnodes if dm.dim == 2 else 8 * dm.nbcells
+            self._cs = torch.empty(n, dtype=torch.float64, device=dm.device)
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
 
@@ -659,8 +661,6 @@ class ShallowWaterSolver:
     def _setup(self):
         if self._dm is None:
             self._dm = self.domain.device_mesh
-            if self.launch != "auto":
-                self._dm.struct.variant = int(self.launch)
             dev = self._dm.device
             # dt double buffer: slot _cur holds the dt of the current state when _dt_key matches
             self._dt_buf = torch.zeros(2, dtype=torch.float64, device=dev)
