@@ -116,16 +116,6 @@ typedef struct mb_mesh {
   const float *n2c_sell_alpha_f32;
   /* [nbfaces][4] = {n_x, n_y, 1/mesure, 0} rounded to FP32 (FP32-compensated shallow water, 2D) */
   const float *face_nm_f32;
-  /* node-sum least-squares gradient of the fused 2D step (NULL: the stencil form above):
-   * cell_lsq [nbcells][4] = {a, b, c, 0}, the inverse of M = sum d d^T over the cell's
-   * vertex neighbours and stencil ghosts; cell_lsqs [nbcells][2] = sum over the vertex
-   * neighbours of d = x_j - x_i.  The first launch then forms per node v the sums
-   * A_v = sum_{j in cells(v)} (x_j - x_v) w_j and B_v = sum_{j in cells(v)} w_j, and per cell
-   * sum_{j in stencil} d w_j = sum_{v in vertices} (A_v + (x_v - x_i) B_v) - sum over the face
-   * neighbours of d w_j (each face neighbour is in two vertex lists, the cell itself has
-   * d = 0), so a cell reads three node sums instead of its ~12 neighbours. */
-  const double *cell_lsq;
-  const double *cell_lsqs;
 } mb_mesh;
 
 typedef struct mb_bc {
@@ -271,7 +261,7 @@ typedef struct mb_advdiff_params {
  * tetrahedra at order 2 add a pack pass before 1 (rows {centre, value} of every cell).
  * w_in is read, w_out written (distinct buffers).  sign_cf[4*i+j] = u.n of the j-th
  * local face of cell i in manapy's face orientation (mb_cell_face_sign); src may be
- * NULL (zero source).  Scratch: cell_scratch [4*nbcells + 4*nbnodes] in 2D, [8*nbcells] in 3D
+ * NULL (zero source).  Scratch: cell_scratch [4*nbcells] in 2D, [8*nbcells] in 3D
  * (order 2), node_scratch [nbnodes] (diffusion); NULL where not needed. */
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
@@ -499,7 +489,7 @@ int mb_halo_unpack(double *const *fields, int32_t nfields, const int64_t *idx, i
  * host application owns every device allocation through its own pool, a service
  * that reserves its device-memory budget up front, or a loop where a cudaMalloc
  * (which can synchronise the device) is not acceptable.  Its scratch
- * (4*nbcells + 5*nbnodes doubles in 2D, 8*nbcells + nbnodes in 3D) lives in a fixed
+ * (4*nbcells + nbnodes doubles in 2D, 8*nbcells + nbnodes in 3D) lives in a fixed
  * array inside the library,
  * MB_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), which every GPU that loads the
  * library keeps reserved until the process exits; larger meshes get MB_ETOOBIG.

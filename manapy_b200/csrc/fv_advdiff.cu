@@ -754,130 +754,6 @@ __global__ void __launch_bounds__(kP2B[VAR], kP2M[VAR]) k_f2_phase2(mb_mesh m, m
   f2_phase2<ORDER2, DIFF, WROWS>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x, rows_out);
 }
 
-// ---------------------------------------------------------------- node-sum first phase (2D)
-//
-// The least-squares gradient of cell i needs J_i = sum_{j in stencil} d_ij (w_j - w_i),
-// d_ij = x_j - x_i, over its vertex neighbours (manapy/ast/functions2d.py:5-104).  The
-// stencil is the union of the cells of its three vertices minus i; a face neighbour lies
-// in two of those vertex lists and i itself has d = 0, so
-//   sum_j d_ij w_j = sum_{v in vertices(i)} (A_v + (x_v - x_i) B_v) - sum_{face nbrs} d_ij w_j
-// with the node sums A_v = sum_{j in cells(v)} (x_j - x_v) w_j, B_v = sum_{j in cells(v)} w_j,
-// and J_i = sum_j d_ij w_j - w_i S_i, S_i = sum_j d_ij (a mesh constant, cell_lsqs).  The
-// matrix of the least-squares system is a mesh constant too (its inverse in cell_lsq).  A
-// cell then reads three node records instead of its ~12 neighbours; offsets from the
-// node keep the terms O(h w), so nothing cancels beyond the direct sum's rounding.
-
-#ifndef MB_N2_NODE_MIN_BLOCKS
-#define MB_N2_NODE_MIN_BLOCKS 6
-#endif
-#ifndef MB_N2_CELL_MIN_BLOCKS
-#define MB_N2_CELL_MIN_BLOCKS 5
-#endif
-
-// node pass: node sums {A_x, A_y, B, 0} of every node and (DIFF) its centre -> vertex value
-template <bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_N2_NODE_MIN_BLOCKS)
-    k_f2n_nodes(mb_mesh m, mb_bc bc, const double *__restrict__ w, double *__restrict__ nrec,
-                double *__restrict__ wn) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= m.nbnodes) return;
-  const GhostRule ghost = make_rule(m, bc, w);
-  const int lane = threadIdx.x & 31;
-  const double2 xv = ldd2(m.node_coord + 2 * n);
-  const int len = ld(m.n2c_ptr + n + 1) - ld(m.n2c_ptr + n);
-  const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
-  const uint64_t pst = l2_stream();
-  double acc = 0., ax = 0., ay = 0., bs = 0.;
-  int e = 0;
-#pragma unroll 4
-  for (int k = sb + lane; k < se; k += 32, ++e) {
-    const int cc = ld1_stream(m.n2c_sell_idx + k, pst);
-    const double wc = ld(w + cc);
-    // padding repeats the row's first cell with weight 0: an exact zero term of the value
-    if (DIFF) acc += ldd_stream(m.n2c_sell_alpha + k, pst) * wc;
-    if (e < len) {
-      const double2 xc = ldd2(m.cell_xy + 2 * cc);
-      ax += (xc.x - xv.x) * wc;
-      ay += (xc.y - xv.y) * wc;
-      bs += wc;
-    }
-  }
-  const uint64_t keep = l2_keep();
-  if (DIFF) {
-    const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
-    for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
-    st1_keep(wn + n, acc, keep);
-  }
-  st4_keep(nrec + 4 * (long long)n, ax, ay, bs, 0.0, keep);
-}
-
-// cell pass: gradient from the node sums, Barth limiter, record {w, gx, gy, psi}
-__global__ void __launch_bounds__(kBlock, MB_N2_CELL_MIN_BLOCKS)
-    k_f2n_cells(mb_mesh m, mb_bc bc, const double *__restrict__ w, const double *__restrict__ nrec,
-                double *__restrict__ rec) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m.nbcells) return;
-  const GhostRule ghost = make_rule(m, bc, w);
-  const double2 c = ldd2(m.cell_xy + 2 * i);
-  const double wi = ld(w + i);
-  const int4 vt = ld4(m.cell_vtx + 4 * i);
-  const int4 nb = ld4(m.cell_nbr + 4 * i);
-  const double2 P0 = ldd2(m.node_coord + 2 * vt.x), P1 = ldd2(m.node_coord + 2 * vt.y),
-                P2 = ldd2(m.node_coord + 2 * vt.z);
-  double sx = 0., sy = 0.;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const double2 P = j == 0 ? P0 : (j == 1 ? P1 : P2);
-    double ax, ay, bs, pad;
-    ld4d(nrec + 4 * (long long)comp(vt, j), ax, ay, bs, pad);
-    sx += ax + (P.x - c.x) * bs;
-    sy += ay + (P.y - c.y) * bs;
-  }
-  double wmax = wi, wmin = wi;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const int o = comp(nb, j);
-    double b;
-    if (o >= 0) {
-      const double2 co = ldd2(m.cell_xy + 2 * o);
-      b = ld(w + o);
-      sx -= (co.x - c.x) * b;     // the face neighbour was counted by both of its vertices
-      sy -= (co.y - c.y) * b;
-    } else {
-      b = ghost(-1 - o);
-    }
-    wmax = pmax(wmax, b);
-    wmin = pmin(wmin, b);
-  }
-  const double2 S = ldd2(m.cell_lsqs + 2 * i);
-  double jx = sx - wi * S.x, jy = sy - wi * S.y;
-  const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
-  for (int k = gb; k < ge; ++k) {
-    const int f = ld(m.ghostnid_idx + k);
-    const double dx = ld(m.face_ghostcenter + 3 * f) - c.x, dy = ld(m.face_ghostcenter + 3 * f + 1) - c.y;
-    const double dw = ghost(f) - wi;
-    jx += dx * dw;
-    jy += dy * dw;
-  }
-  double a, b, cc, pad;
-  ld4d(m.cell_lsq + 4 * (long long)i, a, b, cc, pad);
-  const double x = a * jx + b * jy, y = b * jx + cc * jy;
-  double ps = 1.;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const double2 pa = j == 0 ? P0 : (j == 1 ? P1 : P2), pb = j == 0 ? P1 : (j == 1 ? P2 : P0);
-    const double r1 = 0.5 * (pa.x + pb.x) - c.x, r2 = 0.5 * (pa.y + pb.y) - c.y;
-    const double delta = x * r1 + y * r2;
-    double psi_ij = 1.;
-    if (!(fabs(delta) < 1e-8)) {
-      if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
-      if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
-    }
-    ps = pmin(ps, psi_ij);
-  }
-  st4_keep(rec + 4 * (long long)i, wi, x, y, ps, l2_keep());
-}
-
 // ---------------------------------------------------------------- batches of triangle meshes, FP64
 //
 // Block b of a launch belongs to item map[b] (blocks never straddle two meshes) and runs
@@ -1226,10 +1102,6 @@ inline int grid_for(long long n) {
 
 inline int check_launch() { return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA; }
 
-inline bool nodesum_tables(const mb_mesh &m) {
-  return m.dim == 2 && m.cell_lsq && m.cell_lsqs && m.n2c_ptr;
-}
-
 inline bool compact_tables(const mb_mesh &m) {
   return m.cell_vtx && m.cell_nbr && m.cell_flags && m.node_coord && m.cell_xy && m.lsq_sell_ptr &&
          m.lsq_sell_idx && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
@@ -1307,9 +1179,8 @@ inline void f3_p2_pick(int v, const mb_mesh &m, const mb_bc &bc, const mb_advdif
 }
 
 // cell scratch: [4][nbcells] planes gx, gy, gz, psi (face-table path), [nbcells][4]
-// records {w, gx, gy, psi} then [nbnodes][4] node sums (compact 2D path) or [nbcells][4]
-// records {w, psi gx, psi gy, psi gz} then [nbcells][4] rows {x, y, z, w} (compact 3D path);
-// node scratch: [nbnodes]
+// records {w, gx, gy, psi} (compact 2D path) or [nbcells][4] records {w, psi gx, psi gy,
+// psi gz} then [nbcells][4] rows {x, y, z, w} (compact 3D path); node scratch: [nbnodes]
 template <int DIM, bool O2, bool DF>
 int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                 double *w_out, const double *sign, const double *src, const double *dt, double *cs,
@@ -1330,12 +1201,7 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
     // launch-shape variants (second order with diffusion only): bits 0-1 phase 1, bits 2-3 phase 2
     const int v1 = (O2 && DF) ? (m.variant & 3) : 0, v2 = (O2 && DF) ? ((m.variant >> 2) & 3) : 0;
     if (DIM == 2) {
-      if (O2 && nodesum_tables(m)) {
-        // node-sum gradient: node pass (sums and node values), then the cell pass
-        double *nrec = cs + 4 * (long long)m.nbcells;
-        k_f2n_nodes<DF><<<ceil_div(m.nbnodes, kBlock), kBlock, 0, st>>>(m, bc, w_in, nrec, wn);
-        k_f2n_cells<<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, w_in, nrec, cs);
-      } else if (O2 || DF) {
+      if (O2 || DF) {
         if (rows_in) f2_p1_pick<O2, DF, true>(v1, m, bc, w_in, cs, wn, rows_in, st);
         else f2_p1_pick<O2, DF, false>(v1, m, bc, w_in, cs, wn, nullptr, st);
       }
@@ -1592,7 +1458,7 @@ int mb_advdiff_batch_step(const mb_advdiff_item_f64 *items, const int32_t *p1_ma
 
 // ---------------------------------------------------------------- no-allocation variant
 //
-// mb_advdiff_step needs 4*nbcells + 5*nbnodes (3D: 8*nbcells + nbnodes) doubles of scratch that the caller
+// mb_advdiff_step needs 4*nbcells (3D: 8*nbcells) + nbnodes doubles of scratch that the caller
 // allocates.  Some callers cannot allocate device memory at all: a plugin that
 // lives inside a host application owning every device allocation through its
 // own pool, a service that reserves its whole device-memory budget up front,
@@ -1617,8 +1483,8 @@ extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const 
                                        const double *src, const double *dt_dev, void *stream) {
   MB_NVTX();
   if (!mesh_ok(m) || !bc || !p) return MB_EINVAL;
-  // cell scratch 4*nbcells + 4*nbnodes (2D) or 8*nbcells (3D), then the node scratch
-  const long long cell_need = m->dim == 2 ? 4LL * m->nbcells + 4LL * m->nbnodes : 8LL * m->nbcells;
+  // cell scratch 4*nbcells (2D) or 8*nbcells (3D), then the node scratch
+  const long long cell_need = (m->dim == 2 ? 4LL : 8LL) * m->nbcells;
   const long long need = cell_need + m->nbnodes;
   if (need > (long long)MB_NOALLOC_SCRATCH_DOUBLES) return MB_ETOOBIG;
   int dev = 0;

@@ -104,35 +104,6 @@ def sell32(ptr, idx, vals=None, fill=-1):
     return gptr.astype(np.int32), out, outv
 
 
-def nodesum_tables_2d(T):
-    """Per-cell constants of the node-sum least-squares gradient (device numbering):
-    ``cell_lsq`` [nc][4] = {a, b, c, 0}, the inverse of the least-squares matrix
-    M = sum d d^T over the vertex neighbours and stencil ghosts (gradient = [[a, b], [b, c]] J),
-    and ``cell_lsqs`` [nc][2] = sum over the vertex neighbours of d = x_j - x_i."""
-    ptr = np.asarray(T["cellnid_ptr"], dtype=np.int64)
-    idx = np.asarray(T["cellnid_idx"], dtype=np.int64)
-    X = np.asarray(T["cell_xy"], dtype=np.float64).reshape(-1, 2)
-    nc = len(ptr) - 1
-    row = np.repeat(np.arange(nc), np.diff(ptr))
-    d = X[idx] - X[row]
-    m = np.zeros((nc, 3))
-    np.add.at(m, row, np.stack([d[:, 0] * d[:, 0], d[:, 1] * d[:, 1], d[:, 0] * d[:, 1]], axis=1))
-    S = np.zeros((nc, 2))
-    np.add.at(S, row, d)
-    gptr = np.asarray(T["ghostnid_ptr"], dtype=np.int64)
-    gidx = np.asarray(T["ghostnid_idx"], dtype=np.int64)
-    grow = np.repeat(np.arange(nc), np.diff(gptr))
-    if len(gidx):
-        gc = np.asarray(T["face_ghostcenter"], dtype=np.float64).reshape(-1, 3)[gidx, :2] - X[grow]
-        np.add.at(m, grow, np.stack([gc[:, 0] * gc[:, 0], gc[:, 1] * gc[:, 1], gc[:, 0] * gc[:, 1]], axis=1))
-    dia = m[:, 0] * m[:, 1] - m[:, 2] * m[:, 2]
-    lsq = np.zeros((nc, 4))
-    lsq[:, 0] = m[:, 1] / dia
-    lsq[:, 1] = -m[:, 2] / dia
-    lsq[:, 2] = m[:, 0] / dia
-    return lsq, S
-
-
 def vertex_weights(A):
     """Centre->vertex weight of every node->cell and node->ghost incidence, in
     manapy's expression order (manapy/ast/functions2d.py:219, functions3d.py:272-274)."""
@@ -250,7 +221,6 @@ class DeviceMesh:
             T["cell_vertex1"] = _t(A["nodes_vertex"][A["cells_nodeid"][cp, 1], :2], f64, dev)
         if dim == 2:
             self._compact_2d(A, T, dev)
-            self._add_nodesum(T, dev)
         else:
             self._compact_3d(A, T, dev)
         self.t = T
@@ -304,7 +274,6 @@ class DeviceMesh:
         self.reordered = bool(reorder)
         dev = torch.device(device) if device is not None else None
         self.device = dev
-        self._add_nodesum(T, None)
         self.t = {k: _t(v, v.dtype, dev) for k, v in T.items()}
         self.perm = {k: _t(v, np.int64, dev) for k, v in perm.items()}
         self.inv = {k: _t(v, np.int64, dev) for k, v in inv.items()}
@@ -363,17 +332,6 @@ class DeviceMesh:
         """Drop the host arrays ``A`` (before sending host-built tables to another process)."""
         self.A = None
         return self
-
-    def _add_nodesum(self, T, dev):
-        """Constant tables of the node-sum least-squares gradient of the fused 2D step
-        (``cell_lsq``, ``cell_lsqs``, see ``mb_mesh``), from the device-numbered stencils."""
-        if self.dim != 2 or "cellnid_ptr" not in T or "cell_xy" not in T:
-            return
-        host = {k: (T[k].cpu().numpy() if isinstance(T[k], torch.Tensor) else np.asarray(T[k]))
-                for k in ("cellnid_ptr", "cellnid_idx", "ghostnid_ptr", "ghostnid_idx", "cell_xy", "face_ghostcenter")}
-        lsq, lsqs = nodesum_tables_2d(host)
-        T["cell_lsq"] = _t(lsq, np.float64, dev)
-        T["cell_lsqs"] = _t(lsqs, np.float64, dev)
 
     def _compact_2d(self, A, T, dev):
         """Cell-centred tables of the fused 2D step (see ``mb_mesh`` in the C header)."""

@@ -120,8 +120,8 @@ class ShardedAdvectionDiffusion(_Sharded):
         f64 = torch.float64
         self.w = [torch.zeros(nc, dtype=f64, device=self.dev) for _ in range(2)]
         self.cur = 0
-        # cell scratch of the fused step: 4 nbcells + 4 nbnodes (2D) or 8 nbcells (3D) doubles
-        self.cs = torch.empty(4 * nc + 4 * nn if dim == 2 else 8 * nc, dtype=f64, device=self.dev)
+        # cell scratch of the fused step: 4 nbcells (2D) or 8 nbcells (3D) doubles
+        self.cs = torch.empty((4 if dim == 2 else 8) * nc, dtype=f64, device=self.dev)
         self.ns = torch.empty(nn, dtype=f64, device=self.dev)
         self.sign = torch.empty(4 * nc, dtype=f64, device=self.dev)
         self.dt = torch.zeros(1, dtype=f64, device=self.dev)

@@ -278,9 +278,8 @@ class AdvectionDiffusionSolver:
     def _scratch(self):
         dm = self._dm
         if getattr(self, "_cs", None) is None:
-            # 4 nbcells + 4 nbnodes (2D: records, node sums) or 8 nbcells (3D: records, rows)
-            n = 4 * dm.nbcells + 4 * dm.nbnodes if dm.dim == 2 else 8 * dm.nbcells
-            self._cs = torch.empty(n, dtype=torch.float64, device=dm.device)
+            # 4 nbcells (2D: records) or 8 nbcells (3D: records, rows)
+            self._cs = torch.empty((4 if dm.dim == 2 else 8) * dm.nbcells, dtype=torch.float64, device=dm.device)
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
 

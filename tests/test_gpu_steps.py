@@ -297,7 +297,7 @@ def test_row_carrying_step_matches_the_plain_step(wl, cuda):
     U.call("mb_time_step", dm.struct, *[U.P(c) for c in cells], wl.cfl, *wl.diffusion, U.P(dt), st)
     prm = _lib.MbAdvDiffParams(wl.order, 1, *wl.diffusion)
     w0 = U.T(wl.init(A["cells_center"])[R.cperm])
-    cs, ns = U.Z(4 * nc + 4 * nn if wl.dim == 2 else 8 * nc), U.Z(nn)
+    cs, ns = U.Z((4 if wl.dim == 2 else 8) * nc), U.Z(nn)
     ref = U.Z(nc)
     U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w0), U.P(ref), U.P(sign), None, U.P(dt), U.P(cs),
            U.P(ns), st)

@@ -44,7 +44,7 @@ def _setup(wl):
 def _regular(U, A, dm, db, prm, sign, dt, w_in, st):
     nc, nn = A["nbcells"], A["nbnodes"]
     out = U.Z(nc)
-    cell_scratch = U.Z(4 * nc + 4 * nn if A["dim"] == 2 else 8 * nc)
+    cell_scratch = U.Z((4 if A["dim"] == 2 else 8) * nc)
     node_scratch = U.Z(nn)
     U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w_in), U.P(out), U.P(sign), None, U.P(dt),
            U.P(cell_scratch), U.P(node_scratch), st)
@@ -72,11 +72,11 @@ def test_noalloc_step_matches_regular_step_twice(wl, cuda):
 @pytest.mark.parametrize("wl", [W.C2.scaled(n=20), W.C4.scaled(n=4)])
 def test_noalloc_size_gate_at_its_limit(wl, cuda):
     """A mesh one double beyond the scratch array is refused with MB_ETOOBIG (2D needs
-    4*cells + 5*nodes doubles, 3D 8*cells + nodes); a mesh exactly at the limit passes the
+    4*cells + nodes doubles, 3D 8*cells + nodes); a mesh exactly at the limit passes the
     size gate and is then refused for w_in == w_out (MB_EINVAL), before any launch."""
     U, A, dm, db, prm, sign, dt, w0, st = _setup(wl)
-    # doubles needed: a cells + b nodes, (a, b) = (4, 5) for triangles, (8, 1) for tetrahedra
-    a, b = (4, 5) if wl.dim == 2 else (8, 1)
+    # doubles needed: a cells + b nodes, (a, b) = (4, 1) for triangles, (8, 1) for tetrahedra
+    a, b = (4, 1) if wl.dim == 2 else (8, 1)
     limit = _lib.NOALLOC_SCRATCH_DOUBLES
     lib = _lib.lib()
     at = _lib.MbMesh.from_buffer_copy(dm.struct)
