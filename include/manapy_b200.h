@@ -105,8 +105,10 @@ typedef struct mb_mesh {
   const double *cell_xy;
   /* the same neighbour lists as cellnid_* and n2c_*, stored SELL-32: rows are taken
    * in groups of 32 (one warp); group g occupies idx[ptr[g] .. ptr[g+1]) as
-   * [len_g][32] (entry k of row 32g+l at ptr[g] + 32k + l); lsq rows are padded
-   * with -1, n2c rows with their first cell and weight 0 */
+   * [len_g][32] (entry k of row 32g+l at ptr[g] + 32k + l).  An lsq row holds each of
+   * its neighbours once, in any slots, and -1 in the others (the kernels sum a row's
+   * terms in slot order); n2c rows are padded at their end with their first cell and
+   * weight 0 */
   const int32_t *lsq_sell_ptr;
   const int32_t *lsq_sell_idx;
   const int32_t *n2c_sell_ptr;

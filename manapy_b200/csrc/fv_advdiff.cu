@@ -856,16 +856,30 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
     const int32_t *ix = m.lsq_sell_idx + sb + lane;
     const uint64_t pst = l2_stream();
     int k = 0;
-    // batches of MB_F3_LSQ_BATCH neighbours: their gathers in flight together, terms added in order
-    for (; k + MB_F3_LSQ_BATCH <= L; k += MB_F3_LSQ_BATCH) {
-      int cc[MB_F3_LSQ_BATCH];
-      D3 pc[MB_F3_LSQ_BATCH];
-      double wc[MB_F3_LSQ_BATCH];
+    // batches of MB_F3_LSQ_BATCH neighbours: the next batch's indices are loaded before this
+    // batch's row gathers are issued, the terms are accumulated in stencil order
+    constexpr int B = MB_F3_LSQ_BATCH;
+    int nx[B];
 #pragma unroll
-      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) cc[u] = ld1_stream(ix + 32 * (k + u), pst);
+    for (int u = 0; u < B; ++u) nx[u] = u < L ? ld1_stream(ix + 32 * u, pst) : -1;
+    auto acc = [&](const D3 &pc, double wc) {
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z, dw = wc - wi;
+      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+      ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+      jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
+    };
+    for (; k + B <= L; k += B) {
+      int cc[B];
 #pragma unroll
-      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) {
-        if (cc[u] < 0) {            // padding: the cell itself, no gather issued
+      for (int u = 0; u < B; ++u) {
+        cc[u] = nx[u];
+        nx[u] = k + B + u < L ? ld1_stream(ix + 32 * (k + B + u), pst) : -1;
+      }
+      D3 pc[B];
+      double wc[B];
+#pragma unroll
+      for (int u = 0; u < B; ++u) {
+        if (cc[u] < 0) {            // padding: the cell itself, no gather issued, exact zero terms
           pc[u] = c;
           wc[u] = wi;
         } else {
@@ -873,22 +887,17 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
         }
       }
 #pragma unroll
-      for (int u = 0; u < MB_F3_LSQ_BATCH; ++u) {
-        const double dx = pc[u].x - c.x, dy = pc[u].y - c.y, dz = pc[u].z - c.z, dw = wc[u] - wi;
-        ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
-        ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
-        jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
-      }
+      for (int u = 0; u < B; ++u) acc(pc[u], wc[u]);
     }
-    for (; k < L; ++k) {
-      const int cc = ld1_stream(ix + 32 * k, pst);
-      D3 pc = c;
-      double wcc = wi;
-      if (cc >= 0) ld_row(rows + 4 * (long long)cc, pc.x, pc.y, pc.z, wcc);
-      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z, dw = wcc - wi;
-      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
-      ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
-      jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
+    // the last L - k < B entries, whose indices are in nx
+#pragma unroll
+    for (int u = 0; u < B - 1; ++u) {
+      if (k + u < L) {
+        D3 pc = c;
+        double wcc = wi;
+        if (nx[u] >= 0) ld_row(rows + 4 * (long long)nx[u], pc.x, pc.y, pc.z, wcc);
+        acc(pc, wcc);
+      }
     }
     const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
     for (int k = gb; k < ge; ++k) {

@@ -104,6 +104,27 @@ def sell32(ptr, idx, vals=None, fill=-1):
     return gptr.astype(np.int32), out, outv
 
 
+STENCILS = ("shared", "manapy")
+
+
+def lsq_sell(ptr, idx, stencil):
+    """(group_ptr, idx) of the least-squares stencil (vertex neighbours of every cell) in
+    SELL-32.  ``"manapy"``: each row keeps manapy's neighbour order, padded with -1 at its
+    end, so a cell's sums are formed in the same order whatever the numbering of the other
+    cells.  ``"shared"``: a neighbour held by several cells of one warp is placed in the
+    same slot for all of them where their free slots allow (``native.sell_aligned``), so a
+    warp-wide gather touches fewer distinct rows; each cell's sums are then formed in slot
+    order, which depends on the cells it shares a warp with (results differ from the
+    ``"manapy"`` layout by rounding)."""
+    if stencil == "manapy":
+        gp, gi, _ = sell32(ptr, idx)
+        return gp, gi
+    if stencil == "shared":
+        from . import native
+        return native.sell_aligned(ptr, idx)
+    raise ValueError("stencil must be one of %s" % (STENCILS,))
+
+
 def vertex_weights(A):
     """Centre->vertex weight of every node->cell and node->ghost incidence, in
     manapy's expression order (manapy/ast/functions2d.py:219, functions3d.py:272-274)."""
@@ -141,9 +162,13 @@ class DeviceMesh:
     arrays between that numbering and manapy's.
     """
 
-    def __init__(self, A, device="cuda", reorder=True):
+    def __init__(self, A, device="cuda", reorder=True, stencil="shared"):
         """``device=None`` builds the tables as numpy arrays on the host (``upload`` moves
-        them to a device later, e.g. after building in a worker process)."""
+        them to a device later, e.g. after building in a worker process); ``stencil``: the
+        layout of the least-squares stencil (``lsq_sell``)."""
+        if stencil not in STENCILS:
+            raise ValueError("stencil must be one of %s" % (STENCILS,))
+        self.stencil = stencil
         from .reorder import Renumbering
         dev = torch.device(device) if device is not None else None
         self.device = dev
@@ -173,7 +198,7 @@ class DeviceMesh:
             ptr, idx, _ = R.relabel_csr(A["cellnid_ptr"], A["cellnid_idx"], cp, ci)
             T["cellnid_ptr"] = _t(ptr, i32, dev)
             T["cellnid_idx"] = _t(idx, i32, dev)
-            gp, gi, _ = sell32(ptr, idx)
+            gp, gi = lsq_sell(ptr, idx, stencil)
             T["lsq_sell_ptr"], T["lsq_sell_idx"] = _t(gp, i32, dev), _t(gi, i32, dev)
         ptr, idx, _ = R.relabel_csr(A["ghostnid_ptr"], A["ghostnid_idx"], cp, fi)
         T["ghostnid_ptr"] = _t(ptr, i32, dev)
@@ -243,6 +268,7 @@ class DeviceMesh:
         self.A = A
         self.R = R
         self.reordered = bool(R.enabled)
+        self.stencil = str(T.pop("stencil", np.array("manapy")))
         dev = torch.device(device) if device is not None else None
         self.device = dev
         self.t = {k: _t(v, v.dtype, dev) for k, v in T.items()}
@@ -253,7 +279,7 @@ class DeviceMesh:
         return self
 
     @classmethod
-    def from_native(cls, elements, vertex, device=None, reorder=True, full=False):
+    def from_native(cls, elements, vertex, device=None, reorder=True, full=False, stencil="shared"):
         """The tables of a 2D triangle mesh from the native host builder (``native.tables2d``),
         bit-identical to ``DeviceMesh(geometry.build(...))``; ``A`` then holds only the
         manapy-numbered arrays the boundary set-up reads, or with ``full`` every array of
@@ -261,7 +287,10 @@ class DeviceMesh:
         from types import SimpleNamespace
         from . import native
         T = native.tables2d(elements, vertex, reorder=reorder, full=full)
+        if stencil != "manapy":          # the builder writes the manapy layout
+            T["lsq_sell_ptr"], T["lsq_sell_idx"] = lsq_sell(T["cellnid_ptr"], T["cellnid_idx"], stencil)
         self = cls.__new__(cls)
+        self.stencil = stencil
         nc, nf, nn = len(T["cell_volume"]), len(T["face_name"]), len(T["node_coord"])
         self.dim, self.nbcells, self.nbfaces, self.nbnodes, self.nlf = 2, nc, nf, nn, 3
         self.A = {"dim": 2, "nbcells": nc, "nbfaces": nf, "nbnodes": nn}

@@ -47,7 +47,7 @@ class _OneRankComm:
         return x
 
 
-def build_host_mesh(elements, vertex, dim):
+def build_host_mesh(elements, vertex, dim, stencil="shared"):
     """(A, host-built DeviceMesh or None) through the native host builder, bit-identical to
     the Python builder: for triangles every ``geometry.build`` array and device table in one
     C++ pass; for tetrahedra the ``geometry.build`` arrays (the device tables then come from
@@ -58,7 +58,7 @@ def build_host_mesh(elements, vertex, dim):
         if native.available():
             if dim == 2:
                 from .device import DeviceMesh
-                dm = DeviceMesh.from_native(elements, vertex, device=None, full=True)
+                dm = DeviceMesh.from_native(elements, vertex, device=None, full=True, stencil=stencil)
                 return dm.A, dm
             if dim == 3:
                 return native.geometry3d(elements, vertex), None
@@ -79,6 +79,11 @@ class Domain:
         ("mesh_cache", "str", None, None, "directory of the persistent mesh cache (geometry and device tables "
                                            "stored once per mesh; also MANAPY_B200_MESH_CACHE); no counterpart "
                                            "in manapy"),
+        ("stencil", "str", "shared", None, "layout of the least-squares stencil: 'shared' (neighbours shared by "
+                                           "the cells of one warp read in one slot; fastest) or 'manapy' (each "
+                                           "cell's neighbours in manapy's order, so results do not depend on the "
+                                           "numbering of other cells, e.g. when the mesh is sharded); no "
+                                           "counterpart in manapy"),
     ]
 
     @classmethod
@@ -101,6 +106,10 @@ class Domain:
         self.int_precision = "i4" if get("int_precision") == "signed" else "u4"
         self.signature = get("signature")
         self.device = get("device")
+        self.stencil = get("stencil")
+        from .device import STENCILS
+        if self.stencil not in STENCILS:
+            raise ValueError("stencil must be one of %s" % (STENCILS,))
         if mesh is None:
             mesh = getattr(conf, "mesh", None)
         if mesh is None:
@@ -114,9 +123,9 @@ class Domain:
         if cache_dir:
             from . import meshcache
             self._A, self._host_dm, self.mesh_cache_hit = meshcache.load_or_build(elements, vertex, int(dim),
-                                                                                  cache_dir)
+                                                                                  cache_dir, stencil=self.stencil)
         else:
-            self._A, self._host_dm = build_host_mesh(elements, vertex, int(dim))
+            self._A, self._host_dm = build_host_mesh(elements, vertex, int(dim), self.stencil)
         if len(self._A["unmatched_boundary_faces"]):
             raise ValueError("%d boundary faces match no boundary side (their vertices carry "
                              "incompatible tags)" % len(self._A["unmatched_boundary_faces"]))
@@ -191,7 +200,7 @@ class Domain:
                 self._dmesh, self._host_dm = self._host_dm.upload(self.device), None
             else:
                 from .device import DeviceMesh
-                self._dmesh = DeviceMesh(self._A, self.device)
+                self._dmesh = DeviceMesh(self._A, self.device, stencil=self.stencil)
         return self._dmesh
 
     @property

@@ -171,6 +171,101 @@ inline void sell32(const std::vector<i64> &ptr, const std::vector<i64> &idx, con
   for (i64 g = 0; g <= ng; ++g) gptr[g] = (i32)g64[g];
 }
 
+// SELL-32 whose slots are shared across each warp's 32 rows: a value that several rows of
+// the warp hold is placed, where their free slots allow, in one slot for all of them, so
+// that a warp-wide gather of slot k touches few distinct addresses.  Per warp: every
+// distinct value with the mask of rows holding it, taken in order of decreasing row count
+// (then ascending value); each goes to the slot with the most of its remaining rows free
+// (the first such slot), and what stays unplaced goes on the same way.  A row keeps each
+// of its entries exactly once; the slot count is the warp's longest row + slack (a row
+// with fewer entries than slots always has a free slot).  Empty slots hold -1.  The order
+// of a row's entries is the slot order (not the CSR order).  Warps in parallel threads.
+inline void sell32_aligned(const std::vector<i64> &ptr, const std::vector<i64> &idx, int slack,
+                           std::vector<i32> &gptr, std::vector<i32> &out) {
+  const i64 n = (i64)ptr.size() - 1;
+  const i64 ng = (n + 31) / 32;
+  std::vector<i64> g64(ng + 1, 0);
+  for (i64 g = 0; g < ng; ++g) {
+    i64 len = 0;
+    for (i64 r = 32 * g; r < std::min(n, 32 * g + 32); ++r) len = std::max(len, ptr[r + 1] - ptr[r]);
+    g64[g + 1] = g64[g] + 32 * (len + (len ? slack : 0));
+  }
+  out.assign(g64[ng], -1);
+  auto warps = [&](i64 g0, i64 g1) {
+    std::vector<std::pair<i64, int>> pairs;        // (value, row in warp)
+    std::vector<std::pair<i64, uint32_t>> els;     // (value, rows mask)
+    std::vector<uint32_t> occ;
+    for (i64 g = g0; g < g1; ++g) {
+      const i64 L = (g64[g + 1] - g64[g]) / 32;
+      if (!L) continue;
+      pairs.clear();
+      for (i64 r = 32 * g; r < std::min(n, 32 * g + 32); ++r)
+        for (i64 e = ptr[r]; e < ptr[r + 1]; ++e) pairs.emplace_back(idx[e], (int)(r - 32 * g));
+      std::sort(pairs.begin(), pairs.end());
+      // a value repeated within one row counts as distinct values (its k-th copies grouped)
+      els.clear();
+      std::vector<std::pair<std::pair<i64, int>, uint32_t>> keyed;
+      keyed.reserve(pairs.size());
+      for (size_t a = 0; a < pairs.size();) {
+        size_t b = a;
+        while (b < pairs.size() && pairs[b].first == pairs[a].first) ++b;
+        // rows of this value, with the copy number of each occurrence
+        int copy = 0;
+        for (size_t c = a; c < b; ++c) {
+          copy = (c > a && pairs[c].second == pairs[c - 1].second) ? copy + 1 : 0;
+          bool merged = false;
+          for (auto &kv : keyed)
+            if (kv.first.first == pairs[c].first && kv.first.second == copy && !(kv.second >> pairs[c].second & 1u)) {
+              kv.second |= 1u << pairs[c].second;
+              merged = true;
+              break;
+            }
+          if (!merged) keyed.push_back({{pairs[c].first, copy}, 1u << pairs[c].second});
+        }
+        for (auto &kv : keyed) els.emplace_back(kv.first.first, kv.second);
+        keyed.clear();
+        a = b;
+      }
+      std::stable_sort(els.begin(), els.end(), [](const std::pair<i64, uint32_t> &x, const std::pair<i64, uint32_t> &y) {
+        const int cx = __builtin_popcount(x.second), cy = __builtin_popcount(y.second);
+        return cx != cy ? cx > cy : x.first < y.first;
+      });
+      occ.assign(L, 0u);
+      for (const auto &el : els) {
+        uint32_t rem = el.second;
+        while (rem) {
+          i64 best = -1;
+          int bc = 0;
+          for (i64 k = 0; k < L; ++k) {
+            const uint32_t f = rem & ~occ[k];
+            const int c = __builtin_popcount(f);
+            if (c > bc) {
+              bc = c;
+              best = k;
+              if (f == rem) break;
+            }
+          }
+          const uint32_t f = rem & ~occ[best];
+          occ[best] |= f;
+          for (uint32_t m = f; m; m &= m - 1) out[g64[g] + 32 * best + __builtin_ctz(m)] = (i32)el.first;
+          rem &= ~f;
+        }
+      }
+    }
+  };
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const i64 nthreads = ng >= 2048 ? (i64)hw : 1;
+  if (nthreads == 1) {
+    warps(0, ng);
+  } else {
+    std::vector<std::thread> pool;
+    for (i64 t = 0; t < nthreads; ++t) pool.emplace_back([&, t] { warps(ng * t / nthreads, ng * (t + 1) / nthreads); });
+    for (auto &th : pool) th.join();
+  }
+  gptr.assign(ng + 1, 0);
+  for (i64 g = 0; g <= ng; ++g) gptr[g] = (i32)g64[g];
+}
+
 inline uint64_t part1by1(uint64_t v) {
   v &= 0xFFFFFFFFull;
   v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;

@@ -560,6 +560,30 @@ void *mbh_build2d(const int32_t *elements, int64_t nbcells, const double *vertex
   return build2d(elements, nbcells, vertex, nbnodes, reorder != 0, full != 0);
 }
 
+// the slot-shared SELL-32 (sell32_aligned) of a CSR table: tables "gptr" and "idx"
+void *mbh_sell_aligned(const int64_t *ptr, int64_t n, const int32_t *idx, int32_t slack) {
+  if (!ptr || n < 0 || slack < 0) return nullptr;
+  auto *res = new Result();
+  std::vector<i64> p(ptr, ptr + n + 1), ix(ptr[n]);
+  for (i64 e = 0; e < ptr[n]; ++e) ix[e] = idx[e];
+  std::vector<i64> len(n);
+  i64 total = 0;
+  for (i64 g = 0; g < (n + 31) / 32; ++g) {
+    i64 m = 0;
+    for (i64 r = 32 * g; r < std::min(n, 32 * g + 32); ++r) m = std::max(m, p[r + 1] - p[r]);
+    total += 32 * (m + (m ? slack : 0));
+  }
+  if (total >= ((i64)1 << 31)) {
+    res->error = "neighbour table too large for 32-bit offsets";
+    return res;
+  }
+  std::vector<i32> gp, gi;
+  sell32_aligned(p, ix, slack, gp, gi);
+  res->add("gptr", 'i', {(i64)gp.size()}, gp);
+  res->add("idx", 'i', {(i64)gi.size()}, gi);
+  return res;
+}
+
 const char *mbh_error(void *h) { return h ? static_cast<Result *>(h)->error.c_str() : "null handle"; }
 
 int32_t mbh_count(void *h) { return h ? (int32_t) static_cast<Result *>(h)->tables.size() : 0; }

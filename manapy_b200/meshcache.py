@@ -43,10 +43,10 @@ def _sources_digest():
     return _digest
 
 
-def mesh_key(elements, vertex, dim, reorder=True):
-    """Hex key of (mesh, dimension, renumbering, builder sources)."""
+def mesh_key(elements, vertex, dim, reorder=True, stencil="shared"):
+    """Hex key of (mesh, dimension, renumbering, stencil layout, builder sources)."""
     h = hashlib.sha256()
-    h.update(b"manapy_b200 mesh cache %d %d %d " % (FORMAT, int(dim), int(bool(reorder))))
+    h.update(b"manapy_b200 mesh cache %d %d %d %s " % (FORMAT, int(dim), int(bool(reorder)), stencil.encode()))
     h.update(_sources_digest().encode())
     for a in (np.ascontiguousarray(elements, dtype=np.int32), np.ascontiguousarray(vertex, dtype=np.float64)):
         h.update(str(a.shape).encode())
@@ -67,6 +67,7 @@ def _save(path, A, dm):
     for k in ("cperm", "cinv", "fperm", "finv", "nperm", "ninv"):
         arrays["R/" + k] = np.asarray(getattr(dm.R, k))
     arrays["R/enabled"] = np.asarray(bool(dm.R.enabled))
+    arrays["T/stencil"] = np.asarray(dm.stencil)
     d = os.path.dirname(path)
     fd, tmp = tempfile.mkstemp(prefix=".mesh-", suffix=".npz.tmp", dir=d)
     try:
@@ -98,24 +99,24 @@ def _load(path):
     return A, dm
 
 
-def load_or_build(elements, vertex, dim, cache_dir, reorder=True):
+def load_or_build(elements, vertex, dim, cache_dir, reorder=True, stencil="shared"):
     """(A, host-built DeviceMesh, hit) for the mesh, through the cache in ``cache_dir``."""
     from . import geometry
     from .device import DeviceMesh
     os.makedirs(cache_dir, exist_ok=True)
-    path = entry_path(cache_dir, mesh_key(elements, vertex, dim, reorder))
+    path = entry_path(cache_dir, mesh_key(elements, vertex, dim, reorder, stencil))
     if os.path.exists(path):
         A, dm = _load(path)
         return A, dm, True
     dm = None
     if reorder:
         from .domain import build_host_mesh
-        A, dm = build_host_mesh(elements, vertex, int(dim))
+        A, dm = build_host_mesh(elements, vertex, int(dim), stencil)
     else:
         A = geometry.build(elements, vertex, int(dim))
     if len(A["unmatched_boundary_faces"]):
         return A, None, False          # the caller raises manapy's error; nothing is cached
     if dm is None:
-        dm = DeviceMesh(A, device=None, reorder=reorder)
+        dm = DeviceMesh(A, device=None, reorder=reorder, stencil=stencil)
     _save(path, A, dm)
     return A, dm, False

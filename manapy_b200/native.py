@@ -39,6 +39,8 @@ def lib():
         L.mbh_data.restype = ctypes.c_void_p
         L.mbh_data.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.mbh_free.argtypes = [ctypes.c_void_p]
+        L.mbh_sell_aligned.restype = ctypes.c_void_p
+        L.mbh_sell_aligned.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32]
         L.mbh_geometry3d.restype = ctypes.c_void_p
         L.mbh_geometry3d.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]
         _lib = L
@@ -66,6 +68,23 @@ def tables2d(elements, vertex, reorder=True, full=False):
     if not h:
         raise ValueError("empty mesh")
     return _read(L, h)
+
+
+def sell_aligned(ptr, idx, slack=0):
+    """(group_ptr, idx) of the slot-shared SELL-32 layout of a CSR table (``host/common.hpp``
+    ``sell32_aligned``): rows in warps of 32, values that several rows of a warp hold placed
+    in one slot for all of them where their free slots allow; ``slack`` extra slots per warp;
+    empty slots -1."""
+    p = np.ascontiguousarray(ptr, dtype=np.int64)
+    ix = np.ascontiguousarray(idx, dtype=np.int32)
+    if p.ndim != 1 or len(p) < 1 or p[0] != 0 or len(ix) != p[-1] or np.any(np.diff(p) < 0):
+        raise ValueError("expected a CSR table (ptr from 0, ascending, idx of length ptr[-1])")
+    L = lib()
+    h = L.mbh_sell_aligned(p.ctypes.data, len(p) - 1, ix.ctypes.data, int(slack))
+    if not h:
+        raise ValueError("bad arguments")
+    T = _read(L, h)
+    return T["gptr"], T["idx"]
 
 
 def geometry3d(elements, vertex):

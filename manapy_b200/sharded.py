@@ -41,7 +41,8 @@ class _Sharded:
         self.shard = P.build_shards(elements, vertex, dim, self.world, A=A, extra_cells=extra_cells)[self.rank]
         A = G.build(self.shard.elements, self.shard.vertex, dim, halo_rim=True)
         self.A = A
-        self.dm = DeviceMesh(A, self.dev)
+        # manapy's stencil order: every cell's sums formed as in the single-domain run
+        self.dm = DeviceMesh(A, self.dev, stencil="manapy")
         inv = self.dm.inv["cell"].cpu().numpy()
         self.exchanger = P.HaloExchange(self._to_device_numbering(inv), group, device=self.dev)
         self.monitor = P.FailureMonitor(self.rank, store, world=self.world)

@@ -71,6 +71,32 @@ def test_advance_matches_oracle(wl, cuda):
     assert rel_max(w.cell, o.w) < TOL
 
 
+@pytest.mark.parametrize("wl", [W.C2.scaled(n=120, steps=30), W.C4.scaled(n=10, steps=15)])
+def test_stencil_layouts_agree(wl, cuda):
+    """The slot-shared least-squares stencil (the default) and manapy's order give the same
+    states to rounding, and both the oracle's."""
+    el, vx = wl.mesh()
+    runs = []
+    for stencil in ("shared", "manapy"):
+        dom = M.Domain(dim=wl.dim, mesh=(el, vx), stencil=stencil)
+        assert dom.device_mesh.stencil == stencil
+        w = M.Variable(domain=dom, BC=wl.bc, values=wl.bc_values)
+        vel = [M.Variable(domain=dom) for _ in range(3)]
+        for var, a in zip(vel, wl.velocity(dom.faces.center)):
+            var.face = a
+            var.interpolate_facetocell()
+        w.cell = wl.init(dom.cells.center)
+        S = M.AdvectionDiffusionSolver(w, vel=tuple(vel), conf=M.Struct(
+            Dxx=wl.diffusion[0], Dyy=wl.diffusion[1], Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl))
+        S.advance(wl.steps, graph=True)
+        runs.append(w.cell)
+    o = _oracle(el, vx, wl)
+    for _ in range(wl.steps):
+        o.step()
+    assert rel_max(runs[0], runs[1]) < 1e-13
+    assert rel_max(runs[0], o.w) < TOL and rel_max(runs[1], o.w) < TOL
+
+
 def test_graph_and_eager_agree_bitwise(cuda):
     wl = W.C2.scaled(n=40, steps=9)
     el, vx = wl.mesh()
