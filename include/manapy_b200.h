@@ -118,6 +118,12 @@ typedef struct mb_mesh {
   const float *n2c_sell_alpha_f32;
   /* [nbfaces][4] = {n_x, n_y, 1/mesure, 0} rounded to FP32 (FP32-compensated shallow water, 2D) */
   const float *face_nm_f32;
+  /* tetrahedra, optional: [nbcells][8] the least-squares moment matrix of each cell's
+   * stencil (the lsq_sell neighbours, then its stencil ghosts) as {c_xx, c_xy, c_xz, c_yy,
+   * c_yz, c_zz, det, 0}, cofactors and determinant (mb_lsq_matrix_3d).  The matrix depends
+   * on the geometry only; when given, the fused 3D step reads it instead of forming it
+   * every step.  Must come from the lsq_sell table of this struct. */
+  const double *cell_lsq;
 } mb_mesh;
 
 typedef struct mb_bc {
@@ -272,6 +278,12 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
 /* Rows {centre, value} of a state, [nbcells][4] doubles, 32-byte aligned: {x, y, w, 0} for
  * triangles, {x, y, z, w} for tetrahedra (no counterpart in manapy). */
 int mb_pack_rows(const mb_mesh *m, const double *w, double *rows, void *stream);
+
+/* The cell_lsq table of a tetrahedral mesh with compact tables ([nbcells][8] doubles, 32-byte
+ * aligned): the moment matrix sum over the stencil of d d^T, d = centre offset, of
+ * manapy/ast/functions3d.py:4-120 (cell_gradient_3d), as cofactors and determinant, summed
+ * in the order the fused step sums its right-hand side.  Once per mesh. */
+int mb_lsq_matrix_3d(const mb_mesh *m, double *out, void *stream);
 
 /* mb_advdiff_step for a run of consecutive steps (no counterpart in manapy): rows_in holds
  * the rows of w_in (mb_pack_rows, or the previous step's rows_out), from which the first

@@ -36,7 +36,7 @@ class MbMesh(ctypes.Structure):
                 ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp),
                 ("cell_vtx", _vp), ("cell_nbr", _vp), ("cell_flags", _vp), ("node_coord", _vp), ("cell_xy", _vp),
                 ("lsq_sell_ptr", _vp), ("lsq_sell_idx", _vp), ("n2c_sell_ptr", _vp), ("n2c_sell_idx", _vp),
-                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp)]
+                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp), ("cell_lsq", _vp)]
 
 
 class MbBC(ctypes.Structure):
@@ -106,6 +106,7 @@ _SIGS = {
     "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_pack_rows": [_M, _vp, _vp, _vp],
+    "mb_lsq_matrix_3d": [_M, _vp, _vp],
     "mb_advdiff_step_rows": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                              _vp],
     "mb_cell_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],

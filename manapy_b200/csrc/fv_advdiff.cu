@@ -837,7 +837,7 @@ __device__ __forceinline__ void ld_row(const double *p, double &x, double &y, do
 constexpr int kQ1B[4] = {kBlock, 128, 256, 128};
 constexpr int kQ1M[4] = {MB_P1_3D_MIN_BLOCKS, 8, 3, 6};
 
-template <bool ORDER2, bool DIFF, int VAR>
+template <bool ORDER2, bool DIFF, int VAR, bool PRE = false>
 __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                                         double *__restrict__ rec,
                                                                         const double *__restrict__ rows,
@@ -862,10 +862,13 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
     int nx[B];
 #pragma unroll
     for (int u = 0; u < B; ++u) nx[u] = u < L ? ld1_stream(ix + 32 * u, pst) : -1;
+    // PRE: the moment matrix comes from m.cell_lsq; only the right-hand side is summed here
     auto acc = [&](const D3 &pc, double wc) {
       const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z, dw = wc - wi;
-      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
-      ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+      if (!PRE) {
+        ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+        ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+      }
       jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
     };
     for (; k + B <= L; k += B) {
@@ -903,16 +906,22 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
     for (int k = gb; k < ge; ++k) {
       const int f = ld(m.ghostnid_idx + k);
       const double *gc = m.face_ghostcenter + 3 * f;
-      const double dx = ld(gc) - c.x, dy = ld(gc + 1) - c.y, dz = ld(gc + 2) - c.z;
-      const double dw = ghost(f) - wi;
-      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
-      ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
-      jx += (dx * dw); jy += (dy * dw); jz += (dz * dw);
+      acc(d3(ld(gc), ld(gc + 1), ld(gc + 2)), ghost(f));
     }
-    const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) - izz * (ixy * ixy);
-    const double gx = ((iyy * izz - iyz * iyz) * jx + (ixz * iyz - ixy * izz) * jy + (ixy * iyz - ixz * iyy) * jz) / dia;
-    const double gy = ((ixz * iyz - ixy * izz) * jx + (ixx * izz - ixz * ixz) * jy + (ixy * ixz - iyz * ixx) * jz) / dia;
-    const double gz = ((ixy * iyz - ixz * iyy) * jx + (ixy * ixz - iyz * ixx) * jy + (ixx * iyy - ixy * ixy) * jz) / dia;
+    double gx, gy, gz;
+    if (PRE) {
+      double a, b, cc, d, e, ff, dia, pad;
+      ld4d(m.cell_lsq + 8 * (long long)i, a, b, cc, d);
+      ld4d(m.cell_lsq + 8 * (long long)i + 4, e, ff, dia, pad);
+      gx = (a * jx + b * jy + cc * jz) / dia;
+      gy = (b * jx + d * jy + e * jz) / dia;
+      gz = (cc * jx + e * jy + ff * jz) / dia;
+    } else {
+      const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) - izz * (ixy * ixy);
+      gx = ((iyy * izz - iyz * iyz) * jx + (ixz * iyz - ixy * izz) * jy + (ixy * iyz - ixz * iyy) * jz) / dia;
+      gy = ((ixz * iyz - ixy * izz) * jx + (ixx * izz - ixz * ixz) * jy + (ixy * ixz - iyz * ixx) * jz) / dia;
+      gz = ((ixy * iyz - ixz * iyy) * jx + (ixy * ixz - iyz * ixx) * jy + (ixx * iyy - ixy * ixy) * jz) / dia;
+    }
     // Barth limiter over the four faces
     const int4 vt = ld4(m.cell_vtx + 4 * i);
     const int4 nb = ld4(m.cell_nbr + 4 * i);
@@ -954,6 +963,36 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
     for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
     wn[n] = acc;
   }
+}
+
+// cell_lsq of a tetrahedral mesh: the moment matrix of each cell's stencil summed in the
+// order of k_f3_phase1 (SELL slots, then stencil ghosts), as cofactors and determinant with
+// the expressions k_f3_phase1 uses when it forms the matrix itself
+__global__ void __launch_bounds__(kBlock) k_lsq_matrix3(mb_mesh m, double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const int lane = threadIdx.x & 31;
+  const D3 c = ld3(m.cell_xy + 4 * (long long)i);
+  double ixx = 0., iyy = 0., izz = 0., ixy = 0., ixz = 0., iyz = 0.;
+  auto acc = [&](const D3 &pc) {
+    const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z;
+    ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+    ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
+  };
+  const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
+  for (int k = 0; k < (se - sb) >> 5; ++k) {
+    const int cc = ld(m.lsq_sell_idx + sb + lane + 32 * k);
+    acc(cc < 0 ? c : ld3(m.cell_xy + 4 * (long long)cc));
+  }
+  const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+  for (int k = gb; k < ge; ++k) {
+    const double *gc = m.face_ghostcenter + 3 * ld(m.ghostnid_idx + k);
+    acc(d3(ld(gc), ld(gc + 1), ld(gc + 2)));
+  }
+  const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) - izz * (ixy * ixy);
+  double *o = out + 8 * (long long)i;
+  st4d_plain(o, iyy * izz - iyz * iyz, ixz * iyz - ixy * izz, ixy * iyz - ixz * iyy, ixx * izz - ixz * ixz);
+  st4d_plain(o + 4, ixy * ixz - iyz * ixx, ixx * iyy - ixy * ixy, dia, 0.0);
 }
 
 #ifndef MB_P2_3D_MIN_BLOCKS
@@ -1155,8 +1194,12 @@ inline void f2_p2_pick(int v, const mb_mesh &m, const mb_bc &bc, const mb_advdif
 template <bool O2, bool DF, int V>
 inline void f3_p1_run(const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows, double *wn,
                       cudaStream_t st) {
-  const int ncb = O2 ? ceil_div(m.nbcells, kQ1B[V]) : 0, nnb = DF ? ceil_div(m.nbnodes, kQ1B[V]) : 0;
-  k_f3_phase1<O2, DF, V><<<ncb + nnb, kQ1B[V], 0, st>>>(m, bc, w, cs, rows, wn, ncb);
+  const int B = kQ1B[V];
+  const int ncb = O2 ? ceil_div(m.nbcells, B) : 0, nnb = DF ? ceil_div(m.nbnodes, B) : 0;
+  if (O2 && m.cell_lsq)
+    k_f3_phase1<O2, DF, V, true><<<ncb + nnb, B, 0, st>>>(m, bc, w, cs, rows, wn, ncb);
+  else
+    k_f3_phase1<O2, DF, V, false><<<ncb + nnb, B, 0, st>>>(m, bc, w, cs, rows, wn, ncb);
 }
 template <bool O2, bool DF>
 inline void f3_p1_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows,
@@ -1201,7 +1244,7 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
     // 256-bit loads of [n][4] rows: the phase-1 records (2D) and the centre and vertex
     // tables (3D) must start on 32-byte boundaries
     auto a32 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 31) == 0; };
-    if ((O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord)))) return MB_EINVAL;
+    if ((O2 && !a32(cs)) || (DIM == 3 && (!a32(m.cell_xy) || !a32(m.node_coord) || !a32(m.cell_lsq)))) return MB_EINVAL;
     if ((rows_in && !a32(rows_in)) || (rows_out && !a32(rows_out))) return MB_EINVAL;
 #endif
 #if MB_V4_IO
@@ -1403,6 +1446,15 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
     else { if (df) MB_STEP(3, false, true); else MB_STEP(3, false, false); }
   }
 #undef MB_STEP
+}
+
+int mb_lsq_matrix_3d(const mb_mesh *m, double *out, void *stream) {
+  MB_NVTX();
+  if (!mesh_ok(m) || m->dim != 3 || !out || !compact_tables(*m) || !m->ghostnid_ptr || !m->ghostnid_idx ||
+      !m->face_ghostcenter || (reinterpret_cast<uintptr_t>(out) & 31) != 0)
+    return MB_EINVAL;
+  k_lsq_matrix3<<<ceil_div(m->nbcells, kBlock), kBlock, 0, ST(stream)>>>(*m, out);
+  return check_launch();
 }
 
 int mb_pack_rows(const mb_mesh *m, const double *w, double *rows, void *stream) {

@@ -143,6 +143,8 @@ class AdvectionDiffusionSolver:
     def _setup(self):
         if self._dm is None:
             self._dm = self.domain.device_mesh
+            if self.order == 2:
+                self._dm.ensure_lsq_matrix(self._stream())
             if self.launch != "auto":
                 self._dm.struct.variant = int(self.launch)
             dev = self._dm.device

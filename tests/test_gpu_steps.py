@@ -361,3 +361,67 @@ def test_every_launch_variant_gives_the_default_result(wl, cuda):
     w0 = w.cell.copy()
     assert autotune.launch_variant(S, steps=4) in range(16)
     assert np.array_equal(w.cell, w0)
+
+
+def test_precomputed_moment_matrix(cuda):
+    """mb_lsq_matrix_3d: every tetrahedron's moment matrix (cofactors, determinant) matches
+    the sum over its stencil formed on the host, and the second-order step that reads it
+    gives the step that forms the matrix itself, to rounding."""
+    import gpuutil as U
+    from manapy_b200 import _lib
+    wl = W.C4.scaled(n=7)
+    el, vx = wl.mesh()
+    A = G.build(el, vx, 3)
+    dm = U.mesh(A, reorder=True)
+    db = U.bc(A, B.resolve(A, wl.bc, wl.bc_values), dm)
+    R = dm.R
+    nc, nn = A["nbcells"], A["nbnodes"]
+    st = U.stream()
+    lsq = U.Z(8 * nc)
+    U.call("mb_lsq_matrix_3d", dm.struct, U.P(lsq), st)
+    got = U.H(lsq).reshape(nc, 8)[R.cinv]          # manapy numbering
+    c = A["cells_center"][:, :3]
+    ptr, idx = A["cellnid_ptr"], A["cellnid_idx"]
+    gptr, gidx = A["ghostnid_ptr"], A["ghostnid_idx"]
+    M_ = np.zeros((nc, 3, 3))
+    for i in range(nc):
+        pts = np.concatenate([c[idx[ptr[i]:ptr[i + 1]]], A["faces_ghostcenter"][gidx[gptr[i]:gptr[i + 1]], :3]])
+        d = pts - c[i]
+        M_[i] = d.T @ d
+    det = np.linalg.det(M_)
+    cof = np.stack([M_[:, 1, 1] * M_[:, 2, 2] - M_[:, 1, 2] ** 2, M_[:, 0, 2] * M_[:, 1, 2] - M_[:, 0, 1] * M_[:, 2, 2],
+                    M_[:, 0, 1] * M_[:, 1, 2] - M_[:, 0, 2] * M_[:, 1, 1], M_[:, 0, 0] * M_[:, 2, 2] - M_[:, 0, 2] ** 2,
+                    M_[:, 0, 1] * M_[:, 0, 2] - M_[:, 1, 2] * M_[:, 0, 0], M_[:, 0, 0] * M_[:, 1, 1] - M_[:, 0, 1] ** 2],
+                   axis=1)
+    assert rel_max(got[:, :6], cof) < 1e-12
+    assert rel_max(got[:, 6], det) < 1e-12
+    assert np.all(got[:, 7] == 0)
+    # the step with and without the table
+    uf, vf, wf = wl.velocity(A["faces_center"])
+    sign = U.Z(4 * nc)
+    u_, v_, w_ = U.T(uf[R.fperm]), U.T(vf[R.fperm]), U.T(wf[R.fperm])
+    U.call("mb_cell_face_sign", dm.struct, U.P(u_), U.P(v_), U.P(w_), U.P(sign), st)
+    cells = [U.Z(nc) for _ in range(3)]
+    for f, cc in zip((u_, v_, w_), cells):
+        U.call("mb_facetocell", dm.struct, U.P(f), U.P(cc), st)
+    dt = U.Z(1)
+    U.call("mb_time_step", dm.struct, *[U.P(x) for x in cells], wl.cfl, *wl.diffusion, U.P(dt), st)
+    prm = _lib.MbAdvDiffParams(2, 1, *wl.diffusion)
+    w0 = U.T(wl.init(A["cells_center"])[R.cperm])
+    cs, ns = U.Z(8 * nc), U.Z(nn)
+    outs = []
+    for table in (None, lsq):
+        dm.struct.cell_lsq = U.P(table) if table is not None else None
+        out = U.Z(nc)
+        U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w0), U.P(out), U.P(sign), None, U.P(dt), U.P(cs),
+               U.P(ns), st)
+        outs.append(U.H(out))
+    dm.struct.cell_lsq = None
+    assert rel_max(outs[1], outs[0]) < 1e-14
+    assert not np.array_equal(outs[0], U.H(w0))
+    # a table not 32-byte aligned is refused
+    dm.struct.cell_lsq = U.P(lsq) + 8
+    out = U.Z(nc)
+    assert _lib.lib().mb_advdiff_step(dm.struct, db.struct, prm, U.P(w0), U.P(out), U.P(sign), None, U.P(dt),
+                                      U.P(cs), U.P(ns), st) == _lib.MB_EINVAL
+    dm.struct.cell_lsq = None
