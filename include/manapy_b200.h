@@ -279,6 +279,19 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
  * triangles, {x, y, z, w} for tetrahedra (no counterpart in manapy). */
 int mb_pack_rows(const mb_mesh *m, const double *w, double *rows, void *stream);
 
+/* mb_advdiff_step in two parts, so that the values of cells [0, nfirst) are final before the
+ * rest are computed (a sharded run numbers the cells its peers read first and sends them
+ * while part 1 runs): part 0 runs the first phase over every cell and node and the second
+ * phase over cells [0, nfirst); part 1 the second phase over cells [nfirst, nbcells),
+ * reading the first phase's results that part 0 left in cell_scratch / node_scratch (both
+ * parts with the same arguments, part 1 after part 0 on the same stream or ordered after
+ * it).  Together they compute exactly what mb_advdiff_step computes.  Compact tables only.
+ * Replaces the same step as mb_advdiff_step (manapy/solvers/advecdiff/system.py:156-172);
+ * the split has no counterpart in manapy, whose halo exchange follows the whole step. */
+int mb_advdiff_step_split(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p, const double *w_in,
+                          double *w_out, const double *sign_cf, const double *src, const double *dt_dev,
+                          double *cell_scratch, double *node_scratch, int32_t part, int32_t nfirst, void *stream);
+
 /* The cell_lsq table of a tetrahedral mesh with compact tables ([nbcells][8] doubles, 32-byte
  * aligned): the moment matrix sum over the stencil of d d^T, d = centre offset, of
  * manapy/ast/functions3d.py:4-120 (cell_gradient_3d), as cofactors and determinant, summed

@@ -626,9 +626,10 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
                                           const double *__restrict__ sign, const double *__restrict__ src,
                                           const double *__restrict__ dt_dev, const double *__restrict__ rec,
                                           const double *__restrict__ wn, int bid,
-                                          double *__restrict__ rows_out = nullptr) {
-  const int i = bid * blockDim.x + threadIdx.x;
-  if (i >= m.nbcells) return;
+                                          double *__restrict__ rows_out = nullptr, int c0 = 0, int c1 = -1) {
+  // cells [c0, c1) (c1 < 0: to the last cell)
+  const int i = c0 + bid * blockDim.x + threadIdx.x;
+  if (i >= (c1 < 0 ? m.nbcells : c1)) return;
   const GhostRule ghost = make_rule(m, bc, w);
   const int4 vt = ld4(m.cell_vtx + 4 * i);
   const int4 nb = ld4(m.cell_nbr + 4 * i);
@@ -750,8 +751,8 @@ __global__ void __launch_bounds__(kP2B[VAR], kP2M[VAR]) k_f2_phase2(mb_mesh m, m
                                                          const double *__restrict__ dt_dev,
                                                          const double *__restrict__ rec,
                                                          const double *__restrict__ wn,
-                                                         double *__restrict__ rows_out) {
-  f2_phase2<ORDER2, DIFF, WROWS>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x, rows_out);
+                                                         double *__restrict__ rows_out, int c0, int c1) {
+  f2_phase2<ORDER2, DIFF, WROWS>(m, bc, p, w, w_out, sign, src, dt_dev, rec, wn, blockIdx.x, rows_out, c0, c1);
 }
 
 // ---------------------------------------------------------------- batches of triangle meshes, FP64
@@ -1013,9 +1014,9 @@ __global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, m
                                                          const double *__restrict__ dt_dev,
                                                          const double *__restrict__ rec,
                                                          const double *__restrict__ wn,
-                                                         double *__restrict__ rows_out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m.nbcells) return;
+                                                         double *__restrict__ rows_out, int c0, int c1) {
+  const int i = c0 + blockIdx.x * blockDim.x + threadIdx.x;   // cells [c0, c1)
+  if (i >= c1) return;
   const GhostRule ghost = make_rule(m, bc, w);
   const int4 vt = ld4(m.cell_vtx + 4 * i);
   const int4 nb = ld4(m.cell_nbr + 4 * i);
@@ -1176,20 +1177,21 @@ inline void f2_p1_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w
 template <bool O2, bool DF, bool WROWS, int V>
 inline void f2_p2_run(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                       double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
-                      const double *wn, double *rows_out, cudaStream_t st) {
-  k_f2_phase2<O2, DF, WROWS, V><<<ceil_div(m.nbcells, kP2B[V]), kP2B[V], 0, st>>>(m, bc, p, w_in, w_out, sign, src,
-                                                                                   dt, cs, wn, rows_out);
+                      const double *wn, double *rows_out, int c0, int c1, cudaStream_t st) {
+  if (c1 <= c0) return;
+  k_f2_phase2<O2, DF, WROWS, V><<<ceil_div(c1 - c0, kP2B[V]), kP2B[V], 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt,
+                                                                                 cs, wn, rows_out, c0, c1);
 }
 template <bool O2, bool DF, bool WROWS>
 inline void f2_p2_pick(int v, const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                        double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
-                       const double *wn, double *rows_out, cudaStream_t st) {
+                       const double *wn, double *rows_out, int c0, int c1, cudaStream_t st) {
   if constexpr (O2 && DF) {
-    if (v == 1) return f2_p2_run<O2, DF, WROWS, 1>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
-    if (v == 2) return f2_p2_run<O2, DF, WROWS, 2>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
-    if (v == 3) return f2_p2_run<O2, DF, WROWS, 3>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+    if (v == 1) return f2_p2_run<O2, DF, WROWS, 1>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
+    if (v == 2) return f2_p2_run<O2, DF, WROWS, 2>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
+    if (v == 3) return f2_p2_run<O2, DF, WROWS, 3>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
   }
-  f2_p2_run<O2, DF, WROWS, 0>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+  f2_p2_run<O2, DF, WROWS, 0>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
 }
 template <bool O2, bool DF, int V>
 inline void f3_p1_run(const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows, double *wn,
@@ -1214,29 +1216,36 @@ inline void f3_p1_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w
 template <bool O2, bool DF, bool WROWS, int V>
 inline void f3_p2_run(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                       double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
-                      const double *wn, double *rows_out, cudaStream_t st) {
-  k_f3_phase2<O2, DF, WROWS, V><<<ceil_div(m.nbcells, kQ2B[V]), kQ2B[V], 0, st>>>(m, bc, p, w_in, w_out, sign, src,
-                                                                                   dt, cs, wn, rows_out);
+                      const double *wn, double *rows_out, int c0, int c1, cudaStream_t st) {
+  if (c1 <= c0) return;
+  k_f3_phase2<O2, DF, WROWS, V><<<ceil_div(c1 - c0, kQ2B[V]), kQ2B[V], 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt,
+                                                                                 cs, wn, rows_out, c0, c1);
 }
 template <bool O2, bool DF, bool WROWS>
 inline void f3_p2_pick(int v, const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                        double *w_out, const double *sign, const double *src, const double *dt, const double *cs,
-                       const double *wn, double *rows_out, cudaStream_t st) {
+                       const double *wn, double *rows_out, int c0, int c1, cudaStream_t st) {
   if constexpr (O2 && DF) {
-    if (v == 1) return f3_p2_run<O2, DF, WROWS, 1>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
-    if (v == 2) return f3_p2_run<O2, DF, WROWS, 2>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
-    if (v == 3) return f3_p2_run<O2, DF, WROWS, 3>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+    if (v == 1) return f3_p2_run<O2, DF, WROWS, 1>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
+    if (v == 2) return f3_p2_run<O2, DF, WROWS, 2>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
+    if (v == 3) return f3_p2_run<O2, DF, WROWS, 3>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
   }
-  f3_p2_run<O2, DF, WROWS, 0>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
+  f3_p2_run<O2, DF, WROWS, 0>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
 }
 
 // cell scratch: [4][nbcells] planes gx, gy, gz, psi (face-table path), [nbcells][4]
 // records {w, gx, gy, psi} (compact 2D path) or [nbcells][4] records {w, psi gx, psi gy,
 // psi gz} then [nbcells][4] rows {x, y, z, w} (compact 3D path); node scratch: [nbnodes]
+// part < 0: the whole step; part 0: phase 1 and phase 2 of cells [0, nfirst); part 1: phase 2
+// of cells [nfirst, nbcells), reading what part 0 left in the scratch (compact tables only)
 template <int DIM, bool O2, bool DF>
 int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, const double *w_in,
                 double *w_out, const double *sign, const double *src, const double *dt, double *cs,
-                double *wn, cudaStream_t st, const double *rows_in = nullptr, double *rows_out = nullptr) {
+                double *wn, cudaStream_t st, const double *rows_in = nullptr, double *rows_out = nullptr,
+                int part = -1, int nfirst = 0) {
+  if (part >= 0 && (!compact_tables(m) || nfirst < 0 || nfirst > m.nbcells)) return MB_EINVAL;
+  const int c0 = part == 1 ? nfirst : 0, c1 = part == 0 ? nfirst : m.nbcells;
+  const bool p1 = part != 1;
   const int ncb = O2 ? ceil_div(m.nbcells, kBlock) : 0;
   const int nnb = DF ? ceil_div(m.nbnodes, kBlock) : 0;
   if (compact_tables(m)) {
@@ -1253,23 +1262,23 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
     // launch-shape variants (second order with diffusion only): bits 0-1 phase 1, bits 2-3 phase 2
     const int v1 = (O2 && DF) ? (m.variant & 3) : 0, v2 = (O2 && DF) ? ((m.variant >> 2) & 3) : 0;
     if (DIM == 2) {
-      if (O2 || DF) {
+      if ((O2 || DF) && p1) {
         if (rows_in) f2_p1_pick<O2, DF, true>(v1, m, bc, w_in, cs, wn, rows_in, st);
         else f2_p1_pick<O2, DF, false>(v1, m, bc, w_in, cs, wn, nullptr, st);
       }
-      if (rows_out) f2_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
-      else f2_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, st);
+      if (rows_out) f2_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
+      else f2_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, c0, c1, st);
     } else {
       // cell scratch: records [0, 4 nbcells), then (without rows_in) the pack pass's rows
       const double *rows = rows_in;
-      if (O2 && !rows) {
+      if (O2 && !rows && p1) {
         double *pk = cs + 4 * (long long)m.nbcells;
         k_pack_rows<3><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, w_in, pk);
         rows = pk;
       }
-      if (O2 || DF) f3_p1_pick<O2, DF>(v1, m, bc, w_in, cs, rows, wn, st);
-      if (rows_out) f3_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, st);
-      else f3_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, st);
+      if ((O2 || DF) && p1) f3_p1_pick<O2, DF>(v1, m, bc, w_in, cs, rows, wn, st);
+      if (rows_out) f3_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
+      else f3_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, c0, c1, st);
     }
     return check_launch();
   }
@@ -1438,6 +1447,31 @@ int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *
   cudaStream_t st = ST(stream);
 #define MB_STEP(D, O, F) \
   return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, st)
+  if (m->dim == 2) {
+    if (o2) { if (df) MB_STEP(2, true, true); else MB_STEP(2, true, false); }
+    else { if (df) MB_STEP(2, false, true); else MB_STEP(2, false, false); }
+  } else {
+    if (o2) { if (df) MB_STEP(3, true, true); else MB_STEP(3, true, false); }
+    else { if (df) MB_STEP(3, false, true); else MB_STEP(3, false, false); }
+  }
+#undef MB_STEP
+}
+
+int mb_advdiff_step_split(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p, const double *w_in,
+                          double *w_out, const double *sign_cf, const double *src, const double *dt_dev,
+                          double *cell_scratch, double *node_scratch, int32_t part, int32_t nfirst, void *stream) {
+  MB_NVTX();
+  if (!mesh_ok(m) || !bc || !p || !w_in || !w_out || w_in == w_out || !sign_cf || !dt_dev) return MB_EINVAL;
+  if ((part != 0 && part != 1) || !compact_tables(*m) || nfirst < 0 || nfirst > m->nbcells) return MB_EINVAL;
+  if (p->order != 1 && p->order != 2) return MB_EINVAL;
+  const bool o2 = p->order == 2, df = p->diffusion != 0;
+  if (o2 && !cell_scratch) return MB_EINVAL;
+  if (df && (!node_scratch || !bc->face_grad_on)) return MB_EINVAL;
+  if (!bc->kind || !bc->value) return MB_EINVAL;
+  cudaStream_t st = ST(stream);
+#define MB_STEP(D, O, F)                                                                                     \
+  return launch_step<D, O, F>(*m, *bc, *p, w_in, w_out, sign_cf, src, dt_dev, cell_scratch, node_scratch, st, \
+                              nullptr, nullptr, part, nfirst)
   if (m->dim == 2) {
     if (o2) { if (df) MB_STEP(2, true, true); else MB_STEP(2, true, false); }
     else { if (df) MB_STEP(2, false, true); else MB_STEP(2, false, false); }

@@ -162,10 +162,11 @@ class DeviceMesh:
     arrays between that numbering and manapy's.
     """
 
-    def __init__(self, A, device="cuda", reorder=True, stencil="shared"):
+    def __init__(self, A, device="cuda", reorder=True, stencil="shared", first_cells=None):
         """``device=None`` builds the tables as numpy arrays on the host (``upload`` moves
         them to a device later, e.g. after building in a worker process); ``stencil``: the
-        layout of the least-squares stencil (``lsq_sell``)."""
+        layout of the least-squares stencil (``lsq_sell``); ``first_cells``: boolean mask of
+        cells numbered first (``nfirst`` of them; ``mb_advdiff_step_split``)."""
         if stencil not in STENCILS:
             raise ValueError("stencil must be one of %s" % (STENCILS,))
         self.stencil = stencil
@@ -180,8 +181,9 @@ class DeviceMesh:
             raise ValueError("mesh has boundary faces that match no boundary side (manapy names them "
                              "100/200 and leaves them out of every face list)")
         self.dim, self.nbcells, self.nbfaces, self.nbnodes, self.nlf = dim, nc, nf, nn, nlf
-        R = Renumbering(A, enabled=reorder)
+        R = Renumbering(A, enabled=reorder, first=first_cells)
         self.R = R
+        self.nfirst = int(np.count_nonzero(first_cells)) if first_cells is not None else 0
         cp, fp, np_ = R.cperm, R.fperm, R.nperm
         ci, fi, ni = R.cinv, R.finv, R.ninv
         f64, i32 = np.float64, np.int32

@@ -144,6 +144,13 @@ class HaloExchange:
     def exchange(self, fields):
         """In place: fields[halo] = owners' values.  ``fields``: one 1-D float64 tensor over
         the submesh cells, or a list of them (exchanged together)."""
+        return self.finish(self.start(fields))
+
+    def start(self, fields):
+        """First half of ``exchange``: pack the send entries (ordered on the current stream
+        after what it has queued) and post the sends and receives.  Work queued on the
+        stream before ``finish`` runs while the messages travel; it must not write the send
+        entries.  Returns the handle ``finish`` takes."""
         import torch
         from . import _lib
         dist = self.dist
@@ -172,11 +179,18 @@ class HaloExchange:
                 ops.append(dist.P2POp(dist.irecv, rbuf[ro * nf:(ro + n_r) * nf], q, group=self.group))
             so += n_s
             ro += n_r
-        if ops:
-            for w in dist.batch_isend_irecv(ops):
-                w.wait()
+        works = dist.batch_isend_irecv(ops) if ops else []
+        return (fields, fl, nf, nr, cuda, st, ptrs, sbuf, rbuf, rdev if (self.stage and cuda) else None, works)
+
+    def finish(self, handle):
+        """Second half of ``exchange``: wait for the messages (NCCL: the current stream
+        waits; gloo: the host) and scatter the received values into the halo entries."""
+        from . import _lib
+        fields, fl, nf, nr, cuda, st, ptrs, sbuf, rbuf, rdev, works = handle
+        for w in works:
+            w.wait()
         if cuda:
-            if self.stage:
+            if rdev is not None:
                 rdev.copy_(rbuf)
                 rbuf = rdev
             _lib.call("mb_halo_unpack", ptrs, nf, self.recv_idx.data_ptr(), nr, rbuf.data_ptr(), st)

@@ -76,12 +76,17 @@ def node_order(n2c_ptr, n2c_idx, cinv, nnodes):
 class Renumbering:
     """perm (new -> old) and inv (old -> new) of cells, faces and nodes."""
 
-    def __init__(self, A, enabled=True):
+    def __init__(self, A, enabled=True, first=None):
+        """``first``: optional boolean mask of cells numbered before all others (each group
+        in the order it would have otherwise)."""
         nc, nf, nn = int(A["nbcells"]), int(A["nbfaces"]), int(A["nbnodes"])
         if enabled:
             self.cperm = morton_cells(A["cells_center"], int(A["dim"]))
         else:
             self.cperm = np.arange(nc)
+        if first is not None:
+            first = np.asarray(first, dtype=bool)
+            self.cperm = np.concatenate([self.cperm[first[self.cperm]], self.cperm[~first[self.cperm]]])
         self.cinv = np.empty(nc, dtype=np.int64)
         self.cinv[self.cperm] = np.arange(nc)
         if enabled:

@@ -8,6 +8,10 @@ ranks of each rank's CFL dt (``manapy/solvers/advecdiff/system.py:152`` and
 ``manapy/solvers/shallowater/system.py:188``: manapy's ``allreduce(MIN)``).  The owned
 cells' results are bit-identical to the single-GPU run of the whole mesh.
 
+Advection-diffusion overlaps the exchange with the step: each shard numbers the cells its
+peers read first, computes them (``mb_advdiff_step_split`` part 0), posts the exchange, and
+computes the other cells (part 1) while the messages travel; the halo is written after both.
+
 Before each step every rank checks the run's failure record (``partition.FailureMonitor``):
 a rank that failed between steps has posted it, and the others raise ``RankFailure``
 instead of entering an exchange that would wait for it.
@@ -31,7 +35,7 @@ class _Sharded:
     """Shard, device mesh, halo exchange and failure monitor of one rank."""
 
     def __init__(self, elements, vertex, dim, group, device, store, extra_cells=None, sync_every=0, check_every=1,
-                 A=None):
+                 A=None, send_first=False):
         import torch.distributed as dist
         self.dist, self.group = dist, group
         self.rank = dist.get_rank(group)
@@ -41,8 +45,14 @@ class _Sharded:
         self.shard = P.build_shards(elements, vertex, dim, self.world, A=A, extra_cells=extra_cells)[self.rank]
         A = G.build(self.shard.elements, self.shard.vertex, dim, halo_rim=True)
         self.A = A
-        # manapy's stencil order: every cell's sums formed as in the single-domain run
-        self.dm = DeviceMesh(A, self.dev, stencil="manapy")
+        # manapy's stencil order: every cell's sums formed as in the single-domain run;
+        # with send_first the cells peers read are numbered first
+        first = None
+        if send_first:
+            first = np.zeros(len(self.shard.cells), dtype=bool)
+            for idx in self.shard.send.values():
+                first[np.asarray(idx, dtype=np.int64)] = True
+        self.dm = DeviceMesh(A, self.dev, stencil="manapy", first_cells=first)
         inv = self.dm.inv["cell"].cpu().numpy()
         self.exchanger = P.HaloExchange(self._to_device_numbering(inv), group, device=self.dev)
         self.monitor = P.FailureMonitor(self.rank, store, world=self.world)
@@ -109,9 +119,10 @@ class ShardedAdvectionDiffusion(_Sharded):
     options as ``AdvectionDiffusionSolver`` (Dxx, Dyy, Dzz, order, cfl)."""
 
     def __init__(self, elements, vertex, dim, BC, values, velocity, Dxx=0., Dyy=0., Dzz=0., order=1, cfl=0.4,
-                 group=None, device=None, store=None, sync_every=0, check_every=1, A=None):
+                 group=None, device=None, store=None, sync_every=0, check_every=1, A=None, overlap=True):
         super().__init__(elements, vertex, dim, group, device, store, sync_every=sync_every, check_every=check_every,
-                         A=A)
+                         A=A, send_first=overlap)
+        self.overlap = bool(overlap)
         A = self.A
         self.bc = DeviceBC(A, B.resolve(A, BC, values), self.dev, mesh=self.dm)
         self.params = _lib.MbAdvDiffParams(int(order), int(not (Dxx == Dyy == Dzz == 0)), float(Dxx), float(Dyy),
@@ -153,10 +164,18 @@ class ShardedAdvectionDiffusion(_Sharded):
         self._before_step()
         with self.monitor.guard():
             x, y = self.w[self.cur], self.w[1 - self.cur]
-            _lib.call("mb_advdiff_step", self.dm.struct, self.bc.struct, self.params, _p(x), _p(y), _p(self.sign),
-                      None, _p(self.dt), _p(self.cs), _p(self.ns), self._stream())
+            args = (self.dm.struct, self.bc.struct, self.params, _p(x), _p(y), _p(self.sign), None, _p(self.dt),
+                    _p(self.cs), _p(self.ns))
+            if self.overlap:
+                # the cells peers read, the exchange posted, the other cells while it travels
+                _lib.call("mb_advdiff_step_split", *args, 0, self.dm.nfirst, self._stream())
+                pending = self.exchanger.start(y)
+                _lib.call("mb_advdiff_step_split", *args, 1, self.dm.nfirst, self._stream())
+                self.exchanger.finish(pending)
+            else:
+                _lib.call("mb_advdiff_step", *args, self._stream())
+                self.exchanger.exchange(y)
             self.cur = 1 - self.cur
-            self.exchanger.exchange(self.w[self.cur])
 
     def owned_values(self):
         """(global cell ids, values) of the cells this rank owns."""

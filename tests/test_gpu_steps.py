@@ -425,3 +425,48 @@ def test_precomputed_moment_matrix(cuda):
     assert _lib.lib().mb_advdiff_step(dm.struct, db.struct, prm, U.P(w0), U.P(out), U.P(sign), None, U.P(dt),
                                       U.P(cs), U.P(ns), st) == _lib.MB_EINVAL
     dm.struct.cell_lsq = None
+
+
+@pytest.mark.parametrize("wl", [W.C2.scaled(n=40), W.C4.scaled(n=6)])
+def test_split_step_equals_the_whole_step(wl, cuda):
+    """mb_advdiff_step_split part 0 (first phase, second phase of cells [0, nfirst)) then
+    part 1 (second phase of the rest) computes exactly mb_advdiff_step's result, with the
+    first cells numbered first as a sharded run numbers the cells its peers read."""
+    import gpuutil as U
+    from manapy_b200 import _lib
+    from manapy_b200.device import DeviceMesh
+    el, vx = wl.mesh()
+    A = G.build(el, vx, wl.dim)
+    nc, nn = A["nbcells"], A["nbnodes"]
+    first = np.random.default_rng(3).random(nc) < 0.2
+    dm = DeviceMesh(A, "cuda", first_cells=first)
+    assert dm.nfirst == int(first.sum())
+    assert np.all(first[dm.R.cperm[:dm.nfirst]]) and not np.any(first[dm.R.cperm[dm.nfirst:]])
+    db = U.bc(A, B.resolve(A, wl.bc, wl.bc_values), dm)
+    R = dm.R
+    st = U.stream()
+    uf, vf, wf = wl.velocity(A["faces_center"])
+    sign = U.Z(4 * nc)
+    u_, v_, w_ = U.T(uf[R.fperm]), U.T(vf[R.fperm]), U.T(wf[R.fperm])
+    U.call("mb_cell_face_sign", dm.struct, U.P(u_), U.P(v_), U.P(w_), U.P(sign), st)
+    cells = [U.Z(nc) for _ in range(3)]
+    for f, c in zip((u_, v_, w_), cells):
+        U.call("mb_facetocell", dm.struct, U.P(f), U.P(c), st)
+    dt = U.Z(1)
+    U.call("mb_time_step", dm.struct, *[U.P(c) for c in cells], wl.cfl, *wl.diffusion, U.P(dt), st)
+    w0 = U.T(wl.init(A["cells_center"])[R.cperm])
+    for order in (1, 2):
+        prm = _lib.MbAdvDiffParams(order, 1, *wl.diffusion)
+        cs, ns = U.Z((4 if wl.dim == 2 else 8) * nc), U.Z(nn)
+        ref, got = U.Z(nc), U.Z(nc)
+        U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(w0), U.P(ref), U.P(sign), None, U.P(dt), U.P(cs),
+               U.P(ns), st)
+        args = (dm.struct, db.struct, prm, U.P(w0), U.P(got), U.P(sign), None, U.P(dt), U.P(cs), U.P(ns))
+        U.call("mb_advdiff_step_split", *args, 0, dm.nfirst, st)
+        part0 = U.H(got)[:dm.nfirst].copy()
+        U.call("mb_advdiff_step_split", *args, 1, dm.nfirst, st)
+        assert np.array_equal(U.H(got), U.H(ref))
+        assert np.array_equal(part0, U.H(ref)[:dm.nfirst])
+    L = _lib.lib()
+    assert L.mb_advdiff_step_split(*args, 2, dm.nfirst, st) == _lib.MB_EINVAL
+    assert L.mb_advdiff_step_split(*args, 0, nc + 1, st) == _lib.MB_EINVAL

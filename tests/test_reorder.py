@@ -4,6 +4,7 @@ import pytest
 
 from manapy_b200 import geometry as G, meshgen
 from manapy_b200.device import DeviceBC, DeviceMesh, cell_order_codes
+from manapy_b200.reorder import Renumbering
 from manapy_b200 import boundary as B
 
 
@@ -82,3 +83,17 @@ def test_sell32_layout_round_trips():
                 assert np.all(row[cnt[r]:] == -1)
             elif cnt[r]:
                 assert np.all(row[cnt[r]:] == idx[ptr[r]])
+
+
+def test_first_cells_are_numbered_first():
+    el, vx = meshgen.square_triangles(20, seed=4)
+    A = G.build(el, vx, 2)
+    base = Renumbering(A)
+    first = np.random.default_rng(0).random(A["nbcells"]) < 0.3
+    R = Renumbering(A, first=first)
+    k = int(first.sum())
+    assert np.all(first[R.cperm[:k]]) and not np.any(first[R.cperm[k:]])
+    # each group keeps the locality order
+    assert np.array_equal(R.cperm[:k], base.cperm[first[base.cperm]])
+    assert np.array_equal(R.cperm[k:], base.cperm[~first[base.cperm]])
+    assert np.array_equal(R.cinv[R.cperm], np.arange(A["nbcells"]))
