@@ -120,9 +120,10 @@ typedef struct mb_mesh {
   const float *face_nm_f32;
   /* tetrahedra, optional: [nbcells][8] the least-squares moment matrix of each cell's
    * stencil (the lsq_sell neighbours, then its stencil ghosts) as {c_xx, c_xy, c_xz, c_yy,
-   * c_yz, c_zz, det, 0}, cofactors and determinant (mb_lsq_matrix_3d).  The matrix depends
-   * on the geometry only; when given, the fused 3D step reads it instead of forming it
-   * every step.  Must come from the lsq_sell table of this struct. */
+   * c_yz, c_zz, det, 0}, cofactors and determinant, 32-byte aligned (mb_lsq_matrix).  The
+   * matrix depends on the geometry only; when given, the second-order fused 3D step reads
+   * it instead of forming it every step.  Must come from the lsq_sell table of this
+   * struct.  Triangles: NULL (their step forms the matrix; reading it measured slower). */
   const double *cell_lsq;
 } mb_mesh;
 
@@ -292,11 +293,12 @@ int mb_advdiff_step_split(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_pa
                           double *w_out, const double *sign_cf, const double *src, const double *dt_dev,
                           double *cell_scratch, double *node_scratch, int32_t part, int32_t nfirst, void *stream);
 
-/* The cell_lsq table of a tetrahedral mesh with compact tables ([nbcells][8] doubles, 32-byte
- * aligned): the moment matrix sum over the stencil of d d^T, d = centre offset, of
- * manapy/ast/functions3d.py:4-120 (cell_gradient_3d), as cofactors and determinant, summed
- * in the order the fused step sums its right-hand side.  Once per mesh. */
-int mb_lsq_matrix_3d(const mb_mesh *m, double *out, void *stream);
+/* The cell_lsq table of a tetrahedral mesh with compact tables ([nbcells][8] doubles,
+ * 32-byte aligned): the moment matrix sum over the stencil of d d^T, d = centre offset, of
+ * manapy/ast/functions3d.py:4-120 (cell_gradient_3d), as cofactors and determinant, summed in
+ * the order the fused step sums its right-hand side.  Once per mesh.  MB_EINVAL for
+ * triangles. */
+int mb_lsq_matrix(const mb_mesh *m, double *out, void *stream);
 
 /* mb_advdiff_step for a run of consecutive steps (no counterpart in manapy): rows_in holds
  * the rows of w_in (mb_pack_rows, or the previous step's rows_out), from which the first

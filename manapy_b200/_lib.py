@@ -106,7 +106,7 @@ _SIGS = {
     "mb_advdiff_step": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_pack_rows": [_M, _vp, _vp, _vp],
-    "mb_lsq_matrix_3d": [_M, _vp, _vp],
+    "mb_lsq_matrix": [_M, _vp, _vp],
     "mb_advdiff_step_split": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32,
                               _i32, _vp],
     "mb_advdiff_step_rows": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

@@ -1482,7 +1482,7 @@ int mb_advdiff_step_split(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_pa
 #undef MB_STEP
 }
 
-int mb_lsq_matrix_3d(const mb_mesh *m, double *out, void *stream) {
+int mb_lsq_matrix(const mb_mesh *m, double *out, void *stream) {
   MB_NVTX();
   if (!mesh_ok(m) || m->dim != 3 || !out || !compact_tables(*m) || !m->ghostnid_ptr || !m->ghostnid_idx ||
       !m->face_ghostcenter || (reinterpret_cast<uintptr_t>(out) & 31) != 0)

@@ -323,14 +323,14 @@ class DeviceMesh:
 
     def ensure_lsq_matrix(self, stream=None):
         """Tetrahedra with compact tables: the ``cell_lsq`` table (the least-squares moment
-        matrix of every cell, ``mb_lsq_matrix_3d``), formed once on the device and pointed at by
+        matrix of every cell, ``mb_lsq_matrix``), formed once on the device and pointed at by
         the struct, so that the second-order fused step reads it instead of forming it every
         step.  No-op for triangles, host-built tables, or when it is there already."""
         if self.dim != 3 or self.device is None or "cell_lsq" in self.t or "lsq_sell_idx" not in self.t:
             return
         out = torch.empty(8 * self.nbcells, dtype=torch.float64, device=self.device)
         st = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
-        _lib.call("mb_lsq_matrix_3d", self.struct, out.data_ptr(), st)
+        _lib.call("mb_lsq_matrix", self.struct, out.data_ptr(), st)
         self.t["cell_lsq"] = out
         self.struct.cell_lsq = out.data_ptr()
 

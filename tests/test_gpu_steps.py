@@ -364,7 +364,7 @@ def test_every_launch_variant_gives_the_default_result(wl, cuda):
 
 
 def test_precomputed_moment_matrix(cuda):
-    """mb_lsq_matrix_3d: every tetrahedron's moment matrix (cofactors, determinant) matches
+    """mb_lsq_matrix: every tetrahedron's moment matrix (cofactors, determinant) matches
     the sum over its stencil formed on the host, and the second-order step that reads it
     gives the step that forms the matrix itself, to rounding."""
     import gpuutil as U
@@ -378,7 +378,7 @@ def test_precomputed_moment_matrix(cuda):
     nc, nn = A["nbcells"], A["nbnodes"]
     st = U.stream()
     lsq = U.Z(8 * nc)
-    U.call("mb_lsq_matrix_3d", dm.struct, U.P(lsq), st)
+    U.call("mb_lsq_matrix", dm.struct, U.P(lsq), st)
     got = U.H(lsq).reshape(nc, 8)[R.cinv]          # manapy numbering
     c = A["cells_center"][:, :3]
     ptr, idx = A["cellnid_ptr"], A["cellnid_idx"]
