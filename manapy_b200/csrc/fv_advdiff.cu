@@ -695,19 +695,21 @@ __device__ __forceinline__ void f2_phase2(const mb_mesh &m, const mb_bc &bc, con
       if (!b || ld(bc.face_grad_on + f)) {
         const double2 v1 = own ? ci : co, v2 = own ? co : ci;   // centres of cellid[f][0], [1]
         const double vl = own ? wi : vo, vr = own ? vo : wi;
-        const double f1x = v1.x - Xa.x, f1y = v1.y - Xa.y;
-        const double f2x = Xb.x - v1.x, f2y = Xb.y - v1.y;
-        const double f3x = v2.x - Xb.x, f3y = v2.y - Xb.y;
-        const double f4x = Xa.x - v2.x, f4y = Xa.y - v2.y;
         const double air = 0.5 * ((Xb.x - Xa.x) * (v2.y - v1.y) + (v1.x - v2.x) * (Xb.y - Xa.y));
         const int ia = rev ? comp(vt, (j + 1) % 3) : comp(vt, j);
         const int ib = rev ? comp(vt, j) : comp(vt, (j + 1) % 3);
         const double vi1 = ld(wn + ia), vi2 = ld(wn + ib);
-        const double t1 = vi1 + vl, t2 = vl + vi2, t3 = vi2 + vr, t4 = vr + vi1;
+        // manapy's diamond gradient (manapy/ast/functions2d.py:108-196, face_gradient_2d) sums
+        // (V_i1 + V_L) f_1 + (V_L + V_i2) f_2 + (V_i2 + V_R) f_3 + (V_R + V_i1) f_4 with
+        // f_1 = v1 - Xa, f_2 = Xb - v1, f_3 = v2 - Xb, f_4 = Xa - v2; grouped by value, the
+        // same sum is (V_i1 - V_i2) (v1 - v2) + (V_L - V_R) (Xb - Xa) (equal up to rounding)
+        const double dab = vi1 - vi2, dlr = vl - vr;
+        const double sx = dab * (v1.x - v2.x) + dlr * (Xb.x - Xa.x);
+        const double sy = dab * (v1.y - v2.y) + dlr * (Xb.y - Xa.y);
         // -1 / (2 air) is exactly -(1 / (2 air)): one division serves both components
         const double rda = 1 / (2 * air);
-        const double fgx = rda * (t1 * f1y + t2 * f2y + t3 * f3y + t4 * f4y);
-        const double fgy = -rda * (t1 * f1x + t2 * f2x + t3 * f3x + t4 * f4x);
+        const double fgx = rda * sy;
+        const double fgy = -rda * sx;
         double n0 = Xa.y - Xb.y, n1 = Xb.x - Xa.x;
         if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
         v = p.Dxx * fgx * n0 + p.Dyy * fgy * n1;
@@ -996,6 +998,25 @@ __global__ void __launch_bounds__(kBlock) k_lsq_matrix3(mb_mesh m, double *__res
   st4d_plain(o + 4, ixy * ixz - iyz * ixx, ixx * iyy - ixy * ixy, dia, 0.0);
 }
 
+// manapy's dissipative flux of one tetrahedron face, D (grad w . N) with the diamond
+// gradient of manapy/ast/functions3d.py:122-248 (face_gradient_3d, its f_1 / f_2 vectors from
+// manapy/ddm/ddm_utils3d.py) and manapy/solvers/advecdiff/fvm_utils.py:5-26: the same
+// quantity with the algebra folded, so that no vector of the gradient is formed.
+// f_1 = (s1 x s2 + s2 x s3) / 2 with s1 = v2 - Q2, s2 = Q3 - Q2, s3 = v1 - Q2 equals
+// (Q3 - Q2) x (v1 - v2) / 2, likewise f_2 = (Q1 - Q3) x (v1 - v2) / 2, and
+// (a x e) . d = a . (e x d); so with DN = (Dxx N_x, Dyy N_y, Dzz N_z), t = (v1 - v2) x DN:
+//   D grad . N = [(V_A - V_C) (Q3 - Q2).t / 2 + (V_B - V_C) (Q1 - Q3).t / 2
+//                 + (V_R - V_L) N.DN] / (N . (v2 - v1))
+// (V_D = V_C on triangular faces).  Equal to manapy's expression up to rounding.
+__device__ __forceinline__ double diamond3(const mb_advdiff_params &p, const D3 &N, const D3 &Q1, const D3 &Q2,
+                                           const D3 &Q3, const D3 &v1, const D3 &v2, double VA, double VB,
+                                           double VC, double VL, double VR) {
+  const D3 DN = d3(p.Dxx * N.x, p.Dyy * N.y, p.Dzz * N.z);
+  const D3 t = cross(v1 - v2, DN);
+  const double f1d = 0.5 * dot(Q3 - Q2, t), f2d = 0.5 * dot(Q1 - Q3, t);
+  return ((VA - VC) * f1d + (VB - VC) * f2d + (VR - VL) * dot(N, DN)) / dot(N, v2 - v1);
+}
+
 #ifndef MB_P2_3D_MIN_BLOCKS
 #define MB_P2_3D_MIN_BLOCKS 2
 #endif
@@ -1077,20 +1098,9 @@ __global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, m
         const int i1 = d0, i2 = swp ? d2 : d1, i3 = swp ? d1 : d2;   // faces.nodeid order
         const D3 Q2 = pick4(P, i2), Q3 = pick4(P, i3), Q1 = pick4(P, i1);
         const D3 v1 = own ? ci : co, v2 = own ? co : ci;
-        const D3 s1 = v2 - Q2, s2 = Q3 - Q2, s3 = v1 - Q2;
-        const D3 f1 = 0.5 * cross(s1, s2) + 0.5 * cross(s2, s3);
-        const D3 s4 = v2 - Q3, s5 = Q1 - Q3, s6 = v1 - Q3;
-        const D3 f2 = 0.5 * cross(s4, s5) + 0.5 * cross(s5, s6);
-        // one reciprocal of the diamond volume instead of three divisions (rounding only)
-        const double rair = 1 / dot(N, v2 - v1);
         const int gi1 = comp(vt, i1), gi2 = comp(vt, i2), gi3 = comp(vt, i3);
-        const double VA = ld(wn + gi1), VB = ld(wn + gi2), VC = ld(wn + gi3), VD = VC;
         const double VL = own ? wi : vo, VR = own ? vo : wi;
-        const double dAC = VA - VC, dBD = VB - VD, dRL = VR - VL;
-        const double fgx = (f1.x * dAC + f2.x * dBD + N.x * dRL) * rair;
-        const double fgy = (f1.y * dAC + f2.y * dBD + N.y * dRL) * rair;
-        const double fgz = (f1.z * dAC + f2.z * dBD + N.z * dRL) * rair;
-        v = p.Dxx * fgx * N.x + p.Dyy * fgy * N.y + p.Dzz * fgz * N.z;
+        v = diamond3(p, N, Q1, Q2, Q3, v1, v2, ld(wn + gi1), ld(wn + gi2), ld(wn + gi3), VL, VR);
       }
       q[j] = own ? v : -v;
     }
