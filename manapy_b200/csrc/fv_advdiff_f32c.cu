@@ -301,26 +301,22 @@ __device__ __forceinline__ void f2c_phase2(const mb_mesh &m, const mb_bc &bc, co
       float v = 0.f;
       if (!b || ld(bc.face_grad_on + f)) {
         const double2 v1 = own ? ci : co, v2 = own ? co : ci;
-        const double f1x = v1.x - Xa.x, f1y = v1.y - Xa.y;
-        const double f2x = Xb.x - v1.x, f2y = Xb.y - v1.y;
-        const double f3x = v2.x - Xb.x, f3y = v2.y - Xb.y;
-        const double f4x = Xa.x - v2.x, f4y = Xa.y - v2.y;
         const double air = 0.5 * ((Xb.x - Xa.x) * (v2.y - v1.y) + (v1.x - v2.x) * (Xb.y - Xa.y));
         double n0 = Xa.y - Xb.y, n1 = Xb.x - Xa.x;
         if (f2_flip(fl, j)) { n0 = -1 * n0; n1 = -1 * n1; }
-        // Dxx n0 gx + Dyy n1 gy = sum_k c_k t_k, t = (vi1 + vl, vl + vi2, vi2 + vr, vr + vi1);
-        // regrouped per value: a1 vi1 + a2 vi2 + al vl + ar vr
+        // Dxx n0 gx + Dyy n1 gy with manapy's diamond gradient, whose sum over f_1..f_4 of
+        // (vi1 + vl) f_1 + (vl + vi2) f_2 + (vi2 + vr) f_3 + (vr + vi1) f_4 is, grouped by
+        // value, (vi1 - vi2)(v1 - v2) + (vl - vr)(Xb - Xa): coefficients in FP64, the
+        // differences of values in FP32
         const double r2a = 1. / (2 * air);
         const double gxk = p.Dxx * n0 * r2a, gyk = p.Dyy * n1 * r2a;
-        const double c1 = gxk * f1y - gyk * f1x, c2 = gxk * f2y - gyk * f2x;
-        const double c3 = gxk * f3y - gyk * f3x, c4 = gxk * f4y - gyk * f4x;
-        const double a1 = c1 + c4, a2 = c2 + c3, al = c1 + c2, ar = c3 + c4;
-        const float ao = (float)(own ? ar : al);  // coefficient of the other side's value
-        const float sa = (float)(a1 + a2 + al + ar);
+        const double a1 = gxk * (v1.y - v2.y) - gyk * (v1.x - v2.x);
+        const double al = gxk * (Xb.y - Xa.y) - gyk * (Xb.x - Xa.x);
+        const float ao = (float)(own ? -al : al);  // coefficient of (other side - this cell)
         const int ia = rev ? comp(vt, (j + 1) % 3) : comp(vt, j);
         const int ib = rev ? comp(vt, j) : comp(vt, (j + 1) % 3);
         const float vi1 = ld(wn + ia), vi2 = ld(wn + ib);
-        v = (float)a1 * (vi1 - wi) + (float)a2 * (vi2 - wi) + ao * (vo - wi) + sa * wi;
+        v = (float)a1 * (vi1 - vi2) + ao * (vo - wi);
       }
       q[j] = own ? v : -v;
     }
@@ -558,14 +554,13 @@ __global__ void __launch_bounds__(kBlock, 2)
         const int i1 = d0, i2 = swp ? d2 : d1, i3 = swp ? d1 : d2;
         const D3 Q2 = pick4(P, i2), Q3 = pick4(P, i3), Q1 = pick4(P, i1);
         const D3 v1 = own ? ci : co, v2 = own ? co : ci;
-        const D3 s1 = v2 - Q2, s2 = Q3 - Q2, s3 = v1 - Q2;
-        const D3 f1 = 0.5 * cross(s1, s2) + 0.5 * cross(s2, s3);
-        const D3 s4v = v2 - Q3, s5 = Q1 - Q3, s6 = v1 - Q3;
-        const D3 f2 = 0.5 * cross(s4v, s5) + 0.5 * cross(s5, s6);
         const double rair = 1. / dot(N, v2 - v1);
-        // sum_d D_d g_d N_d = ca (V_A - V_C) + cb (V_B - V_D) + cr (V_R - V_L)
+        // sum_d D_d g_d N_d = ca (V_A - V_C) + cb (V_B - V_D) + cr (V_R - V_L), with manapy's
+        // f_1 = (Q3 - Q2) x (v1 - v2) / 2, f_2 = (Q1 - Q3) x (v1 - v2) / 2 folded into triple
+        // products with t = (v1 - v2) x DN
         const D3 DN = d3(p.Dxx * N.x, p.Dyy * N.y, p.Dzz * N.z);
-        const float ca = (float)(dot(DN, f1) * rair), cb = (float)(dot(DN, f2) * rair),
+        const D3 t = cross(v1 - v2, DN);
+        const float ca = (float)(0.5 * dot(Q3 - Q2, t) * rair), cb = (float)(0.5 * dot(Q1 - Q3, t) * rair),
                     cr = (float)(dot(DN, N) * rair);
         const float VA = ld(wn + comp(vt, i1)), VB = ld(wn + comp(vt, i2)), VC = ld(wn + comp(vt, i3));
         const float VL = own ? wi : vo, VR = own ? vo : wi;
