@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--n", "--mesh-n", dest="n", type=int, default=None,
                     help="mesh resolution override (small profiling cases; --mesh-n under torchrun, whose own "
                          "options start with --n)")
+    ap.add_argument("--launch", type=int, default=None,
+                    help="launch-shape variant of the fused phases (0-15; default: tuned per mesh), for "
+                         "profiling one shape")
     ap.add_argument("--min-timed-steps", type=int, default=500,
                     help="repeat the K timed steps until at least this many steps are timed (median reported)")
     ap.add_argument("--no-extras", action="store_true",
@@ -208,7 +211,7 @@ def repeats_for(K, args):
     return max(1, -(-int(args.min_timed_steps) // max(int(K), 1)))
 
 
-def build_advdiff(wl, seed):
+def build_advdiff(wl, seed, launch="auto"):
     import manapy_b200 as M
     el, vx = wl.scaled(seed=seed).mesh()
     dom = M.Domain(dim=wl.dim, mesh=(el, vx))
@@ -222,7 +225,7 @@ def build_advdiff(wl, seed):
         x.interpolate_facetocell()
     w.cell = wl.init(dom.cells.center)
     S = M.AdvectionDiffusionSolver(w, vel=(u, v, wz), conf=M.Struct(
-        Dxx=wl.diffusion[0], Dyy=wl.diffusion[1], Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl))
+        Dxx=wl.diffusion[0], Dyy=wl.diffusion[1], Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl, launch=launch))
     return dom, w, (u, v, wz), S, (uf, vf)
 
 
@@ -416,7 +419,8 @@ def measure_workload(wl, args, world, rank, local, K, fp32c=True, seed_offset=0)
     import torch
     Wm = max(args.warmup, 3)
     if wl.kind == "advdiff":
-        dom, w, vel, S, (uf, vf) = build_advdiff(wl, seed=wl.seed + seed_offset)
+        dom, w, vel, S, (uf, vf) = build_advdiff(wl, seed=wl.seed + seed_offset,
+                                                  launch="auto" if args.launch is None else args.launch)
     else:
         dom, vs, S = build_sw(wl, seed=wl.seed + seed_offset)
     # warm-up: also tunes the steps per graph replay and captures the step graph, so that
