@@ -380,6 +380,18 @@ int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q
                   double cfl, double grav, int32_t order, int32_t walls, double *scratch,
                   double *face_flux, const double *dt_cur, double *dt_next, void *stream);
 
+/* mb_sw_step_ex in two parts, so that the values of cells [0, nfirst) are final before the
+ * rest are computed (a sharded run numbers the cells its peers read first and sends them
+ * while part 1 runs): part 0 computes every face flux (and, for order 2, the gradients) and
+ * updates cells [0, nfirst); part 1 updates cells [nfirst, nbcells) from the face fluxes that
+ * part 0 left in face_flux (both parts with the same arguments, part 1 after part 0 on the
+ * same stream or ordered after it).  Together they compute exactly what mb_sw_step_ex
+ * computes, dt_next included.  Replaces the same step (manapy/solvers/shallowater/
+ * system.py:186-281); the split has no counterpart in manapy. */
+int mb_sw_step_split(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl,
+                     double grav, int32_t order, int32_t walls, double *scratch, double *face_flux,
+                     const double *dt_cur, double *dt_next, int32_t part, int32_t nfirst, void *stream);
+
 /* FP32-compensated twin of mb_sw_step (no counterpart in manapy), first order, Neumann
  * ghosts: FP32 state (q_in, q_out: h, hu, hv, hc, Z), FP32 SRNH flux arithmetic and face
  * fluxes (face_flux [nbfaces][4] floats), residuals summed per cell with compensated
@@ -541,6 +553,22 @@ int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_
  * zeroed by the caller).  The host reads flags after the stream: MB_ENONFINITE /
  * MB_ENEGATIVE. */
 int mb_check_state(const double *f64, const float *f32, int64_t n, int32_t nonneg, int32_t *flags, void *stream);
+
+/* Debug check of a mesh's index tables (no counterpart in manapy, whose Numba kernels do
+ * not check their indices either): every entry of every index table the struct holds is
+ * compared with the range the kernels gather with it, and every CSR / SELL-32 offset table
+ * with being non-decreasing from 0 (SELL group offsets: multiples of 32), one launch per
+ * table, reading nothing outside the tables.  *first (device) receives UINT64_MAX, or the
+ * first bad entry as table << 40 | offsets << 39 | position, the smallest such key.
+ * Tables, in this order (dense tables: position = row * stride + column; CSR / SELL:
+ * position in the index array, or with bit 39 the position in the offsets):
+ *   0 cell_faces [0, nbfaces)   1 cellnid [0, nbcells)   2 ghostnid [0, nbfaces)
+ *   3 face_cellid[.][0] [0, nbcells)   4 face_cellid[.][1] [-1, nbcells) (position counted
+ *   from face_cellid + 1)   5 face_nodeid [0, nbnodes)   6 n2c [0, nbcells)   7 n2g [0, nbfaces)
+ *   8 cell_cellfid [0, nbcells)   9 cell_vtx [0, nbnodes)   10 cell_nbr [-nbfaces, nbcells)
+ *   11 lsq_sell [-1, nbcells)   12 n2c_sell [0, nbcells)
+ * A CSR or SELL table's last offset is taken as the length of its index array. */
+int mb_check_tables(const mb_mesh *m, uint64_t *first, void *stream);
 
 /* Library build information (architecture string), for diagnostics. */
 const char *mb_build_info(void);

@@ -74,6 +74,39 @@ class MbSwItemF64(ctypes.Structure):
 
 WALLS = {"neumann": 0, "reflective": 1}
 
+# mb_check_tables: table ids -> (device table holding the checked values, offsets table or
+# None, first checked column offset, accepted range as a function of (nbcells, nbfaces,
+# nbnodes))
+CHECK_TABLES = (
+    ("cell_faces", None, 0, lambda c, f, n: (0, f)),
+    ("cellnid_idx", "cellnid_ptr", 0, lambda c, f, n: (0, c)),
+    ("ghostnid_idx", "ghostnid_ptr", 0, lambda c, f, n: (0, f)),
+    ("face_cellid", None, 0, lambda c, f, n: (0, c)),
+    ("face_cellid", None, 1, lambda c, f, n: (-1, c)),
+    ("face_nodeid", None, 0, lambda c, f, n: (0, n)),
+    ("n2c_idx", "n2c_ptr", 0, lambda c, f, n: (0, c)),
+    ("n2g_idx", "n2g_ptr", 0, lambda c, f, n: (0, f)),
+    ("cell_cellfid", None, 0, lambda c, f, n: (0, c)),
+    ("cell_vtx", None, 0, lambda c, f, n: (0, n)),
+    ("cell_nbr", None, 0, lambda c, f, n: (-f, c)),
+    ("lsq_sell_idx", "lsq_sell_ptr", 0, lambda c, f, n: (-1, c)),
+    ("n2c_sell_idx", "n2c_sell_ptr", 0, lambda c, f, n: (0, c)),
+)
+
+
+def decode_table_check(key):
+    """mb_check_tables' result -> None (all tables valid) or (table, offsets?, position):
+    the device table name (the offsets table's name when offsets? is true) and the flat
+    position of the first bad entry in it."""
+    key = int(key)
+    if key == 2 ** 64 - 1:
+        return None
+    tid, offs, pos = key >> 40, bool((key >> 39) & 1), key & ((1 << 39) - 1)
+    name, ptr, col, _ = CHECK_TABLES[tid]
+    if offs:
+        return ptr, True, pos
+    return name, False, pos + col
+
 _M = ctypes.POINTER(MbMesh)
 _B = ctypes.POINTER(MbBC)
 _P5 = _vp * 5
@@ -107,6 +140,7 @@ _SIGS = {
     "mb_face_sign": [_M, _vp, _vp, _vp, _vp, _vp],
     "mb_pack_rows": [_M, _vp, _vp, _vp],
     "mb_lsq_matrix": [_M, _vp, _vp],
+    "mb_check_tables": [_M, _vp, _vp],
     "mb_advdiff_step_split": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32,
                               _i32, _vp],
     "mb_advdiff_step_rows": [_M, _B, ctypes.POINTER(MbAdvDiffParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
@@ -122,6 +156,7 @@ _SIGS = {
     "mb_sw_step": [_M, _P5, _P5, _d, _d, _i32, _vp, _vp, _vp, _vp, _vp],
     "mb_sw_dt": [_M, _vp, _vp, _vp, _d, _d, _vp, _vp],
     "mb_sw_step_ex": [_M, _P5, _P5, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp, _vp],
+    "mb_sw_step_split": [_M, _P5, _P5, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp, _i32, _i32, _vp],
     "mb_sw_step_f32c_ex": [_M, _P5, _P5, _P4, _P4, _d, _d, _i32, _i32, _vp, _vp, _vp, _vp],
     "mb_advdiff_batch_step": [_vp, _vp, _i32, _vp, _i32, _i32, _i32, _vp, _vp],
     "mb_sw_batch_step": [_vp, _vp, _i32, _vp, _i32, _vp, _vp],

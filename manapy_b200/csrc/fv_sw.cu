@@ -632,11 +632,11 @@ __device__ __forceinline__ double sw2_cell_body(const mb_mesh &m, const SWState 
 
 __global__ void __launch_bounds__(kBlock, MB_SW_CELL_MIN_BLOCKS) k_sw2_cell(mb_mesh m, SWState s, SWQ out, const double *ff,
                                                      const double *dt_cur, double *dt_next, double cfl,
-                                                     double grav) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                     double grav, int c0, int c1) {
+  const int i = c0 + blockIdx.x * blockDim.x + threadIdx.x;   // cells [c0, c1)
   // every thread of the block reaches the dt reduction below (it synchronises the block)
   double best = 1e300;
-  if (i < m.nbcells) best = sw2_cell_body(m, s, out, ff, dt_cur, dt_next != nullptr, cfl, grav, i);
+  if (i < c1) best = sw2_cell_body(m, s, out, ff, dt_cur, dt_next != nullptr, cfl, grav, i);
   if (dt_next) {
     best = block_min(best);
     if (threadIdx.x == 0 && best < 1e300) atomic_min_pos(dt_next, best);
@@ -919,11 +919,13 @@ int mb_sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_ou
                        stream);
 }
 
-int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
-                  int32_t order, int32_t walls, double *scratch, double *face_flux, const double *dt_cur,
-                  double *dt_next, void *stream) {
-  MB_NVTX();
+// part < 0: the whole step; part 0: the face fluxes and the cells [0, nfirst); part 1: the
+// cells [nfirst, nbcells), reading the face fluxes part 0 left in face_flux
+static int sw_step(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
+                   int32_t order, int32_t walls, double *scratch, double *face_flux, const double *dt_cur,
+                   double *dt_next, int part, int nfirst, void *stream) {
   if (!sw_mesh_ok(m) || !q_in || !q_out || !face_flux || !dt_cur || (order != 1 && order != 2)) return MB_EINVAL;
+  if (part >= 0 && (nfirst < 0 || nfirst > m->nbcells)) return MB_EINVAL;
   if (walls != MB_WALLS_NEUMANN && walls != MB_WALLS_REFLECT) return MB_EINVAL;
   if (!m->cell_cellfid || !m->cell_vtx || !m->cell_nbr || !m->cell_flags || !m->node_coord || !m->cell_xy)
     return MB_EINVAL;
@@ -942,6 +944,13 @@ int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q
 #endif
   cudaStream_t st = ST(stream);
   const int fb = ceil_div(m->nbfaces, MB_SW_FLUX_BLOCK);
+  const int c0 = part == 1 ? nfirst : 0, c1 = part == 0 ? nfirst : m->nbcells;
+  if (part == 1) {
+    if (c1 > c0)
+      k_sw2_cell<<<ceil_div(c1 - c0, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_cur, dt_next, cfl, grav, c0,
+                                                                c1);
+    return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+  }
   if (order == 2) {
     if (!scratch) return MB_EINVAL;
     const long long n = m->nbcells;
@@ -954,8 +963,24 @@ int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q
   } else {
     k_sw2_flux<false, MB_SW_FAST><<<fb, MB_SW_FLUX_BLOCK, 0, st>>>(*m, s, grav, face_flux, dt_next);
   }
-  k_sw2_cell<<<ceil_div(m->nbcells, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_cur, dt_next, cfl, grav);
+  if (c1 > c0)
+    k_sw2_cell<<<ceil_div(c1 - c0, kBlock), kBlock, 0, st>>>(*m, s, out, face_flux, dt_cur, dt_next, cfl, grav, c0, c1);
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
+}
+
+int mb_sw_step_ex(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl, double grav,
+                  int32_t order, int32_t walls, double *scratch, double *face_flux, const double *dt_cur,
+                  double *dt_next, void *stream) {
+  MB_NVTX();
+  return sw_step(m, q_in, q_out, cfl, grav, order, walls, scratch, face_flux, dt_cur, dt_next, -1, 0, stream);
+}
+
+int mb_sw_step_split(const mb_mesh *m, const double *const q_in[5], double *const q_out[5], double cfl,
+                     double grav, int32_t order, int32_t walls, double *scratch, double *face_flux,
+                     const double *dt_cur, double *dt_next, int32_t part, int32_t nfirst, void *stream) {
+  MB_NVTX();
+  if (part != 0 && part != 1) return MB_EINVAL;
+  return sw_step(m, q_in, q_out, cfl, grav, order, walls, scratch, face_flux, dt_cur, dt_next, part, nfirst, stream);
 }
 
 int mb_sw_dt(const mb_mesh *m, const double *h, const double *hu, const double *hv, double cfl, double grav,

@@ -321,6 +321,23 @@ class DeviceMesh:
                 setattr(s, name, self.t[name].data_ptr())
         return s
 
+    def check_tables(self, stream=None):
+        """Debug check of every index table on the device (``mb_check_tables``): raises
+        ValueError naming the first entry outside the range the kernels gather with."""
+        first = torch.empty(1, dtype=torch.int64, device=self.device)
+        st = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        _lib.call("mb_check_tables", self.struct, first.data_ptr(), st)
+        torch.cuda.synchronize(self.device)
+        bad = _lib.decode_table_check(int(first.item()) & (2 ** 64 - 1))
+        if bad is None:
+            return
+        name, offs, pos = bad
+        value = int(self.t[name].reshape(-1)[pos].item())
+        tid = [t[1] if offs else t[0] for t in _lib.CHECK_TABLES].index(name)
+        lo, hi = _lib.CHECK_TABLES[tid][3](self.nbcells, self.nbfaces, self.nbnodes)
+        what = "is out of order" if offs else "is outside [%d, %d)" % (lo, hi)
+        raise ValueError("mesh table %s: entry %d = %d %s" % (name, pos, value, what))
+
     def ensure_lsq_matrix(self, stream=None):
         """Tetrahedra with compact tables: the ``cell_lsq`` table (the least-squares moment
         matrix of every cell, ``mb_lsq_matrix``), formed once on the device and pointed at by

@@ -79,6 +79,8 @@ class Domain:
         ("mesh_cache", "str", None, None, "directory of the persistent mesh cache (geometry and device tables "
                                            "stored once per mesh; also MANAPY_B200_MESH_CACHE); no counterpart "
                                            "in manapy"),
+        ("check_tables", "bool", False, False, "check every index table of the mesh on the device once, when "
+                                                "it is first used (mb_check_tables); no counterpart in manapy"),
         ("stencil", "str", "shared", None, "layout of the least-squares stencil: 'shared' (neighbours shared by "
                                            "the cells of one warp read in one slot; fastest) or 'manapy' (each "
                                            "cell's neighbours in manapy's order, so results do not depend on the "
@@ -107,6 +109,7 @@ class Domain:
         self.signature = get("signature")
         self.device = get("device")
         self.stencil = get("stencil")
+        self.check_tables = bool(get("check_tables"))
         from .device import STENCILS
         if self.stencil not in STENCILS:
             raise ValueError("stencil must be one of %s" % (STENCILS,))
@@ -201,6 +204,8 @@ class Domain:
             else:
                 from .device import DeviceMesh
                 self._dmesh = DeviceMesh(self._A, self.device, stencil=self.stencil)
+            if self.check_tables:
+                self._dmesh.check_tables()
         return self._dmesh
 
     @property

@@ -8,9 +8,10 @@ ranks of each rank's CFL dt (``manapy/solvers/advecdiff/system.py:152`` and
 ``manapy/solvers/shallowater/system.py:188``: manapy's ``allreduce(MIN)``).  The owned
 cells' results are bit-identical to the single-GPU run of the whole mesh.
 
-Advection-diffusion overlaps the exchange with the step: each shard numbers the cells its
-peers read first, computes them (``mb_advdiff_step_split`` part 0), posts the exchange, and
-computes the other cells (part 1) while the messages travel; the halo is written after both.
+Both solvers overlap the exchange with the step: each shard numbers the cells its peers
+read first, computes them (``mb_advdiff_step_split`` / ``mb_sw_step_split`` part 0), posts
+the exchange, and computes the other cells (part 1) while the messages travel; the halo is
+written after both.
 
 Before each step every rank checks the run's failure record (``partition.FailureMonitor``):
 a rank that failed between steps has posted it, and the others raise ``RankFailure``
@@ -194,10 +195,11 @@ class ShardedShallowWater(_Sharded):
     formula, min over ranks; the fused step; the exchange of h, hu, hv, hc."""
 
     def __init__(self, elements, vertex, cfl=0.8, grav=9.81, walls="neumann", group=None, device=None, store=None,
-                 sync_every=0, check_every=1, A=None):
+                 sync_every=0, check_every=1, A=None, overlap=True):
         # every shard holds the mesh's last cell: the source term reads it for cellfid padding
         super().__init__(elements, vertex, 2, group, device, store, extra_cells=[len(elements) - 1],
-                         sync_every=sync_every, check_every=check_every, A=A)
+                         sync_every=sync_every, check_every=check_every, A=A, send_first=overlap)
+        self.overlap = bool(overlap)
         if walls not in _lib.WALLS:
             raise ValueError("walls must be 'neumann' or 'reflective'")
         self.walls = _lib.WALLS[walls]
@@ -224,11 +226,19 @@ class ShardedShallowWater(_Sharded):
             _lib.call("mb_sw_dt", self.dm.struct, _p(qi[0]), _p(qi[1]), _p(qi[2]), self.cfl, self.grav, _p(self.dt),
                       st)
             self._all_min(self.dt)
-            _lib.call("mb_sw_step_ex", self.dm.struct, _lib.p5([_p(t) for t in qi] + [_p(self.Z)]),
-                      _lib.p5([_p(t) for t in qo] + [_p(self.Z)]), self.cfl, self.grav, 1, self.walls, None,
-                      _p(self.ff), _p(self.dt), None, st)
+            args = (self.dm.struct, _lib.p5([_p(t) for t in qi] + [_p(self.Z)]),
+                    _lib.p5([_p(t) for t in qo] + [_p(self.Z)]), self.cfl, self.grav, 1, self.walls, None,
+                    _p(self.ff), _p(self.dt), None)
+            if self.overlap:
+                # the cells peers read, the exchange posted, the other cells while it travels
+                _lib.call("mb_sw_step_split", *args, 0, self.dm.nfirst, st)
+                pending = self.exchanger.start(qo)
+                _lib.call("mb_sw_step_split", *args, 1, self.dm.nfirst, st)
+                self.exchanger.finish(pending)
+            else:
+                _lib.call("mb_sw_step_ex", *args, st)
+                self.exchanger.exchange(qo)
             self.cur = 1 - self.cur
-            self.exchanger.exchange(self.q[self.cur])
 
     def gather(self):
         """[h, hu, hv] whole-mesh cell arrays on every rank (manapy numbering)."""

@@ -76,3 +76,13 @@ def test_entry_points_reject_null_arguments():
                 args.append(None)
         rc = getattr(L, name)(*args)
         assert rc == (_lib.MB_OK if name == "mb_srnh_flux" else _lib.MB_EINVAL), (name, rc)
+
+
+def test_table_check_keys_decode():
+    from manapy_b200 import _lib
+    assert _lib.decode_table_check(2 ** 64 - 1) is None
+    assert _lib.decode_table_check((11 << 40) | 5) == ("lsq_sell_idx", False, 5)
+    assert _lib.decode_table_check((1 << 40) | (1 << 39) | 9) == ("cellnid_ptr", True, 9)
+    # face_cellid's second column is checked from face_cellid + 1
+    assert _lib.decode_table_check((4 << 40) | 22) == ("face_cellid", False, 23)
+    assert len(_lib.CHECK_TABLES) == 13

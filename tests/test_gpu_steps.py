@@ -470,3 +470,40 @@ def test_split_step_equals_the_whole_step(wl, cuda):
     L = _lib.lib()
     assert L.mb_advdiff_step_split(*args, 2, dm.nfirst, st) == _lib.MB_EINVAL
     assert L.mb_advdiff_step_split(*args, 0, nc + 1, st) == _lib.MB_EINVAL
+
+
+@pytest.mark.parametrize("walls", ["neumann", "reflective"])
+def test_split_shallow_water_step_equals_the_whole_step(walls, cuda):
+    """mb_sw_step_split part 0 (every face flux, cells [0, nfirst)) then part 1 (the other
+    cells) computes exactly mb_sw_step_ex's new state and next dt."""
+    import gpuutil as U
+    import torch
+    from manapy_b200 import _lib
+    from manapy_b200.device import DeviceMesh
+    wl = W.C3.scaled(n=30)
+    el, vx = wl.mesh()
+    A = G.build(el, vx, 2)
+    nc, nf = A["nbcells"], A["nbfaces"]
+    first = np.random.default_rng(7).random(nc) < 0.25
+    dm = DeviceMesh(A, "cuda", first_cells=first)
+    R = dm.R
+    st = U.stream()
+    q = [U.T(a[R.cperm]) for a in wl.init_sw(A["cells_center"])]      # h, hu, hv, hc, Z
+    dt = U.Z(1)
+    U.call("mb_sw_dt", dm.struct, U.P(q[0]), U.P(q[1]), U.P(q[2]), wl.cfl, wl.grav, U.P(dt), st)
+    ff = torch.empty(4 * nf, dtype=torch.float64, device="cuda")
+    outs = []
+    for split in (False, True):
+        qo = [U.Z(nc) for _ in range(4)] + [q[4]]
+        dn = U.Z(1)
+        args = (dm.struct, _lib.p5([U.P(t) for t in q]), _lib.p5([U.P(t) for t in qo]), wl.cfl, wl.grav, 1,
+                _lib.WALLS[walls], None, U.P(ff), U.P(dt), U.P(dn))
+        if split:
+            U.call("mb_sw_step_split", *args, 0, dm.nfirst, st)
+            U.call("mb_sw_step_split", *args, 1, dm.nfirst, st)
+        else:
+            U.call("mb_sw_step_ex", *args, st)
+        outs.append([U.H(t) for t in qo[:4]] + [U.H(dn)])
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    assert _lib.lib().mb_sw_step_split(*args, 2, dm.nfirst, st) == _lib.MB_EINVAL
