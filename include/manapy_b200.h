@@ -125,6 +125,20 @@ typedef struct mb_mesh {
    * it instead of forming it every step.  Must come from the lsq_sell table of this
    * struct.  Triangles: NULL (their step forms the matrix; reading it measured slower). */
   const double *cell_lsq;
+  /* tetrahedra, optional: the edges of the mesh, with which the second-order step forms each
+   * cell's least-squares right-hand side from node, edge and face-neighbour sums instead of
+   * gathering its whole stencil (needs cell_lsq; see mb_advdiff_step):
+   *   cell_edges [nbcells][8] the edge of local vertex pair (0,1), (0,2), (0,3), (1,2), (1,3),
+   *              (2,3), then -1, -1;
+   *   edge_origin [nbedges] the edge's vertex with the smaller index (the origin of its sums);
+   *   edge_sell_ptr / edge_sell_idx: the cells of each edge, SELL-32 as lsq_sell (-1 in
+   *              empty slots). */
+  const int32_t *cell_edges;
+  const int32_t *edge_origin;
+  const int32_t *edge_sell_ptr;
+  const int32_t *edge_sell_idx;
+  int32_t nbedges;
+  int32_t pad_;
 } mb_mesh;
 
 typedef struct mb_bc {

@@ -36,7 +36,9 @@ class MbMesh(ctypes.Structure):
                 ("cell_cellfid", _vp), ("cell_nf", _vp), ("cell_vertex1", _vp),
                 ("cell_vtx", _vp), ("cell_nbr", _vp), ("cell_flags", _vp), ("node_coord", _vp), ("cell_xy", _vp),
                 ("lsq_sell_ptr", _vp), ("lsq_sell_idx", _vp), ("n2c_sell_ptr", _vp), ("n2c_sell_idx", _vp),
-                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp), ("cell_lsq", _vp)]
+                ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp), ("cell_lsq", _vp),
+                ("cell_edges", _vp), ("edge_origin", _vp), ("edge_sell_ptr", _vp), ("edge_sell_idx", _vp),
+                ("nbedges", _i32), ("pad_", _i32)]
 
 
 class MbBC(ctypes.Structure):

@@ -914,8 +914,8 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
     double gx, gy, gz;
     if (PRE) {
       double a, b, cc, d, e, ff, dia, pad;
-      ld4d(m.cell_lsq + 8 * (long long)i, a, b, cc, d);
-      ld4d(m.cell_lsq + 8 * (long long)i + 4, e, ff, dia, pad);
+      ld4d(m.cell_lsq + 12 * (long long)i, a, b, cc, d);
+      ld4d(m.cell_lsq + 12 * (long long)i + 4, e, ff, dia, pad);
       gx = (a * jx + b * jy + cc * jz) / dia;
       gy = (b * jx + d * jy + e * jz) / dia;
       gz = (cc * jx + e * jy + ff * jz) / dia;
@@ -982,10 +982,14 @@ __global__ void __launch_bounds__(kBlock) k_lsq_matrix3(mb_mesh m, double *__res
     ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
     ixy += (dx * dy); ixz += (dx * dz); iyz += (dy * dz);
   };
+  // D = sum over the cell stencil (ghosts excluded) of the centre offsets
+  double sx = 0., sy = 0., sz = 0.;
   const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
   for (int k = 0; k < (se - sb) >> 5; ++k) {
     const int cc = ld(m.lsq_sell_idx + sb + lane + 32 * k);
-    acc(cc < 0 ? c : ld3(m.cell_xy + 4 * (long long)cc));
+    const D3 pc = cc < 0 ? c : ld3(m.cell_xy + 4 * (long long)cc);
+    acc(pc);
+    sx += pc.x - c.x; sy += pc.y - c.y; sz += pc.z - c.z;
   }
   const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
   for (int k = gb; k < ge; ++k) {
@@ -993,9 +997,164 @@ __global__ void __launch_bounds__(kBlock) k_lsq_matrix3(mb_mesh m, double *__res
     acc(d3(ld(gc), ld(gc + 1), ld(gc + 2)));
   }
   const double dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) - izz * (ixy * ixy);
-  double *o = out + 8 * (long long)i;
+  double *o = out + 12 * (long long)i;
   st4d_plain(o, iyy * izz - iyz * iyz, ixz * iyz - ixy * izz, ixy * iyz - ixz * iyy, ixx * izz - ixz * ixz);
   st4d_plain(o + 4, ixy * ixz - iyz * ixx, ixx * iyy - ixy * ixy, dia, 0.0);
+  st4d_plain(o + 8, sx, sy, sz, 0.0);
+}
+
+// ---------------------------------------------------------------- tetrahedra: LSQ sums by inclusion-exclusion
+//
+// The stencil of tetrahedron i (manapy's cells.cellnid: the cells that share a vertex with i,
+// i excluded) is the union of its four vertices' cell lists.  Two of the lists meet in the
+// cells of an edge, three in the cells of a face (i and its face neighbour), four in i alone,
+// so by inclusion-exclusion, for any f,
+//   sum_stencil f = sum_4 vertices F_v - sum_6 edges F_e + sum_face neighbours f(o),
+// f(i) appearing 4 - 6 + 4 - 1 - 1 = 0 times.  With sums kept relative to an origin x of each
+// vertex or edge, F = P + (x - c_i) Q, P = sum_j (c_j - x) w_j, Q = sum_j w_j, and the
+// right-hand side of manapy's gradient (manapy/ast/functions3d.py:4-120) is
+//   sum_stencil (c_j - c_i)(w_j - w_i) = sum_stencil (c_j - c_i) w_j - w_i D_i
+// with D_i = sum_stencil (c_j - c_i) (cell_lsq), then the stencil ghosts as before.  It
+// equals the direct sum up to rounding; a cell gathers 4 vertex and 6 edge records and its
+// face neighbours instead of about 60 neighbours, and each cell's row is read by its 4
+// vertices' and 6 edges' sums.
+
+// vertex blocks [0, nnb): the vertex's sums and (DIFF) its centre->vertex value; edge blocks:
+// the edge's sums.  Records {P, Q} (32 bytes).
+template <bool DIFF>
+__global__ void __launch_bounds__(kBlock) k_f3_sums(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+                                                    const double *__restrict__ rows, double *__restrict__ nrec,
+                                                    double *__restrict__ erec, double *__restrict__ wn, int nnb) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t pst = l2_stream();
+  double px = 0., py = 0., pz = 0., q = 0.;
+  if ((int)blockIdx.x < nnb) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.nbnodes) return;
+    const D3 X = ld3(m.node_coord + 4 * (long long)n);
+    const int len = ld(m.n2c_ptr + n + 1) - ld(m.n2c_ptr + n);
+    const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
+    double acc = 0.;
+    for (int k = 0; sb + lane + 32 * k < se; ++k) {
+      const int e = sb + lane + 32 * k;
+      // entries past the row's length repeat its first cell with weight 0
+      const int cc = ld1_stream(m.n2c_sell_idx + e, pst);
+      double x, y, z, wc;
+      ld_row(rows + 4 * (long long)cc, x, y, z, wc);
+      if (DIFF) acc += ldd_stream(m.n2c_sell_alpha + e, pst) * wc;
+      if (k < len) {
+        px += (x - X.x) * wc; py += (y - X.y) * wc; pz += (z - X.z) * wc;
+        q += wc;
+      }
+    }
+    if (DIFF) {
+      const GhostRule ghost = make_rule(m, bc, w);
+      const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
+      for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * ghost(ld(m.n2g_idx + k));
+      wn[n] = acc;
+    }
+    st4_keep(nrec + 4 * (long long)n, px, py, pz, q, l2_keep());
+    return;
+  }
+  const int e = (blockIdx.x - nnb) * blockDim.x + threadIdx.x;
+  if (e >= m.nbedges) return;
+  const D3 X = ld3(m.node_coord + 4 * (long long)ld(m.edge_origin + e));
+  const int sb = ld(m.edge_sell_ptr + (e >> 5)), se = ld(m.edge_sell_ptr + (e >> 5) + 1);
+  for (int k = sb + lane; k < se; k += 32) {
+    const int cc = ld1_stream(m.edge_sell_idx + k, pst);
+    if (cc < 0) continue;
+    double x, y, z, wc;
+    ld_row(rows + 4 * (long long)cc, x, y, z, wc);
+    px += (x - X.x) * wc; py += (y - X.y) * wc; pz += (z - X.z) * wc;
+    q += wc;
+  }
+  st4_keep(erec + 4 * (long long)e, px, py, pz, q, l2_keep());
+}
+
+// cell pass: the gradient from the vertex, edge and face-neighbour sums, the Barth limiter;
+// the same record as k_f3_phase1
+template <int VAR>
+__global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_grad(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+                                                                    double *__restrict__ rec,
+                                                                    const double *__restrict__ rows,
+                                                                    const double *__restrict__ nrec,
+                                                                    const double *__restrict__ erec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRule ghost = make_rule(m, bc, w);
+  D3 c;
+  double wi;
+  ld_row(rows + 4 * (long long)i, c.x, c.y, c.z, wi);
+  const int4 vt = ld4(m.cell_vtx + 4 * i);
+  const int4 nb = ld4(m.cell_nbr + 4 * i);
+  const int4 ea = ld4(m.cell_edges + 8 * (long long)i), eb = ld4(m.cell_edges + 8 * (long long)i + 4);
+  const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
+                   ld3(m.node_coord + 4 * vt.w)};
+  double sx = 0., sy = 0., sz = 0.;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double px, py, pz, q;
+    ld4d(nrec + 4 * (long long)comp(vt, v), px, py, pz, q);
+    const D3 d = P[v] - c;
+    sx += px + d.x * q; sy += py + d.y * q; sz += pz + d.z * q;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    // local vertex pairs (0,1), (0,2), (0,3), (1,2), (1,3), (2,3); origin: the vertex of smaller index
+    const int a = k < 3 ? 0 : (k < 5 ? 1 : 2), b = k < 3 ? k + 1 : (k < 5 ? k - 1 : 3);
+    const int e = k == 0 ? ea.x : (k == 1 ? ea.y : (k == 2 ? ea.z : (k == 3 ? ea.w : (k == 4 ? eb.x : eb.y))));
+    double px, py, pz, q;
+    ld4d(erec + 4 * (long long)e, px, py, pz, q);
+    const D3 d = (comp(vt, a) < comp(vt, b) ? P[a] : P[b]) - c;
+    sx -= px + d.x * q; sy -= py + d.y * q; sz -= pz + d.z * q;
+  }
+  double wmax = wi, wmin = wi;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int o = comp(nb, j);
+    double b;
+    if (o >= 0) {
+      double x, y, z;
+      ld_row(rows + 4 * (long long)o, x, y, z, b);
+      sx += (x - c.x) * b; sy += (y - c.y) * b; sz += (z - c.z) * b;
+    } else {
+      b = ghost(-1 - o);
+    }
+    wmax = pmax(wmax, b);
+    wmin = pmin(wmin, b);
+  }
+  double a0, a1, a2, a3, a4, a5, dia, pad, Dx, Dy, Dz;
+  ld4d(m.cell_lsq + 12 * (long long)i, a0, a1, a2, a3);
+  ld4d(m.cell_lsq + 12 * (long long)i + 4, a4, a5, dia, pad);
+  ld4d(m.cell_lsq + 12 * (long long)i + 8, Dx, Dy, Dz, pad);
+  double jx = sx - wi * Dx, jy = sy - wi * Dy, jz = sz - wi * Dz;
+  const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+  for (int k = gb; k < ge; ++k) {
+    const int f = ld(m.ghostnid_idx + k);
+    const double *gc = m.face_ghostcenter + 3 * f;
+    const double dw = ghost(f) - wi;
+    jx += (ld(gc) - c.x) * dw; jy += (ld(gc + 1) - c.y) * dw; jz += (ld(gc + 2) - c.z) * dw;
+  }
+  const double gx = (a0 * jx + a1 * jy + a2 * jz) / dia;
+  const double gy = (a1 * jx + a3 * jy + a4 * jz) / dia;
+  const double gz = (a2 * jx + a4 * jy + a5 * jz) / dia;
+  // Barth limiter over the four faces (as k_f3_phase1)
+  const uint32_t fl = ld(m.cell_flags + i);
+  double ps = 1.;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    int d0, d1, d2;
+    face_desc(fl, j, d0, d1, d2);
+    const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
+    const double delta = gx * (fc.x - c.x) + gy * (fc.y - c.y) + gz * (fc.z - c.z);
+    double psi_ij = 1.;
+    if (!(fabs(delta) < 1e-10)) {
+      if (delta > 0.) psi_ij = pmin(1., (wmax - wi) / delta);
+      if (delta < 0.) psi_ij = pmin(1., (wmin - wi) / delta);
+    }
+    ps = pmin(ps, psi_ij);
+  }
+  st4_keep(rec + 4 * (long long)i, wi, ps * gx, ps * gy, ps * gz, l2_keep());
 }
 
 // manapy's dissipative flux of one tetrahedron face, D (grad w . N) with the diamond
@@ -1213,6 +1372,28 @@ inline void f3_p1_run(const mb_mesh &m, const mb_bc &bc, const double *w, double
   else
     k_f3_phase1<O2, DF, V, false><<<ncb + nnb, B, 0, st>>>(m, bc, w, cs, rows, wn, ncb);
 }
+// the first phase by inclusion-exclusion: vertex and edge sums (and node values), then the
+// cells; records of the sums after the cell records and rows in the cell scratch
+inline bool f3_sums_tables(const mb_mesh &m) {
+  return m.cell_edges && m.edge_origin && m.edge_sell_ptr && m.edge_sell_idx && m.nbedges > 0 && m.cell_lsq &&
+         m.n2c_ptr && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
+}
+template <bool DF, int V>
+inline void f3_sums_run(const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows,
+                        double *wn, cudaStream_t st) {
+  double *nrec = cs + 8 * (long long)m.nbcells, *erec = nrec + 4 * (long long)m.nbnodes;
+  const int nnb = ceil_div(m.nbnodes, kBlock), neb = ceil_div(m.nbedges, kBlock);
+  k_f3_sums<DF><<<nnb + neb, kBlock, 0, st>>>(m, bc, w, rows, nrec, erec, wn, nnb);
+  k_f3_grad<V><<<ceil_div(m.nbcells, kQ1B[V]), kQ1B[V], 0, st>>>(m, bc, w, cs, rows, nrec, erec);
+}
+template <bool DF>
+inline void f3_sums_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows,
+                         double *wn, cudaStream_t st) {
+  if (v == 1) return f3_sums_run<DF, 1>(m, bc, w, cs, rows, wn, st);
+  if (v == 2) return f3_sums_run<DF, 2>(m, bc, w, cs, rows, wn, st);
+  if (v == 3) return f3_sums_run<DF, 3>(m, bc, w, cs, rows, wn, st);
+  f3_sums_run<DF, 0>(m, bc, w, cs, rows, wn, st);
+}
 template <bool O2, bool DF>
 inline void f3_p1_pick(int v, const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows,
                        double *wn, cudaStream_t st) {
@@ -1286,7 +1467,11 @@ int launch_step(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params &p, c
         k_pack_rows<3><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, w_in, pk);
         rows = pk;
       }
-      if ((O2 || DF) && p1) f3_p1_pick<O2, DF>(v1, m, bc, w_in, cs, rows, wn, st);
+      if (O2 && p1 && f3_sums_tables(m)) {
+        f3_sums_pick<DF>((m.variant & 3), m, bc, w_in, cs, rows, wn, st);
+      } else if ((O2 || DF) && p1) {
+        f3_p1_pick<O2, DF>(v1, m, bc, w_in, cs, rows, wn, st);
+      }
       if (rows_out) f3_p2_pick<O2, DF, true>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, rows_out, c0, c1, st);
       else f3_p2_pick<O2, DF, false>(v2, m, bc, p, w_in, w_out, sign, src, dt, cs, wn, nullptr, c0, c1, st);
     }
@@ -1608,6 +1793,9 @@ extern "C" int mb_advdiff_step_noalloc(const mb_mesh *m, const mb_bc *bc, const 
     base = g_noalloc_base[dev];
   }
   // Every slice is written by the first launch of the step before the second
-  // launch reads it, so nothing has to be cleared between calls.
-  return mb_advdiff_step(m, bc, p, w_in, w_out, sign_cf, src, dt_dev, base, base + cell_need, stream);
+  // launch reads it, so nothing has to be cleared between calls.  The scratch holds the
+  // step without the edge sums (their records need more), so their tables are left out.
+  mb_mesh mm = *m;
+  mm.cell_edges = nullptr;
+  return mb_advdiff_step(&mm, bc, p, w_in, w_out, sign_cf, src, dt_dev, base, base + cell_need, stream);
 }

@@ -271,6 +271,7 @@ class DeviceMesh:
         self.R = R
         self.reordered = bool(R.enabled)
         self.stencil = str(T.pop("stencil", np.array("manapy")))
+        self.nbedges = len(T["edge_origin"]) if "edge_origin" in T else 0
         dev = torch.device(device) if device is not None else None
         self.device = dev
         self.t = {k: _t(v, v.dtype, dev) for k, v in T.items()}
@@ -317,9 +318,33 @@ class DeviceMesh:
                                                          self.nlf)
         s.variant = int(getattr(self, "variant", 0))
         for name, _ in _lib.MbMesh._fields_:
-            if name in self.t:
+            if name in self.t and name not in self.EDGE_TABLES:
                 setattr(s, name, self.t[name].data_ptr())
         return s
+
+    # the edge tables change the scratch a second-order 3D step needs, so a struct carries
+    # them only once its user asks (use_edge_sums)
+    EDGE_TABLES = ("cell_edges", "edge_origin", "edge_sell_ptr", "edge_sell_idx")
+
+    def use_edge_sums(self):
+        """Tetrahedra: point the struct at the edge tables, so that the second-order step
+        forms the least-squares sums by inclusion-exclusion (it then needs ``cell_lsq`` and
+        ``cell_scratch_size()`` doubles of cell scratch).  Returns False where the tables are
+        absent."""
+        if self.dim != 3 or "cell_edges" not in self.t or self.device is None:
+            return False
+        for name in self.EDGE_TABLES:
+            setattr(self.struct, name, self.t[name].data_ptr())
+        self.struct.nbedges = int(self.nbedges)
+        return True
+
+    def cell_scratch_size(self):
+        """Doubles of cell scratch a fused step needs with this struct: 4 nbcells (2D), 8 nbcells
+        (3D), plus 4 (nbnodes + nbedges) when the edge sums are in use."""
+        if self.dim == 2:
+            return 4 * self.nbcells
+        extra = 4 * (self.nbnodes + int(self.nbedges)) if self.struct is not None and self.struct.cell_edges else 0
+        return 8 * self.nbcells + extra
 
     def check_tables(self, stream=None):
         """Debug check of every index table on the device (``mb_check_tables``): raises
@@ -345,7 +370,7 @@ class DeviceMesh:
         step.  No-op for triangles, host-built tables, or when it is there already."""
         if self.dim != 3 or self.device is None or "cell_lsq" in self.t or "lsq_sell_idx" not in self.t:
             return
-        out = torch.empty(8 * self.nbcells, dtype=torch.float64, device=self.device)
+        out = torch.empty(12 * self.nbcells, dtype=torch.float64, device=self.device)
         st = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
         _lib.call("mb_lsq_matrix", self.struct, out.data_ptr(), st)
         self.t["cell_lsq"] = out
@@ -491,6 +516,39 @@ class DeviceMesh:
         cc4 = np.zeros((nc, 4))
         cc4[:, :3] = A["cells_center"][cp]
         T["cell_xy"] = _t(cc4, np.float64, dev)
+        self._edge_tables(ni[nodes], T, dev)
+
+    # the six edges of a tetrahedron as pairs of local vertices
+    TET_EDGES = np.array([[0, 1], [0, 2], [0, 3], [1, 2], [1, 3], [2, 3]])
+
+    def _edge_tables(self, vt, T, dev):
+        """Edges of a tetrahedral mesh for the least-squares sums by inclusion-exclusion:
+        ``cell_edges`` [nc][8] (the edge of each local vertex pair in TET_EDGES order, then
+        -1, -1), ``edge_origin`` [ne] (the edge's vertex of smaller device number, the origin
+        of its sums), ``edge_sell_ptr`` / ``edge_sell_idx`` (edge -> cells, SELL-32,
+        slot-shared, -1 in empty slots).  Edges are numbered by their first cell."""
+        nc, nn = len(vt), self.nbnodes
+        ends = np.sort(vt[:, self.TET_EDGES], axis=2).reshape(-1, 2).astype(np.int64)   # [nc*6, 2]
+        key = ends[:, 0] * nn + ends[:, 1]
+        uk, first, inv = np.unique(key, return_index=True, return_inverse=True)
+        # number edges by their first cell (the device cell numbering keeps locality)
+        order = np.argsort(first // 6, kind="stable")
+        rank = np.empty(len(uk), dtype=np.int64)
+        rank[order] = np.arange(len(uk))
+        eid = rank[inv].reshape(nc, 6)
+        ce = np.full((nc, 8), -1, dtype=np.int32)
+        ce[:, :6] = eid
+        T["cell_edges"] = _t(ce, np.int32, dev)
+        T["edge_origin"] = _t((uk[order] // nn).astype(np.int32), np.int32, dev)
+        cells = np.repeat(np.arange(nc, dtype=np.int64), 6)
+        flat = eid.reshape(-1)
+        srt = np.argsort(flat, kind="stable")
+        ptr = np.zeros(len(uk) + 1, dtype=np.int64)
+        np.cumsum(np.bincount(flat, minlength=len(uk)), out=ptr[1:])
+        gp, gi = lsq_sell(ptr, cells[srt].astype(np.int32), "shared")
+        T["edge_sell_ptr"] = _t(gp, np.int32, dev)
+        T["edge_sell_idx"] = _t(gi, np.int32, dev)
+        self.nbedges = len(uk)
 
     @classmethod
     def _perm_codes(cls, order):

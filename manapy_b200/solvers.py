@@ -67,7 +67,10 @@ class AdvectionDiffusionSolver:
                                                       "even number, or 'auto' (measured by manapy_b200.autotune)"),
                    ("launch", object, "auto", 0, "launch shapes of the fused phases: 'auto' (measured by "
                                                  "manapy_b200.autotune at the first graph advance), or a variant "
-                                                 "number (bits 0-1 first phase, 2-3 second; 0 = defaults)")]
+                                                 "number (bits 0-1 first phase, 2-3 second; 0 = defaults)"),
+                   ("lsq_sums", bool, True, 0, "tetrahedra, second order: least-squares sums by inclusion-"
+                                               "exclusion over vertex and edge sums instead of gathering each "
+                                               "cell's stencil (equal up to rounding; no counterpart in manapy)")]
 
     @classmethod
     def process_conf(cls, conf, kwargs):
@@ -116,6 +119,7 @@ class AdvectionDiffusionSolver:
             raise ValueError("launch must be 'auto' or a variant number 0-15")
         self.launch = launch if launch == "auto" else int(launch)
         self.launch_variant = 0 if launch == "auto" else int(launch)
+        self.lsq_sums = bool(get("lsq_sums"))
         self.diffusion = not (self.Dxx == self.Dyy == self.Dzz == 0)
         self.backend = self.domain.backend
         self.signature = self.domain.signature
@@ -145,6 +149,8 @@ class AdvectionDiffusionSolver:
             self._dm = self.domain.device_mesh
             if self.order == 2:
                 self._dm.ensure_lsq_matrix(self._stream())
+                if self.lsq_sums:
+                    self._dm.use_edge_sums()
             if self.launch != "auto":
                 self._dm.struct.variant = int(self.launch)
             dev = self._dm.device
@@ -280,8 +286,9 @@ class AdvectionDiffusionSolver:
     def _scratch(self):
         dm = self._dm
         if getattr(self, "_cs", None) is None:
-            # 4 nbcells (2D: records) or 8 nbcells (3D: records, rows)
-            self._cs = torch.empty((4 if dm.dim == 2 else 8) * dm.nbcells, dtype=torch.float64, device=dm.device)
+            # 4 nbcells (2D: records) or 8 nbcells (3D: records, rows), plus the vertex and edge
+            # records when the 3D step uses the edge sums
+            self._cs = torch.empty(dm.cell_scratch_size(), dtype=torch.float64, device=dm.device)
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
 

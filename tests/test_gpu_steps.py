@@ -377,17 +377,19 @@ def test_precomputed_moment_matrix(cuda):
     R = dm.R
     nc, nn = A["nbcells"], A["nbnodes"]
     st = U.stream()
-    lsq = U.Z(8 * nc)
+    lsq = U.Z(12 * nc)
     U.call("mb_lsq_matrix", dm.struct, U.P(lsq), st)
-    got = U.H(lsq).reshape(nc, 8)[R.cinv]          # manapy numbering
+    got = U.H(lsq).reshape(nc, 12)[R.cinv]         # manapy numbering
     c = A["cells_center"][:, :3]
     ptr, idx = A["cellnid_ptr"], A["cellnid_idx"]
     gptr, gidx = A["ghostnid_ptr"], A["ghostnid_idx"]
     M_ = np.zeros((nc, 3, 3))
+    D_ = np.zeros((nc, 3))
     for i in range(nc):
         pts = np.concatenate([c[idx[ptr[i]:ptr[i + 1]]], A["faces_ghostcenter"][gidx[gptr[i]:gptr[i + 1]], :3]])
         d = pts - c[i]
         M_[i] = d.T @ d
+        D_[i] = (c[idx[ptr[i]:ptr[i + 1]]] - c[i]).sum(axis=0)
     det = np.linalg.det(M_)
     cof = np.stack([M_[:, 1, 1] * M_[:, 2, 2] - M_[:, 1, 2] ** 2, M_[:, 0, 2] * M_[:, 1, 2] - M_[:, 0, 1] * M_[:, 2, 2],
                     M_[:, 0, 1] * M_[:, 1, 2] - M_[:, 0, 2] * M_[:, 1, 1], M_[:, 0, 0] * M_[:, 2, 2] - M_[:, 0, 2] ** 2,
@@ -395,7 +397,8 @@ def test_precomputed_moment_matrix(cuda):
                    axis=1)
     assert rel_max(got[:, :6], cof) < 1e-12
     assert rel_max(got[:, 6], det) < 1e-12
-    assert np.all(got[:, 7] == 0)
+    assert np.all(got[:, 7] == 0) and np.all(got[:, 11] == 0)
+    assert np.abs(got[:, 8:11] - D_).max() < 1e-12 * np.abs(c).max()
     # the step with and without the table
     uf, vf, wf = wl.velocity(A["faces_center"])
     sign = U.Z(4 * nc)
@@ -507,3 +510,46 @@ def test_split_shallow_water_step_equals_the_whole_step(walls, cuda):
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
     assert _lib.lib().mb_sw_step_split(*args, 2, dm.nfirst, st) == _lib.MB_EINVAL
+
+
+@pytest.mark.parametrize("order", [2])
+def test_edge_sums_step_equals_the_stencil_step(order, cuda):
+    """Tetrahedra: the second-order step with the least-squares sums by inclusion-exclusion
+    (vertex, edge and face-neighbour sums; the struct's edge tables) gives the step that
+    gathers every stencil neighbour, to rounding, over several steps."""
+    import gpuutil as U
+    from manapy_b200 import _lib
+    wl = W.C4.scaled(n=8)
+    el, vx = wl.mesh()
+    A = G.build(el, vx, 3)
+    dm = U.mesh(A, reorder=True)
+    db = U.bc(A, B.resolve(A, wl.bc, wl.bc_values), dm)
+    R = dm.R
+    nc, nn = A["nbcells"], A["nbnodes"]
+    st = U.stream()
+    dm.ensure_lsq_matrix(st)
+    uf, vf, wf = wl.velocity(A["faces_center"])
+    sign = U.Z(4 * nc)
+    u_, v_, w_ = U.T(uf[R.fperm]), U.T(vf[R.fperm]), U.T(wf[R.fperm])
+    U.call("mb_cell_face_sign", dm.struct, U.P(u_), U.P(v_), U.P(w_), U.P(sign), st)
+    cells = [U.Z(nc) for _ in range(3)]
+    for f, cc in zip((u_, v_, w_), cells):
+        U.call("mb_facetocell", dm.struct, U.P(f), U.P(cc), st)
+    dt = U.Z(1)
+    U.call("mb_time_step", dm.struct, *[U.P(x) for x in cells], wl.cfl, *wl.diffusion, U.P(dt), st)
+    prm = _lib.MbAdvDiffParams(order, 1, *wl.diffusion)
+    w0 = U.T(wl.init(A["cells_center"])[R.cperm])
+    runs = []
+    for sums in (False, True):
+        if sums:
+            assert dm.use_edge_sums()
+        cs, ns = U.Z(dm.cell_scratch_size()), U.Z(nn)
+        a, b = w0.clone(), U.Z(nc)
+        for _ in range(6):
+            U.call("mb_advdiff_step", dm.struct, db.struct, prm, U.P(a), U.P(b), U.P(sign), None, U.P(dt),
+                   U.P(cs), U.P(ns), st)
+            a, b = b, a
+        runs.append(U.H(a))
+    assert dm.cell_scratch_size() == 8 * nc + 4 * (nn + dm.nbedges)
+    assert rel_max(runs[1], runs[0]) < 1e-13
+    assert not np.array_equal(runs[0], U.H(w0))
