@@ -419,8 +419,11 @@ class AdvectionDiffusionSolver:
     def launches_per_step(self):
         """Kernel launches of one fused step."""
         # (tetrahedra at order 2 through mb_advdiff_step pack rows first; the solver's steps
-        # carry them from one step to the next instead)
-        return 1 + int(self.order == 2 or bool(self.diffusion))
+        # carry them from one step to the next instead; with the edge sums the first phase is
+        # two launches: vertex and edge sums, then the cells)
+        dm = self._dm
+        sums = dm is not None and self.order == 2 and dm.struct is not None and bool(dm.struct.cell_edges)
+        return 1 + int(self.order == 2 or bool(self.diffusion)) + int(sums)
 
     def release_graphs(self):
         self._graph = None
