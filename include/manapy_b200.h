@@ -580,7 +580,8 @@ int mb_check_state(const double *f64, const float *f32, int64_t n, int32_t nonne
  *   3 face_cellid[.][0] [0, nbcells)   4 face_cellid[.][1] [-1, nbcells) (position counted
  *   from face_cellid + 1)   5 face_nodeid [0, nbnodes)   6 n2c [0, nbcells)   7 n2g [0, nbfaces)
  *   8 cell_cellfid [0, nbcells)   9 cell_vtx [0, nbnodes)   10 cell_nbr [-nbfaces, nbcells)
- *   11 lsq_sell [-1, nbcells)   12 n2c_sell [0, nbcells)
+ *   11 lsq_sell [-1, nbcells)   12 n2c_sell [0, nbcells)   and, when cell_edges is set,
+ *   13 cell_edges [0, nbedges)   14 edge_origin [0, nbnodes)   15 edge_sell [-1, nbcells)
  * A CSR or SELL table's last offset is taken as the length of its index array. */
 int mb_check_tables(const mb_mesh *m, uint64_t *first, void *stream);
 

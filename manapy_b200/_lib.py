@@ -93,6 +93,9 @@ CHECK_TABLES = (
     ("cell_nbr", None, 0, lambda c, f, n: (-f, c)),
     ("lsq_sell_idx", "lsq_sell_ptr", 0, lambda c, f, n: (-1, c)),
     ("n2c_sell_idx", "n2c_sell_ptr", 0, lambda c, f, n: (0, c)),
+    ("cell_edges", None, 0, lambda c, f, n: (0, None)),
+    ("edge_origin", None, 0, lambda c, f, n: (0, n)),
+    ("edge_sell_idx", "edge_sell_ptr", 0, lambda c, f, n: (-1, c)),
 )
 
 

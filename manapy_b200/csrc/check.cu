@@ -108,5 +108,11 @@ extern "C" int mb_check_tables(const mb_mesh *m, uint64_t *first, void *stream) 
   mb::check_one(TableCheck{m->cell_nbr, nullptr, nc, 4, nlf, -nf, nc, 0}, 10, f, st);
   mb::check_one(TableCheck{m->lsq_sell_idx, m->lsq_sell_ptr, ncg, 0, 0, -1, nc, 1}, 11, f, st);
   mb::check_one(TableCheck{m->n2c_sell_idx, m->n2c_sell_ptr, nng, 0, 0, 0, nc, 1}, 12, f, st);
+  if (m->cell_edges && m->nbedges > 0) {
+    const int ne = m->nbedges;
+    mb::check_one(TableCheck{m->cell_edges, nullptr, nc, 8, 6, 0, ne, 0}, 13, f, st);
+    mb::check_one(TableCheck{m->edge_origin, nullptr, ne, 1, 1, 0, nn, 0}, 14, f, st);
+    mb::check_one(TableCheck{m->edge_sell_idx, m->edge_sell_ptr, (ne + 31) / 32, 0, 0, -1, nc, 1}, 15, f, st);
+  }
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }

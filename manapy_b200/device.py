@@ -360,6 +360,8 @@ class DeviceMesh:
         value = int(self.t[name].reshape(-1)[pos].item())
         tid = [t[1] if offs else t[0] for t in _lib.CHECK_TABLES].index(name)
         lo, hi = _lib.CHECK_TABLES[tid][3](self.nbcells, self.nbfaces, self.nbnodes)
+        if hi is None:                       # cell_edges: the edge count
+            hi = int(getattr(self, "nbedges", 0))
         what = "is out of order" if offs else "is outside [%d, %d)" % (lo, hi)
         raise ValueError("mesh table %s: entry %d = %d %s" % (name, pos, value, what))
 

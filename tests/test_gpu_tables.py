@@ -50,6 +50,15 @@ def test_a_planted_bad_entry_is_named(dim, name, where, value, msg, cuda):
         dm.check_tables()
 
 
+def test_edge_tables_are_checked_when_in_use(cuda):
+    dm = _mesh(3)
+    assert dm.use_edge_sums()
+    dm.check_tables()
+    _plant(dm, "edge_sell_idx", 5, dm.nbcells)
+    with pytest.raises(ValueError, match="edge_sell_idx: entry 5"):
+        dm.check_tables()
+
+
 def test_offsets_out_of_order_are_named(cuda):
     dm = _mesh(2)
     ptr = dm.t["cellnid_ptr"]
