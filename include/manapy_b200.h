@@ -139,6 +139,11 @@ typedef struct mb_mesh {
   const int32_t *edge_sell_idx;
   int32_t nbedges;
   int32_t pad_;
+  /* with the edge tables: the vertex -> cells lists (as n2c_*) in the slot-shared SELL-32
+   * layout of lsq_sell, with their centre->vertex weights (-1 and weight 0 in empty slots) */
+  const int32_t *n2c_sum_ptr;
+  const int32_t *n2c_sum_idx;
+  const double *n2c_sum_alpha;
 } mb_mesh;
 
 typedef struct mb_bc {
@@ -582,6 +587,7 @@ int mb_check_state(const double *f64, const float *f32, int64_t n, int32_t nonne
  *   8 cell_cellfid [0, nbcells)   9 cell_vtx [0, nbnodes)   10 cell_nbr [-nbfaces, nbcells)
  *   11 lsq_sell [-1, nbcells)   12 n2c_sell [0, nbcells)   and, when cell_edges is set,
  *   13 cell_edges [0, nbedges)   14 edge_origin [0, nbnodes)   15 edge_sell [-1, nbcells)
+ *   16 n2c_sum [-1, nbcells)
  * A CSR or SELL table's last offset is taken as the length of its index array. */
 int mb_check_tables(const mb_mesh *m, uint64_t *first, void *stream);
 

@@ -38,7 +38,8 @@ class MbMesh(ctypes.Structure):
                 ("lsq_sell_ptr", _vp), ("lsq_sell_idx", _vp), ("n2c_sell_ptr", _vp), ("n2c_sell_idx", _vp),
                 ("n2c_sell_alpha", _vp), ("n2c_sell_alpha_f32", _vp), ("face_nm_f32", _vp), ("cell_lsq", _vp),
                 ("cell_edges", _vp), ("edge_origin", _vp), ("edge_sell_ptr", _vp), ("edge_sell_idx", _vp),
-                ("nbedges", _i32), ("pad_", _i32)]
+                ("nbedges", _i32), ("pad_", _i32), ("n2c_sum_ptr", _vp), ("n2c_sum_idx", _vp),
+                ("n2c_sum_alpha", _vp)]
 
 
 class MbBC(ctypes.Structure):
@@ -96,6 +97,7 @@ CHECK_TABLES = (
     ("cell_edges", None, 0, lambda c, f, n: (0, None)),
     ("edge_origin", None, 0, lambda c, f, n: (0, n)),
     ("edge_sell_idx", "edge_sell_ptr", 0, lambda c, f, n: (-1, c)),
+    ("n2c_sum_idx", "n2c_sum_ptr", 0, lambda c, f, n: (-1, c)),
 )
 
 

@@ -113,6 +113,7 @@ extern "C" int mb_check_tables(const mb_mesh *m, uint64_t *first, void *stream) 
     mb::check_one(TableCheck{m->cell_edges, nullptr, nc, 8, 6, 0, ne, 0}, 13, f, st);
     mb::check_one(TableCheck{m->edge_origin, nullptr, ne, 1, 1, 0, nn, 0}, 14, f, st);
     mb::check_one(TableCheck{m->edge_sell_idx, m->edge_sell_ptr, (ne + 31) / 32, 0, 0, -1, nc, 1}, 15, f, st);
+    mb::check_one(TableCheck{m->n2c_sum_idx, m->n2c_sum_ptr, nng, 0, 0, -1, nc, 1}, 16, f, st);
   }
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
 }

@@ -1032,20 +1032,16 @@ __global__ void __launch_bounds__(kBlock) k_f3_sums(mb_mesh m, mb_bc bc, const d
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.nbnodes) return;
     const D3 X = ld3(m.node_coord + 4 * (long long)n);
-    const int len = ld(m.n2c_ptr + n + 1) - ld(m.n2c_ptr + n);
-    const int sb = ld(m.n2c_sell_ptr + (n >> 5)), se = ld(m.n2c_sell_ptr + (n >> 5) + 1);
+    const int sb = ld(m.n2c_sum_ptr + (n >> 5)), se = ld(m.n2c_sum_ptr + (n >> 5) + 1);
     double acc = 0.;
-    for (int k = 0; sb + lane + 32 * k < se; ++k) {
-      const int e = sb + lane + 32 * k;
-      // entries past the row's length repeat its first cell with weight 0
-      const int cc = ld1_stream(m.n2c_sell_idx + e, pst);
+    for (int k = sb + lane; k < se; k += 32) {
+      const int cc = ld1_stream(m.n2c_sum_idx + k, pst);
+      if (cc < 0) continue;       // empty slot
       double x, y, z, wc;
       ld_row(rows + 4 * (long long)cc, x, y, z, wc);
-      if (DIFF) acc += ldd_stream(m.n2c_sell_alpha + e, pst) * wc;
-      if (k < len) {
-        px += (x - X.x) * wc; py += (y - X.y) * wc; pz += (z - X.z) * wc;
-        q += wc;
-      }
+      if (DIFF) acc += ldd_stream(m.n2c_sum_alpha + k, pst) * wc;
+      px += (x - X.x) * wc; py += (y - X.y) * wc; pz += (z - X.z) * wc;
+      q += wc;
     }
     if (DIFF) {
       const GhostRule ghost = make_rule(m, bc, w);
@@ -1376,7 +1372,7 @@ inline void f3_p1_run(const mb_mesh &m, const mb_bc &bc, const double *w, double
 // cells; records of the sums after the cell records and rows in the cell scratch
 inline bool f3_sums_tables(const mb_mesh &m) {
   return m.cell_edges && m.edge_origin && m.edge_sell_ptr && m.edge_sell_idx && m.nbedges > 0 && m.cell_lsq &&
-         m.n2c_ptr && m.n2c_sell_ptr && m.n2c_sell_idx && m.n2c_sell_alpha;
+         m.n2c_sum_ptr && m.n2c_sum_idx && m.n2c_sum_alpha;
 }
 template <bool DF, int V>
 inline void f3_sums_run(const mb_mesh &m, const mb_bc &bc, const double *w, double *cs, const double *rows,

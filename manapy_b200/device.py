@@ -232,6 +232,8 @@ class DeviceMesh:
         a_c, a_g = vertex_weights(A)
         ptr, idx, src = R.relabel_csr(A["n2c_ptr"], A["n2c_idx"], np_, ci)
         T["n2c_ptr"], T["n2c_idx"], T["n2c_alpha"] = _t(ptr, i32, dev), _t(idx, i32, dev), _t(a_c[src], f64, dev)
+        if dim == 3:
+            self._node_sum_tables(ptr, idx, a_c[src], T, dev)
         gp, gi, gv = sell32(ptr, idx, a_c[src], fill="first")
         T["n2c_sell_ptr"], T["n2c_sell_idx"], T["n2c_sell_alpha"] = _t(gp, i32, dev), _t(gi, i32, dev), _t(gv, f64, dev)
         T["n2c_sell_alpha_f32"] = _t(gv, np.float32, dev)
@@ -324,7 +326,8 @@ class DeviceMesh:
 
     # the edge tables change the scratch a second-order 3D step needs, so a struct carries
     # them only once its user asks (use_edge_sums)
-    EDGE_TABLES = ("cell_edges", "edge_origin", "edge_sell_ptr", "edge_sell_idx")
+    EDGE_TABLES = ("cell_edges", "edge_origin", "edge_sell_ptr", "edge_sell_idx", "n2c_sum_ptr", "n2c_sum_idx",
+                   "n2c_sum_alpha")
 
     def use_edge_sums(self):
         """Tetrahedra: point the struct at the edge tables, so that the second-order step
@@ -519,6 +522,31 @@ class DeviceMesh:
         cc4[:, :3] = A["cells_center"][cp]
         T["cell_xy"] = _t(cc4, np.float64, dev)
         self._edge_tables(ni[nodes], T, dev)
+
+    def _node_sum_tables(self, ptr, idx, alpha, T, dev):
+        """Tetrahedra: the vertex -> cells lists in the slot-shared SELL-32 layout with their
+        centre->vertex weights (``n2c_sum_ptr`` / ``n2c_sum_idx`` / ``n2c_sum_alpha``; -1 and
+        weight 0 in empty slots), read by the vertex sums of the edge-sum step."""
+        from . import native
+        ptr = np.asarray(ptr, dtype=np.int64)
+        idx = np.asarray(idx, dtype=np.int64)
+        nrow, ncell = len(ptr) - 1, int(self.nbcells)
+        gp, gi = native.sell_aligned(ptr, idx.astype(np.int32))
+        gp64 = np.asarray(gp, dtype=np.int64)
+        # the CSR position of every (row, cell) slot
+        slot = np.arange(int(gp64[-1]), dtype=np.int64)
+        grp = np.searchsorted(gp64, slot, side="right") - 1
+        row = 32 * grp + (slot - gp64[grp]) % 32
+        key_csr = np.repeat(np.arange(nrow, dtype=np.int64), np.diff(ptr)) * ncell + idx
+        order = np.argsort(key_csr, kind="stable")
+        gi64 = np.asarray(gi, dtype=np.int64)
+        used = gi64 >= 0
+        pos = order[np.searchsorted(key_csr[order], row[used] * ncell + gi64[used])]
+        al = np.zeros(len(gi64))
+        al[used] = np.asarray(alpha)[pos]
+        T["n2c_sum_ptr"] = _t(gp, np.int32, dev)
+        T["n2c_sum_idx"] = _t(gi, np.int32, dev)
+        T["n2c_sum_alpha"] = _t(al, np.float64, dev)
 
     # the six edges of a tetrahedron as pairs of local vertices
     TET_EDGES = np.array([[0, 1], [0, 2], [0, 3], [1, 2], [1, 3], [2, 3]])

@@ -85,4 +85,4 @@ def test_table_check_keys_decode():
     assert _lib.decode_table_check((1 << 40) | (1 << 39) | 9) == ("cellnid_ptr", True, 9)
     # face_cellid's second column is checked from face_cellid + 1
     assert _lib.decode_table_check((4 << 40) | 22) == ("face_cellid", False, 23)
-    assert len(_lib.CHECK_TABLES) == 16
+    assert len(_lib.CHECK_TABLES) == 17

@@ -95,3 +95,23 @@ def test_layout_choice_reaches_the_device_tables():
     assert not np.array_equal(a.t["lsq_sell_idx"], b.t["lsq_sell_idx"])
     with pytest.raises(ValueError):
         DeviceMesh(A, device=None, stencil="sorted")
+
+
+def test_vertex_sum_lists_keep_cells_and_weights():
+    """Tetrahedra: the slot-shared vertex -> cells lists of the edge-sum step hold, per
+    vertex, exactly its CSR cells with their centre->vertex weights."""
+    el, vx = meshgen.cube_tetrahedra(5, seed=3)
+    dm = DeviceMesh(G.build(el, vx, 3), device=None)
+    ptr, idx, al = (np.asarray(dm.t[k]) for k in ("n2c_ptr", "n2c_idx", "n2c_alpha"))
+    gp, gi, ga = (np.asarray(dm.t[k]) for k in ("n2c_sum_ptr", "n2c_sum_idx", "n2c_sum_alpha"))
+    n = len(ptr) - 1
+    for g in range(len(gp) - 1):
+        bi = gi[gp[g]:gp[g + 1]].reshape(-1, 32)
+        ba = ga[gp[g]:gp[g + 1]].reshape(-1, 32)
+        for lane in range(32):
+            r = 32 * g + lane
+            col, wts = bi[:, lane], ba[:, lane]
+            assert np.all(wts[col < 0] == 0)
+            got = sorted(zip(col[col >= 0].tolist(), wts[col >= 0].tolist()))
+            ref = sorted(zip(idx[ptr[r]:ptr[r + 1]].tolist(), al[ptr[r]:ptr[r + 1]].tolist())) if r < n else []
+            assert got == ref
