@@ -56,8 +56,10 @@ def test_sharded_equals_single_gpu(tmp_path, key, n, steps, cuda):
         var.face = a
         var.interpolate_facetocell()
     w.cell = wl.init(dom.cells.center)
+    # the shards gather each cell's whole stencil (no edge sums), as this run does
     S = M.AdvectionDiffusionSolver(w, vel=tuple(vel), conf=M.Struct(Dxx=wl.diffusion[0], Dyy=wl.diffusion[1],
-                                                                     Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl))
+                                                                     Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl,
+                                                                     lsq_sums=False))
     S.advance(steps)
     out = str(tmp_path / "w.npy")
     tmp.spawn(_rank, args=(2, _free_port(), key, n, steps, out), nprocs=2, join=True)
