@@ -898,9 +898,11 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
-def _serial_fp64(reqs, steps, warmup=3):
+def _serial_fp64(reqs, steps, warmup=None):
     """Each request's plain FP64 solve through the public API, one after another (CUDA
-    graphs, inputs resident); device time of ``steps`` steps per request, summed."""
+    graphs, inputs resident); device time of ``steps`` steps per request, summed.  The
+    warm-up runs the same number of steps first (default), so that tuning and the graph
+    capture happen before the timed steps."""
     import torch
     import manapy_b200 as M
     from manapy_b200 import meshgen, serving as SV
@@ -923,7 +925,7 @@ def _serial_fp64(reqs, steps, warmup=3):
             S = M.ShallowWaterSolver(vs[0], hvel=(vs[1], vs[2]), hc=vs[3], Z=vs[4],
                                      conf=M.Struct(order=1, cfl=0.5, grav=9.81))
             run = S.advance
-        run(warmup)
+        run(steps if warmup is None else warmup)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
