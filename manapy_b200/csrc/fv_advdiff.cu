@@ -1179,8 +1179,8 @@ __device__ __forceinline__ double diamond3(const mb_advdiff_params &p, const D3 
 #define MB_P2_3D_BLOCK kBlock
 #endif
 
-constexpr int kQ2B[4] = {MB_P2_3D_BLOCK, 128, 128, 64};
-constexpr int kQ2M[4] = {MB_P2_3D_MIN_BLOCKS, 4, 5, 8};
+constexpr int kQ2B[4] = {MB_P2_3D_BLOCK, 128, 128, 128};
+constexpr int kQ2M[4] = {MB_P2_3D_MIN_BLOCKS, 4, 5, 6};
 
 template <bool ORDER2, bool DIFF, bool WROWS, int VAR>
 __global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p,
@@ -1197,8 +1197,6 @@ __global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, m
   const int4 vt = ld4(m.cell_vtx + 4 * i);
   const int4 nb = ld4(m.cell_nbr + 4 * i);
   const uint32_t fl = ld(m.cell_flags + i);
-  const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
-                   ld3(m.node_coord + 4 * vt.w)};
   const D3 ci = ld3(m.cell_xy + 4 * i);
   const double2 sa = ldd2(sign + 4 * i), sb = ldd2(sign + 4 * i + 2);
   // order 2: the record {w, psi gx, psi gy, psi gz} of phase 1
@@ -1217,7 +1215,10 @@ __global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, m
     const bool own = (fl >> (6 * j)) & 1u;
     int d0, d1, d2;
     face_desc(fl, j, d0, d1, d2);
-    const D3 V0 = pick4(P, d0), V1 = pick4(P, d1), V2 = pick4(P, d2);
+    // the face's vertices gathered by index (L1 hits after the first face) instead of
+    // selected among four held in registers
+    const int g0 = comp(vt, d0), g1 = comp(vt, d1), g2 = comp(vt, d2);
+    const D3 V0 = ld3(m.node_coord + 4 * g0), V1 = ld3(m.node_coord + 4 * g1), V2 = ld3(m.node_coord + 4 * g2);
     const D3 fc = (1. / 3) * ((V0 + V1) + V2);
     double vo, gxo = 0., gyo = 0., gzo = 0.;
     D3 co;
@@ -1250,12 +1251,12 @@ __global__ void __launch_bounds__(kQ2B[VAR], kQ2M[VAR]) k_f3_phase2(mb_mesh m, m
         const D3 Nd = 0.5 * cross(V1 - V0, V2 - V0);
         const D3 N = ((fl >> (6 * j + 5)) & 1u) ? (-1.0) * Nd : Nd;
         const bool swp = (fl >> (6 * j + 4)) & 1u;
-        const int i1 = d0, i2 = swp ? d2 : d1, i3 = swp ? d1 : d2;   // faces.nodeid order
-        const D3 Q2 = pick4(P, i2), Q3 = pick4(P, i3), Q1 = pick4(P, i1);
+        // faces.nodeid order: (d0, d1, d2), or (d0, d2, d1) when swapped
+        const D3 Q2 = swp ? V2 : V1, Q3 = swp ? V1 : V2;
         const D3 v1 = own ? ci : co, v2 = own ? co : ci;
-        const int gi1 = comp(vt, i1), gi2 = comp(vt, i2), gi3 = comp(vt, i3);
+        const int gi2 = swp ? g2 : g1, gi3 = swp ? g1 : g2;
         const double VL = own ? wi : vo, VR = own ? vo : wi;
-        v = diamond3(p, N, Q1, Q2, Q3, v1, v2, ld(wn + gi1), ld(wn + gi2), ld(wn + gi3), VL, VR);
+        v = diamond3(p, N, V0, Q2, Q3, v1, v2, ld(wn + g0), ld(wn + gi2), ld(wn + gi3), VL, VR);
       }
       q[j] = own ? v : -v;
     }
