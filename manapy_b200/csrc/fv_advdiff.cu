@@ -944,7 +944,7 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_phase1(mb_mesh m, m
     for (int j = 0; j < 4; ++j) {
       int d0, d1, d2;
       face_desc(fl, j, d0, d1, d2);
-      const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
+      const D3 fc = (1. / 3) * tet_face_sum(P, j, d2);
       const double delta = gx * (fc.x - c.x) + gy * (fc.y - c.y) + gz * (fc.z - c.z);
       double psi_ij = 1.;
       if (!(fabs(delta) < 1e-10)) {
@@ -1141,7 +1141,7 @@ __global__ void __launch_bounds__(kQ1B[VAR], kQ1M[VAR]) k_f3_grad(mb_mesh m, mb_
   for (int j = 0; j < 4; ++j) {
     int d0, d1, d2;
     face_desc(fl, j, d0, d1, d2);
-    const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
+    const D3 fc = (1. / 3) * tet_face_sum(P, j, d2);
     const double delta = gx * (fc.x - c.x) + gy * (fc.y - c.y) + gz * (fc.z - c.z);
     double psi_ij = 1.;
     if (!(fabs(delta) < 1e-10)) {

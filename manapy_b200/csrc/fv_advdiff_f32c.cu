@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kBlock, MB_P1C_3D_MIN_BLOCKS)
     for (int j = 0; j < 4; ++j) {
       int d0, d1, d2;
       face_desc(fl, j, d0, d1, d2);
-      const D3 fc = (1. / 3) * ((pick4(P, d0) + pick4(P, d1)) + pick4(P, d2));
+      const D3 fc = (1. / 3) * tet_face_sum(P, j, d2);
       const float delta = gx * (float)(fc.x - c.x) + gy * (float)(fc.y - c.y) + gz * (float)(fc.z - c.z);
       float psi_ij = 1.f;
       if (!(fabsf(delta) < 1e-10f)) {
@@ -491,8 +491,6 @@ __global__ void __launch_bounds__(kBlock, 2)
   const int4 vt = ld4(m.cell_vtx + 4 * i);
   const int4 nb = ld4(m.cell_nbr + 4 * i);
   const uint32_t fl = ld(m.cell_flags + i);
-  const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
-                   ld3(m.node_coord + 4 * vt.w)};
   const D3 ci = ld3(m.cell_xy + 4 * i);
   const float4 s4 = ldf4(sign + 4 * (long long)i);
   const long long nc = m.nbcells;
@@ -513,7 +511,9 @@ __global__ void __launch_bounds__(kBlock, 2)
     const bool own = (fl >> (6 * j)) & 1u;
     int d0, d1, d2;
     face_desc(fl, j, d0, d1, d2);
-    const D3 V0 = pick4(P, d0), V1 = pick4(P, d1), V2 = pick4(P, d2);
+    // the face's vertices gathered by index instead of selected among four in registers
+    const int g0 = comp(vt, d0), g1 = comp(vt, d1), g2 = comp(vt, d2);
+    const D3 V0 = ld3(m.node_coord + 4 * g0), V1 = ld3(m.node_coord + 4 * g1), V2 = ld3(m.node_coord + 4 * g2);
     const D3 fc = (1. / 3) * ((V0 + V1) + V2);
     float vo, gxo = 0.f, gyo = 0.f, gzo = 0.f, pso = 0.f;
     D3 co;
@@ -551,8 +551,8 @@ __global__ void __launch_bounds__(kBlock, 2)
         const D3 Nd = 0.5 * cross(V1 - V0, V2 - V0);
         const D3 N = ((fl >> (6 * j + 5)) & 1u) ? (-1.0) * Nd : Nd;
         const bool swp = (fl >> (6 * j + 4)) & 1u;
-        const int i1 = d0, i2 = swp ? d2 : d1, i3 = swp ? d1 : d2;
-        const D3 Q2 = pick4(P, i2), Q3 = pick4(P, i3), Q1 = pick4(P, i1);
+        const D3 Q1 = V0, Q2 = swp ? V2 : V1, Q3 = swp ? V1 : V2;   // faces.nodeid order
+        const int gi2 = swp ? g2 : g1, gi3 = swp ? g1 : g2;
         const D3 v1 = own ? ci : co, v2 = own ? co : ci;
         const double rair = 1. / dot(N, v2 - v1);
         // sum_d D_d g_d N_d = ca (V_A - V_C) + cb (V_B - V_D) + cr (V_R - V_L), with manapy's
@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(kBlock, 2)
         const D3 t = cross(v1 - v2, DN);
         const float ca = (float)(0.5 * dot(Q3 - Q2, t) * rair), cb = (float)(0.5 * dot(Q1 - Q3, t) * rair),
                     cr = (float)(dot(DN, N) * rair);
-        const float VA = ld(wn + comp(vt, i1)), VB = ld(wn + comp(vt, i2)), VC = ld(wn + comp(vt, i3));
+        const float VA = ld(wn + g0), VB = ld(wn + gi2), VC = ld(wn + gi3);
         const float VL = own ? wi : vo, VR = own ? vo : wi;
         v = ca * (VA - VC) + cb * (VB - VC) + cr * (VR - VL);  // already differences
       }

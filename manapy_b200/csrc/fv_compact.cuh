@@ -156,6 +156,18 @@ __device__ __forceinline__ D3 pick4(const D3 *P, int k) { return k == 0 ? P[0] :
 template <class T>
 __device__ __forceinline__ T pick4v(T a, T b, T c, T d, int k) { return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d)); }
 
+// (V_d0 + V_d1) + V_d2 for local face j, d = face_desc's descending order: the pair added
+// first is the face's two vertices other than d2 (an addition of two commutes exactly), so
+// the sum is one of three candidates chosen by d2, with no 4-way selects of coordinates
+// (j a compile-time constant after unrolling)
+__device__ __forceinline__ D3 tet_face_sum(const D3 *P, int j, int d2) {
+  const int a = tet_face(j, 0), b = tet_face(j, 1), c = tet_face(j, 2);
+  const D3 x = P[a], y = P[b], z = P[c];
+  if (d2 == a) return (y + z) + x;
+  if (d2 == b) return (x + z) + y;
+  return (x + y) + z;
+}
+
 // manapy's descending-order vertices of local face j: (d0, d1, d2), as local vertex indices
 __device__ __forceinline__ void face_desc(uint32_t fl, int j, int &d0, int &d1, int &d2) {
   const int code = (fl >> (6 * j + 1)) & 7u;
