@@ -115,3 +115,28 @@ def test_vertex_sum_lists_keep_cells_and_weights():
             got = sorted(zip(col[col >= 0].tolist(), wts[col >= 0].tolist()))
             ref = sorted(zip(idx[ptr[r]:ptr[r + 1]].tolist(), al[ptr[r]:ptr[r + 1]].tolist())) if r < n else []
             assert got == ref
+
+
+def test_edge_tables_of_a_tetrahedral_mesh():
+    """cell_edges names the edge of each local vertex pair, edge_origin its vertex of
+    smaller index, and each edge's cell list holds exactly the cells that contain it."""
+    el, vx = meshgen.cube_tetrahedra(4, seed=2)
+    dm = DeviceMesh(G.build(el, vx, 3), device=None)
+    vt = np.asarray(dm.t["cell_vtx"]).astype(np.int64)
+    ce = np.asarray(dm.t["cell_edges"]).astype(np.int64)
+    org = np.asarray(dm.t["edge_origin"]).astype(np.int64)
+    gp, gi = np.asarray(dm.t["edge_sell_ptr"]), np.asarray(dm.t["edge_sell_idx"])
+    ne, nc = dm.nbedges, dm.nbcells
+    assert np.all(ce[:, 6:] == -1) and ce[:, :6].min() == 0 and ce[:, :6].max() == ne - 1
+    ends = {}
+    for i in range(nc):
+        for k, (a, b) in enumerate(DeviceMesh.TET_EDGES):
+            e, pair = ce[i, k], tuple(sorted((vt[i, a], vt[i, b])))
+            assert ends.setdefault(e, pair) == pair          # one pair per edge id
+            assert org[e] == pair[0]
+    assert len(ends) == ne and len(set(ends.values())) == ne
+    rows, _ = _rows(gp, gi, ne)
+    for e in range(ne):
+        a, b = ends[e]
+        holders = sorted(np.nonzero(np.any(vt == a, axis=1) & np.any(vt == b, axis=1))[0].tolist())
+        assert sorted(rows[e].tolist()) == holders
