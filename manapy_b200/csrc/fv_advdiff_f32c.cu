@@ -399,7 +399,9 @@ __global__ void k_clock_tick(int32_t *clock) { *clock += 1; }
 #endif
 
 // record layout: float4 {w, gx, gy, gz} at rec[4i], psi at rec[4 nbcells + i]
-template <bool ORDER2, bool DIFF>
+// PRE: the moment matrix's cofactors and determinant come from m.cell_lsq ([nbcells][12],
+// mb_lsq_matrix) and only the right-hand side is summed over the stencil
+template <bool ORDER2, bool DIFF, bool PRE = false>
 __global__ void __launch_bounds__(kBlock, MB_P1C_3D_MIN_BLOCKS)
     k_f3c_phase1(mb_mesh m, mb_bc bc, const float *__restrict__ w, float *__restrict__ rec, float *__restrict__ wn,
                  int ncb) {
@@ -415,32 +417,53 @@ __global__ void __launch_bounds__(kBlock, MB_P1C_3D_MIN_BLOCKS)
     const int sb = ld(m.lsq_sell_ptr + (i >> 5)), se = ld(m.lsq_sell_ptr + (i >> 5) + 1);
     const int L = (se - sb) >> 5;
     const int32_t *ix = m.lsq_sell_idx + sb + lane;
-    for (int k = 0; k < L; ++k) {
+    auto acc = [&](const D3 &pc, float dw) {
+      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z;
+      if (!PRE) {
+        ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
+        ixy += dx * dy; ixz += dx * dz; iyz += dy * dz;
+      }
+      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy); jz = fmaf((float)dz, dw, jz);
+    };
+    // batches of four neighbours: their indices, then their centres and values in flight
+    // together, then the terms in stencil order (padding: the cell itself, exact zeros)
+    int k = 0;
+    for (; k + 4 <= L; k += 4) {
+      int cc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { cc[u] = ld(ix + 32 * (k + u)); cc[u] = cc[u] < 0 ? i : cc[u]; }
+      D3 pc[4];
+      float wc[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { pc[u] = ld3(m.cell_xy + 4 * cc[u]); wc[u] = ld(w + cc[u]); }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc(pc[u], wc[u] - wi);
+    }
+    for (; k < L; ++k) {
       int cc = ld(ix + 32 * k);
       cc = cc < 0 ? i : cc;
-      const D3 pc = ld3(m.cell_xy + 4 * cc);
-      const double dx = pc.x - c.x, dy = pc.y - c.y, dz = pc.z - c.z;
-      const float dw = ld(w + cc) - wi;
-      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
-      ixy += dx * dy; ixz += dx * dz; iyz += dy * dz;
-      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy); jz = fmaf((float)dz, dw, jz);
+      acc(ld3(m.cell_xy + 4 * cc), ld(w + cc) - wi);
     }
     const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
     for (int k = gb; k < ge; ++k) {
       const int f = ld(m.ghostnid_idx + k);
       const double *gc = m.face_ghostcenter + 3 * f;
-      const double dx = ld(gc) - c.x, dy = ld(gc + 1) - c.y, dz = ld(gc + 2) - c.z;
-      const float dw = ghost(f) - wi;
-      ixx += dx * dx; iyy += dy * dy; izz += dz * dz;
-      ixy += dx * dy; ixz += dx * dz; iyz += dy * dz;
-      jx = fmaf((float)dx, dw, jx); jy = fmaf((float)dy, dw, jy); jz = fmaf((float)dz, dw, jz);
+      acc(d3(ld(gc), ld(gc + 1), ld(gc + 2)), ghost(f) - wi);
     }
-    const double rdia = 1. / (ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) -
-                              izz * (ixy * ixy));
     // inverse moment matrix (symmetric cofactors / determinant), rounded once
-    const float a11 = (float)((iyy * izz - iyz * iyz) * rdia), a12 = (float)((ixz * iyz - ixy * izz) * rdia);
-    const float a13 = (float)((ixy * iyz - ixz * iyy) * rdia), a22 = (float)((ixx * izz - ixz * ixz) * rdia);
-    const float a23 = (float)((ixy * ixz - iyz * ixx) * rdia), a33 = (float)((ixx * iyy - ixy * ixy) * rdia);
+    double c11, c12, c13, c22, c23, c33, dia;
+    if (PRE) {
+      double pad;
+      ld4d(m.cell_lsq + 12 * (long long)i, c11, c12, c13, c22);
+      ld4d(m.cell_lsq + 12 * (long long)i + 4, c23, c33, dia, pad);
+    } else {
+      dia = ixx * iyy * izz + 2. * ixy * ixz * iyz - ixx * (iyz * iyz) - iyy * (ixz * ixz) - izz * (ixy * ixy);
+      c11 = iyy * izz - iyz * iyz; c12 = ixz * iyz - ixy * izz; c13 = ixy * iyz - ixz * iyy;
+      c22 = ixx * izz - ixz * ixz; c23 = ixy * ixz - iyz * ixx; c33 = ixx * iyy - ixy * ixy;
+    }
+    const double rdia = 1. / dia;
+    const float a11 = (float)(c11 * rdia), a12 = (float)(c12 * rdia), a13 = (float)(c13 * rdia);
+    const float a22 = (float)(c22 * rdia), a23 = (float)(c23 * rdia), a33 = (float)(c33 * rdia);
     const float gx = a11 * jx + a12 * jy + a13 * jz;
     const float gy = a12 * jx + a22 * jy + a23 * jz;
     const float gz = a13 * jx + a23 * jy + a33 * jz;
@@ -623,7 +646,12 @@ int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params 
     k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2C_BLOCK), MB_P2C_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
                                                                            lo_in, lo_out);
   } else {
-    if (ncb + nnb > 0) k_f3c_phase1<O2, DF><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+    if (ncb + nnb > 0) {
+      if (O2 && m.cell_lsq)
+        k_f3c_phase1<O2, DF, true><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+      else
+        k_f3c_phase1<O2, DF, false><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
+    }
     k_f3c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
                                                                            lo_in, lo_out);
   }
