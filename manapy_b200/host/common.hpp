@@ -39,6 +39,64 @@ struct Result {
   }
 };
 
+// Host threads for n independent items: up to 16, one below min_n items.
+inline i64 pool_size(i64 n, i64 min_n) {
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  return n >= min_n ? std::max<i64>(1, std::min<i64>((i64)hw, n)) : 1;
+}
+
+// fn(t, i0, i1) for t < nt over the contiguous ranges [n t / nt, n (t+1) / nt), each on its
+// own thread (range 0 on the calling one).  fn writes only what its range owns, so the
+// result does not depend on nt.
+template <class F>
+inline void run_ranges(i64 nt, i64 n, F &&fn) {
+  if (nt <= 1) {
+    fn((i64)0, (i64)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  pool.reserve(nt - 1);
+  for (i64 t = 1; t < nt; ++t) pool.emplace_back([&, t] { fn(t, n * t / nt, n * (t + 1) / nt); });
+  fn((i64)0, (i64)0, n / nt);
+  for (auto &th : pool) th.join();
+}
+
+// fn(i) for every i in [0, n), split over host threads when n is large.
+template <class F>
+inline void parallel_for(i64 n, F &&fn) {
+  run_ranges(pool_size(n, (i64)1 << 15), n, [&](i64, i64 i0, i64 i1) {
+    for (i64 i = i0; i < i1; ++i) fn(i);
+  });
+}
+
+// Stable argsort of integer keys in [0, n): a counting sort (equal keys keep their order).
+inline std::vector<i64> counting_argsort(const std::vector<i64> &key, i64 n) {
+  std::vector<i64> pos(n + 1, 0), o(key.size());
+  for (i64 k : key) pos[k + 1]++;
+  for (i64 i = 0; i < n; ++i) pos[i + 1] += pos[i];
+  for (size_t e = 0; e < key.size(); ++e) o[pos[key[e]]++] = (i64)e;
+  return o;
+}
+
+// CSR rows taken in `rows` order with values mapped through vinv, each row's entry order
+// kept; src (optional) gets each new entry's position in the old table.
+inline void relabel_csr(const std::vector<i64> &ptr, const std::vector<i64> &idx, const std::vector<i64> &rows,
+                        const std::vector<i64> &vinv, std::vector<i64> &optr, std::vector<i64> &oidx,
+                        std::vector<i64> *src) {
+  const i64 n = (i64)rows.size();
+  optr.assign(n + 1, 0);
+  for (i64 r = 0; r < n; ++r) optr[r + 1] = optr[r] + (ptr[rows[r] + 1] - ptr[rows[r]]);
+  oidx.resize(optr[n]);
+  if (src) src->resize(optr[n]);
+  parallel_for(n, [&](i64 r) {
+    i64 e = optr[r];
+    for (i64 a = ptr[rows[r]]; a < ptr[rows[r] + 1]; ++a, ++e) {
+      oidx[e] = vinv[idx[a]];
+      if (src) (*src)[e] = a;
+    }
+  });
+}
+
 // CSR from (key, value) pairs grouped by key in [0, n), values kept in input order (a
 // stable counting sort, as numpy's stable argsort of the keys)
 inline void group_csr(const std::vector<i64> &key, const std::vector<i64> &val, i64 n, std::vector<i64> &ptr,
@@ -118,17 +176,9 @@ inline void ragged_union(i64 nrows, const std::vector<i64> &row_items_ptr, const
     }
   };
   std::vector<i64> cnt(nrows);
-  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  const i64 nthreads = nrows >= (i64)1 << 16 ? (i64)hw : 1;
+  const i64 nthreads = pool_size(nrows, (i64)1 << 16);
   std::vector<std::vector<i64>> parts(nthreads);
-  if (nthreads == 1) {
-    rows(0, nrows, cnt.data(), parts[0]);
-  } else {
-    std::vector<std::thread> pool;
-    for (i64 t = 0; t < nthreads; ++t)
-      pool.emplace_back([&, t] { rows(nrows * t / nthreads, nrows * (t + 1) / nthreads, cnt.data(), parts[t]); });
-    for (auto &th : pool) th.join();
-  }
+  run_ranges(nthreads, nrows, [&](i64 t, i64 r0, i64 r1) { rows(r0, r1, cnt.data(), parts[t]); });
   ptr.assign(nrows + 1, 0);
   for (i64 r = 0; r < nrows; ++r) ptr[r + 1] = ptr[r] + cnt[r];
   idx.clear();
@@ -151,7 +201,7 @@ inline void sell32(const std::vector<i64> &ptr, const std::vector<i64> &idx, con
   }
   out.assign(g64[ng], -1);
   outv.assign(vals ? g64[ng] : 0, 0.0);
-  for (i64 g = 0; g < ng; ++g) {
+  parallel_for(ng, [&](i64 g) {
     const i64 len = (g64[g + 1] - g64[g]) / 32;
     for (i64 l = 0; l < 32; ++l) {
       const i64 r = 32 * g + l;
@@ -167,7 +217,7 @@ inline void sell32(const std::vector<i64> &ptr, const std::vector<i64> &idx, con
         }
       }
     }
-  }
+  });
   for (i64 g = 0; g <= ng; ++g) gptr[g] = (i32)g64[g];
 }
 
@@ -253,15 +303,7 @@ inline void sell32_aligned(const std::vector<i64> &ptr, const std::vector<i64> &
       }
     }
   };
-  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  const i64 nthreads = ng >= 2048 ? (i64)hw : 1;
-  if (nthreads == 1) {
-    warps(0, ng);
-  } else {
-    std::vector<std::thread> pool;
-    for (i64 t = 0; t < nthreads; ++t) pool.emplace_back([&, t] { warps(ng * t / nthreads, ng * (t + 1) / nthreads); });
-    for (auto &th : pool) th.join();
-  }
+  run_ranges(pool_size(ng, 2048), ng, [&](i64, i64 g0, i64 g1) { warps(g0, g1); });
   gptr.assign(ng + 1, 0);
   for (i64 g = 0; g <= ng; ++g) gptr[g] = (i32)g64[g];
 }

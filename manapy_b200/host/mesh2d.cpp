@@ -42,13 +42,13 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
 
   // ---- cell centre and volume
   std::vector<double> cx(nc), cy(nc), vol(nc);
-  for (i64 c = 0; c < nc; ++c) {
+  parallel_for(nc, [&](i64 c) {
     const double x1 = X(node(c, 0)), x2 = X(node(c, 1)), x3 = X(node(c, 2));
     const double y1 = Y(node(c, 0)), y2 = Y(node(c, 1)), y3 = Y(node(c, 2));
     cx[c] = 1.0 / 3 * (x1 + x2 + x3);
     cy[c] = 1.0 / 3 * (y1 + y2 + y3);
     vol[c] = 0.5 * std::fabs((x1 - x2) * (y1 - y3) - (x1 - x3) * (y1 - y2));
-  }
+  });
   // ---- node -> cells, cell -> vertex neighbours
   std::vector<i64> flat_nodes(3 * nc), flat_cells(3 * nc), c2n_ptr(nc + 1);
   for (i64 c = 0; c < nc; ++c)
@@ -110,20 +110,20 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   const i64 nf = (i64)fa.size();
   // face neighbours, compacted (boundary faces skipped)
   std::vector<i64> cellfid(3 * nc, -1);
-  for (i64 c = 0; c < nc; ++c) {
+  parallel_for(nc, [&](i64 c) {
     int k = 0;
     for (int j = 0; j < 3; ++j) {
       const i64 f = inv[3 * c + j];
       if (f1[f] == -1) continue;
       cellfid[3 * c + k++] = f0[f] == c ? f1[f] : f0[f];
     }
-  }
+  });
   // ---- names, normals, areas, centres
   std::vector<i32> namen(nn);
   for (i64 n = 0; n < nn; ++n) namen[n] = (i32)vx[4 * n + 3];
   std::vector<i32> name(nf, 0);
   std::vector<double> nx(nf), ny(nf), nz(nf), mes(nf), fcx(nf), fcy(nf), fcz(nf);
-  for (i64 f = 0; f < nf; ++f) {
+  parallel_for(nf, [&](i64 f) {
     if (f1[f] == -1) {
       const i32 a = namen[fa[f]], b = namen[fb[f]];
       i32 r = 100;
@@ -142,15 +142,16 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     ny[f] = flip ? -1 * n1 : n1;
     nz[f] = flip ? -1 * 0.0 : 0.0;
     mes[f] = std::sqrt(nx[f] * nx[f] + ny[f] * ny[f]);
+  });
+  for (i64 f = 0; f < nf; ++f)
     if (f1[f] == -1 && (name[f] >= 100 || name[f] == 0)) {
       res->error = "mesh has boundary faces that match no boundary side (manapy names them 100/200 and "
                    "leaves them out of every face list)";
       return res;
     }
-  }
   // outward normal of each local face (cells.nf)
   std::vector<double> cnf(9 * nc);
-  for (i64 c = 0; c < nc; ++c)
+  parallel_for(nc, [&](i64 c) {
     for (int j = 0; j < 3; ++j) {
       const i64 f = inv[3 * c + j];
       const double s = (cx[c] - fcx[f]) * nx[f] + (cy[c] - fcy[f]) * ny[f] + (0.0 - fcz[f]) * nz[f];
@@ -159,6 +160,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       cnf[9 * c + 3 * j + 1] = keep ? ny[f] : -1.0 * ny[f];
       cnf[9 * c + 3 * j + 2] = keep ? nz[f] : -1.0 * nz[f];
     }
+  });
   // ---- face lists (manapy numbering)
   std::vector<i64> lists[5];
   std::vector<i64> bfaces;
@@ -168,7 +170,8 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   }
   // ---- ghost centres
   std::vector<double> gc(3 * nf, -1.0);
-  for (i64 f : bfaces) {
+  parallel_for((i64)bfaces.size(), [&](i64 i) {
+    const i64 f = bfaces[i];
     const double x1x = X(fb[f]), x1y = Y(fb[f]), x2x = X(fa[f]), x2y = Y(fa[f]);
     const double v1x = cx[f0[f]], v1y = cy[f0[f]];
     const double gamma = ((v1x - x2x) * (x1x - x2x) + (v1y - x2y) * (x1y - x2y)) /
@@ -177,7 +180,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     gc[3 * f] = 2 * kk0 + (-1 * v1x);
     gc[3 * f + 1] = 2 * kk1 + (-1 * v1y);
     gc[3 * f + 2] = gamma;
-  }
+  });
   // node -> boundary faces (ascending face), cell -> stencil ghosts
   std::vector<i64> gkey, gval;
   for (i64 f : bfaces) {
@@ -193,7 +196,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   // ---- centre -> vertex weights
   std::vector<double> lx(nn), ly(nn), Rx(nn), Ry(nn);
   std::vector<i64> number(nn);
-  for (i64 n = 0; n < nn; ++n) {
+  parallel_for(nn, [&](i64 n) {
     double xx = 0, yy = 0, xy = 0, sx = 0, sy = 0;
     auto acc = [&](double px, double py) {
       const double rx = px - X(n), ry = py - Y(n);
@@ -211,7 +214,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     Rx[n] = sx;
     Ry[n] = sy;
     number[n] = (n2c_ptr[n + 1] - n2c_ptr[n]) + (n2g_ptr[n + 1] - n2g_ptr[n]);
-  }
+  });
   auto alpha = [&](i64 n, double px, double py) {
     const double den = (double)number[n] + lx[n] * Rx[n] + ly[n] * Ry[n];
     const double xd = px - X(n), yd = py - Y(n);
@@ -226,7 +229,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     const double z0 = cx[K] - px, z1 = cy[K] - py;
     return std::sqrt(z0 * z0 + z1 * z1);
   };
-  for (i64 f = 0; f < nf; ++f) {
+  parallel_for(nf, [&](i64 f) {
     const bool inner = name[f] == 0;
     const double v1x = cx[f0[f]], v1y = cy[f0[f]];
     const double v2x = inner ? cx[f1[f]] : gc[3 * f], v2y = inner ? cy[f1[f]] : gc[3 * f + 1];
@@ -241,7 +244,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       dist[f] = proj(f0[f], f) + proj(f1[f], f);
     else if (name[f] >= 1 && name[f] <= 4)
       dist[f] = 2 * proj(f0[f], f);
-  }
+  });
 
   // ---- locality numbering
   std::vector<i64> cperm(nc), fperm(nf), nperm(nn);
@@ -254,10 +257,10 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     const double sp0 = std::max(hi0 - lo0, 1e-300), sp1 = std::max(hi1 - lo1, 1e-300);
     const double scale = (double)((1 << 20) - 1);
     std::vector<uint64_t> mk(nc);
-    for (i64 c = 0; c < nc; ++c) {
+    parallel_for(nc, [&](i64 c) {
       const i64 q0 = (i64)std::floor((cx[c] - lo0) / sp0 * scale), q1 = (i64)std::floor((cy[c] - lo1) / sp1 * scale);
       mk[c] = part1by1((uint64_t)q0) | (part1by1((uint64_t)q1) << 1);
-    }
+    });
     cperm = stable_argsort(mk);
   } else {
     std::iota(cperm.begin(), cperm.end(), 0);
@@ -266,18 +269,23 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   for (i64 k = 0; k < nc; ++k) cinv[cperm[k]] = k;
   if (reorder) {
     std::vector<i64> lo(nf), hi(nf);
-    for (i64 f = 0; f < nf; ++f) {
+    parallel_for(nf, [&](i64 f) {
       const i64 a = cinv[f0[f]], b = f1[f] >= 0 ? cinv[f1[f]] : a;
       lo[f] = std::min(a, b);
       hi[f] = std::max(a, b);
-    }
-    std::iota(fperm.begin(), fperm.end(), 0);
-    std::stable_sort(fperm.begin(), fperm.end(),
-                     [&](i64 a, i64 b) { return lo[a] < lo[b] || (lo[a] == lo[b] && hi[a] < hi[b]); });
-    std::vector<i64> first(nn, INT64_MAX);
-    for (i64 n = 0; n < nn; ++n)
+    });
+    // stable order of (lo, hi): by hi, then stably by lo
+    const std::vector<i64> byhi = counting_argsort(hi, nc);
+    std::vector<i64> lo2(nf);
+    for (i64 k = 0; k < nf; ++k) lo2[k] = lo[byhi[k]];
+    const std::vector<i64> bylo = counting_argsort(lo2, nc);
+    for (i64 k = 0; k < nf; ++k) fperm[k] = byhi[bylo[k]];
+    // nodes by their first cell (nodes in no cell last)
+    std::vector<i64> first(nn, nc);
+    parallel_for(nn, [&](i64 n) {
       for (i64 a = n2c_ptr[n]; a < n2c_ptr[n + 1]; ++a) first[n] = std::min(first[n], cinv[n2c_idx[a]]);
-    nperm = stable_argsort(first);
+    });
+    nperm = counting_argsort(first, nc + 1);
   } else {
     std::iota(fperm.begin(), fperm.end(), 0);
     std::iota(nperm.begin(), nperm.end(), 0);
@@ -286,36 +294,28 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   for (i64 k = 0; k < nf; ++k) finv[fperm[k]] = k;
   for (i64 k = 0; k < nn; ++k) ninv[nperm[k]] = k;
 
-  // relabelled CSR: rows in `rows` order, values mapped, entry order kept
   auto relabel = [](const std::vector<i64> &ptr, const std::vector<i64> &idx, const std::vector<i64> &rows,
                     const std::vector<i64> &vinv, std::vector<i64> &optr, std::vector<i64> &oidx,
-                    std::vector<i64> *src) {
-    optr.assign(rows.size() + 1, 0);
-    oidx.clear();
-    if (src) src->clear();
-    for (size_t r = 0; r < rows.size(); ++r) {
-      for (i64 a = ptr[rows[r]]; a < ptr[rows[r] + 1]; ++a) {
-        oidx.push_back(vinv[idx[a]]);
-        if (src) src->push_back(a);
-      }
-      optr[r + 1] = (i64)oidx.size();
-    }
+                    std::vector<i64> *src) { relabel_csr(ptr, idx, rows, vinv, optr, oidx, src); };
+  auto to32 = [](const std::vector<i64> &v) {
+    std::vector<i32> o(v.size());
+    parallel_for((i64)v.size(), [&](i64 i) { o[i] = (i32)v[i]; });
+    return o;
   };
-  auto to32 = [](const std::vector<i64> &v) { return std::vector<i32>(v.begin(), v.end()); };
 
   // ---- device tables
   {
     std::vector<double> t(3 * nc);
-    for (i64 k = 0; k < nc; ++k) { t[3 * k] = cx[cperm[k]]; t[3 * k + 1] = cy[cperm[k]]; t[3 * k + 2] = 0.0; }
+    parallel_for(nc, [&](i64 k) { t[3 * k] = cx[cperm[k]]; t[3 * k + 1] = cy[cperm[k]]; t[3 * k + 2] = 0.0; });
     res->add("cell_center", 'd', {nc, 3}, t);
     std::vector<double> v(nc);
-    for (i64 k = 0; k < nc; ++k) v[k] = vol[cperm[k]];
+    parallel_for(nc, [&](i64 k) { v[k] = vol[cperm[k]]; });
     res->add("cell_volume", 'd', {nc}, v);
   }
   {
     std::vector<i32> cf(4 * nc, -1);
     std::vector<uint8_t> code(nc);
-    for (i64 k = 0; k < nc; ++k) {
+    parallel_for(nc, [&](i64 k) {
       const i64 c = cperm[k];
       i64 fo[3];
       for (int j = 0; j < 3; ++j) { fo[j] = inv[3 * c + j]; cf[4 * k + j] = (i32)finv[fo[j]]; }
@@ -324,7 +324,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       if (fo[o[2]] < fo[o[1]]) std::swap(o[1], o[2]);
       if (fo[o[1]] < fo[o[0]]) std::swap(o[0], o[1]);
       code[k] = (uint8_t)(o[0] | (o[1] << 2) | (o[2] << 4));
-    }
+    });
     res->add("cell_faces", 'i', {nc, 4}, cf);
     res->add("cell_order", 'b', {nc}, code);
   }
@@ -346,7 +346,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     std::vector<i32> cid(2 * nf), fn(4 * nf, -1), nm(nf);
     std::vector<double> nrm(3 * nf), fc(3 * nf), ms(nf), g(3 * nf), a(nf), F(8 * nf), d(nf);
     std::vector<float> nm32(4 * nf, 0.f);
-    for (i64 k = 0; k < nf; ++k) {
+    parallel_for(nf, [&](i64 k) {
       const i64 f = fperm[k];
       cid[2 * k] = (i32)cinv[f0[f]];
       cid[2 * k + 1] = f1[f] >= 0 ? (i32)cinv[f1[f]] : -1;
@@ -363,7 +363,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       a[k] = air[f];
       for (int c = 0; c < 8; ++c) F[8 * k + c] = ff[8 * f + c];
       d[k] = dist[f];
-    }
+    });
     res->add("face_cellid", 'i', {nf, 2}, cid);
     res->add("face_nodeid", 'i', {nf, 4}, fn);
     res->add("face_name", 'i', {nf}, nm);
@@ -380,13 +380,13 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     std::vector<i64> p, ix, src;
     relabel(n2c_ptr, n2c_idx, nperm, cinv, p, ix, &src);
     std::vector<double> al(ix.size());
-    for (i64 r = 0; r < nn; ++r) {  // row r of the new table is node nperm[r]
+    parallel_for(nn, [&](i64 r) {  // row r of the new table is node nperm[r]
       const i64 n = nperm[r];
       for (i64 e = p[r]; e < p[r + 1]; ++e) {
         const i64 c = n2c_idx[src[e]];
         al[e] = alpha(n, cx[c], cy[c]);
       }
-    }
+    });
     res->add("n2c_ptr", 'i', {nn + 1}, to32(p));
     res->add("n2c_idx", 'i', {(i64)ix.size()}, to32(ix));
     res->add("n2c_alpha", 'd', {(i64)al.size()}, al);
@@ -400,13 +400,13 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     res->add("n2c_sell_alpha_f32", 'f', {(i64)gv32.size()}, gv32);
     relabel(n2g_ptr, n2g_idx, nperm, finv, p, ix, &src);
     std::vector<double> ag(ix.size());
-    for (i64 r = 0; r < nn; ++r) {
+    parallel_for(nn, [&](i64 r) {
       const i64 n = nperm[r];
       for (i64 e = p[r]; e < p[r + 1]; ++e) {
         const i64 f = n2g_idx[src[e]];
         ag[e] = alpha(n, gc[3 * f], gc[3 * f + 1]);
       }
-    }
+    });
     res->add("n2g_ptr", 'i', {nn + 1}, to32(p));
     res->add("n2g_idx", 'i', {(i64)ix.size()}, to32(ix));
     res->add("n2g_alpha", 'd', {(i64)ag.size()}, ag);
@@ -415,7 +415,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     std::vector<i32> cf(4 * nc, -1), vtx(4 * nc, 0), nbr(4 * nc, -1);
     std::vector<uint32_t> flags(nc, 0);
     std::vector<double> nf_(9 * nc), v1(2 * nc), xy(2 * nc), ncoord(2 * nn);
-    for (i64 k = 0; k < nc; ++k) {
+    parallel_for(nc, [&](i64 k) {
       const i64 c = cperm[k];
       for (int j = 0; j < 3; ++j) {
         const i64 o = cellfid[3 * c + j];
@@ -443,8 +443,8 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
               ((uint32_t)nfneg << (9 + j));
       }
       flags[k] = fl;
-    }
-    for (i64 r = 0; r < nn; ++r) { ncoord[2 * r] = X(nperm[r]); ncoord[2 * r + 1] = Y(nperm[r]); }
+    });
+    parallel_for(nn, [&](i64 r) { ncoord[2 * r] = X(nperm[r]); ncoord[2 * r + 1] = Y(nperm[r]); });
     res->add("cell_cellfid", 'i', {nc, 4}, cf);
     res->add("cell_nf", 'd', {nc, 3, 3}, nf_);
     res->add("cell_vertex1", 'd', {nc, 2}, v1);
