@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
@@ -39,10 +40,15 @@ struct Result {
   }
 };
 
-// Host threads for n independent items: up to 16, one below min_n items.
+// Host threads for n independent items: up to 16 (or MANAPY_B200_HOST_THREADS, for a process
+// that shares the cores with others), one below min_n items.
 inline i64 pool_size(i64 n, i64 min_n) {
-  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  return n >= min_n ? std::max<i64>(1, std::min<i64>((i64)hw, n)) : 1;
+  i64 cap = (i64)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (const char *env = std::getenv("MANAPY_B200_HOST_THREADS")) {
+    const long v = std::strtol(env, nullptr, 10);
+    if (v > 0) cap = v;
+  }
+  return n >= min_n ? std::max<i64>(1, std::min<i64>(cap, n)) : 1;
 }
 
 // fn(t, i0, i1) for t < nt over the contiguous ranges [n t / nt, n (t+1) / nt), each on its

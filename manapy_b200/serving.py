@@ -25,9 +25,14 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import dataclasses
+import functools
 import math
 import multiprocessing as mp
 import os
+import pickle
+import queue
+import tempfile
+import threading
 import time
 
 import numpy as np
@@ -50,6 +55,7 @@ class Request:
     uy: float = 0.0
     D: float = 0.0
     ratio: float = 2.0    # dam-break height ratio (left / right)
+    prep_window: tuple = None  # (start, end) of its preparation, time.perf_counter() of the worker
 
     @property
     def cells(self):
@@ -131,6 +137,7 @@ def prepare(req, precision="fp32c"):
     (as host arrays), boundary rules and the initial state in the device numbering."""
     from . import boundary as B, meshgen
     from .device import DeviceBC, DeviceMesh
+    t_start = time.perf_counter()
     el, vx = meshgen.square_triangles(req.n, seed=req.seed)
     dm = DeviceMesh.from_native(el, vx)       # the native host builder (C++)
     A = dm.A
@@ -142,7 +149,84 @@ def prepare(req, precision="fp32c"):
         bc.resolved = None
     init = [a[dm.R.cperm] for a in initial_state(req, A["cells_center"])]
     dm.strip()
+    req = dataclasses.replace(req, prep_window=(t_start, time.perf_counter()))
     return req, dm, bc, init
+
+
+# Prepared requests cross from the workers in shared memory: the pickle stream of the
+# (req, mesh, bc, init) tuple keeps only a header of each numpy array (protocol 5, buffers
+# out of band), the buffers go to one file on a tmpfs, and the serving process reads the file
+# back in one read.  Through the pool's result pipe a 500k-cell mesh's ~200 MB took about a
+# quarter of a second and held up every other result behind it.
+_SHM_DIR = "/dev/shm"
+_ALIGN = 64
+
+
+@dataclasses.dataclass
+class _Shipped:
+    path: str
+    head: bytes
+    sizes: list
+
+
+def _ship(obj):
+    """Worker side: ``obj`` with its array buffers moved to a file in shared memory, or
+    ``obj`` itself when no tmpfs with room for them is there."""
+    bufs = []
+    head = pickle.dumps(obj, protocol=5, buffer_callback=bufs.append)
+    raws = [b.raw() for b in bufs]
+    sizes = [r.nbytes for r in raws]
+    total = sum(-(-n // _ALIGN) * _ALIGN for n in sizes)
+    path = None
+    try:
+        st = os.statvfs(_SHM_DIR)
+        if st.f_bavail * st.f_frsize < 2 * total + (256 << 20):
+            return obj
+        fd, path = tempfile.mkstemp(prefix="manapy_b200_prep_", dir=_SHM_DIR)
+        with os.fdopen(fd, "wb") as f:
+            for r in raws:
+                f.write(r)
+                pad = -r.nbytes % _ALIGN
+                if pad:
+                    f.write(bytes(pad))
+    except OSError:
+        if path is not None and os.path.exists(path):
+            os.unlink(path)
+        return obj
+    return _Shipped(path, head, sizes)
+
+
+def _receive(x):
+    """Serving side of ``_ship``: the object rebuilt on one read of its buffer file (the
+    arrays are views of that read, each 64-byte aligned), the file removed."""
+    if not isinstance(x, _Shipped):
+        return x
+    total = sum(-(-n // _ALIGN) * _ALIGN for n in x.sizes)
+    raw = np.empty(total + _ALIGN, dtype=np.uint8)
+    start = -raw.ctypes.data % _ALIGN
+    data = raw[start:start + total]
+    try:
+        with open(x.path, "rb", buffering=0) as f:
+            got = f.readinto(memoryview(data))
+    finally:
+        os.unlink(x.path)
+    if got != total:
+        raise RuntimeError("prepared request %s: short read (%d of %d bytes)" % (x.path, got, total))
+    views, off = [], 0
+    for n in x.sizes:
+        views.append(memoryview(data[off:off + n]))
+        off += -(-n // _ALIGN) * _ALIGN
+    return pickle.loads(x.head, buffers=views)
+
+
+def prepare_shipped(req, precision="fp32c"):
+    """``prepare`` in a worker process, its result handed back through shared memory."""
+    return _ship(prepare(req, precision))
+
+
+def _init_worker(host_threads):
+    """Worker initialiser: the thread count of the native builder in this process."""
+    os.environ["MANAPY_B200_HOST_THREADS"] = str(int(host_threads))
 
 
 def _warm(_):
@@ -284,11 +368,16 @@ class BatchServer:
     ``max_active``: slots; ``chunk``: steps per graph replay between admission points;
     ``workers``: host processes preparing meshes (0: prepare in this process);
     ``precision``: "fp32c" (FP32 state with compensated sums, the serving default) or "fp64"
-    (manapy's plain arithmetic, each result bit-identical to the single-mesh FP64 solver).
+    (manapy's plain arithmetic, each result bit-identical to the single-mesh FP64 solver);
+    ``host_threads``: native-builder threads per worker (default: host cores / workers);
+    ``poll``: a dispatcher thread hands each request to the workers at its arrival, and the
+    serving loop polls the device while two chunks are queued instead of blocking on the
+    older one, so that meshes prepared meanwhile are admitted at once (False: requests are
+    handed over and admitted only between chunks).
     """
 
     def __init__(self, device="cuda:0", hbm_budget=40e9, max_active=256, chunk=16, workers=None,
-                 graphs=True, precision="fp32c"):
+                 graphs=True, precision="fp32c", host_threads=None, poll=True):
         if precision not in ("fp32c", "fp64"):
             raise ValueError("precision must be 'fp32c' or 'fp64'")
         self.precision = precision
@@ -297,7 +386,11 @@ class BatchServer:
         self.max_active = int(max_active)
         self.chunk = int(chunk)
         self.graphs = bool(graphs)
+        self.poll = bool(poll)
         self.workers = (os.cpu_count() or 1) if workers is None else int(workers)
+        # native-builder threads per preparation process: the host cores shared out
+        self.host_threads = (max(1, (os.cpu_count() or 1) // max(1, self.workers)) if host_threads is None
+                             else int(host_threads))
         self.stream = torch.cuda.Stream(device=self.dev)
         self.upload_stream = torch.cuda.Stream(device=self.dev)
         # one step counter per family: [advection-diffusion, shallow water]
@@ -315,7 +408,8 @@ class BatchServer:
     def start_pool(self):
         """Start the mesh-preparation worker processes (and load their modules) ahead of a run."""
         if self.workers > 0 and self.pool is None:
-            self.pool = cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn"))
+            self.pool = cf.ProcessPoolExecutor(max_workers=self.workers, mp_context=mp.get_context("spawn"),
+                                               initializer=_init_worker, initargs=(self.host_threads,))
             list(self.pool.map(_warm, range(self.workers)))
         return self
 
@@ -451,7 +545,8 @@ class BatchServer:
         if self.workers > 0:
             own = self.pool is None
             self.start_pool()
-            prepared = list(self.pool.map(prepare, requests, [self.precision] * len(requests)))
+            prepared = [_receive(x) for x in
+                        self.pool.map(prepare_shipped, requests, [self.precision] * len(requests))]
             if own:
                 self.stop_pool()
         else:
@@ -496,21 +591,47 @@ class BatchServer:
         done = []
         pending_done = []      # (event, slots)
         t0 = time.perf_counter()
+        self._t0, self._t_sub, self._t_recv = t0, {}, {}
         used = 0.0
+        arrived = queue.SimpleQueue()   # (rid, future) of finished preparations
+        n_recv = 0
+        stop = threading.Event()
+        dispatcher = None
+        if pool is not None and self.poll:
+            def dispatch():
+                for r in reqs:
+                    while (wait := r.arrival - (time.perf_counter() - t0)) > 0:
+                        if stop.wait(wait):
+                            return
+                    self._t_sub[r.rid] = time.perf_counter() - t0
+                    fut = pool.submit(prepare_shipped, r, self.precision)
+                    fut.add_done_callback(functools.partial(self._arrived, arrived, r.rid))
+            dispatcher = threading.Thread(target=dispatch, daemon=True)
+            dispatcher.start()
+            nxt = len(reqs)
         try:
             while len(done) < len(reqs):
                 now = time.perf_counter() - t0
                 # hand arrived requests to the preparation pool
                 while nxt < len(reqs) and reqs[nxt].arrival <= now:
                     r = reqs[nxt]
+                    self._t_sub[r.rid] = time.perf_counter() - t0
                     if pool is not None:
-                        futures[r.rid] = pool.submit(prepare, r, self.precision)
+                        futures[r.rid] = pool.submit(prepare_shipped, r, self.precision)
                     else:
                         prepared.append(prepare(r, self.precision))
                     nxt += 1
                 ta = time.perf_counter()
                 for rid in [k for k, f in futures.items() if f.done()]:
-                    prepared.append(futures.pop(rid).result())
+                    prepared.append(_receive(futures.pop(rid).result()))
+                    self._t_recv[rid] = time.perf_counter() - t0
+                while not arrived.empty():
+                    rid, item, err = arrived.get()
+                    if err is not None:
+                        raise err
+                    prepared.append(item)
+                    self._t_recv[rid] = time.perf_counter() - t0
+                    n_recv += 1
                 prepared.sort(key=lambda x: x[0].arrival)
                 tb = time.perf_counter()
                 st["receive"] += tb - ta
@@ -537,7 +658,8 @@ class BatchServer:
                 td = time.perf_counter()
                 st["retable"] += td - tc
                 if not self.active:
-                    if nxt >= len(reqs) and not futures and not prepared and not pending_done:
+                    if (nxt >= len(reqs) and not futures and not prepared and not pending_done
+                            and (dispatcher is None or n_recv == len(reqs))):
                         break
                     used -= self._complete(pending_done, done, t0, keep_results, log)
                     time.sleep(0.002)
@@ -545,6 +667,14 @@ class BatchServer:
                     continue
                 # keep at most two chunks queued on the device, so that admissions and
                 # retirements take effect within about one chunk
+                if self.poll:
+                    while inflight and inflight[0].query():
+                        inflight.pop(0)
+                    if len(inflight) >= 2:
+                        used -= self._complete(pending_done, done, t0, keep_results, log)
+                        time.sleep(0.0002)
+                        st["throttle"] += time.perf_counter() - td
+                        continue
                 while len(inflight) >= 2:
                     inflight.pop(0).synchronize()
                 te = time.perf_counter()
@@ -577,9 +707,21 @@ class BatchServer:
             torch.cuda.synchronize(self.dev)
             used -= self._complete(pending_done, done, t0, keep_results, log)
         finally:
+            stop.set()
+            if dispatcher is not None:
+                dispatcher.join()
             if own_pool:
                 self.stop_pool()
         return done
+
+    @staticmethod
+    def _arrived(out, rid, fut):
+        """Done-callback of a preparation (on the pool's thread): the request read back from
+        shared memory, or the error, queued for the serving loop."""
+        try:
+            out.put((rid, _receive(fut.result()), None))
+        except BaseException as e:  # handed to the serving loop, which raises it
+            out.put((rid, None, e))
 
     def _retable(self):
         """New item tables and block maps for the current active set (the old ones stay
@@ -603,6 +745,11 @@ class BatchServer:
                 rec = {"rid": s.req.rid, "kind": s.req.kind, "cells": s.dm.nbcells, "steps": s.req.steps,
                        "arrival": s.req.arrival, "admitted": s.admitted, "done": tdone,
                        "latency": tdone - s.req.arrival}
+                # the preparation's course: handed to the pool, run in a worker, back in this process
+                rec["submitted"] = self._t_sub.get(s.req.rid)
+                if s.req.prep_window is not None:
+                    rec["prep_start"], rec["prep_end"] = (x - self._t0 for x in s.req.prep_window)
+                rec["received"] = self._t_recv.get(s.req.rid, rec["submitted"])
                 if keep_results:
                     inv = np.asarray(s.dm.inv["cell"])
                     rec["result"] = [x.numpy()[inv] for x in o]

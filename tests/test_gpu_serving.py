@@ -51,14 +51,18 @@ def test_staggered_admission_and_worker_pool(cuda):
     for k, r in enumerate(reqs):
         r.arrival = 0.05 * k
     staggered = _by_rid(BatchServer(workers=2, chunk=4, max_active=3).serve(reqs, keep_results=True))
+    blocking = _by_rid(BatchServer(workers=2, chunk=4, max_active=3, poll=False).serve(reqs, keep_results=True))
     for r in reqs:
         r.arrival = 0.0
     at_once = _by_rid(BatchServer(workers=0, chunk=16).serve(reqs, keep_results=True))
     for r in reqs:
-        for a, b in zip(staggered[r.rid]["result"], at_once[r.rid]["result"]):
-            assert np.array_equal(a, b), r
-        rec = staggered[r.rid]
-        assert rec["done"] >= rec["admitted"] >= 0 and rec["latency"] > 0
+        for a, b, c in zip(staggered[r.rid]["result"], at_once[r.rid]["result"], blocking[r.rid]["result"]):
+            assert np.array_equal(a, b) and np.array_equal(c, b), r
+        for rec in (staggered[r.rid], blocking[r.rid]):
+            assert rec["done"] >= rec["admitted"] >= 0 and rec["latency"] > 0
+            # handed over at arrival or later, prepared in a worker, received, then admitted
+            assert rec["arrival"] <= rec["submitted"] <= rec["prep_start"] <= rec["prep_end"] <= rec["received"]
+            assert rec["received"] <= rec["admitted"]
 
 
 def test_batched_equals_the_single_mesh_solver_and_the_oracle(cuda):

@@ -1,6 +1,10 @@
-"""Host side of the serving loop, on the CPU: the seeded request stream and the per-request
-preparation a worker process runs (native tables, boundary rules, initial state)."""
+"""Host side of the serving loop, on the CPU: the seeded request stream, the per-request
+preparation a worker process runs (native tables, boundary rules, initial state), and its
+hand-over back to the serving process through shared memory."""
+import os
+
 import numpy as np
+import pytest
 
 from manapy_b200 import serving as SV
 from manapy_b200.device import DeviceMesh
@@ -57,7 +61,6 @@ def test_batched_items_are_checked_for_the_tables_their_step_reads():
     """The batched kernels read mesh tables through pointers held in device memory, which no
     kernel can check: the server checks each item on the host.  A mesh prepared for the FP32c
     batches lacks the FP64 centre->vertex weights of the FP64 batches."""
-    import pytest
     for kind in ("advdiff", "sw"):
         req = SV.Request(rid=0, kind=kind, n=10, seed=5, steps=10, ux=0.3, uy=0.1, D=1e-3)
         for prec in ("fp32c", "fp64"):
@@ -67,3 +70,45 @@ def test_batched_items_are_checked_for_the_tables_their_step_reads():
         if kind == "advdiff":
             with pytest.raises(ValueError, match="n2c_sell_alpha"):
                 SV.check_item_tables(kind, "fp64", _struct_of(dm32))
+
+def _arrays(obj, path="x"):
+    """Every numpy array reachable from obj, by path."""
+    if isinstance(obj, np.ndarray):
+        return {path: obj}
+    out = {}
+    if isinstance(obj, (list, tuple)):
+        for i, v in enumerate(obj):
+            out.update(_arrays(v, "%s[%d]" % (path, i)))
+    elif isinstance(obj, dict):
+        for k, v in obj.items():
+            out.update(_arrays(v, "%s.%s" % (path, k)))
+    elif hasattr(obj, "__dict__") and not isinstance(obj, type):
+        out.update(_arrays(vars(obj), path))
+    return out
+
+
+@pytest.mark.skipif(not os.path.isdir(SV._SHM_DIR), reason="no tmpfs at /dev/shm")
+@pytest.mark.parametrize("kind_seed", [3, 4])
+def test_prepared_request_crosses_shared_memory(kind_seed):
+    req = SV.make_requests(1, 0.0, seed=kind_seed, cells=(3e3, 6e3))[0]
+    a = SV.prepare(req)
+    x = SV._ship(a)
+    assert isinstance(x, SV._Shipped) and os.path.exists(x.path) and len(x.head) < 16384
+    b = SV._receive(x)
+    assert not os.path.exists(x.path)
+    aa, bb = _arrays(a), _arrays(b)
+    assert aa.keys() == bb.keys() and len(aa) > 30
+    for k in aa:
+        assert aa[k].dtype == bb[k].dtype and aa[k].shape == bb[k].shape, k
+        assert np.array_equal(aa[k], bb[k], equal_nan=True), k
+        if bb[k].nbytes:
+            assert bb[k].ctypes.data % 64 == 0, k
+    assert b[0].prep_window is not None and b[0].rid == req.rid
+
+
+def test_hand_over_without_tmpfs(monkeypatch, tmp_path):
+    monkeypatch.setattr(SV, "_SHM_DIR", str(tmp_path / "absent"))
+    req = SV.make_requests(1, 0.0, seed=5, cells=(2e3, 3e3))[0]
+    a = SV.prepare(req)
+    assert SV._ship(a) is a
+    assert SV._receive(a) is a
