@@ -267,7 +267,7 @@ __device__ __forceinline__ double sw2c_cell_body(const mb_mesh &m, const SWState
 #define MB_SW2C_CELL_MIN_BLOCKS 4
 #endif
 #ifndef MB_SW2C_BATCH_CELL_MIN_BLOCKS
-#define MB_SW2C_BATCH_CELL_MIN_BLOCKS 1
+#define MB_SW2C_BATCH_CELL_MIN_BLOCKS 4
 #endif
 
 __global__ void __launch_bounds__(kBlock, MB_SW2C_CELL_MIN_BLOCKS) k_sw2c_cell(mb_mesh m, SWStateF s, SWOutF out, const float *ff,
