@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(kP2B[VAR], kP2M[VAR]) k_f2_phase2(mb_mesh m, m
 // ping-pong state and skips items outside their [start_step, end_step) window.
 
 #ifndef MB_P2_BATCH_MIN_BLOCKS
-#define MB_P2_BATCH_MIN_BLOCKS 3
+#define MB_P2_BATCH_MIN_BLOCKS 4
 #endif
 
 template <bool ORDER2, bool DIFF>

@@ -131,7 +131,7 @@ __device__ __forceinline__ void node_value_f32(const mb_mesh &m, const GhostRule
 #define MB_P2C_BLOCK 128   // threads per block of the single-mesh phase 2 (batches: kBlock)
 #endif
 #ifndef MB_P2C_BATCH_MIN_BLOCKS
-#define MB_P2C_BATCH_MIN_BLOCKS 4
+#define MB_P2C_BATCH_MIN_BLOCKS 5
 #endif
 #ifndef MB_P2C_MIN_BLOCKS
 #define MB_P2C_MIN_BLOCKS 7
