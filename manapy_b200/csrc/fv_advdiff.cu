@@ -767,9 +767,12 @@ __global__ void __launch_bounds__(kP2B[VAR], kP2M[VAR]) k_f2_phase2(mb_mesh m, m
 #ifndef MB_P2_BATCH_MIN_BLOCKS
 #define MB_P2_BATCH_MIN_BLOCKS 4
 #endif
+#ifndef MB_P1_BATCH_MIN_BLOCKS
+#define MB_P1_BATCH_MIN_BLOCKS MB_P1_MIN_BLOCKS
+#endif
 
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P1_MIN_BLOCKS)
+__global__ void __launch_bounds__(kBlock, MB_P1_BATCH_MIN_BLOCKS)
     k_f2_batch_phase1(const mb_advdiff_item_f64 *__restrict__ items, const int32_t *__restrict__ map,
                       const int32_t *__restrict__ clock) {
   const mb_advdiff_item_f64 &it = items[map[blockIdx.x]];

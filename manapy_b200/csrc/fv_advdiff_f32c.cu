@@ -365,8 +365,11 @@ __global__ void __launch_bounds__(MB_P2C_BLOCK, MB_P2C_MIN_BLOCKS)
 
 __device__ __forceinline__ bool item_active(int t, int start, int end) { return t >= start && t < end; }
 
+#ifndef MB_P1C_BATCH_MIN_BLOCKS
+#define MB_P1C_BATCH_MIN_BLOCKS 8
+#endif
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_P1C_MIN_BLOCKS)
+__global__ void __launch_bounds__(kBlock, MB_P1C_BATCH_MIN_BLOCKS)
     k_f2c_batch_phase1(const mb_advdiff_item *__restrict__ items, const int32_t *__restrict__ map,
                        const int32_t *__restrict__ clock) {
   const mb_advdiff_item &it = items[map[blockIdx.x]];

@@ -219,8 +219,11 @@ def _receive(x):
     return pickle.loads(x.head, buffers=views)
 
 
-def prepare_shipped(req, precision="fp32c"):
-    """``prepare`` in a worker process, its result handed back through shared memory."""
+def prepare_shipped(req, precision="fp32c", host_threads=None):
+    """``prepare`` in a worker process (its native builder on ``host_threads`` threads when
+    given), its result handed back through shared memory."""
+    if host_threads is not None:
+        os.environ["MANAPY_B200_HOST_THREADS"] = str(max(1, int(host_threads)))
     return _ship(prepare(req, precision))
 
 
@@ -369,7 +372,9 @@ class BatchServer:
     ``workers``: host processes preparing meshes (0: prepare in this process);
     ``precision``: "fp32c" (FP32 state with compensated sums, the serving default) or "fp64"
     (manapy's plain arithmetic, each result bit-identical to the single-mesh FP64 solver);
-    ``host_threads``: native-builder threads per worker (default: host cores / workers);
+    ``host_threads``: native-builder threads per worker; default: with ``poll``, the host cores
+    shared among the preparations in flight when a request is handed over (one when many
+    are), else host cores / workers;
     ``poll``: a dispatcher thread hands each request to the workers at its arrival, and the
     serving loop polls the device while two chunks are queued instead of blocking on the
     older one, so that meshes prepared meanwhile are admitted at once (False: requests are
@@ -389,7 +394,9 @@ class BatchServer:
         self.poll = bool(poll)
         self.workers = (os.cpu_count() or 1) if workers is None else int(workers)
         # native-builder threads per preparation process: the host cores shared out
-        self.host_threads = (max(1, (os.cpu_count() or 1) // max(1, self.workers)) if host_threads is None
+        self.cores = os.cpu_count() or 1
+        self.adaptive_threads = host_threads is None
+        self.host_threads = (max(1, self.cores // max(1, self.workers)) if host_threads is None
                              else int(host_threads))
         self.stream = torch.cuda.Stream(device=self.dev)
         self.upload_stream = torch.cuda.Stream(device=self.dev)
@@ -603,8 +610,12 @@ class BatchServer:
                     while (wait := r.arrival - (time.perf_counter() - t0)) > 0:
                         if stop.wait(wait):
                             return
+                    threads = None
+                    if self.adaptive_threads:
+                        busy = len(self._t_sub) - n_recv + 1    # preparations in flight, this one included
+                        threads = max(1, self.cores // busy)
                     self._t_sub[r.rid] = time.perf_counter() - t0
-                    fut = pool.submit(prepare_shipped, r, self.precision)
+                    fut = pool.submit(prepare_shipped, r, self.precision, threads)
                     fut.add_done_callback(functools.partial(self._arrived, arrived, r.rid))
             dispatcher = threading.Thread(target=dispatch, daemon=True)
             dispatcher.start()
