@@ -814,7 +814,10 @@ __global__ void __launch_bounds__(MB_SW_FLUX_BLOCK, MB_SW_FLUX_MIN_BLOCKS)
   sw2_flux_face<false, MB_SW_FAST>(it.m, s, it.grav, it.face_flux, f);
 }
 
-__global__ void __launch_bounds__(kBlock, MB_SW_CELL_MIN_BLOCKS)
+#ifndef MB_SW_BATCH_CELL_MIN_BLOCKS
+#define MB_SW_BATCH_CELL_MIN_BLOCKS MB_SW_CELL_MIN_BLOCKS
+#endif
+__global__ void __launch_bounds__(kBlock, MB_SW_BATCH_CELL_MIN_BLOCKS)
     k_sw2_batch_cell(const mb_sw_item_f64 *__restrict__ items, const int32_t *__restrict__ map,
                      const int32_t *__restrict__ clock) {
   const mb_sw_item_f64 &it = items[map[blockIdx.x]];
