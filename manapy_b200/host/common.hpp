@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -18,25 +19,59 @@ namespace mbh {
 using i32 = int32_t;
 using i64 = int64_t;
 
+// An allocator whose value-less construct() leaves scalars uninitialised: a vector sized
+// with it is not zero-filled, so the (parallel) loop that fills it is the first to touch
+// its pages.
+template <class T>
+struct NoInit : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInit<U>;
+  };
+  NoInit() = default;
+  template <class U>
+  NoInit(const NoInit<U> &) {}
+  template <class U>
+  void construct(U *p) noexcept {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using uvec = std::vector<T, NoInit<T>>;
+
 struct Table {
   std::string name;
   char dtype;  // 'i' int32, 'l' int64, 'd' float64, 'f' float32, 'b' uint8
   std::vector<i64> shape;
-  std::vector<unsigned char> bytes;
+  std::shared_ptr<void> owner;  // the storage of the table's bytes
+  const void *data = nullptr;
+  size_t nbytes = 0;
 };
 
 struct Result {
   std::vector<Table> tables;
   std::string error;
-  template <class T>
-  void add(const std::string &name, char dt, std::vector<i64> shape, const std::vector<T> &v) {
+  // the table takes over v's storage (no copy)
+  template <class T, class A>
+  void add(const std::string &name, char dt, std::vector<i64> shape, std::vector<T, A> &&v) {
+    auto held = std::make_shared<std::vector<T, A>>(std::move(v));
     Table t;
     t.name = name;
     t.dtype = dt;
     t.shape = std::move(shape);
-    t.bytes.resize(v.size() * sizeof(T));
-    if (!v.empty()) std::memcpy(t.bytes.data(), v.data(), t.bytes.size());
+    t.data = held->data();
+    t.nbytes = held->size() * sizeof(T);
+    t.owner = std::move(held);
     tables.push_back(std::move(t));
+  }
+  // a table of a vector that the builder still uses: copied
+  template <class T, class A>
+  void add(const std::string &name, char dt, std::vector<i64> shape, const std::vector<T, A> &v) {
+    add(name, dt, std::move(shape), std::vector<T, A>(v));
   }
 };
 

@@ -298,35 +298,36 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
                     const std::vector<i64> &vinv, std::vector<i64> &optr, std::vector<i64> &oidx,
                     std::vector<i64> *src) { relabel_csr(ptr, idx, rows, vinv, optr, oidx, src); };
   auto to32 = [](const std::vector<i64> &v) {
-    std::vector<i32> o(v.size());
+    uvec<i32> o(v.size());
     parallel_for((i64)v.size(), [&](i64 i) { o[i] = (i32)v[i]; });
     return o;
   };
 
   // ---- device tables
   {
-    std::vector<double> t(3 * nc);
+    uvec<double> t(3 * nc);
     parallel_for(nc, [&](i64 k) { t[3 * k] = cx[cperm[k]]; t[3 * k + 1] = cy[cperm[k]]; t[3 * k + 2] = 0.0; });
-    res->add("cell_center", 'd', {nc, 3}, t);
-    std::vector<double> v(nc);
+    res->add("cell_center", 'd', {nc, 3}, std::move(t));
+    uvec<double> v(nc);
     parallel_for(nc, [&](i64 k) { v[k] = vol[cperm[k]]; });
-    res->add("cell_volume", 'd', {nc}, v);
+    res->add("cell_volume", 'd', {nc}, std::move(v));
   }
   {
-    std::vector<i32> cf(4 * nc, -1);
-    std::vector<uint8_t> code(nc);
+    uvec<i32> cf(4 * nc);
+    uvec<uint8_t> code(nc);
     parallel_for(nc, [&](i64 k) {
       const i64 c = cperm[k];
       i64 fo[3];
       for (int j = 0; j < 3; ++j) { fo[j] = inv[3 * c + j]; cf[4 * k + j] = (i32)finv[fo[j]]; }
+      cf[4 * k + 3] = -1;
       int o[3] = {0, 1, 2};  // stable order of the three face ids
       if (fo[o[1]] < fo[o[0]]) std::swap(o[0], o[1]);
       if (fo[o[2]] < fo[o[1]]) std::swap(o[1], o[2]);
       if (fo[o[1]] < fo[o[0]]) std::swap(o[0], o[1]);
       code[k] = (uint8_t)(o[0] | (o[1] << 2) | (o[2] << 4));
     });
-    res->add("cell_faces", 'i', {nc, 4}, cf);
-    res->add("cell_order", 'b', {nc}, code);
+    res->add("cell_faces", 'i', {nc, 4}, std::move(cf));
+    res->add("cell_order", 'b', {nc}, std::move(code));
   }
   {
     std::vector<i64> p, ix;
@@ -336,22 +337,24 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     std::vector<i32> gp, gi;
     std::vector<double> gv;
     sell32(p, ix, nullptr, false, gp, gi, gv);
-    res->add("lsq_sell_ptr", 'i', {(i64)gp.size()}, gp);
-    res->add("lsq_sell_idx", 'i', {(i64)gi.size()}, gi);
+    res->add("lsq_sell_ptr", 'i', {(i64)gp.size()}, std::move(gp));
+    res->add("lsq_sell_idx", 'i', {(i64)gi.size()}, std::move(gi));
     relabel(gnid_ptr, gnid_idx, cperm, finv, p, ix, nullptr);
     res->add("ghostnid_ptr", 'i', {nc + 1}, to32(p));
     res->add("ghostnid_idx", 'i', {(i64)ix.size()}, to32(ix));
   }
   {
-    std::vector<i32> cid(2 * nf), fn(4 * nf, -1), nm(nf);
-    std::vector<double> nrm(3 * nf), fc(3 * nf), ms(nf), g(3 * nf), a(nf), F(8 * nf), d(nf);
-    std::vector<float> nm32(4 * nf, 0.f);
+    uvec<i32> cid(2 * nf), fn(4 * nf), nm(nf);
+    uvec<double> nrm(3 * nf), fc(3 * nf), ms(nf), g(3 * nf), a(nf), F(8 * nf), d(nf);
+    uvec<float> nm32(4 * nf);
     parallel_for(nf, [&](i64 k) {
       const i64 f = fperm[k];
       cid[2 * k] = (i32)cinv[f0[f]];
       cid[2 * k + 1] = f1[f] >= 0 ? (i32)cinv[f1[f]] : -1;
       fn[4 * k] = (i32)ninv[fa[f]];
       fn[4 * k + 1] = (i32)ninv[fb[f]];
+      fn[4 * k + 2] = -1;
+      fn[4 * k + 3] = -1;
       nm[k] = name[f];
       nrm[3 * k] = nx[f]; nrm[3 * k + 1] = ny[f]; nrm[3 * k + 2] = nz[f];
       fc[3 * k] = fcx[f]; fc[3 * k + 1] = fcy[f]; fc[3 * k + 2] = fcz[f];
@@ -359,27 +362,28 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       nm32[4 * k] = (float)nx[f];
       nm32[4 * k + 1] = (float)ny[f];
       nm32[4 * k + 2] = (float)(1.0 / mes[f]);
+      nm32[4 * k + 3] = 0.f;
       for (int c = 0; c < 3; ++c) g[3 * k + c] = gc[3 * f + c];
       a[k] = air[f];
       for (int c = 0; c < 8; ++c) F[8 * k + c] = ff[8 * f + c];
       d[k] = dist[f];
     });
-    res->add("face_cellid", 'i', {nf, 2}, cid);
-    res->add("face_nodeid", 'i', {nf, 4}, fn);
-    res->add("face_name", 'i', {nf}, nm);
-    res->add("face_normal", 'd', {nf, 3}, nrm);
-    res->add("face_center", 'd', {nf, 3}, fc);
-    res->add("face_mesure", 'd', {nf}, ms);
-    res->add("face_nm_f32", 'f', {nf, 4}, nm32);
-    res->add("face_ghostcenter", 'd', {nf, 3}, g);
-    res->add("face_air", 'd', {nf}, a);
-    res->add("face_f", 'd', {nf, 8}, F);
-    res->add("face_dist", 'd', {nf}, d);
+    res->add("face_cellid", 'i', {nf, 2}, std::move(cid));
+    res->add("face_nodeid", 'i', {nf, 4}, std::move(fn));
+    res->add("face_name", 'i', {nf}, std::move(nm));
+    res->add("face_normal", 'd', {nf, 3}, std::move(nrm));
+    res->add("face_center", 'd', {nf, 3}, std::move(fc));
+    res->add("face_mesure", 'd', {nf}, std::move(ms));
+    res->add("face_nm_f32", 'f', {nf, 4}, std::move(nm32));
+    res->add("face_ghostcenter", 'd', {nf, 3}, std::move(g));
+    res->add("face_air", 'd', {nf}, std::move(a));
+    res->add("face_f", 'd', {nf, 8}, std::move(F));
+    res->add("face_dist", 'd', {nf}, std::move(d));
   }
   {
     std::vector<i64> p, ix, src;
     relabel(n2c_ptr, n2c_idx, nperm, cinv, p, ix, &src);
-    std::vector<double> al(ix.size());
+    uvec<double> al(ix.size());
     parallel_for(nn, [&](i64 r) {  // row r of the new table is node nperm[r]
       const i64 n = nperm[r];
       for (i64 e = p[r]; e < p[r + 1]; ++e) {
@@ -389,17 +393,19 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     });
     res->add("n2c_ptr", 'i', {nn + 1}, to32(p));
     res->add("n2c_idx", 'i', {(i64)ix.size()}, to32(ix));
-    res->add("n2c_alpha", 'd', {(i64)al.size()}, al);
+    std::vector<double> alv(al.begin(), al.end());
+    res->add("n2c_alpha", 'd', {(i64)al.size()}, std::move(al));
     std::vector<i32> gp, gi;
     std::vector<double> gv;
-    sell32(p, ix, &al, true, gp, gi, gv);
-    res->add("n2c_sell_ptr", 'i', {(i64)gp.size()}, gp);
-    res->add("n2c_sell_idx", 'i', {(i64)gi.size()}, gi);
-    res->add("n2c_sell_alpha", 'd', {(i64)gv.size()}, gv);
-    std::vector<float> gv32(gv.begin(), gv.end());
-    res->add("n2c_sell_alpha_f32", 'f', {(i64)gv32.size()}, gv32);
+    sell32(p, ix, &alv, true, gp, gi, gv);
+    uvec<float> gv32(gv.size());
+    parallel_for((i64)gv.size(), [&](i64 i) { gv32[i] = (float)gv[i]; });
+    res->add("n2c_sell_ptr", 'i', {(i64)gp.size()}, std::move(gp));
+    res->add("n2c_sell_idx", 'i', {(i64)gi.size()}, std::move(gi));
+    res->add("n2c_sell_alpha", 'd', {(i64)gv.size()}, std::move(gv));
+    res->add("n2c_sell_alpha_f32", 'f', {(i64)gv32.size()}, std::move(gv32));
     relabel(n2g_ptr, n2g_idx, nperm, finv, p, ix, &src);
-    std::vector<double> ag(ix.size());
+    uvec<double> ag(ix.size());
     parallel_for(nn, [&](i64 r) {
       const i64 n = nperm[r];
       for (i64 e = p[r]; e < p[r + 1]; ++e) {
@@ -409,14 +415,17 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     });
     res->add("n2g_ptr", 'i', {nn + 1}, to32(p));
     res->add("n2g_idx", 'i', {(i64)ix.size()}, to32(ix));
-    res->add("n2g_alpha", 'd', {(i64)ag.size()}, ag);
+    res->add("n2g_alpha", 'd', {(i64)ag.size()}, std::move(ag));
   }
   {
-    std::vector<i32> cf(4 * nc, -1), vtx(4 * nc, 0), nbr(4 * nc, -1);
-    std::vector<uint32_t> flags(nc, 0);
-    std::vector<double> nf_(9 * nc), v1(2 * nc), xy(2 * nc), ncoord(2 * nn);
+    uvec<i32> cf(4 * nc), vtx(4 * nc), nbr(4 * nc);
+    uvec<uint32_t> flags(nc);
+    uvec<double> nf_(9 * nc), v1(2 * nc), xy(2 * nc), ncoord(2 * nn);
     parallel_for(nc, [&](i64 k) {
       const i64 c = cperm[k];
+      cf[4 * k + 3] = -1;
+      vtx[4 * k + 3] = 0;
+      nbr[4 * k + 3] = -1;
       for (int j = 0; j < 3; ++j) {
         const i64 o = cellfid[3 * c + j];
         cf[4 * k + j] = (i32)(o >= 0 ? cinv[o] : cinv[nc - 1]);
@@ -445,14 +454,14 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       flags[k] = fl;
     });
     parallel_for(nn, [&](i64 r) { ncoord[2 * r] = X(nperm[r]); ncoord[2 * r + 1] = Y(nperm[r]); });
-    res->add("cell_cellfid", 'i', {nc, 4}, cf);
-    res->add("cell_nf", 'd', {nc, 3, 3}, nf_);
-    res->add("cell_vertex1", 'd', {nc, 2}, v1);
-    res->add("cell_vtx", 'i', {nc, 4}, vtx);
-    res->add("cell_nbr", 'i', {nc, 4}, nbr);
-    res->add("cell_flags", 'i', {nc}, flags);
-    res->add("node_coord", 'd', {nn, 2}, ncoord);
-    res->add("cell_xy", 'd', {nc, 2}, xy);
+    res->add("cell_cellfid", 'i', {nc, 4}, std::move(cf));
+    res->add("cell_nf", 'd', {nc, 3, 3}, std::move(nf_));
+    res->add("cell_vertex1", 'd', {nc, 2}, std::move(v1));
+    res->add("cell_vtx", 'i', {nc, 4}, std::move(vtx));
+    res->add("cell_nbr", 'i', {nc, 4}, std::move(nbr));
+    res->add("cell_flags", 'i', {nc}, std::move(flags));
+    res->add("node_coord", 'd', {nn, 2}, std::move(ncoord));
+    res->add("cell_xy", 'd', {nc, 2}, std::move(xy));
   }
   // permutations and the manapy-numbered arrays the boundary set-up reads
   res->add("perm_cell", 'l', {nc}, cperm);
@@ -597,7 +606,7 @@ int32_t mbh_info(void *h, int32_t k, const char **name, char *dtype, int64_t sha
   return (int32_t)t.shape.size();
 }
 
-const void *mbh_data(void *h, int32_t k) { return static_cast<Result *>(h)->tables[k].bytes.data(); }
+const void *mbh_data(void *h, int32_t k) { return static_cast<Result *>(h)->tables[k].data; }
 
 void mbh_free(void *h) { delete static_cast<Result *>(h); }
 
