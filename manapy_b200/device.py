@@ -291,9 +291,9 @@ class DeviceMesh:
         ``geometry.build`` (bit-identical too)."""
         from types import SimpleNamespace
         from . import native
-        T = native.tables2d(elements, vertex, reorder=reorder, full=full)
-        if stencil != "manapy":          # the builder writes the manapy layout
-            T["lsq_sell_ptr"], T["lsq_sell_idx"] = lsq_sell(T["cellnid_ptr"], T["cellnid_idx"], stencil)
+        if stencil not in STENCILS:
+            raise ValueError("stencil must be one of %s" % (STENCILS,))
+        T = native.tables2d(elements, vertex, reorder=reorder, full=full, stencil=stencil)
         self = cls.__new__(cls)
         self.stencil = stencil
         nc, nf, nn = len(T["cell_volume"]), len(T["face_name"]), len(T["node_coord"])

@@ -28,7 +28,7 @@ namespace {
 
 using namespace mbh;
 
-Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, bool full) {
+Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, bool full, bool shared) {
   auto *res = new Result();
   for (i64 c = 0; c < nc; ++c)
     if (el[4 * c + 3] != 3) {
@@ -336,7 +336,10 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     res->add("cellnid_idx", 'i', {(i64)ix.size()}, to32(ix));
     std::vector<i32> gp, gi;
     std::vector<double> gv;
-    sell32(p, ix, nullptr, false, gp, gi, gv);
+    if (shared)
+      sell32_aligned(p, ix, 0, gp, gi);  // the slot-shared layout
+    else
+      sell32(p, ix, nullptr, false, gp, gi, gv);  // manapy's order, -1 after each row
     res->add("lsq_sell_ptr", 'i', {(i64)gp.size()}, std::move(gp));
     res->add("lsq_sell_idx", 'i', {(i64)gi.size()}, std::move(gi));
     relabel(gnid_ptr, gnid_idx, cperm, finv, p, ix, nullptr);
@@ -562,11 +565,13 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
 
 extern "C" {
 
-// full != 0 also returns every array of geometry.build as "A.<name>" (manapy numbering)
+// full != 0 also returns every array of geometry.build as "A.<name>" (manapy numbering);
+// shared != 0 writes the least-squares stencil (lsq_sell_*) in the slot-shared SELL-32
+// layout of sell32_aligned, else in manapy's neighbour order
 void *mbh_build2d(const int32_t *elements, int64_t nbcells, const double *vertex, int64_t nbnodes, int32_t reorder,
-                  int32_t full) {
+                  int32_t full, int32_t shared) {
   if (!elements || !vertex || nbcells <= 0 || nbnodes <= 0) return nullptr;
-  return build2d(elements, nbcells, vertex, nbnodes, reorder != 0, full != 0);
+  return build2d(elements, nbcells, vertex, nbnodes, reorder != 0, full != 0, shared != 0);
 }
 
 // the slot-shared SELL-32 (sell32_aligned) of a CSR table: tables "gptr" and "idx"

@@ -28,7 +28,7 @@ def lib():
         L = ctypes.CDLL(HOST_OUT)
         L.mbh_build2d.restype = ctypes.c_void_p
         L.mbh_build2d.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
-                                  ctypes.c_int32]
+                                  ctypes.c_int32, ctypes.c_int32]
         L.mbh_error.restype = ctypes.c_char_p
         L.mbh_error.argtypes = [ctypes.c_void_p]
         L.mbh_count.restype = ctypes.c_int32
@@ -56,15 +56,20 @@ def available():
         return False
 
 
-def tables2d(elements, vertex, reorder=True, full=False):
+def tables2d(elements, vertex, reorder=True, full=False, stencil="manapy"):
     """dict name -> numpy array (see ``host/mesh2d.cpp``); raises ValueError on a bad mesh.
-    ``full``: also every array of ``geometry.build`` as ``"A.<name>"``."""
+    ``full``: also every array of ``geometry.build`` as ``"A.<name>"``; ``stencil``: the
+    layout of ``lsq_sell_*``, ``"manapy"`` (manapy's neighbour order) or ``"shared"`` (the
+    slot-shared layout of ``sell_aligned``)."""
+    if stencil not in ("manapy", "shared"):
+        raise ValueError("stencil must be 'manapy' or 'shared'")
     el = np.ascontiguousarray(elements, dtype=np.int32)
     vx = np.ascontiguousarray(vertex, dtype=np.float64)
     if el.ndim != 2 or el.shape[1] != 4 or vx.ndim != 2 or vx.shape[1] != 4:
         raise ValueError("expected elements [nc, 4] and vertex [nn, 4]")
     L = lib()
-    h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)), int(bool(full)))
+    h = L.mbh_build2d(el.ctypes.data, len(el), vx.ctypes.data, len(vx), int(bool(reorder)), int(bool(full)),
+                      int(stencil == "shared"))
     if not h:
         raise ValueError("empty mesh")
     return _read(L, h)

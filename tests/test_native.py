@@ -98,3 +98,21 @@ def test_native_3d_rejects_untagged_boundaries_like_the_python_builder():
         native.geometry3d(el, vx)
     with pytest.raises(ValueError, match="match no boundary side"):
         M.Domain(dim=3, mesh=(el, vx))
+
+
+def test_native_builder_writes_either_stencil_layout():
+    """The builder's slot-shared stencil equals the layout ``lsq_sell`` forms from its own
+    vertex-neighbour tables; every other table does not depend on the layout."""
+    from manapy_b200 import native
+    el, vx = meshgen.square_triangles(60, seed=8)
+    a = native.tables2d(el, vx, stencil="shared")
+    b = native.tables2d(el, vx)
+    gp, gi = D.lsq_sell(b["cellnid_ptr"], b["cellnid_idx"], "shared")
+    assert np.array_equal(a["lsq_sell_ptr"], gp) and np.array_equal(a["lsq_sell_idx"], gi)
+    mp, mi = D.lsq_sell(b["cellnid_ptr"], b["cellnid_idx"], "manapy")
+    assert np.array_equal(b["lsq_sell_ptr"], mp) and np.array_equal(b["lsq_sell_idx"], mi)
+    for k in a:
+        if not k.startswith("lsq_sell"):
+            assert np.array_equal(a[k], b[k]), k
+    with pytest.raises(ValueError):
+        native.tables2d(el, vx, stencil="sorted")
