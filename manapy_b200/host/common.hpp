@@ -359,6 +359,31 @@ inline uint64_t part1by1(uint64_t v) {
   return v;
 }
 
+// Stable argsort of unsigned keys: LSD radix passes of 11 bits up to the largest key's top
+// bit (each pass a stable counting sort), the same order as a stable comparison sort.
+inline std::vector<i64> radix_argsort(const std::vector<uint64_t> &key) {
+  const i64 n = (i64)key.size();
+  uint64_t top = 0;
+  for (uint64_t k : key) top |= k;
+  int bits = 0;
+  while (bits < 64 && (top >> bits)) ++bits;
+  std::vector<i64> o(n), tmp(n);
+  std::iota(o.begin(), o.end(), 0);
+  constexpr int D = 11;
+  std::vector<i64> cnt((1 << D) + 1);
+  for (int sh = 0; sh < bits; sh += D) {
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (i64 e = 0; e < n; ++e) cnt[((key[e] >> sh) & ((1u << D) - 1)) + 1]++;
+    for (int d = 0; d < (1 << D); ++d) cnt[d + 1] += cnt[d];
+    for (i64 e = 0; e < n; ++e) {
+      const i64 x = o[e];
+      tmp[cnt[(key[x] >> sh) & ((1u << D) - 1)]++] = x;
+    }
+    o.swap(tmp);
+  }
+  return o;
+}
+
 template <class K>
 inline std::vector<i64> stable_argsort(const std::vector<K> &key) {
   std::vector<i64> o(key.size());

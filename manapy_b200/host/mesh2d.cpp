@@ -65,7 +65,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   // ---- faces: descending node pairs, numbered by ascending key
   static const int LOC[3][2] = {{0, 1}, {1, 2}, {2, 0}};
   std::vector<i64> key(3 * nc), pa(3 * nc), pb(3 * nc);
-  for (i64 c = 0; c < nc; ++c)
+  parallel_for(nc, [&](i64 c) {
     for (int j = 0; j < 3; ++j) {
       i64 a = node(c, LOC[j][0]), b = node(c, LOC[j][1]);
       if (a < b) std::swap(a, b);
@@ -73,6 +73,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       pb[3 * c + j] = b;
       key[3 * c + j] = a * nn + b;
     }
+  });
   // stable order of the keys (a, b): two counting-sort passes, by b then by a
   std::vector<i64> ord(3 * nc);
   {
@@ -150,7 +151,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       return res;
     }
   // outward normal of each local face (cells.nf)
-  std::vector<double> cnf(9 * nc);
+  uvec<double> cnf(9 * nc);
   parallel_for(nc, [&](i64 c) {
     for (int j = 0; j < 3; ++j) {
       const i64 f = inv[3 * c + j];
@@ -221,7 +222,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     return (1. + lx[n] * xd + ly[n] * yd) / den;
   };
   // ---- diamond vectors and areas, orthogonal distances
-  std::vector<double> ff(8 * nf), air(nf), dist(nf, 0.0);
+  uvec<double> ff(8 * nf), air(nf), dist(nf);
   auto proj = [&](i64 K, i64 f) {
     const double vx_ = cx[K] - fcx[f], vy_ = cy[K] - fcy[f];
     const double s = vx_ * nx[f] + vy_ * ny[f];
@@ -244,6 +245,8 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       dist[f] = proj(f0[f], f) + proj(f1[f], f);
     else if (name[f] >= 1 && name[f] <= 4)
       dist[f] = 2 * proj(f0[f], f);
+    else
+      dist[f] = 0.0;
   });
 
   // ---- locality numbering
@@ -261,7 +264,7 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       const i64 q0 = (i64)std::floor((cx[c] - lo0) / sp0 * scale), q1 = (i64)std::floor((cy[c] - lo1) / sp1 * scale);
       mk[c] = part1by1((uint64_t)q0) | (part1by1((uint64_t)q1) << 1);
     });
-    cperm = stable_argsort(mk);
+    cperm = radix_argsort(mk);
   } else {
     std::iota(cperm.begin(), cperm.end(), 0);
   }
@@ -474,11 +477,11 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
   res->add("inv_face", 'l', {nf}, finv);
   res->add("inv_node", 'l', {nn}, ninv);
   {
-    std::vector<double> fc(3 * nf), cc(3 * nc);
-    for (i64 f = 0; f < nf; ++f) { fc[3 * f] = fcx[f]; fc[3 * f + 1] = fcy[f]; fc[3 * f + 2] = fcz[f]; }
-    for (i64 c = 0; c < nc; ++c) { cc[3 * c] = cx[c]; cc[3 * c + 1] = cy[c]; cc[3 * c + 2] = 0.0; }
-    res->add("A.faces_center", 'd', {nf, 3}, fc);
-    res->add("A.cells_center", 'd', {nc, 3}, cc);
+    uvec<double> fc(3 * nf), cc(3 * nc);
+    parallel_for(nf, [&](i64 f) { fc[3 * f] = fcx[f]; fc[3 * f + 1] = fcy[f]; fc[3 * f + 2] = fcz[f]; });
+    parallel_for(nc, [&](i64 c) { cc[3 * c] = cx[c]; cc[3 * c + 1] = cy[c]; cc[3 * c + 2] = 0.0; });
+    res->add("A.faces_center", 'd', {nf, 3}, std::move(fc));
+    res->add("A.cells_center", 'd', {nc, 3}, std::move(cc));
     static const char *LN[5] = {"A.innerfaces", "A.infaces", "A.outfaces", "A.upperfaces", "A.bottomfaces"};
     for (int t = 0; t < 5; ++t) res->add(LN[t], 'i', {(i64)lists[t].size()}, to32(lists[t]));
   }
