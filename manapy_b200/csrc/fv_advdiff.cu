@@ -1024,11 +1024,8 @@ __global__ void __launch_bounds__(kBlock) k_lsq_matrix3(mb_mesh m, double *__res
 
 // vertex blocks [0, nnb): the vertex's sums and (DIFF) its centre->vertex value; edge blocks:
 // the edge's sums.  Records {P, Q} (32 bytes).
-#ifndef MB_F3_SUMS_MIN_BLOCKS
-#define MB_F3_SUMS_MIN_BLOCKS 1
-#endif
 template <bool DIFF>
-__global__ void __launch_bounds__(kBlock, MB_F3_SUMS_MIN_BLOCKS) k_f3_sums(mb_mesh m, mb_bc bc, const double *__restrict__ w,
+__global__ void __launch_bounds__(kBlock) k_f3_sums(mb_mesh m, mb_bc bc, const double *__restrict__ w,
                                                     const double *__restrict__ rows, double *__restrict__ nrec,
                                                     double *__restrict__ erec, double *__restrict__ wn, int nnb) {
   const int lane = threadIdx.x & 31;
