@@ -110,12 +110,50 @@ inline void parallel_for(i64 n, F &&fn) {
   });
 }
 
+// out = the elements of `in` (or 0, 1, ... when in is null) in stable order of digit[e] in
+// [0, n): a counting sort.  Large inputs are counted and scattered by host threads, each over
+// a contiguous range of the input, from per-thread offsets (digit-major, then thread), so
+// the order is the serial one.
+inline void stable_by_digit(const std::vector<i64> &digit, const std::vector<i64> *in, i64 m, i64 n,
+                            std::vector<i64> &out) {
+  out.resize(m);
+  auto elem = [&](i64 e) { return in ? (*in)[e] : e; };
+  const i64 nt = std::min<i64>(pool_size(m, (i64)1 << 18), std::max<i64>(1, m / std::max<i64>(n, 1)));
+  if (nt <= 1) {
+    std::vector<i64> pos(n + 1, 0);
+    for (i64 e = 0; e < m; ++e) pos[digit[elem(e)] + 1]++;
+    for (i64 d = 0; d < n; ++d) pos[d + 1] += pos[d];
+    for (i64 e = 0; e < m; ++e) {
+      const i64 x = elem(e);
+      out[pos[digit[x]]++] = x;
+    }
+    return;
+  }
+  std::vector<i64> cnt(nt * n, 0);  // cnt[t * n + d]
+  run_ranges(nt, m, [&](i64 t, i64 e0, i64 e1) {
+    i64 *c = &cnt[t * n];
+    for (i64 e = e0; e < e1; ++e) c[digit[elem(e)]]++;
+  });
+  i64 run = 0;
+  for (i64 d = 0; d < n; ++d)
+    for (i64 t = 0; t < nt; ++t) {
+      const i64 c = cnt[t * n + d];
+      cnt[t * n + d] = run;
+      run += c;
+    }
+  run_ranges(nt, m, [&](i64 t, i64 e0, i64 e1) {
+    i64 *c = &cnt[t * n];
+    for (i64 e = e0; e < e1; ++e) {
+      const i64 x = elem(e);
+      out[c[digit[x]]++] = x;
+    }
+  });
+}
+
 // Stable argsort of integer keys in [0, n): a counting sort (equal keys keep their order).
 inline std::vector<i64> counting_argsort(const std::vector<i64> &key, i64 n) {
-  std::vector<i64> pos(n + 1, 0), o(key.size());
-  for (i64 k : key) pos[k + 1]++;
-  for (i64 i = 0; i < n; ++i) pos[i + 1] += pos[i];
-  for (size_t e = 0; e < key.size(); ++e) o[pos[key[e]]++] = (i64)e;
+  std::vector<i64> o;
+  stable_by_digit(key, nullptr, (i64)key.size(), n, o);
   return o;
 }
 
@@ -145,9 +183,10 @@ inline void group_csr(const std::vector<i64> &key, const std::vector<i64> &val, 
   ptr.assign(n + 1, 0);
   for (i64 k : key) ptr[k + 1]++;
   for (i64 i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+  std::vector<i64> order;
+  stable_by_digit(key, nullptr, (i64)key.size(), n, order);
   idx.resize(key.size());
-  std::vector<i64> pos(ptr.begin(), ptr.end() - 1);
-  for (size_t e = 0; e < key.size(); ++e) idx[pos[key[e]]++] = val[e];
+  parallel_for((i64)key.size(), [&](i64 e) { idx[e] = val[order[e]]; });
 }
 
 // for each row r: sorted unique union of the lists of its items (CSR), optionally without r.

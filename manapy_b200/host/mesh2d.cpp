@@ -75,19 +75,11 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
     }
   });
   // stable order of the keys (a, b): two counting-sort passes, by b then by a
-  std::vector<i64> ord(3 * nc);
+  std::vector<i64> ord;
   {
-    std::vector<i64> tmp(3 * nc), cnt(nn + 1);
-    auto pass = [&](const std::vector<i64> &digit, const std::vector<i64> &in, std::vector<i64> &out) {
-      std::fill(cnt.begin(), cnt.end(), 0);
-      for (i64 e : in) cnt[digit[e] + 1]++;
-      for (i64 d = 0; d < nn; ++d) cnt[d + 1] += cnt[d];
-      for (i64 e : in) out[cnt[digit[e]]++] = e;
-    };
-    std::vector<i64> id(3 * nc);
-    std::iota(id.begin(), id.end(), 0);
-    pass(pb, id, tmp);
-    pass(pa, tmp, ord);
+    std::vector<i64> tmp;
+    stable_by_digit(pb, nullptr, 3 * nc, nn, tmp);
+    stable_by_digit(pa, &tmp, 3 * nc, nn, ord);
   }
   std::vector<i64> inv(3 * nc);
   std::vector<i64> fa, fb;  // face nodes (descending)
@@ -278,11 +270,9 @@ Result *build2d(const i32 *el, i64 nc, const double *vx, i64 nn, bool reorder, b
       hi[f] = std::max(a, b);
     });
     // stable order of (lo, hi): by hi, then stably by lo
-    const std::vector<i64> byhi = counting_argsort(hi, nc);
-    std::vector<i64> lo2(nf);
-    for (i64 k = 0; k < nf; ++k) lo2[k] = lo[byhi[k]];
-    const std::vector<i64> bylo = counting_argsort(lo2, nc);
-    for (i64 k = 0; k < nf; ++k) fperm[k] = byhi[bylo[k]];
+    std::vector<i64> byhi;
+    stable_by_digit(hi, nullptr, nf, nc, byhi);
+    stable_by_digit(lo, &byhi, nf, nc, fperm);
     // nodes by their first cell (nodes in no cell last)
     std::vector<i64> first(nn, nc);
     parallel_for(nn, [&](i64 n) {
