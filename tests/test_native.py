@@ -116,3 +116,19 @@ def test_native_builder_writes_either_stencil_layout():
             assert np.array_equal(a[k], b[k]), k
     with pytest.raises(ValueError):
         native.tables2d(el, vx, stencil="sorted")
+
+
+def test_native_builder_threads_do_not_change_the_tables(monkeypatch):
+    """Every threaded path of the builder (per-element loops, unions, the SELL layouts, the
+    counting sorts, which switch to threads above 2^18 entries) gives the bytes of the
+    one-thread build."""
+    from manapy_b200 import native
+    el, vx = meshgen.square_triangles(230, seed=12)          # 105,800 triangles
+    monkeypatch.setenv("MANAPY_B200_HOST_THREADS", "1")
+    one = native.tables2d(el, vx, stencil="shared", full=True)
+    monkeypatch.setenv("MANAPY_B200_HOST_THREADS", "7")
+    many = native.tables2d(el, vx, stencil="shared", full=True)
+    assert one.keys() == many.keys()
+    for k in one:
+        assert one[k].dtype == many[k].dtype and one[k].shape == many[k].shape, k
+        assert one[k].tobytes() == many[k].tobytes(), k
