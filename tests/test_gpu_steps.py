@@ -553,3 +553,37 @@ def test_edge_sums_step_equals_the_stencil_step(order, cuda):
     assert dm.cell_scratch_size() == 8 * nc + 4 * (nn + dm.nbedges)
     assert rel_max(runs[1], runs[0]) < 1e-13
     assert not np.array_equal(runs[0], U.H(w0))
+
+
+def test_pinned_uploads_between_steps_match_host_arrays(cuda):
+    """manapy's driver loop with the face velocities uploaded from pinned host memory every
+    step and the state fetched into pinned memory gives the bits of the same loop fed numpy
+    arrays."""
+    import torch
+    wl = W.C2.scaled(n=40)
+    el, vx = wl.mesh()
+    runs = []
+    for pinned in (False, True):
+        dom = M.Domain(dim=2, mesh=(el, vx))
+        w = M.Variable(domain=dom, BC=wl.bc, values=wl.bc_values)
+        u, v = M.Variable(domain=dom), M.Variable(domain=dom)
+        uf, vf, _ = wl.velocity(dom.faces.center)
+        w.cell = wl.init(dom.cells.center)
+        S = M.AdvectionDiffusionSolver(w, vel=(u, v), conf=M.Struct(Dxx=5e-4, Dyy=5e-4, order=2, cfl=0.8))
+        out = torch.empty(int(dom.nbcells), dtype=torch.float64, pin_memory=True)
+        states = []
+        for k in range(6):
+            a, b = (1.0 + 0.1 * k) * uf, (1.0 - 0.05 * k) * vf     # a new velocity every step
+            if pinned:
+                pa, pb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
+                u.face, v.face = pa, pb
+            else:
+                u.face, v.face = a, b
+            u.interpolate_facetocell(); v.interpolate_facetocell()
+            S.stepper(); S.compute_fluxes(); S.compute_new_val()
+            w.fetch("cell", out=out)
+            torch.cuda.synchronize()
+            states.append(out.numpy().copy())
+        runs.append(states)
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
