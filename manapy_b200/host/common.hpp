@@ -320,11 +320,13 @@ inline void sell32_aligned(const std::vector<i64> &ptr, const std::vector<i64> &
     for (i64 r = 32 * g; r < std::min(n, 32 * g + 32); ++r) len = std::max(len, ptr[r + 1] - ptr[r]);
     g64[g + 1] = g64[g] + 32 * (len + (len ? slack : 0));
   }
-  out.assign(g64[ng], -1);
+  out.resize(g64[ng]);
   auto warps = [&](i64 g0, i64 g1) {
     std::vector<std::pair<i64, int>> pairs;        // (value, row in warp)
     std::vector<std::pair<i64, uint32_t>> els;     // (value, rows mask)
+    std::vector<std::pair<std::pair<i64, int>, uint32_t>> keyed;
     std::vector<uint32_t> occ;
+    std::fill(out.begin() + g64[g0], out.begin() + g64[g1], -1);   // this range's slots, empty
     for (i64 g = g0; g < g1; ++g) {
       const i64 L = (g64[g + 1] - g64[g]) / 32;
       if (!L) continue;
@@ -334,8 +336,7 @@ inline void sell32_aligned(const std::vector<i64> &ptr, const std::vector<i64> &
       std::sort(pairs.begin(), pairs.end());
       // a value repeated within one row counts as distinct values (its k-th copies grouped)
       els.clear();
-      std::vector<std::pair<std::pair<i64, int>, uint32_t>> keyed;
-      keyed.reserve(pairs.size());
+      keyed.clear();
       for (size_t a = 0; a < pairs.size();) {
         size_t b = a;
         while (b < pairs.size() && pairs[b].first == pairs[a].first) ++b;
