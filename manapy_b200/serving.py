@@ -219,6 +219,14 @@ def _receive(x):
     return pickle.loads(x.head, buffers=views)
 
 
+def _discard(fut):
+    """Done-callback of a preparation nobody will admit: its shared-memory file removed."""
+    try:
+        _receive(fut.result())
+    except BaseException:  # a failed or cancelled preparation left no file
+        pass
+
+
 def prepare_shipped(req, precision="fp32c", host_threads=None):
     """``prepare`` in a worker process (its native builder on ``host_threads`` threads when
     given), its result handed back through shared memory."""
@@ -721,6 +729,11 @@ class BatchServer:
             stop.set()
             if dispatcher is not None:
                 dispatcher.join()
+            # preparations that were never received (an error ended the loop): their
+            # shared-memory files are removed as they finish
+            for f in futures.values():
+                if not f.cancel():
+                    f.add_done_callback(_discard)
             if own_pool:
                 self.stop_pool()
         return done

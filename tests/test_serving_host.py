@@ -112,3 +112,17 @@ def test_hand_over_without_tmpfs(monkeypatch, tmp_path):
     a = SV.prepare(req)
     assert SV._ship(a) is a
     assert SV._receive(a) is a
+
+
+@pytest.mark.skipif(not os.path.isdir(SV._SHM_DIR), reason="no tmpfs at /dev/shm")
+def test_unreceived_preparation_leaves_no_file():
+    """A preparation that nobody admits (the serving loop ended by an error) has its
+    shared-memory file removed when it finishes."""
+    import concurrent.futures as cf
+    req = SV.make_requests(1, 0.0, seed=6, cells=(2e3, 3e3))[0]
+    with cf.ThreadPoolExecutor(1) as ex:
+        fut = ex.submit(SV.prepare_shipped, req)
+        x = fut.result()
+        assert isinstance(x, SV._Shipped) and os.path.exists(x.path)
+        fut.add_done_callback(SV._discard)     # runs at once: the future is done
+    assert not os.path.exists(x.path)
