@@ -235,6 +235,26 @@ def prepare_shipped(req, precision="fp32c", host_threads=None):
     return _ship(prepare(req, precision))
 
 
+def admission_order(waiting, used, budget, slots, active, now, max_skip_wait=1.0):
+    """Which prepared requests to admit now, as indices into ``waiting`` in the order to admit
+    them.  ``waiting``: (ready time, estimated device bytes) of the prepared requests in
+    arrival order; ``used``: bytes the admitted requests hold; ``slots``: free slots;
+    ``active``: admitted requests.  Arrival order, except that a request that does not fit
+    in the budget lets later ones that fit pass it until it has been ready for
+    ``max_skip_wait`` seconds; from then on nothing passes it (0: strict arrival order).
+    With nothing admitted, the first request goes in even if it alone exceeds the budget."""
+    out = []
+    for k, (ready, est) in enumerate(waiting):
+        if len(out) >= slots:
+            break
+        if used + est <= budget or (active == 0 and not out):
+            out.append(k)
+            used += est
+        elif now - ready >= max_skip_wait:
+            break
+    return out
+
+
 def _init_worker(host_threads):
     """Worker initialiser: the thread count of the native builder in this process."""
     os.environ["MANAPY_B200_HOST_THREADS"] = str(int(host_threads))
@@ -383,6 +403,8 @@ class BatchServer:
     ``host_threads``: native-builder threads per worker; default: with ``poll``, the host cores
     shared among the preparations in flight when a request is handed over (one when many
     are), else host cores / workers;
+    ``max_skip_wait``: seconds a prepared request that does not fit in the HBM budget lets
+    later ones that fit pass it (``admission_order``; 0: strict arrival order);
     ``poll``: a dispatcher thread hands each request to the workers at its arrival, and the
     serving loop polls the device while two chunks are queued instead of blocking on the
     older one, so that meshes prepared meanwhile are admitted at once (False: requests are
@@ -390,7 +412,7 @@ class BatchServer:
     """
 
     def __init__(self, device="cuda:0", hbm_budget=40e9, max_active=256, chunk=16, workers=None,
-                 graphs=True, precision="fp32c", host_threads=None, poll=True):
+                 graphs=True, precision="fp32c", host_threads=None, poll=True, max_skip_wait=1.0):
         if precision not in ("fp32c", "fp64"):
             raise ValueError("precision must be 'fp32c' or 'fp64'")
         self.precision = precision
@@ -400,6 +422,7 @@ class BatchServer:
         self.chunk = int(chunk)
         self.graphs = bool(graphs)
         self.poll = bool(poll)
+        self.max_skip_wait = float(max_skip_wait)
         self.workers = (os.cpu_count() or 1) if workers is None else int(workers)
         # native-builder threads per preparation process: the host cores shared out
         self.cores = os.cpu_count() or 1
@@ -654,14 +677,20 @@ class BatchServer:
                 prepared.sort(key=lambda x: x[0].arrival)
                 tb = time.perf_counter()
                 st["receive"] += tb - ta
-                # admission (between steps): FIFO while a slot and the budget allow
+                # admission (between steps): arrival order while a slot and the budget
+                # allow, smaller requests passing one that does not fit for a while
                 changed = False
-                while prepared and len(self.active) < self.max_active:
-                    req, dm, bc, init = prepared[0]
-                    est = dm.nbytes() + 48.0 * dm.nbcells + 16.0 * dm.nbfaces
-                    if used + est > self.budget and self.active:
-                        break
-                    prepared.pop(0)
+                picks = []
+                if prepared and len(self.active) < self.max_active:
+                    waiting = [(self._t_recv.get(x[0].rid, x[0].arrival),
+                                x[1].nbytes() + 48.0 * x[1].nbcells + 16.0 * x[1].nbfaces) for x in prepared]
+                    picks = admission_order(waiting, used, self.budget, self.max_active - len(self.active),
+                                            len(self.active), time.perf_counter() - t0, self.max_skip_wait)
+                chosen = [prepared[k] for k in picks]
+                if picks:
+                    taken = set(picks)
+                    prepared = [x for k, x in enumerate(prepared) if k not in taken]
+                for req, dm, bc, init in chosen:
                     slot = self._admit(req, dm, bc, init)
                     slot.admitted = time.perf_counter() - t0
                     slot.fam = 0 if req.kind == "advdiff" else 1

@@ -164,3 +164,32 @@ def test_batched_fp64_staggered_admission(cuda):
     for r in reqs:
         for a, b in zip(staggered[r.rid]["result"], at_once[r.rid]["result"]):
             assert np.array_equal(a, b), r
+
+
+@pytest.mark.parametrize("skip", [True, False])
+def test_small_requests_pass_one_that_does_not_fit(skip, cuda):
+    """Under an HBM budget that the first request and a large second one exceed together,
+    the later small ones are admitted before the large one (or, with max_skip_wait=0, after
+    it, in arrival order); every result equals the request's result alone."""
+    from manapy_b200 import serving as SV
+    reqs = [Request(rid=0, kind="advdiff", n=20, seed=7, steps=40, ux=0.5, uy=0.3, D=1e-3),
+            Request(rid=1, kind="advdiff", n=60, seed=8, steps=20, ux=0.4, uy=0.2, D=1e-3),
+            Request(rid=2, kind="sw", n=12, seed=9, steps=25, ratio=2.0),
+            Request(rid=3, kind="advdiff", n=14, seed=10, steps=30, ux=0.2, uy=0.6, D=1e-4)]
+
+    def est(r):
+        dm = SV.prepare(r)[1]
+        return dm.nbytes() + 48.0 * dm.nbcells + 16.0 * dm.nbfaces
+    e = [est(r) for r in reqs]
+    budget = 1.2 * (e[0] + e[2] + e[3])
+    assert e[0] + e[1] > budget
+    srv = BatchServer(workers=0, chunk=4, hbm_budget=budget, max_skip_wait=1e9 if skip else 0.0)
+    recs = _by_rid(srv.serve(reqs, keep_results=True))
+    if skip:
+        assert recs[2]["admitted"] < recs[1]["admitted"] and recs[3]["admitted"] < recs[1]["admitted"]
+    else:
+        assert recs[1]["admitted"] <= recs[2]["admitted"] <= recs[3]["admitted"]
+    for r in reqs:
+        alone = BatchServer(workers=0, chunk=4).serve([r], keep_results=True)[0]
+        for a, b in zip(alone["result"], recs[r.rid]["result"]):
+            assert np.array_equal(a, b), r

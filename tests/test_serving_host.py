@@ -126,3 +126,23 @@ def test_unreceived_preparation_leaves_no_file():
         assert isinstance(x, SV._Shipped) and os.path.exists(x.path)
         fut.add_done_callback(SV._discard)     # runs at once: the future is done
     assert not os.path.exists(x.path)
+
+
+def test_admission_order():
+    """Arrival order while the budget allows; a request that does not fit lets later ones
+    that fit pass it until it has waited ``max_skip_wait``; nothing admitted: the first goes
+    in whatever its size; never more than the free slots."""
+    ao = SV.admission_order
+    w = [(0.0, 10.0), (0.1, 10.0), (0.2, 10.0)]
+    assert ao(w, used=0.0, budget=100.0, slots=8, active=0, now=0.3) == [0, 1, 2]
+    assert ao(w, used=0.0, budget=100.0, slots=2, active=0, now=0.3) == [0, 1]
+    big = [(0.0, 80.0), (0.1, 10.0), (0.2, 5.0), (0.3, 40.0)]
+    # 50 bytes in use: the 80-byte head does not fit, the two small ones pass it, the 40-byte
+    # one no longer fits after them
+    assert ao(big, used=50.0, budget=100.0, slots=8, active=3, now=0.5) == [1, 2]
+    # the head has waited long enough: nothing passes it
+    assert ao(big, used=50.0, budget=100.0, slots=8, active=3, now=1.5, max_skip_wait=1.0) == []
+    assert ao(big, used=50.0, budget=100.0, slots=8, active=3, now=0.5, max_skip_wait=0.0) == []
+    # nothing admitted: the oversize head goes in alone, then the budget counts it
+    assert ao([(0.0, 150.0), (0.1, 10.0)], used=0.0, budget=100.0, slots=8, active=0, now=0.2) == [0]
+    assert ao([], used=0.0, budget=100.0, slots=8, active=0, now=0.0) == []
