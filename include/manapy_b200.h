@@ -290,7 +290,8 @@ typedef struct mb_advdiff_params {
  * w_in is read, w_out written (distinct buffers).  sign_cf[4*i+j] = u.n of the j-th
  * local face of cell i in manapy's face orientation (mb_cell_face_sign); src may be
  * NULL (zero source).  Scratch: cell_scratch [4*nbcells] in 2D, [8*nbcells] in 3D
- * (order 2), node_scratch [nbnodes] (diffusion); NULL where not needed. */
+ * (order 2; [8*nbcells + 4*(nbnodes + nbedges)] when m carries the edge tables),
+ * node_scratch [nbnodes] (diffusion); NULL where not needed. */
 int mb_advdiff_step(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_params *p,
                     const double *w_in, double *w_out, const double *sign_cf, const double *src,
                     const double *dt_dev, double *cell_scratch, double *node_scratch, void *stream);
@@ -343,7 +344,11 @@ int mb_cell_face_sign_f32c(const mb_mesh *m, const double *sign_cf, float *sign_
  * per cell with compensated (Neumaier) summation on differences from the cell's own
  * value; coordinates, every geometric coefficient and dt stay FP64.  Scratch:
  * cell_scratch [4*nbcells] floats in 2D, [5*nbcells] in 3D (order 2), node_scratch
- * [nbnodes] floats (diffusion).  Needs the
+ * [nbnodes] floats (diffusion).  Tetrahedra whose struct carries the edge tables (order 2)
+ * form the least-squares sums by inclusion-exclusion as mb_advdiff_step does, in FP64 over
+ * the FP32 state: cell_scratch then holds 5*nbcells floats rounded up to a multiple of 8,
+ * followed by the vertex and edge sums, 8*(nbnodes + nbedges) floats, and must be
+ * 32-byte aligned.  Needs the
  * compact tables of mb_mesh, n2c_sell_alpha_f32 included.
  * Compensated state: lo_in / lo_out (FP32 [nbcells], both or neither) carry the rounding
  * error of the state, w + lo; the update is w_out + lo_out = w_in + (increment + lo_in)

@@ -618,6 +618,158 @@ __global__ void __launch_bounds__(kBlock, 2)
   store_state(wi, inc, lo_in, w_out, lo_out, i);
 }
 
+// ---- tetrahedra, the first phase by inclusion-exclusion (the FP64 step's k_f3_sums /
+// k_f3_grad over the FP32 state): each cell's least-squares right-hand side from the FP64
+// sums of its 4 vertices and 6 edges and its face neighbours, instead of gathering its ~60
+// stencil neighbours.  The sums are FP64 over the FP32 values: a cell's right-hand side is
+// the difference of sums of undifferenced values, which FP32 sums would lose to
+// cancellation.  Scratch after the 5 nbcells floats of records (rounded up to 8 floats):
+// [nbnodes][4] vertex sums, then [nbedges][4] edge sums, doubles {P, Q}.
+
+#ifndef MB_P1C_3D_SUMS_MIN_BLOCKS
+#define MB_P1C_3D_SUMS_MIN_BLOCKS 4
+#endif
+
+inline bool f3c_sums_tables(const mb_mesh &m) {
+  return m.cell_edges && m.edge_origin && m.edge_sell_ptr && m.edge_sell_idx && m.nbedges > 0 && m.cell_lsq &&
+         m.n2c_sum_ptr && m.n2c_sum_idx && m.n2c_sum_alpha;
+}
+inline long long f3c_rec_floats(const mb_mesh &m) { return (5LL * m.nbcells + 7) & ~7LL; }
+
+// vertex blocks [0, nnb): the vertex's sums and (DIFF) its centre->vertex value, FP64 weights
+// rounded once; edge blocks: the edge's sums
+template <bool DIFF>
+__global__ void __launch_bounds__(kBlock) k_f3c_sums(mb_mesh m, mb_bc bc, const float *__restrict__ w,
+                                                     double *__restrict__ nrec, double *__restrict__ erec,
+                                                     float *__restrict__ wn, int nnb) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t pst = l2_stream();
+  double px = 0., py = 0., pz = 0., q = 0.;
+  int sb, se;
+  const int32_t *idx;
+  D3 X;
+  const bool vertex = (int)blockIdx.x < nnb;
+  const int n = (vertex ? blockIdx.x : blockIdx.x - nnb) * blockDim.x + threadIdx.x;
+  if (vertex) {
+    if (n >= m.nbnodes) return;
+    X = ld3(m.node_coord + 4 * (long long)n);
+    sb = ld(m.n2c_sum_ptr + (n >> 5)); se = ld(m.n2c_sum_ptr + (n >> 5) + 1);
+    idx = m.n2c_sum_idx;
+  } else {
+    if (n >= m.nbedges) return;
+    X = ld3(m.node_coord + 4 * (long long)ld(m.edge_origin + n));
+    sb = ld(m.edge_sell_ptr + (n >> 5)); se = ld(m.edge_sell_ptr + (n >> 5) + 1);
+    idx = m.edge_sell_idx;
+  }
+  double acc = 0.;
+  for (int k = sb + lane; k < se; k += 32) {
+    const int cc = ld1_stream(idx + k, pst);
+    if (cc < 0) continue;  // empty slot
+    const D3 x = ld3(m.cell_xy + 4 * (long long)cc);
+    const double wc = ld(w + cc);
+    if (DIFF && vertex) acc += ldd_stream(m.n2c_sum_alpha + k, pst) * wc;
+    px += (x.x - X.x) * wc; py += (x.y - X.y) * wc; pz += (x.z - X.z) * wc;
+    q += wc;
+  }
+  if (vertex) {
+    if (DIFF) {
+      const GhostRuleF ghost = make_rule_f(m, bc, w);
+      const int gb = ld(m.n2g_ptr + n), ge = ld(m.n2g_ptr + n + 1);
+      for (int k = gb; k < ge; ++k) acc += ld(m.n2g_alpha + k) * (double)ghost(ld(m.n2g_idx + k));
+      st1f_keep(wn + n, (float)acc, l2_keep());
+    }
+    st4_keep(nrec + 4 * (long long)n, px, py, pz, q, l2_keep());
+  } else {
+    st4_keep(erec + 4 * (long long)n, px, py, pz, q, l2_keep());
+  }
+}
+
+// cell pass: the gradient from the vertex, edge and face-neighbour sums (FP64, rounded once),
+// the Barth limiter in FP32 as k_f3c_phase1; the same records as k_f3c_phase1
+__global__ void __launch_bounds__(kBlock, MB_P1C_3D_SUMS_MIN_BLOCKS)
+    k_f3c_grad(mb_mesh m, mb_bc bc, const float *__restrict__ w, float *__restrict__ rec,
+               const double *__restrict__ nrec, const double *__restrict__ erec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nbcells) return;
+  const GhostRuleF ghost = make_rule_f(m, bc, w);
+  const D3 c = ld3(m.cell_xy + 4 * (long long)i);
+  const float wf = ld(w + i);
+  const double wi = wf;
+  const int4 vt = ld4(m.cell_vtx + 4 * i);
+  const int4 nb = ld4(m.cell_nbr + 4 * i);
+  const int4 ea = ld4(m.cell_edges + 8 * (long long)i), eb = ld4(m.cell_edges + 8 * (long long)i + 4);
+  const D3 P[4] = {ld3(m.node_coord + 4 * vt.x), ld3(m.node_coord + 4 * vt.y), ld3(m.node_coord + 4 * vt.z),
+                   ld3(m.node_coord + 4 * vt.w)};
+  double sx = 0., sy = 0., sz = 0.;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double px, py, pz, q;
+    ld4d(nrec + 4 * (long long)comp(vt, v), px, py, pz, q);
+    const D3 d = P[v] - c;
+    sx += px + d.x * q; sy += py + d.y * q; sz += pz + d.z * q;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    // local vertex pairs (0,1), (0,2), (0,3), (1,2), (1,3), (2,3); origin: the vertex of smaller index
+    const int a = k < 3 ? 0 : (k < 5 ? 1 : 2), b = k < 3 ? k + 1 : (k < 5 ? k - 1 : 3);
+    const int e = k == 0 ? ea.x : (k == 1 ? ea.y : (k == 2 ? ea.z : (k == 3 ? ea.w : (k == 4 ? eb.x : eb.y))));
+    double px, py, pz, q;
+    ld4d(erec + 4 * (long long)e, px, py, pz, q);
+    const D3 d = (comp(vt, a) < comp(vt, b) ? P[a] : P[b]) - c;
+    sx -= px + d.x * q; sy -= py + d.y * q; sz -= pz + d.z * q;
+  }
+  float wmax = wf, wmin = wf;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int o = comp(nb, j);
+    float bv;
+    if (o >= 0) {
+      const D3 x = ld3(m.cell_xy + 4 * (long long)o);
+      bv = ld(w + o);
+      const double b = bv;
+      sx += (x.x - c.x) * b; sy += (x.y - c.y) * b; sz += (x.z - c.z) * b;
+    } else {
+      bv = ghost(-1 - o);
+    }
+    wmax = fmaxp(wmax, bv);
+    wmin = fminp(wmin, bv);
+  }
+  double a0, a1, a2, a3, a4, a5, dia, pad, Dx, Dy, Dz;
+  ld4d(m.cell_lsq + 12 * (long long)i, a0, a1, a2, a3);
+  ld4d(m.cell_lsq + 12 * (long long)i + 4, a4, a5, dia, pad);
+  ld4d(m.cell_lsq + 12 * (long long)i + 8, Dx, Dy, Dz, pad);
+  double jx = sx - wi * Dx, jy = sy - wi * Dy, jz = sz - wi * Dz;
+  const int gb = ld(m.ghostnid_ptr + i), ge = ld(m.ghostnid_ptr + i + 1);
+  for (int k = gb; k < ge; ++k) {
+    const int f = ld(m.ghostnid_idx + k);
+    const double *gc = m.face_ghostcenter + 3 * f;
+    const double dw = (double)ghost(f) - wi;
+    jx += (ld(gc) - c.x) * dw; jy += (ld(gc + 1) - c.y) * dw; jz += (ld(gc + 2) - c.z) * dw;
+  }
+  const double rdia = 1. / dia;
+  const float gx = (float)((a0 * jx + a1 * jy + a2 * jz) * rdia);
+  const float gy = (float)((a1 * jx + a3 * jy + a4 * jz) * rdia);
+  const float gz = (float)((a2 * jx + a4 * jy + a5 * jz) * rdia);
+  const uint32_t fl = ld(m.cell_flags + i);
+  float ps = 1.f;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    int d0, d1, d2;
+    face_desc(fl, j, d0, d1, d2);
+    const D3 fc = (1. / 3) * tet_face_sum(P, j, d2);
+    const float delta = gx * (float)(fc.x - c.x) + gy * (float)(fc.y - c.y) + gz * (float)(fc.z - c.z);
+    float psi_ij = 1.f;
+    if (!(fabsf(delta) < 1e-10f)) {
+      if (delta > 0.f) psi_ij = fminp(1.f, (wmax - wf) / delta);
+      if (delta < 0.f) psi_ij = fminp(1.f, (wmin - wf) / delta);
+    }
+    ps = fminp(ps, psi_ij);
+  }
+  const uint64_t keep = l2_keep();
+  st4_keep(rec + 4 * (long long)i, make_float4(wf, gx, gy, gz), keep);
+  st1f_keep(rec + 4 * (long long)m.nbcells + i, ps, keep);
+}
+
 // FP32 u.n per cell face and, in FP64 then rounded, the cell's signed sum of them
 // (minus for the faces the cell owns, which the residual subtracts)
 __global__ void __launch_bounds__(kBlock) k_sign_f32c(mb_mesh m, const double *__restrict__ s64,
@@ -649,7 +801,15 @@ int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params 
     k_f2c_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2C_BLOCK), MB_P2C_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
                                                                            lo_in, lo_out);
   } else {
-    if (ncb + nnb > 0) {
+    if (O2 && f3c_sums_tables(m)) {
+      // the sums path: records, then the vertex and edge sums (32-byte aligned doubles)
+      if ((reinterpret_cast<uintptr_t>(cs) & 31) != 0 || (reinterpret_cast<uintptr_t>(m.cell_lsq) & 31) != 0)
+        return MB_EINVAL;
+      double *nrec = reinterpret_cast<double *>(cs + f3c_rec_floats(m)), *erec = nrec + 4 * (long long)m.nbnodes;
+      const int nvb = ceil_div(m.nbnodes, kBlock), neb = ceil_div(m.nbedges, kBlock);
+      k_f3c_sums<DF><<<nvb + neb, kBlock, 0, st>>>(m, bc, w_in, nrec, erec, wn, nvb);
+      k_f3c_grad<<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, w_in, cs, nrec, erec);
+    } else if (ncb + nnb > 0) {
       if (O2 && m.cell_lsq)
         k_f3c_phase1<O2, DF, true><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
       else

@@ -349,6 +349,16 @@ class DeviceMesh:
         extra = 4 * (self.nbnodes + int(self.nbedges)) if self.struct is not None and self.struct.cell_edges else 0
         return 8 * self.nbcells + extra
 
+    def cell_scratch_size_f32c(self):
+        """Floats of cell scratch an FP32-compensated second-order step needs with this struct:
+        4 nbcells (2D), 5 nbcells (3D); with the edge sums in use, 5 nbcells rounded up to 8,
+        plus the FP64 vertex and edge sums, 8 (nbnodes + nbedges) floats."""
+        if self.dim == 2:
+            return 4 * self.nbcells
+        if self.struct is not None and self.struct.cell_edges:
+            return ((5 * self.nbcells + 7) // 8) * 8 + 8 * (self.nbnodes + int(self.nbedges))
+        return 5 * self.nbcells
+
     def check_tables(self, stream=None):
         """Debug check of every index table on the device (``mb_check_tables``): raises
         ValueError naming the first entry outside the range the kernels gather with."""

@@ -285,9 +285,10 @@ class AdvectionDiffusionSolver:
 
     def _scratch(self):
         dm = self._dm
-        if getattr(self, "_cs", None) is None:
+        if getattr(self, "_cs", None) is None or self._cs.numel() < dm.cell_scratch_size():
             # 4 nbcells (2D: records) or 8 nbcells (3D: records, rows), plus the vertex and edge
-            # records when the 3D step uses the edge sums
+            # records when the 3D step uses the edge sums (grown if another solver on this mesh
+            # opted the struct into them since)
             self._cs = torch.empty(dm.cell_scratch_size(), dtype=torch.float64, device=dm.device)
             self._ns = torch.empty(dm.nbnodes, dtype=torch.float64, device=dm.device)
         return self._cs, self._ns
@@ -348,8 +349,7 @@ class AdvectionDiffusionSolver:
             self._w32 = [torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device) for _ in range(2)]
             # rounding errors of the FP32 state (w + lo carries the state to ~48 bits)
             self._lo32 = [torch.empty(dm.nbcells, dtype=torch.float32, device=dm.device) for _ in range(2)]
-            nrec = (4 if dm.dim == 2 else 5) * dm.nbcells
-            self._cs32 = torch.empty(nrec, dtype=torch.float32, device=dm.device)
+            self._cs32 = torch.empty(dm.cell_scratch_size_f32c(), dtype=torch.float32, device=dm.device)
             self._ns32 = torch.empty(dm.nbnodes, dtype=torch.float32, device=dm.device)
             self._sign32 = torch.empty((4 if dm.dim == 2 else 5) * dm.nbcells, dtype=torch.float32,
                                        device=dm.device)
@@ -396,6 +396,10 @@ class AdvectionDiffusionSolver:
     def _call_f32c(self, k, src, st):
         """One step from buffer k into buffer 1 - k."""
         w, lo = self._w32, self._lo32
+        if self._cs32.numel() < self._dm.cell_scratch_size_f32c():
+            # another solver on this mesh opted its struct into the edge sums since the
+            # scratch was sized
+            self._cs32 = torch.empty(self._dm.cell_scratch_size_f32c(), dtype=torch.float32, device=self._dm.device)
         _lib.call("mb_advdiff_step_f32c", self._dm.struct, self.var.device_bc.struct, self._params, _p(w[k]),
                   _p(w[1 - k]), _p(lo[k]), _p(lo[1 - k]), _p(self._sign32), _p(src), _p(self._dt_dev),
                   _p(self._cs32), _p(self._ns32), st)

@@ -24,7 +24,7 @@ def rel_l2(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
 
 
-def _api(el, vx, wl, precision):
+def _api(el, vx, wl, precision, **conf):
     dom = M.Domain(dim=wl.dim, mesh=(el, vx))
     w = M.Variable(domain=dom, BC=wl.bc, values=wl.bc_values)
     vel = [M.Variable(domain=dom) for _ in range(3)]
@@ -34,7 +34,7 @@ def _api(el, vx, wl, precision):
     w.cell = wl.init(dom.cells.center)
     S = M.AdvectionDiffusionSolver(w, vel=tuple(vel), conf=M.Struct(
         Dxx=wl.diffusion[0], Dyy=wl.diffusion[1], Dzz=wl.diffusion[2], order=wl.order, cfl=wl.cfl,
-        precision=precision))
+        precision=precision, **conf))
     return dom, w, S
 
 
@@ -61,6 +61,28 @@ def test_fp32c_error_vs_fp64_oracle(wl, cuda):
     l2, linf = rel_l2(w.cell, o.w), rel_max(w.cell, o.w)
     print("%s fp32c after %d steps: L2 %.2e Linf %.2e" % (wl.name, wl.steps, l2, linf))
     assert l2 <= L2_TOL and linf <= LINF_TOL, (l2, linf)
+
+
+def test_fp32c_tetrahedra_edge_sums_match_stencil_gather(cuda):
+    """Second-order FP32c on tetrahedra: the least-squares sums by inclusion-exclusion over
+    vertex and edge sums (FP64 sums of the FP32 state, the default) and the gather of each
+    cell's whole stencil (lsq_sums=False) agree to FP32 rounding, and both meet the oracle
+    tolerance."""
+    wl = W.C4.scaled(n=10, steps=30)
+    el, vx = wl.mesh()
+    o = _oracle(el, vx, wl)
+    for _ in range(wl.steps):
+        o.step()
+    res = {}
+    for sums in (True, False):
+        dom, w, S = _api(el, vx, wl, "fp32c", lsq_sums=sums)
+        S.advance(wl.steps, graph=True)
+        assert bool(S._dm.struct.cell_edges) == sums
+        res[sums] = np.array(w.cell)
+        l2, linf = rel_l2(res[sums], o.w), rel_max(res[sums], o.w)
+        print("C4 n=10 fp32c lsq_sums=%s after %d steps: L2 %.2e Linf %.2e" % (sums, wl.steps, l2, linf))
+        assert l2 <= L2_TOL and linf <= LINF_TOL, (sums, l2, linf)
+    assert rel_l2(res[True], res[False]) <= L2_TOL
 
 
 def test_fp32c_manapy_loop_and_graph_agree_bitwise(cuda):
