@@ -505,8 +505,17 @@ __global__ void __launch_bounds__(kBlock, MB_P1C_3D_MIN_BLOCKS)
   if (DIFF) node_value_f32(m, ghost, w, wn, (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x, lane);
 }
 
+// 128 x 6: 80 registers, 24 warps per SM (256 x 2: 90 registers, 16 warps, 13 % slower at
+// 1.57M tetrahedra; 256 x 3: 80 registers, 1 % slower than 128 x 6)
+#ifndef MB_P2C_3D_BLOCK
+#define MB_P2C_3D_BLOCK 128
+#endif
+#ifndef MB_P2C_3D_MIN_BLOCKS
+#define MB_P2C_3D_MIN_BLOCKS 6
+#endif
+
 template <bool ORDER2, bool DIFF>
-__global__ void __launch_bounds__(kBlock, 2)
+__global__ void __launch_bounds__(MB_P2C_3D_BLOCK, MB_P2C_3D_MIN_BLOCKS)
     k_f3c_phase2(mb_mesh m, mb_bc bc, mb_advdiff_params p, const float *__restrict__ w, float *__restrict__ w_out,
                  const float *__restrict__ sign, const float *__restrict__ src, const double *__restrict__ dt_dev,
                  const float *__restrict__ rec, const float *__restrict__ wn, const float *__restrict__ lo_in,
@@ -815,7 +824,7 @@ int launch_step_f32c(const mb_mesh &m, const mb_bc &bc, const mb_advdiff_params 
       else
         k_f3c_phase1<O2, DF, false><<<ncb + nnb, kBlock, 0, st>>>(m, bc, w_in, cs, wn, ncb);
     }
-    k_f3c_phase2<O2, DF><<<ceil_div(m.nbcells, kBlock), kBlock, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
+    k_f3c_phase2<O2, DF><<<ceil_div(m.nbcells, MB_P2C_3D_BLOCK), MB_P2C_3D_BLOCK, 0, st>>>(m, bc, p, w_in, w_out, sign, src, dt, cs, wn,
                                                                            lo_in, lo_out);
   }
   return cudaGetLastError() == cudaSuccess ? MB_OK : MB_ECUDA;
