@@ -505,13 +505,13 @@ __global__ void __launch_bounds__(kBlock, MB_P1C_3D_MIN_BLOCKS)
   if (DIFF) node_value_f32(m, ghost, w, wn, (blockIdx.x - (ORDER2 ? ncb : 0)) * blockDim.x + threadIdx.x, lane);
 }
 
-// 128 x 6: 80 registers, 24 warps per SM (256 x 2: 90 registers, 16 warps, 13 % slower at
-// 1.57M tetrahedra; 256 x 3: 80 registers, 1 % slower than 128 x 6)
+// 128 x 7: 72 registers, 28 warps per SM (at 1.57M tetrahedra: 256 x 2, 90 registers, 13 %
+// slower; 128 x 6 and 256 x 3, 80 registers, 2-3 % slower; 64 x 12 2 % slower)
 #ifndef MB_P2C_3D_BLOCK
 #define MB_P2C_3D_BLOCK 128
 #endif
 #ifndef MB_P2C_3D_MIN_BLOCKS
-#define MB_P2C_3D_MIN_BLOCKS 6
+#define MB_P2C_3D_MIN_BLOCKS 7
 #endif
 
 template <bool ORDER2, bool DIFF>
