@@ -97,3 +97,25 @@ def test_first_cells_are_numbered_first():
     assert np.array_equal(R.cperm[:k], base.cperm[first[base.cperm]])
     assert np.array_equal(R.cperm[k:], base.cperm[~first[base.cperm]])
     assert np.array_equal(R.cinv[R.cperm], np.arange(A["nbcells"]))
+
+
+@pytest.mark.parametrize("dim,n", [(2, 12), (3, 3)])
+def test_cell_scratch_sizes_follow_the_edge_tables(dim, n):
+    """Scratch the fused steps need: FP64 4 nbcells (2D) or 8 nbcells (3D), FP32c 4 / 5 nbcells;
+    once a tetrahedral struct carries the edge tables, FP64 adds 4 (nbnodes + nbedges) doubles
+    and FP32c rounds its records up to 8 floats (32 bytes, where the FP64 sums start) and adds
+    8 (nbnodes + nbedges) floats."""
+    el, vx = meshgen.square_triangles(n, seed=3) if dim == 2 else meshgen.cube_tetrahedra(n, seed=3)
+    dm = DeviceMesh(G.build(el, vx, dim), "cpu", reorder=True)
+    nc, nn = dm.nbcells, dm.nbnodes
+    assert dm.cell_scratch_size() == (4 if dim == 2 else 8) * nc
+    assert dm.cell_scratch_size_f32c() == (4 if dim == 2 else 5) * nc
+    assert dm.use_edge_sums() == (dim == 3)
+    if dim == 3:
+        ne = dm.nbedges
+        assert ne > 0 and dm.struct.nbedges == ne
+        rec = dm.cell_scratch_size_f32c() - 8 * (nn + ne)
+        assert rec >= 5 * nc and rec % 8 == 0 and rec - 5 * nc < 8
+        assert dm.cell_scratch_size() == 8 * nc + 4 * (nn + ne)
+    else:
+        assert dm.cell_scratch_size_f32c() == 4 * nc
