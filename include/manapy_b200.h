@@ -118,9 +118,11 @@ typedef struct mb_mesh {
   const float *n2c_sell_alpha_f32;
   /* [nbfaces][4] = {n_x, n_y, 1/mesure, 0} rounded to FP32 (FP32-compensated shallow water, 2D) */
   const float *face_nm_f32;
-  /* tetrahedra, optional: [nbcells][8] the least-squares moment matrix of each cell's
+  /* tetrahedra, optional: [nbcells][12] the least-squares moment matrix of each cell's
    * stencil (the lsq_sell neighbours, then its stencil ghosts) as {c_xx, c_xy, c_xz, c_yy,
-   * c_yz, c_zz, det, 0}, cofactors and determinant, 32-byte aligned (mb_lsq_matrix).  The
+   * c_yz, c_zz, det, 0}, cofactors and determinant, followed by {D_x, D_y, D_z, 0}, the sum
+   * of the lsq_sell neighbours' centre offsets (read by the edge-sum step), 32-byte aligned
+   * (mb_lsq_matrix).  The
    * matrix depends on the geometry only; when given, the second-order fused 3D step reads
    * it instead of forming it every step.  Must come from the lsq_sell table of this
    * struct.  Triangles: NULL (their step forms the matrix; reading it measured slower). */
@@ -313,8 +315,9 @@ int mb_advdiff_step_split(const mb_mesh *m, const mb_bc *bc, const mb_advdiff_pa
                           double *w_out, const double *sign_cf, const double *src, const double *dt_dev,
                           double *cell_scratch, double *node_scratch, int32_t part, int32_t nfirst, void *stream);
 
-/* The cell_lsq table of a tetrahedral mesh with compact tables ([nbcells][8] doubles,
- * 32-byte aligned): the moment matrix sum over the stencil of d d^T, d = centre offset, of
+/* The cell_lsq table of a tetrahedral mesh with compact tables ([nbcells][12] doubles,
+ * 32-byte aligned; layout at mb_mesh.cell_lsq): the moment matrix sum over the stencil of
+ * d d^T, d = centre offset, of
  * manapy/ast/functions3d.py:4-120 (cell_gradient_3d), as cofactors and determinant, summed in
  * the order the fused step sums its right-hand side.  Once per mesh.  MB_EINVAL for
  * triangles. */
