@@ -628,7 +628,8 @@ __global__ void __launch_bounds__(MB_P2C_3D_BLOCK, MB_P2C_3D_MIN_BLOCKS)
 }
 
 // ---- tetrahedra, the first phase by inclusion-exclusion (the FP64 step's k_f3_sums /
-// k_f3_grad over the FP32 state): each cell's least-squares right-hand side from the FP64
+// k_f3_grad over the FP32 state; manapy/ast/functions3d.py:4-120 cell_gradient_3d and
+// :364-408 barthlimiter_3d): each cell's least-squares right-hand side from the FP64
 // sums of its 4 vertices and 6 edges and its face neighbours, instead of gathering its ~60
 // stencil neighbours.  The sums are FP64 over the FP32 values: a cell's right-hand side is
 // the difference of sums of undifferenced values, which FP32 sums would lose to
